@@ -1,0 +1,197 @@
+/*
+ * demsph.h -- C ABI of the B200-native DEMSPH particle-interaction library
+ * (libdemsph_b200.so).
+ *
+ * The reference (kaiqideng/this_studio, DEMSPH/kernel) exposes its per-step
+ * path as two C++ solver classes whose public methods set up a scene and run
+ * the step loop (DEMSolver, DEMSPH/kernel/DEMSolver.h:1633-2049; WCSPHSolver,
+ * DEMSPH/kernel/WCSPHSolver.h:522-624), on top of extern "C" kernel launchers.
+ * This header is the flat C form of that scene-setup / solver-step interface:
+ * one function per public method, plain pointers and sizes, no C++ or torch
+ * types, so cgo / JNI / ctypes / N-API bind it directly.  The C++ facade in
+ * include/demsph/solvers.hpp restores the reference class and method names.
+ *
+ * Conventions
+ *  - Every function returns an int status: DEMSPH_OK (0) or a DEMSPH_ERR_*
+ *    code; nothing exits the process (the reference calls exit(1) when
+ *    cudaSetDevice fails, DEMSolver.h:1974-1981).  demsph_last_error() gives
+ *    the message of the last failure on the calling thread.
+ *  - Vectors are arrays of 3 doubles (x, y, z) per object, packed: n objects
+ *    take 3n doubles.  Quaternions are (q0, q1, q2, q3); symmetric matrices are
+ *    (xx, yy, zz, xy, xz, yz) as in the reference (myQua.h:10-15, myMat.h:15-27).
+ *  - Host arrays are read during the call only.  Getters write into caller
+ *    buffers sized from the matching demsph_*_num_* query.
+ *  - `stream` is a cudaStream_t passed as void*; 0 means the legacy stream.
+ *    All device work of a scene is ordered on its stream.  Getters
+ *    synchronise that stream.
+ *  - A scene owns all device memory it allocates; demsph_*_destroy frees it.
+ */
+#ifndef DEMSPH_H
+#define DEMSPH_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DEMSPH_OK 0
+#define DEMSPH_ERR_INVALID 1     /* bad argument or call order               */
+#define DEMSPH_ERR_SCENE 2       /* malformed scene (empty, NaN, bad sizes)  */
+#define DEMSPH_ERR_OVERFLOW 3    /* a list overflowed and could not regrow   */
+#define DEMSPH_ERR_CUDA 4        /* CUDA runtime error                       */
+#define DEMSPH_ERR_NOT_READY 5   /* scene not initialised                    */
+#define DEMSPH_ERR_TIMEOUT 6     /* a bounded device wait gave up            */
+#define DEMSPH_ERR_ALLOC 7       /* host or device allocation failed         */
+
+/* arithmetic of the force laws (positions, velocities and springs are FP64
+ * in both modes) */
+#define DEMSPH_PRECISION_FP64 0  /* reference arithmetic throughout         */
+#define DEMSPH_PRECISION_MIXED 1 /* FP32 force laws, FP64 state            */
+
+typedef struct demsph_dem_scene* demsph_dem_t;
+typedef struct demsph_sph_scene* demsph_sph_t;
+
+const char* demsph_last_error(void);
+const char* demsph_version(void);
+/* Number of CUDA kernels this library has launched since load (instrumentation). */
+long long demsph_kernel_launches(void);
+
+/* ======================================================================= */
+/* DEM: spheres, clumps, triangle-mesh walls, contact + parallel bonds      */
+/* ======================================================================= */
+
+/* DEMSolver::DEMSolver(cudaStream_t)  -- DEMSolver.h:147 */
+int demsph_dem_create(demsph_dem_t* out, void* stream);
+/* DEMSolver::~DEMSolver -- DEMSolver.h:153 */
+int demsph_dem_destroy(demsph_dem_t s);
+
+/* DEMSolver::setHertzianPair -- DEMSolver.h:1637-1662 */
+int demsph_dem_set_hertzian_pair(demsph_dem_t s, int materialA, int materialB, double effectiveYoungsModulus,
+                                 double effectiveShearModulus, double restitution, double rollingToShearStiffness,
+                                 double torsionToShearStiffness, double slidingFriction, double rollingFriction,
+                                 double torsionFriction);
+/* DEMSolver::setLinearPair -- DEMSolver.h:1667-1700 */
+int demsph_dem_set_linear_pair(demsph_dem_t s, int materialA, int materialB, double kn, double ks, double kr,
+                               double kt, double dn, double ds, double dr, double dt, double slidingFriction,
+                               double rollingFriction, double torsionFriction);
+/* DEMSolver::setBondedPair -- DEMSolver.h:1705-1726 */
+int demsph_dem_set_bonded_pair(demsph_dem_t s, int materialA, int materialB, double bondRadiusMultiplier,
+                               double bondYoungsModulus, double normalToShearStiffness, double tensileStrength,
+                               double cohesion, double friction);
+
+/* DEMSolver::addBall (density > 0) / addFixedBall (fixed != 0), n at once --
+ * DEMSolver.h:1728-1768.  clumpID may be NULL (all -1). */
+int demsph_dem_add_balls(demsph_dem_t s, long n, const double* position, const double* velocity,
+                         const double* angularVelocity, const double* radius, const double* density,
+                         const int* materialID, const int* clumpID, int fixed);
+/* DEMSolver::addClump -- DEMSolver.h:1796-1845 */
+int demsph_dem_add_clump(demsph_dem_t s, long numPebbles, const double* pebblePosition, const double* pebbleRadius,
+                         const double* centroid, const double* velocity, const double* angularVelocity, double mass,
+                         const double* inertiaTensor6, int materialID);
+/* DEMSolver::addMeshWall -- DEMSolver.h:1882-1935.  Like the reference, the
+ * wall starts at rest; use demsph_dem_set_wall_motion to move it. */
+int demsph_dem_add_mesh_wall(demsph_dem_t s, long numVertices, const double* vertexLocal, long numTriangles,
+                             const int* tri0, const int* tri1, const int* tri2, const double* position,
+                             int materialID);
+/* Sets a mesh wall's velocity and angular velocity (the reference writes the
+ * wall body arrays through getMeshWallBody(), DEMSolver.h:1545). */
+int demsph_dem_set_wall_motion(demsph_dem_t s, int wall, const double* velocity, const double* angularVelocity);
+/* DEMSolver::addBondedInteraction -- DEMSolver.h:1937-1942 (bondedInteraction::add, :93-135).
+ * Callable before or after initialisation (the reference's addInitialCondition hook, :1998). */
+int demsph_dem_add_bonds(demsph_dem_t s, long n, const int* objectPointed, const int* objectPointing,
+                         const double* ballPosition, long numBallPositions);
+
+/* The reference's external force hook (virtual addExternalForceTorque,
+ * DEMSolver.h:1372) runs user kernels from DEMSPH/externalForceTorque.cu.
+ * These three configure the same kernels, applied in this order each call:
+ * constant force (launchAddConstantForce, externalForceTorque.cu:14-24; the
+ * force is scaled by min(time/ramp, 1) when ramp > 0), global damping
+ * (launchAddGlobalDampingForceTorque, :41-57), buoyancy + drag against the
+ * plane z = waterLevel (launchAddBuoyancyDrag, :135-160). */
+int demsph_dem_set_constant_force(demsph_dem_t s, long n, const double* force, double rampTime);
+int demsph_dem_set_global_damping(demsph_dem_t s, double dampingCoefficient);
+int demsph_dem_set_buoyancy_drag(demsph_dem_t s, double fluidDensity, double dragCoefficient, const double* gravity,
+                                 const double* fluidVelocity, double waterLevel);
+
+/* The initialisation part of DEMSolver::solve (DEMSolver.h:1961-1997):
+ * upload, grids (cell = 2 r_max; triangle cell >= 2 circumradius),
+ * neighbour search, one force evaluation with dt = 0.  precision is
+ * DEMSPH_PRECISION_*. */
+int demsph_dem_initialize(demsph_dem_t s, const double* minBoundary, const double* maxBoundary,
+                          const double* gravity, double timeStep, int precision);
+/* numSteps passes of the step loop (loop_ball / loop_ball_wall,
+ * DEMSolver.h:1376-1485): neighbour search every 5th step, two force
+ * evaluations and the kick-drift-kick integration per step. */
+int demsph_dem_step(demsph_dem_t s, long numSteps);
+/* Protected step pieces of DEMSolver, exposed for parity checks:
+ * neighborSearch (DEMSolver.h:698-777) and calculateBallContactForceTorque
+ * (:599-695) followed, when walls != 0, by addTriangleContactForceTorque(dtWall) (:428-597). */
+int demsph_dem_neighbor_search(demsph_dem_t s);
+int demsph_dem_eval_forces(demsph_dem_t s, double dt, int walls, double dtWall);
+
+int demsph_dem_num_balls(demsph_dem_t s, long* n);
+int demsph_dem_num_pairs(demsph_dem_t s, int which /*0 ball-ball, 1 ball-triangle*/, long* n);
+int demsph_dem_num_bonds(demsph_dem_t s, long* n);
+int demsph_dem_num_clumps(demsph_dem_t s, long* n);
+int demsph_dem_step_index(demsph_dem_t s, long* step, double* time);
+/* ball_ getters (DEMSolver::getBall, DEMSolver.h:1541); any pointer may be NULL. */
+int demsph_dem_get_balls(demsph_dem_t s, double* position, double* velocity, double* angularVelocity, double* force,
+                         double* torque);
+int demsph_dem_set_balls(demsph_dem_t s, const double* position, const double* velocity,
+                         const double* angularVelocity);
+/* getBallPair* / getBallTrianglePair* (DEMSolver.h:1549-1631), in the
+ * reference's CSR order (rows by objectPointed, stencil order inside a row). */
+int demsph_dem_get_pairs(demsph_dem_t s, int which, int* objectPointed, int* objectPointing, double* sliding,
+                         double* rolling, double* torsion, double* force, double* torque);
+/* Seeds contact history: springs of matching (pointed, pointing) pairs of the
+ * current ball-ball list are set from the given list (the carry rule of
+ * writeBallInteractionsKernel, ballNeighborSearchKernel.cu:130-143). */
+int demsph_dem_import_springs(demsph_dem_t s, long n, const int* objectPointed, const int* objectPointing,
+                              const double* sliding, const double* rolling, const double* torsion);
+/* getBondedInteraction (DEMSolver.h:1547) fields */
+int demsph_dem_get_bonds(demsph_dem_t s, int* objectPointed, int* objectPointing, int* isBonded, double* normalForce,
+                         double* torsionTorque, double* shearForce, double* bendingTorque, double* normal,
+                         double* point);
+/* getClump (DEMSolver.h:1543) */
+int demsph_dem_get_clumps(demsph_dem_t s, double* position, double* velocity, double* angularVelocity,
+                          double* orientation);
+/* getMeshWallBody (DEMSolver.h:1545) and vertex global positions */
+int demsph_dem_get_walls(demsph_dem_t s, double* position, double* orientation, double* vertexGlobal);
+
+/* ======================================================================= */
+/* WCSPH: weakly compressible SPH with fixed dummy wall particles           */
+/* ======================================================================= */
+
+/* WCSPHSolver::WCSPHSolver(cudaStream_t) -- WCSPHSolver.h:21 */
+int demsph_sph_create(demsph_sph_t* out, void* stream);
+int demsph_sph_destroy(demsph_sph_t s);
+/* WCSPHSolver::addSPH / addDummy, n at once -- WCSPHSolver.h:523-541
+ * (m = spacing^3 rho, h = 1.3 spacing; particles with rho <= 0 or c <= 0 are skipped). */
+int demsph_sph_add(demsph_sph_t s, int dummy, long n, const double* position, const double* velocity,
+                   const double* soundSpeed, const double* spacing, const double* density, const double* viscosity);
+/* Initialisation part of WCSPHSolver::solve (WCSPHSolver.h:567-600):
+ * grid (cell = 2 h_max), dummy-dummy pairs and dummy wall normals. */
+int demsph_sph_initialize(demsph_sph_t s, const double* minBoundary, const double* maxBoundary, const double* gravity,
+                          double timeStep, int precision);
+/* numSteps passes of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621). */
+int demsph_sph_step(demsph_sph_t s, long numSteps);
+/* Protected step pieces (WCSPHSolver.h:150-358), for parity checks. */
+int demsph_sph_neighbor_search(demsph_sph_t s);
+int demsph_sph_eval_accel(demsph_sph_t s);
+
+int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
+int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);
+int demsph_sph_step_index(demsph_sph_t s, long* step, double* time);
+/* getSPH / getDummy (WCSPHSolver.h:563-565), in the caller's original order. */
+int demsph_sph_get(demsph_sph_t s, int dummy, double* position, double* velocity, double* acceleration,
+                   double* density, double* pressure, double* densityChange, double* normal);
+int demsph_sph_set(demsph_sph_t s, const double* position, const double* velocity, const double* density,
+                   const double* pressure, const double* densityChange);
+/* Pair lists in the reference's CSR order (countSPHInteractionsKernel and friends,
+ * SPHNeighborSearchKernel.cu:6-228), indices in the caller's original order. */
+int demsph_sph_get_pairs(demsph_sph_t s, int which, int* objectPointed, int* objectPointing);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEMSPH_H */

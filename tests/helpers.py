@@ -1,0 +1,58 @@
+"""Shared test helpers: load a scene into the oracle, compare pair sets and
+force fields."""
+import numpy as np
+
+from oracle.oracle import OracleDEM, OracleSPH
+
+
+def oracle_dem(scene):
+    o = OracleDEM()
+    for r in scene.hertz:
+        o.set_hertzian_pair(*r)
+    for r in scene.linear:
+        o.set_linear_pair(*r)
+    for r in scene.bonded:
+        o.set_bonded_pair(*r)
+    n = scene.position.shape[0]
+    fixed = np.zeros(n, bool) if scene.fixed is None else scene.fixed
+    starts = np.flatnonzero(np.diff(np.r_[-1, fixed.astype(int)]) != 0)
+    bounds = list(starts) + [n]
+    w = getattr(scene, "angvel", None)
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        sl = slice(a, b)
+        vel = None if scene.velocity is None else scene.velocity[sl]
+        o.add_balls(scene.position[sl], vel, None if w is None else w[sl], scene.radius[sl], scene.density[sl],
+                    scene.material[sl], None, fixed=bool(fixed[a]))
+    for c in scene.clumps:
+        o.add_clump(c["point"], c["radius"], c["centroid"], c["velocity"], c["angularVelocity"], c["mass"],
+                    c["inertia"], c["material"])
+    for k, wl in enumerate(scene.walls):
+        o.add_mesh_wall(wl["vertices"], wl["tri0"], wl["tri1"], wl["tri2"], wl["position"], wl["material"])
+        if "velocity" in wl:
+            o.set_wall_motion(k, wl["velocity"], wl.get("angularVelocity", (0, 0, 0)))
+    if scene.buoyancy is not None:
+        o.set_buoyancy_drag(*scene.buoyancy)
+    o.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt)
+    if scene.bond_initial_contacts:
+        p = o.pairs(0)
+        o.add_bonds(p["a"], p["b"], scene.position)
+    return o
+
+
+def oracle_sph(scene):
+    o = OracleSPH()
+    o.add_sph(scene.fluid, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
+    o.add_dummy(scene.dummy, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
+    o.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt)
+    return o
+
+
+def pair_keys(a, b):
+    return np.asarray(a, np.int64) * (1 << 32) + np.asarray(b, np.int64)
+
+
+def rel_err(x, ref):
+    """||x - ref||_2 / ||ref||_2 over all entries (0 when both vanish)."""
+    d = np.linalg.norm(np.asarray(x) - np.asarray(ref))
+    n = np.linalg.norm(ref)
+    return d / n if n > 0 else d

@@ -1,0 +1,123 @@
+"""ctypes binding of libdemsph_b200.so (the C ABI declared in include/demsph.h).
+
+The library is built in-tree by ``python -m this_studio_b200.build``.  There
+is no fallback: importing the solvers without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdemsph_b200.so")
+
+OK = 0
+ERR_INVALID = 1
+ERR_SCENE = 2
+ERR_OVERFLOW = 3
+ERR_CUDA = 4
+ERR_NOT_READY = 5
+ERR_TIMEOUT = 6
+ERR_ALLOC = 7
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+_d = C.POINTER(C.c_double)
+_i = C.POINTER(C.c_int)
+_l = C.POINTER(C.c_long)
+_vp = C.c_void_p
+_pvp = C.POINTER(C.c_void_p)
+_int = C.c_int
+_dbl = C.c_double
+_long = C.c_long
+
+# name -> argument types (all return int unless listed in _RESTYPE)
+SIGNATURES = {
+    "demsph_last_error": [],
+    "demsph_version": [],
+    "demsph_kernel_launches": [],
+    "demsph_dem_create": [_pvp, _vp],
+    "demsph_dem_destroy": [_vp],
+    "demsph_dem_set_hertzian_pair": [_vp, _int, _int] + [_dbl] * 8,
+    "demsph_dem_set_linear_pair": [_vp, _int, _int] + [_dbl] * 11,
+    "demsph_dem_set_bonded_pair": [_vp, _int, _int] + [_dbl] * 6,
+    "demsph_dem_add_balls": [_vp, _long, _d, _d, _d, _d, _d, _i, _i, _int],
+    "demsph_dem_add_clump": [_vp, _long, _d, _d, _d, _d, _d, _dbl, _d, _int],
+    "demsph_dem_add_mesh_wall": [_vp, _long, _d, _long, _i, _i, _i, _d, _int],
+    "demsph_dem_set_wall_motion": [_vp, _int, _d, _d],
+    "demsph_dem_add_bonds": [_vp, _long, _i, _i, _d, _long],
+    "demsph_dem_set_constant_force": [_vp, _long, _d, _dbl],
+    "demsph_dem_set_global_damping": [_vp, _dbl],
+    "demsph_dem_set_buoyancy_drag": [_vp, _dbl, _dbl, _d, _d, _dbl],
+    "demsph_dem_initialize": [_vp, _d, _d, _d, _dbl, _int],
+    "demsph_dem_step": [_vp, _long],
+    "demsph_dem_neighbor_search": [_vp],
+    "demsph_dem_eval_forces": [_vp, _dbl, _int, _dbl],
+    "demsph_dem_num_balls": [_vp, _l],
+    "demsph_dem_num_pairs": [_vp, _int, _l],
+    "demsph_dem_num_bonds": [_vp, _l],
+    "demsph_dem_num_clumps": [_vp, _l],
+    "demsph_dem_step_index": [_vp, _l, _d],
+    "demsph_dem_get_balls": [_vp, _d, _d, _d, _d, _d],
+    "demsph_dem_set_balls": [_vp, _d, _d, _d],
+    "demsph_dem_get_pairs": [_vp, _int, _i, _i, _d, _d, _d, _d, _d],
+    "demsph_dem_import_springs": [_vp, _long, _i, _i, _d, _d, _d],
+    "demsph_dem_get_bonds": [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d],
+    "demsph_dem_get_clumps": [_vp, _d, _d, _d, _d],
+    "demsph_dem_get_walls": [_vp, _d, _d, _d],
+    "demsph_sph_create": [_pvp, _vp],
+    "demsph_sph_destroy": [_vp],
+    "demsph_sph_add": [_vp, _int, _long, _d, _d, _d, _d, _d, _d],
+    "demsph_sph_initialize": [_vp, _d, _d, _d, _dbl, _int],
+    "demsph_sph_step": [_vp, _long],
+    "demsph_sph_neighbor_search": [_vp],
+    "demsph_sph_eval_accel": [_vp],
+    "demsph_sph_num": [_vp, _int, _l],
+    "demsph_sph_num_pairs": [_vp, _int, _l],
+    "demsph_sph_step_index": [_vp, _l, _d],
+    "demsph_sph_get": [_vp, _int, _d, _d, _d, _d, _d, _d, _d],
+    "demsph_sph_set": [_vp, _d, _d, _d, _d, _d],
+    "demsph_sph_get_pairs": [_vp, _int, _i, _i],
+}
+_RESTYPE = {
+    "demsph_last_error": C.c_char_p,
+    "demsph_version": C.c_char_p,
+    "demsph_kernel_launches": C.c_longlong,
+}
+
+_lib = None
+
+
+class DemsphError(RuntimeError):
+    def __init__(self, code, func, msg):
+        super().__init__(f"{func} failed with status {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads the native library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} not found: the CUDA library is not built "
+                "(run `python -m this_studio_b200.build`)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPE.get(name, C.c_int)
+        _lib = L
+    return _lib
+
+
+def call(name, *args):
+    rc = getattr(lib(), name)(*args)
+    if rc != OK:
+        msg = lib().demsph_last_error().decode(errors="replace")
+        raise DemsphError(rc, name, msg)
+    return rc
+
+
+def kernel_launches() -> int:
+    return int(lib().demsph_kernel_launches())

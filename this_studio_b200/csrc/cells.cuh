@@ -1,0 +1,174 @@
+// Counting sort of objects into a dense cell grid, replacing the reference's
+// thrust::sort_by_key + findStartAndEnd (DEMSPH/kernel/buildHashStartEnd.cu:
+// 6-83) and its thrust::inclusive_scan (buildHashStartEnd.cu:85-117).
+//
+// The number of cells is known, so a histogram + exclusive scan + scatter
+// gives the sorted index list and every cell's [start, start+1) range in
+// O(N + C) with no comparison sort.  The scatter uses atomics, so a short
+// per-cell insertion sort restores the reference's stable (key, index) order
+// and makes the result deterministic.
+#pragma once
+#include "common.cuh"
+
+namespace demsph {
+
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+// Histogram: key[i] = clamped cell key of object i; cnt[key]++.
+static __global__ void k_cell_count(const double4* __restrict__ p, int n, GridDesc g, int* __restrict__ key,
+                             int* __restrict__ cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 q = p[i];
+    int k = clamped_key(mk3(q.x, q.y, q.z), g);
+    key[i] = k;
+    atomicAdd(cnt + k, 1);
+}
+
+// One tile of an exclusive scan.  Optionally reads a per-tile offset, writes
+// the tile total, and writes the scanned values (out[n] = grand total).
+static __global__ void __launch_bounds__(kScanBlock) k_scan_tile(const int* __restrict__ in, int* __restrict__ out, int n,
+                                                          const int* __restrict__ tileOffset,
+                                                          int* __restrict__ tileSum) {
+    __shared__ int warpSums[kScanBlock / 32];
+    int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        v[i] = (base + i < n) ? in[base + i] : 0;
+        s += v[i];
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int ws = warpSums[lane];
+        int xs = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, xs, o);
+            if (lane >= o) xs += y;
+        }
+        warpSums[lane] = xs - ws;
+        if (lane == 31 && tileSum) tileSum[blockIdx.x] = xs;
+    }
+    __syncthreads();
+    if (!out) return;
+    int e = x - s + warpSums[w] + (tileOffset ? tileOffset[blockIdx.x] : 0);
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        if (base + i < n) out[base + i] = e;
+        e += v[i];
+        if (base + i == n - 1) out[n] = e;
+    }
+}
+
+// Scatter into cell order: the atomic decrement returns the counters to zero
+// for the next rebuild, so no memset is needed between rebuilds.
+static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const int* __restrict__ start, int* __restrict__ cnt,
+                               int* __restrict__ sorted) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int k = key[i];
+    int slot = start[k] + atomicSub(cnt + k, 1) - 1;
+    sorted[slot] = i;
+}
+
+// Restores ascending order inside each cell, by orderKey[value] (or by the
+// value itself when orderKey is null): the stable order of the reference sort.
+static __global__ void k_cell_order(int ncell, const int* __restrict__ start, int* __restrict__ sorted,
+                             const int* __restrict__ orderKey) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int b = start[c], e = start[c + 1];
+    if (e - b < 2) return;
+    for (int i = b + 1; i < e; i++) {
+        int v = sorted[i];
+        int kv = orderKey ? orderKey[v] : v;
+        int j = i - 1;
+        while (j >= b) {
+            int u = sorted[j];
+            int ku = orderKey ? orderKey[u] : u;
+            if (ku <= kv) break;
+            sorted[j + 1] = u;
+            j--;
+        }
+        sorted[j + 1] = v;
+    }
+}
+
+// Host side: owns the cell arrays of one grid and builds them on a stream.
+struct CellTable {
+    GridDesc g{};
+    int ncell = 0;
+    DBuf<int> key, cnt, start, sorted;
+    std::vector<DBuf<int>*> scanTmp;  // per-level tile sums / offsets
+    int launches = 0;                 // kernels issued by the last build
+
+    ~CellTable() {
+        for (auto* b : scanTmp) delete b;
+    }
+    void setup(const GridDesc& grid, int nobj, cudaStream_t s) {
+        g = grid;
+        ncell = g.ncell();
+        key.alloc(nobj > 0 ? nobj : 1, s, false);
+        sorted.alloc(nobj > 0 ? nobj : 1, s, false);
+        cnt.alloc(ncell, s, true);
+        start.alloc((size_t)ncell + 1, s, true);
+        for (auto* b : scanTmp) delete b;
+        scanTmp.clear();
+        int m = ncell;
+        while (m > kScanTile) {
+            int nt = (m + kScanTile - 1) / kScanTile;
+            auto* sums = new DBuf<int>();
+            sums->alloc(nt, s, true);
+            auto* offs = new DBuf<int>();
+            offs->alloc((size_t)nt + 1, s, true);
+            scanTmp.push_back(sums);
+            scanTmp.push_back(offs);
+            m = nt;
+        }
+    }
+    // Exclusive scan of in[0..n) into out[0..n], recursing over tile sums.
+    void scan(const int* in, int* out, int n, int level, cudaStream_t s) {
+        if (n <= kScanTile) {
+            k_scan_tile<<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, nullptr);
+            launches++;
+            return;
+        }
+        int nt = (n + kScanTile - 1) / kScanTile;
+        int* sums = scanTmp[2 * level]->p;
+        int* offs = scanTmp[2 * level + 1]->p;
+        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, nullptr, n, nullptr, sums);
+        launches++;
+        scan(sums, offs, nt, level + 1, s);
+        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, out, n, offs, nullptr);
+        launches++;
+    }
+    // Sorts objects p[0..n) (positions in .xyz) into cells.
+    void build(const double4* p, int n, cudaStream_t s, const int* orderKey = nullptr) {
+        launches = 0;
+        if (n > 0) {
+            k_cell_count<<<grid_for(n, 256), 256, 0, s>>>(p, n, g, key.p, cnt.p);
+            launches++;
+        }
+        scan(cnt.p, start.p, ncell, 0, s);
+        if (n > 0) {
+            k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, sorted.p);
+            k_cell_order<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, start.p, sorted.p, orderKey);
+            launches += 2;
+        }
+        DEMSPH_LAUNCH_CHECK();
+    }
+};
+
+}  // namespace demsph

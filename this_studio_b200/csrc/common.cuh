@@ -1,0 +1,254 @@
+// Shared device math, status codes and device-buffer ownership for the
+// DEMSPH B200 library.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/demsph.h"
+
+namespace demsph {
+
+// ----------------------------------------------------------------- errors --
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
+};
+struct Status : std::runtime_error {
+    int code;
+    Status(int c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+#define DEMSPH_CUDA(call)                                                                  \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            char b_[512];                                                                  \
+            snprintf(b_, sizeof b_, "%s:%d %s: %s", __FILE__, __LINE__, #call,             \
+                     cudaGetErrorString(e_));                                              \
+            throw ::demsph::CudaError(e_, b_);                                             \
+        }                                                                                  \
+    } while (0)
+
+#define DEMSPH_LAUNCH_CHECK() DEMSPH_CUDA(cudaGetLastError())
+
+// Last error text, per thread, readable through demsph_last_error().
+void set_last_error(const std::string& s);
+
+// Runs f, converting exceptions into the C-ABI status convention.
+template <class F>
+static inline int guarded(F&& f) {
+    try {
+        f();
+        return DEMSPH_OK;
+    } catch (const Status& s) {
+        set_last_error(s.what());
+        return s.code;
+    } catch (const CudaError& e) {
+        set_last_error(e.what());
+        return DEMSPH_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return DEMSPH_ERR_ALLOC;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return DEMSPH_ERR_INVALID;
+    }
+}
+
+// ---------------------------------------------------------- device buffer --
+// Owns a device allocation made with cudaMallocAsync on the owner's stream.
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, cudaStream_t stream, bool zero = true) {
+        release();
+        s = stream;
+        n = count;
+        if (count == 0) return;
+        DEMSPH_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
+        if (zero) DEMSPH_CUDA(cudaMemsetAsync(p, 0, count * sizeof(T), stream));
+    }
+    // Grows to at least count elements, keeping the first n elements.
+    void grow(size_t count, cudaStream_t stream) {
+        if (count <= n) return;
+        T* q = nullptr;
+        DEMSPH_CUDA(cudaMallocAsync((void**)&q, count * sizeof(T), stream));
+        DEMSPH_CUDA(cudaMemsetAsync(q, 0, count * sizeof(T), stream));
+        if (p && n) DEMSPH_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+        if (p) cudaFreeAsync(p, s);
+        p = q;
+        n = count;
+        s = stream;
+    }
+    void upload(const std::vector<T>& h, cudaStream_t stream) {
+        alloc(h.size(), stream, false);
+        if (!h.empty()) DEMSPH_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    }
+    void download(std::vector<T>& h, cudaStream_t stream) const {
+        h.resize(n);
+        if (n) DEMSPH_CUDA(cudaMemcpyAsync(h.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+static inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+// ------------------------------------------------------------ vector math --
+// double3 algebra in the form the reference uses (myVec.h:25-176).
+__host__ __device__ __forceinline__ double3 mk3(double x, double y, double z) { return make_double3(x, y, z); }
+__host__ __device__ __forceinline__ double3 operator+(double3 a, double3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ double3 operator-(double3 a, double3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ double3 operator-(double3 a) { return mk3(-a.x, -a.y, -a.z); }
+__host__ __device__ __forceinline__ double3 operator*(double3 a, double s) { return mk3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ double3 operator*(double s, double3 a) { return mk3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ double3 operator/(double3 a, double s) { double i = 1.0 / s; return mk3(a.x * i, a.y * i, a.z * i); }
+__host__ __device__ __forceinline__ double3& operator+=(double3& a, double3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+__host__ __device__ __forceinline__ double3& operator-=(double3& a, double3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
+__host__ __device__ __forceinline__ double3& operator*=(double3& a, double s) { a.x *= s; a.y *= s; a.z *= s; return a; }
+__host__ __device__ __forceinline__ double dot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ double3 cross(double3 a, double3 b) {
+    return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ double len2(double3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+__host__ __device__ __forceinline__ double len(double3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__host__ __device__ __forceinline__ double3 normalize(double3 v) {
+    double l2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    if (l2 < 1.0e-20) return mk3(0, 0, 0);
+    double inv = 1.0 / sqrt(l2);
+    return mk3(v.x * inv, v.y * inv, v.z * inv);
+}
+__host__ __device__ __forceinline__ double3 xyz(double4 a) { return mk3(a.x, a.y, a.z); }
+__host__ __device__ __forceinline__ double4 d4(double3 a, double w) { return make_double4(a.x, a.y, a.z, w); }
+
+// float3 algebra for the mixed-precision force laws.
+__host__ __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__host__ __device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ float3& operator+=(float3& a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+__host__ __device__ __forceinline__ float3& operator-=(float3& a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
+__host__ __device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ float len(float3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+// Precision traits: V<double> = double3, V<float> = float3.
+template <class R> struct VecOf;
+template <> struct VecOf<double> { using T = double3; };
+template <> struct VecOf<float> { using T = float3; };
+template <class R> using V = typename VecOf<R>::T;
+
+template <class R> __host__ __device__ __forceinline__ V<R> cvt(double3 a);
+template <> __host__ __device__ __forceinline__ double3 cvt<double>(double3 a) { return a; }
+template <> __host__ __device__ __forceinline__ float3 cvt<float>(double3 a) { return make_float3((float)a.x, (float)a.y, (float)a.z); }
+__host__ __device__ __forceinline__ double3 up(double3 a) { return a; }
+__host__ __device__ __forceinline__ double3 up(float3 a) { return mk3(a.x, a.y, a.z); }
+template <class R> __host__ __device__ __forceinline__ V<R> v3r(R x, R y, R z);
+template <> __host__ __device__ __forceinline__ double3 v3r<double>(double x, double y, double z) { return mk3(x, y, z); }
+template <> __host__ __device__ __forceinline__ float3 v3r<float>(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ double rsq(double x) { return sqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rlen(double3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ float rlen(float3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+static constexpr double kPi = 3.14159265358979323846;
+
+// ----------------------------------------------------------------- grid ---
+// spatialGrid (DEMSPH/kernel/boundary.h:70-94): cells of at least the
+// requested size tiling [mn, mx); keys z*ny*nx + y*nx + x.
+struct GridDesc {
+    double3 mn, mx, cs;
+    int nx, ny, nz;
+    int ncell() const { return nx * ny * nz; }
+};
+static inline bool grid_set(GridDesc& g, double3 mn, double3 mx, double cell) {
+    if (mx.x <= mn.x || mx.y <= mn.y || mx.z <= mn.z || cell < 1.e-20) return false;
+    g.mn = mn;
+    g.mx = mx;
+    double3 d = mx - mn;
+    g.nx = d.x > cell ? int(d.x / cell) : 1;
+    g.ny = d.y > cell ? int(d.y / cell) : 1;
+    g.nz = d.z > cell ? int(d.z / cell) : 1;
+    g.cs = mk3(d.x / double(g.nx), d.y / double(g.ny), d.z / double(g.nz));
+    return true;
+}
+// calculateGridPosition (neighborSearchKernel.cuh:4-9): truncation toward zero.
+__device__ __forceinline__ int3 cell_of(double3 p, const GridDesc& g) {
+    return make_int3(int((p.x - g.mn.x) / g.cs.x), int((p.y - g.mn.y) / g.cs.y), int((p.z - g.mn.z) / g.cs.z));
+}
+__device__ __forceinline__ int key_of(int3 c, const GridDesc& g) { return c.z * g.ny * g.nx + c.y * g.nx + c.x; }
+// calculateHash kernel (neighborSearchKernel.cu:6-27): clamp into the domain first.
+__device__ __forceinline__ int clamped_key(double3 p, const GridDesc& g) {
+    if (p.x < g.mn.x) p.x = g.mn.x; else if (p.x >= g.mx.x) p.x = g.mx.x - 0.5 * g.cs.x;
+    if (p.y < g.mn.y) p.y = g.mn.y; else if (p.y >= g.mx.y) p.y = g.mx.y - 0.5 * g.cs.y;
+    if (p.z < g.mn.z) p.z = g.mn.z; else if (p.z >= g.mx.z) p.z = g.mx.z - 0.5 * g.cs.z;
+    int3 c = cell_of(p, g);
+    // A coordinate within an ulp below the max face can round up to index n
+    // (and NaN converts to an arbitrary int); keep the key inside the table.
+    c.x = min(max(c.x, 0), g.nx - 1);
+    c.y = min(max(c.y, 0), g.ny - 1);
+    c.z = min(max(c.z, 0), g.nz - 1);
+    return key_of(c, g);
+}
+// The 27-cell stencil with the reference's index clamping
+// (ballNeighborSearchKernel.cu:25-46).  The three x-neighbours of a row are
+// consecutive keys, so each (y, z) row is ONE contiguous range of the
+// cell-sorted index list: nine ranges instead of 27 lookups, visited in the
+// reference's (z, y, x) order.
+struct Stencil {
+    int3 c, s, e;
+};
+__device__ __forceinline__ Stencil stencil_of(double3 p, const GridDesc& g) {
+    Stencil st;
+    st.c = cell_of(p, g);
+    st.s = make_int3(-1, -1, -1);
+    st.e = make_int3(1, 1, 1);
+    if (st.c.x <= 0) { st.c.x = 0; st.s.x = 0; }
+    if (st.c.x >= g.nx - 1) { st.c.x = g.nx - 1; st.e.x = 0; }
+    if (st.c.y <= 0) { st.c.y = 0; st.s.y = 0; }
+    if (st.c.y >= g.ny - 1) { st.c.y = g.ny - 1; st.e.y = 0; }
+    if (st.c.z <= 0) { st.c.z = 0; st.s.z = 0; }
+    if (st.c.z >= g.nz - 1) { st.c.z = g.nz - 1; st.e.z = 0; }
+    return st;
+}
+// Calls f(begin, end) for each stencil row range of the sorted list.
+// cellStart has ncell+1 entries (exclusive scan of the cell counts).
+template <class F>
+__device__ __forceinline__ void for_stencil_rows(const Stencil& st, const GridDesc& g, const int* __restrict__ cellStart, F&& f) {
+    for (int zz = st.s.z; zz <= st.e.z; zz++)
+        for (int yy = st.s.y; yy <= st.e.y; yy++) {
+            int k0 = key_of(make_int3(st.c.x + st.s.x, st.c.y + yy, st.c.z + zz), g);
+            int k1 = key_of(make_int3(st.c.x + st.e.x, st.c.y + yy, st.c.z + zz), g);
+            int b = __ldg(cellStart + k0), e = __ldg(cellStart + k1 + 1);
+            if (b < e) f(b, e);
+        }
+}
+
+// Device status word shared by the kernels of one scene.  Kernels record
+// capacity overflows here instead of writing out of bounds.
+struct DevStatus {
+    int overflow;      // nonzero: a list overflowed its capacity
+    int need_pairs;    // largest per-row count seen for the ball/fluid list
+    int need_rev;      // largest reverse-list count
+    int need_aux;      // largest per-row count for the secondary list
+};
+
+}  // namespace demsph

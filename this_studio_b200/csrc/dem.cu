@@ -1,0 +1,1555 @@
+// DEM path of the DEMSPH B200 library: neighbour search with contact-history
+// carry, contact / bond forces, mesh-wall contact, clump and sphere
+// integration, and the scene runtime behind the demsph_dem_* C ABI.
+//
+// Layout in HBM (one scene):
+//   balls   pos (x,y,z,r) | vel (vx,vy,vz,1/m) | angv (wx,wy,wz,-) : double4 SoA
+//   pairs   ELL, column-major: slot(k, A) = k*N + A for the k-th partner B>A of
+//           ball A; ids int32, springs double4, per-slot force / B-side torque.
+//           Double-buffered across rebuilds so history carries old -> new.
+//   reverse per-ball list of the slots in which the ball is the B side.
+//   walls   triangle (i0,i1,i2,wall) int4, vertices double4, per-ball ELL of
+//           candidate triangles with their springs (double-buffered per call).
+// Kernels walk balls in cell order (the order array of the last rebuild) so
+// that neighbouring threads touch neighbouring memory.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <map>
+#include <memory>
+
+#include "cells.cuh"
+#include "dem_physics.cuh"
+
+namespace demsph {
+
+extern std::atomic<long long> g_launches;
+
+// Everything a DEM kernel needs, passed by value.
+struct DemDev {
+    int N, K, KR, KT;
+    int nBond, nTri, nVert, nWall, nClump;
+    int nMat, cap;
+    int roll, tors;
+    GridDesc bg, tg;
+    const MatPair* mats;
+    double4* pos;
+    double4* vel;
+    double4* angv;
+    double4* force;
+    double4* torque;
+    double4* forceA;
+    double4* torqueA;
+    const int* mat;
+    const int* clump;
+    const int* order;      // cell-sorted ball list
+    const int* cellStart;  // ball grid
+    // current / previous pair lists
+    int* pj;
+    int* pcnt;
+    double4* spS;
+    double4* spR;
+    double4* spT;
+    const int* pjOld;
+    const int* pcntOld;
+    const double4* spSOld;
+    const double4* spROld;
+    const double4* spTOld;
+    double4* pF;
+    double4* pTB;
+    int* rcnt;
+    int* rslot;
+    // bonds
+    const int2* bab;
+    int* bok;
+    double4* bpoint;
+    double4* bnormal;
+    double4* bFs;
+    double4* bTb;
+    double* bFn;
+    double* bTt;
+    double* bsmax;
+    double* btmax;
+    double4* bF;
+    double4* bTA;
+    double4* bTB;
+    const int* bincStart;
+    const int* binc;
+    // mesh walls
+    double4* wpos;
+    double4* wvel;
+    double4* wangv;
+    double4* wq;
+    const int* wmat;
+    const double4* vlocal;
+    double4* vglobal;
+    const int* vwall;
+    const int4* tris;
+    double4* tcenter;
+    const int* triOrder;
+    const int* triCellStart;
+    int* wtj;
+    int* wcnt;
+    double4* wS;
+    double4* wR;
+    double4* wT;
+    const int* wtjOld;
+    const int* wcntOld;
+    const double4* wSOld;
+    const double4* wROld;
+    const double4* wTOld;
+    // clumps
+    double4* cpos;
+    double4* cvel;
+    double4* cangv;
+    double4* cforce;
+    double4* ctorque;
+    double4* cq;
+    const double4* cinvIa;
+    const double4* cinvIb;
+    const double* cinvm;
+    const int2* cpeb;
+    // external force hook
+    const double4* fconst;
+    double framp;
+    double damp;
+    int buoy;
+    double brho, bcd, blevel;
+    double3 bg3, bu;
+    double3 gravity;
+    DevStatus* status;
+};
+
+// ------------------------------------------------------------ rebuild ------
+// countBallInteractionsKernel + writeBallInteractionsKernel
+// (ballNeighborSearchKernel.cu:6-151) as one pass: candidate B > A, not both
+// fixed, not the same clump, |r_AB| <= 1.1 (r_A + r_B); rows in the
+// reference's stencil order; springs carried from A's previous row.
+__global__ void k_dem_build_pairs(DemDev d) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    const int A = d.order[t];
+    const double4 pa = d.pos[A];
+    const double3 ra = xyz(pa);
+    const double imA = d.vel[A].w;
+    const int clA = d.clump[A];
+    const int oldCnt = d.pcntOld ? d.pcntOld[A] : 0;
+    int cnt = 0;
+    Stencil st = stencil_of(ra, d.bg);
+    for_stencil_rows(st, d.bg, d.cellStart, [&](int b, int e) {
+        for (int k = b; k < e; k++) {
+            const int B = d.order[k];
+            if (A >= B) continue;
+            const double imB = d.vel[B].w;
+            if (imA == 0 && imB == 0) continue;
+            const int clB = d.clump[B];
+            if (clB >= 0 && clA == clB) continue;
+            const double4 pb = d.pos[B];
+            double cut = 1.1 * (pa.w + pb.w);
+            double3 r = ra - xyz(pb);
+            if ((cut * cut - dot(r, r)) >= 0.) {
+                if (cnt < d.K) {
+                    size_t slot = (size_t)cnt * d.N + A;
+                    d.pj[slot] = B;
+                    double4 s = make_double4(0, 0, 0, 0), rr = s, tt = s;
+                    for (int q = 0; q < oldCnt; q++) {
+                        size_t os = (size_t)q * d.N + A;
+                        if (d.pjOld[os] == B) {
+                            s = d.spSOld[os];
+                            if (d.roll) rr = d.spROld[os];
+                            if (d.tors) tt = d.spTOld[os];
+                            break;
+                        }
+                    }
+                    d.spS[slot] = s;
+                    if (d.roll) d.spR[slot] = rr;
+                    if (d.tors) d.spT[slot] = tt;
+                }
+                cnt++;
+            }
+        }
+    });
+    if (cnt > d.K) {
+        atomicMax(&d.status->need_pairs, cnt);
+        atomicExch(&d.status->overflow, 1);
+        cnt = d.K;
+    }
+    d.pcnt[A] = cnt;
+}
+
+// Reverse incidence: for each pair slot, record it in the B ball's list.
+__global__ void k_dem_reverse(DemDev d) {
+    int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= d.N) return;
+    int c = d.pcnt[A];
+    for (int k = 0; k < c; k++) {
+        int slot = k * d.N + A;
+        int B = d.pj[slot];
+        int r = atomicAdd(d.rcnt + B, 1);
+        if (r < d.KR) {
+            d.rslot[(size_t)r * d.N + B] = slot;
+        } else {
+            atomicMax(&d.status->need_rev, r + 1);
+            atomicExch(&d.status->overflow, 1);
+        }
+    }
+}
+// Orders each reverse list by the A ball (the reference's stable sort of the
+// pairs by objectPointing, DEMSolver.h:59-78), for a deterministic sum.
+__global__ void k_dem_reverse_order(DemDev d) {
+    int B = blockIdx.x * blockDim.x + threadIdx.x;
+    if (B >= d.N) return;
+    int c = d.rcnt[B];
+    if (c > d.KR) { c = d.KR; d.rcnt[B] = c; }
+    for (int i = 1; i < c; i++) {
+        int v = d.rslot[(size_t)i * d.N + B];
+        int kv = v % d.N;
+        int j = i - 1;
+        while (j >= 0) {
+            int u = d.rslot[(size_t)j * d.N + B];
+            if (u % d.N <= kv) break;
+            d.rslot[(size_t)(j + 1) * d.N + B] = u;
+            j--;
+        }
+        d.rslot[(size_t)(j + 1) * d.N + B] = v;
+    }
+}
+
+// ------------------------------------------------------- force evaluation --
+// updateBallContactKernel + calBallContactForceTorqueKernel
+// (contactKernel.cu:135-259) for every pair in ball A's row, fused with the
+// A-side sum of sumObjectPointedForceTorqueFromInteractionKernel
+// (contactKernel.cu:657-681).  The pair force and the B-side torque
+// contribution -(T_c + (r_c - r_B) x F_c) are stored for the B side.
+template <class R>
+__global__ void __launch_bounds__(256) k_dem_pair_forces(DemDev d, double dt) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    const int A = d.order[t];
+    const double4 pa = d.pos[A];
+    const double3 ra = xyz(pa);
+    const double4 va4 = d.vel[A];
+    const double3 va = xyz(va4);
+    const double3 wa = xyz(d.angv[A]);
+    const int matA = d.mat[A];
+    const int c = d.pcnt[A];
+    double3 FA = mk3(0, 0, 0), TA = mk3(0, 0, 0);
+    for (int k = 0; k < c; k++) {
+        size_t slot = (size_t)k * d.N + A;
+        int B = d.pj[slot];
+        double4 pb = d.pos[B];
+        double3 rb = xyz(pb);
+        double4 vb4 = d.vel[B];
+        double3 wb = xyz(d.angv[B]);
+        double3 rij = ra - rb;
+        double3 n = normalize(rij);
+        double delta = pa.w + pb.w - len(rij);
+        double3 rc = rb + (pb.w - 0.5 * delta) * n;
+        double Rad = pa.w * pb.w / (pa.w + pb.w);
+        double m = 1. / (va4.w + vb4.w);
+        double3 vc = va + cross(wa, rc - ra) - (xyz(vb4) + cross(wb, rc - rb));
+        double3 wij = wa - wb;
+        const MatPair mp = d.mats[pair_param_index(matA, d.mat[B], d.nMat, d.cap)];
+        double4 s4 = d.spS[slot];
+        double3 es = xyz(s4), er = mk3(0, 0, 0), et = mk3(0, 0, 0);
+        if (d.roll) er = xyz(d.spR[slot]);
+        if (d.tors) et = xyz(d.spT[slot]);
+        V<R> F, T;
+        contact_law<R>(mp, F, T, es, er, et, vc, wij, n, delta, m, Rad, dt, d.roll, d.tors);
+        d.spS[slot] = d4(es, 0);
+        if (d.roll) d.spR[slot] = d4(er, 0);
+        if (d.tors) d.spT[slot] = d4(et, 0);
+        double3 Fd = up(F), Td = up(T);
+        d.pF[slot] = d4(Fd, 0);
+        d.pTB[slot] = d4(-Td - cross(rc - rb, Fd), 0);
+        FA += Fd;
+        TA += Td + cross(rc - ra, Fd);
+    }
+    d.forceA[A] = d4(FA, 0);
+    d.torqueA[A] = d4(TA, 0);
+}
+
+// calBondedForceTorqueKernel (contactKernel.cu:535-655).  Instead of adding
+// into the pair (bond with a contact pair) or FP64 atomics (without), each
+// bond stores its contributions to both balls; the per-ball pass sums them
+// over a static incidence list, so the result is deterministic.
+__global__ void k_dem_bonds(DemDev d, double dt) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.nBond) return;
+    if (d.bok[b] == 0) {
+        d.bFn[b] = 0;
+        d.bTt[b] = 0;
+        d.bFs[b] = make_double4(0, 0, 0, 0);
+        d.bTb[b] = make_double4(0, 0, 0, 0);
+        d.bF[b] = make_double4(0, 0, 0, 0);
+        d.bTA[b] = make_double4(0, 0, 0, 0);
+        d.bTB[b] = make_double4(0, 0, 0, 0);
+        return;
+    }
+    int2 ab = d.bab[b];
+    int i = ab.x, j = ab.y;
+    double4 pi4 = d.pos[i], pj4 = d.pos[j];
+    double3 ri = xyz(pi4), rj = xyz(pj4);
+    double3 n0 = xyz(d.bnormal[b]);
+    double3 n = normalize(ri - rj);
+    double delta = pi4.w + pj4.w - len(ri - rj);
+    double3 rc = rj + (pj4.w - 0.5 * delta) * n;
+    // The reference takes r_c and n from the matching contact pair when one
+    // exists; that pair computed them with these same expressions.
+    bool found = false;
+    int c = d.pcnt[i];
+    for (int k = 0; k < c; k++) {
+        if (d.pj[(size_t)k * d.N + i] == j) { found = true; break; }
+    }
+    d.bpoint[b] = d4(rc, 0);
+    d.bnormal[b] = d4(n, 0);
+    double3 wi = xyz(d.angv[i]), wj = xyz(d.angv[j]);
+    double3 vc = xyz(d.vel[i]) + cross(wi, rc - ri) - (xyz(d.vel[j]) + cross(wj, rc - rj));
+    const MatPair mp = d.mats[pair_param_index(d.mat[i], d.mat[j], d.nMat, d.cap)];
+    double Fn = d.bFn[b], Tt = d.bTt[b];
+    double3 Fs = xyz(d.bFs[b]), Tb = xyz(d.bTb[b]);
+    double smax = d.bsmax[b], tmax = d.btmax[b];
+    d.bok[b] = parallel_bond(Fn, Tt, Fs, Tb, smax, tmax, n0, n, vc, wi, wj, pi4.w, pj4.w, dt, mp);
+    d.bFn[b] = Fn;
+    d.bTt[b] = Tt;
+    d.bFs[b] = d4(Fs, 0);
+    d.bTb[b] = d4(Tb, 0);
+    d.bsmax[b] = smax;
+    d.btmax[b] = tmax;
+    double3 Fb = Fn * n + Fs;
+    double3 Tn = Tt * n + Tb;
+    d.bF[b] = d4(Fb, 0);
+    if (!found) {
+        d.bTA[b] = d4(Tn + cross(rc - ri, Fs), 0);
+        d.bTB[b] = d4(-Tt * n - Tb + cross(rc - rj, -Fs), 0);
+    } else {
+        d.bTA[b] = d4(Tn + cross(rc - ri, Fb), 0);
+        d.bTB[b] = d4(-Tn - cross(rc - rj, Fb), 0);
+    }
+}
+
+// Per-ball finish of one force evaluation:
+//  * B-side pair sum (sumObjectPointingForceTorqueFromInteractionKernel,
+//    contactKernel.cu:683-714) and bond contributions;
+//  * mesh-wall contact: candidate triangles by AABB over the triangle grid
+//    with spring carry (count/writeBallTriangleInteractionsKernel,
+//    ballNeighborSearchKernel.cu:153-338), edge/vertex de-duplication
+//    (updateBallTriangleContact, contactKernel.cu:261-418) and the wall law
+//    (calBallWallContactForceTorqueKernel, contactKernel.cu:420-533);
+//  * the external force hook (externalForceTorque.cu);
+//  * optionally the half-kick (+ drift) of ballIntegrationKernel.cu:30-56,112-121.
+constexpr int kMaxTriPerBall = 32;
+template <class R>
+__global__ void __launch_bounds__(128) k_dem_finalize(DemDev d, double dtWall, double extTime, int ext, int integ,
+                                                      double hdt) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    const int i = d.order[t];
+    double3 F = xyz(d.forceA[i]), T = xyz(d.torqueA[i]);
+    const int rc = d.rcnt[i];
+    for (int r = 0; r < rc; r++) {
+        int slot = d.rslot[(size_t)r * d.N + i];
+        F -= xyz(d.pF[slot]);
+        T += xyz(d.pTB[slot]);
+    }
+    if (d.nBond) {
+        for (int q = d.bincStart[i]; q < d.bincStart[i + 1]; q++) {
+            int e = d.binc[q];
+            int b = e >> 1;
+            if (e & 1) { F -= xyz(d.bF[b]); T += xyz(d.bTB[b]); }
+            else { F += xyz(d.bF[b]); T += xyz(d.bTA[b]); }
+        }
+    }
+    const double4 p4 = d.pos[i];
+    const double3 ri = xyz(p4);
+    const double4 v4 = d.vel[i];
+    if (d.nTri) {
+        // candidate triangles in the reference's stencil order
+        int tri[kMaxTriPerBall];
+        int cnt = 0;
+        Stencil st = stencil_of(ri, d.tg);
+        const double r2 = p4.w * p4.w;
+        for_stencil_rows(st, d.tg, d.triCellStart, [&](int b, int e) {
+            for (int k = b; k < e; k++) {
+                int tj = d.triOrder[k];
+                int4 tv = d.tris[tj];
+                double3 a = xyz(d.vglobal[tv.x]), bb = xyz(d.vglobal[tv.y]), c = xyz(d.vglobal[tv.z]);
+                double cx = fmin(fmax(ri.x, fmin(a.x, fmin(bb.x, c.x))), fmax(a.x, fmax(bb.x, c.x)));
+                double cy = fmin(fmax(ri.y, fmin(a.y, fmin(bb.y, c.y))), fmax(a.y, fmax(bb.y, c.y)));
+                double cz = fmin(fmax(ri.z, fmin(a.z, fmin(bb.z, c.z))), fmax(a.z, fmax(bb.z, c.z)));
+                double dx = ri.x - cx, dy = ri.y - cy, dz = ri.z - cz;
+                if (dx * dx + dy * dy + dz * dz <= r2) {
+                    if (cnt < d.KT && cnt < kMaxTriPerBall) tri[cnt] = tj;
+                    cnt++;
+                }
+            }
+        });
+        if (cnt > d.KT || cnt > kMaxTriPerBall) {
+            atomicMax(&d.status->need_aux, cnt);
+            atomicExch(&d.status->overflow, 1);
+            cnt = min(d.KT, kMaxTriPerBall);
+        }
+        // springs: carry from this ball's previous candidate row
+        double3 sS[kMaxTriPerBall], sR[kMaxTriPerBall], sT[kMaxTriPerBall];
+        double3 cp[kMaxTriPerBall];
+        int type[kMaxTriPerBall];
+        const int oc = d.wcntOld ? d.wcntOld[i] : 0;
+        for (int c = 0; c < cnt; c++) {
+            sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
+            for (int q = 0; q < oc; q++) {
+                size_t os = (size_t)q * d.N + i;
+                if (d.wtjOld[os] == tri[c]) {
+                    sS[c] = xyz(d.wSOld[os]);
+                    if (d.roll) sR[c] = xyz(d.wROld[os]);
+                    if (d.tors) sT[c] = xyz(d.wTOld[os]);
+                    break;
+                }
+            }
+            int4 tv = d.tris[tri[c]];
+            cp[c] = mk3(0, 0, 0);
+            type[c] = classify_sphere_triangle(ri, p4.w, xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]),
+                                               xyz(d.vglobal[tv.z]), cp[c]);
+        }
+        // de-duplication, sequential as in the reference thread
+        unsigned cancel = 0;
+        for (int c = 0; c < cnt; c++) {
+            if (type[c] == kCtNone) {
+                sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
+                cancel |= 1u << c;
+                continue;
+            }
+            if (type[c] == kCtFace) continue;
+            for (int c1 = 0; c1 < cnt; c1++) {
+                if (c1 == c) continue;
+                int t1 = type[c1];
+                bool copy = false;
+                if (t1 == kCtNone) continue;
+                if (t1 == kCtFace) {
+                    int4 tv = d.tris[tri[c1]];
+                    double3 q0 = xyz(d.vglobal[tv.x]), q1 = xyz(d.vglobal[tv.y]), q2 = xyz(d.vglobal[tv.z]);
+                    if (len2(cross(cp[c] - q0, q1 - q0)) < 1.e-20) copy = true;
+                    else if (len2(cross(cp[c] - q1, q2 - q1)) < 1.e-20) copy = true;
+                    else if (len2(cross(cp[c] - q0, q2 - q0)) < 1.e-20) copy = true;
+                } else if (t1 == kCtEdge) {
+                    if (type[c] == t1) { if (c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true; }
+                    else if (len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
+                } else {
+                    if (type[c] == t1 && c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
+                }
+                if (copy) {
+                    sS[c] = sS[c1]; sR[c] = sR[c1]; sT[c] = sT[c1];
+                    cancel |= 1u << c;
+                    break;
+                }
+            }
+        }
+        // wall law (fixed balls skip it, as calBallWallContactForceTorqueKernel returns early)
+        if (!(v4.w < 1.e-20)) {
+            const double3 vi = xyz(v4), wi = xyz(d.angv[i]);
+            const double m = 1. / v4.w;
+            const int mi = d.mat[i];
+            for (int c = 0; c < cnt; c++) {
+                if (cancel & (1u << c)) continue;
+                int wj = d.tris[tri[c]].w;
+                double3 n = normalize(ri - cp[c]);
+                double delta = p4.w - len(ri - cp[c]);
+                double3 rj = xyz(d.wpos[wj]), vj = xyz(d.wvel[wj]), wwj = xyz(d.wangv[wj]);
+                double3 vc = vi + cross(wi, cp[c] - ri) - (vj + cross(wwj, cp[c] - rj));
+                double3 wij = wi - wwj;
+                const MatPair mp = d.mats[pair_param_index(mi, d.wmat[wj], d.nMat, d.cap)];
+                V<R> Fc, Tc;
+                contact_law<R>(mp, Fc, Tc, sS[c], sR[c], sT[c], vc, wij, n, delta, m, p4.w, dtWall, d.roll, d.tors);
+                double3 Fd = up(Fc);
+                F += Fd;
+                T += up(Tc) + cross(cp[c] - ri, Fd);
+            }
+        }
+        for (int c = 0; c < cnt; c++) {
+            size_t s = (size_t)c * d.N + i;
+            d.wtj[s] = tri[c];
+            d.wS[s] = d4(sS[c], 0);
+            if (d.roll) d.wR[s] = d4(sR[c], 0);
+            if (d.tors) d.wT[s] = d4(sT[c], 0);
+        }
+        d.wcnt[i] = cnt;
+    }
+    if (ext) {
+        // launchAddConstantForce (externalForceTorque.cu:4-24)
+        if (d.fconst) {
+            double c = 1.0;
+            if (d.framp > 0) { c = extTime / d.framp; if (c > 1.0) c = 1.0; }
+            F += xyz(d.fconst[i]) * c;
+        }
+        // launchAddGlobalDampingForceTorque (externalForceTorque.cu:26-57)
+        if (d.damp != 0) {
+            double3 f0 = F, t0 = T;
+            F -= d.damp * len(f0) * normalize(xyz(v4));
+            T -= d.damp * len(t0) * normalize(xyz(d.angv[i]));
+        }
+        // addBuoyancyDragKernel (externalForceTorque.cu:66-133)
+        if (d.buoy && !(v4.w <= 0.0)) {
+            double r = p4.w;
+            double dd = d.blevel - ri.z;
+            double Vsub;
+            if (dd <= -r) Vsub = 0.0;
+            else if (dd >= r) Vsub = (4.0 / 3.0) * kPi * r * r * r;
+            else { double h = dd + r; Vsub = (kPi * h * h * (3.0 * r - h)) / 3.0; }
+            if (Vsub > 0.0) {
+                double3 Fb = mk3(-d.brho * Vsub * d.bg3.x, -d.brho * Vsub * d.bg3.y, -d.brho * Vsub * d.bg3.z);
+                double Vs = (4.0 / 3.0) * kPi * r * r * r;
+                double alpha = (Vs > 1.e-30) ? (Vsub / Vs) : 0.0;
+                double3 vr = xyz(v4) - d.bu;
+                double v2 = dot(vr, vr);
+                double3 Fdr = mk3(0, 0, 0);
+                if (v2 > 1.e-30 && d.bcd > 0.0) {
+                    double vm = sqrt(v2);
+                    double Aeff = alpha * (kPi * r * r);
+                    double kk = 0.5 * d.brho * d.bcd * Aeff * vm;
+                    Fdr = mk3(-kk * vr.x, -kk * vr.y, -kk * vr.z);
+                }
+                F.x += Fb.x + Fdr.x;
+                F.y += Fb.y + Fdr.y;
+                F.z += Fb.z + Fdr.z;
+            }
+        }
+    }
+    d.force[i] = d4(F, 0);
+    d.torque[i] = d4(T, 0);
+    if (integ) {
+        // ballVelocityAngularVelocityIntegrationKernel (ballIntegrationKernel.cu:30-56)
+        double3 v = xyz(v4);
+        double im = v4.w;
+        if (d.clump[i] < 0 && !(im < 1.e-20)) {
+            v += (F * im + d.gravity) * hdt;
+            d.vel[i] = d4(v, im);
+            if (!(p4.w < 1.e-20)) {
+                double I = 0.4 * p4.w * p4.w / im;
+                double3 w = xyz(d.angv[i]) + T / I * hdt;
+                d.angv[i] = d4(w, 0);
+            }
+        }
+        // positionIntegrationKernel (ballIntegrationKernel.cu:112-121), first half only
+        if (integ == 1) d.pos[i] = d4(ri + (2.0 * hdt) * v, p4.w);
+    }
+}
+
+// ----------------------------------------------------------- integration --
+// sumClumpForceTorqueKernel (ballIntegrationKernel.cu:3-28, Q1 corrected: the
+// pebble forces are summed) + clumpVelocityAngularVelocityIntegrationKernel
+// (:58-79) + in the first half the clump drift and quaternion update (:101-121).
+__global__ void k_dem_clumps(DemDev d, double hdt, int first) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.nClump) return;
+    int2 pe = d.cpeb[c];
+    double3 cp = xyz(d.cpos[c]);
+    double3 Fc = mk3(0, 0, 0), Tc = mk3(0, 0, 0);
+    for (int i = pe.x; i < pe.y; i++) {
+        double3 Fi = xyz(d.force[i]);
+        Fc += Fi;
+        Tc += xyz(d.torque[i]) + cross(xyz(d.pos[i]) - cp, Fi);
+    }
+    d.cforce[c] = d4(Fc, 0);
+    d.ctorque[c] = d4(Tc, 0);
+    double im = d.cinvm[c];
+    double3 v = xyz(d.cvel[c]), w = xyz(d.cangv[c]);
+    double4 q = d.cq[c];
+    if (im > 1.e-20) {
+        v += (Fc * im + d.gravity) * hdt;
+        w += rot_inv_inertia_apply(q, d.cinvIa[c], d.cinvIb[c], Tc) * hdt;
+        d.cvel[c] = d4(v, 0);
+        d.cangv[c] = d4(w, 0);
+    }
+    if (first) {
+        d.cpos[c] = d4(cp + (2.0 * hdt) * v, 0);
+        d.cq[c] = quat_rotate(q, w, 2.0 * hdt);
+    }
+}
+// setPebbleVelocityAngularVelocityKernel (ballIntegrationKernel.cu:81-99)
+__global__ void k_dem_pebbles(DemDev d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    int c = d.clump[i];
+    if (c < 0) return;
+    double3 w = xyz(d.cangv[c]);
+    d.angv[i] = d4(w, 0);
+    double4 v4 = d.vel[i];
+    d.vel[i] = d4(xyz(d.cvel[c]) + cross(w, xyz(d.pos[i]) - xyz(d.cpos[c])), v4.w);
+}
+// ballVelocityAngularVelocityIntegrationKernel + positionIntegrationKernel
+// (ballIntegrationKernel.cu:30-56,112-121) for scenes with clumps.
+__global__ void k_dem_integrate(DemDev d, double hdt, int first) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    double4 v4 = d.vel[i];
+    double3 v = xyz(v4);
+    double im = v4.w;
+    if (d.clump[i] < 0 && !(im < 1.e-20)) {
+        v += (xyz(d.force[i]) * im + d.gravity) * hdt;
+        d.vel[i] = d4(v, im);
+        double r = d.pos[i].w;
+        if (!(r < 1.e-20)) {
+            double I = 0.4 * r * r / im;
+            d.angv[i] = d4(xyz(d.angv[i]) + xyz(d.torque[i]) / I * hdt, 0);
+        }
+    }
+    if (first) {
+        double4 p = d.pos[i];
+        d.pos[i] = d4(xyz(p) + (2.0 * hdt) * v, p.w);
+    }
+}
+// wallPositionIntegrationKernel + wallOrientationIntegrationKernel (wallIntegrationKernel.cu:3-23)
+__global__ void k_dem_wall_move(DemDev d, double dt) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= d.nWall) return;
+    d.wpos[w] = d4(xyz(d.wpos[w]) + dt * xyz(d.wvel[w]), 0);
+    d.wq[w] = quat_rotate(d.wq[w], xyz(d.wangv[w]), dt);
+}
+// updateWallVertexGlobalPosition (wallIntegrationKernel.cu:25-37)
+__global__ void k_dem_vertices(DemDev d) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= d.nVert) return;
+    int w = d.vwall[v];
+    d.vglobal[v] = d4(xyz(d.wpos[w]) + quat_apply(d.wq[w], xyz(d.vlocal[v])), 0);
+}
+// updateTriangleCircumcenter (wallIntegrationKernel.cu:39-53)
+__global__ void k_dem_circumcenters(DemDev d) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nTri) return;
+    int4 tv = d.tris[t];
+    d.tcenter[t] = d4(circumcenter(xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]), xyz(d.vglobal[tv.z])), 0);
+}
+
+// ================================================================ host =====
+struct HostMatRows {
+    struct Row { int a, b; double v[11]; };
+    std::vector<Row> h, l, bd;
+};
+
+struct DemScene {
+    cudaStream_t s = 0;
+    int precision = DEMSPH_PRECISION_MIXED;
+    bool ready = false;
+    // host staging (the reference's host halves of HostDeviceArray1D)
+    std::vector<double4> hPos, hVel, hAngv;
+    std::vector<int> hMat, hClump;
+    HostMatRows rows;
+    std::vector<double4> hCpos, hCvel, hCangv, hCq, hCinvIa, hCinvIb;
+    std::vector<double> hCinvm;
+    std::vector<int2> hCpeb;
+    std::vector<double4> hWpos, hWvel, hWangv, hWq;
+    std::vector<int> hWmat;
+    std::vector<double4> hVlocal;
+    std::vector<int> hVwall;
+    std::vector<int4> hTris;
+    std::vector<int2> hBab;
+    std::vector<double4> hBpoint, hBnormal;
+    std::vector<double4> hFconst;
+    double framp = 0, damp = 0;
+    int buoy = 0;
+    double brho = 0, bcd = 0, blevel = 0;
+    double3 bg3{0, 0, 0}, bu{0, 0, 0};
+    // parameters
+    double3 gmin{0, 0, 0}, gmax{0, 0, 0}, gravity{0, 0, 0};
+    double dt = 0;
+    long iStep = 0;
+    double time = 0;
+    int K = 16, KR = 16, KT = 8;
+    int nMat = 0, cap = 0, roll = 0, tors = 0;
+    bool wallsMove = false;
+    // device
+    DBuf<MatPair> mats;
+    DBuf<double4> pos, vel, angv, force, torque, forceA, torqueA;
+    DBuf<int> mat, clump;
+    CellTable ballCells, triCells;
+    DBuf<int> pj[2], pcnt[2];
+    DBuf<double4> spS[2], spR[2], spT[2];
+    int cur = 0;
+    bool havePairs = false;
+    DBuf<double4> pF, pTB;
+    DBuf<int> rcnt, rslot;
+    DBuf<int2> bab;
+    DBuf<int> bok;
+    DBuf<double4> bpoint, bnormal, bFs, bTb, bF, bTA, bTB;
+    DBuf<double> bFn, bTt, bsmax, btmax;
+    DBuf<int> bincStart, binc;
+    DBuf<double4> wpos, wvel, wangv, wq, vlocal, vglobal, tcenter;
+    DBuf<int> wmat, vwall;
+    DBuf<int4> tris;
+    DBuf<int> wtj[2], wcnt[2];
+    DBuf<double4> wS[2], wR[2], wT[2];
+    int wcur = 0;
+    bool haveWallRows = false;
+    DBuf<double4> cpos, cvel, cangv, cforce, ctorque, cq, cinvIa, cinvIb;
+    DBuf<double> cinvm;
+    DBuf<int2> cpeb;
+    DBuf<double4> fconst;
+    DBuf<DevStatus> status;
+
+    int N() const { return (int)hPos.size(); }
+
+    DemDev dev(bool withOld) {
+        DemDev d{};
+        d.N = N(); d.K = K; d.KR = KR; d.KT = KT;
+        d.nBond = (int)hBab.size(); d.nTri = (int)hTris.size(); d.nVert = (int)hVlocal.size();
+        d.nWall = (int)hWpos.size(); d.nClump = (int)hCpos.size();
+        d.nMat = nMat; d.cap = cap; d.roll = roll; d.tors = tors;
+        d.bg = ballCells.g; d.tg = triCells.g;
+        d.mats = mats.p;
+        d.pos = pos.p; d.vel = vel.p; d.angv = angv.p; d.force = force.p; d.torque = torque.p;
+        d.forceA = forceA.p; d.torqueA = torqueA.p; d.mat = mat.p; d.clump = clump.p;
+        d.order = ballCells.sorted.p; d.cellStart = ballCells.start.p;
+        int o = cur ^ 1;
+        d.pj = pj[cur].p; d.pcnt = pcnt[cur].p; d.spS = spS[cur].p; d.spR = spR[cur].p; d.spT = spT[cur].p;
+        if (withOld && havePairs) {
+            d.pjOld = pj[o].p; d.pcntOld = pcnt[o].p; d.spSOld = spS[o].p; d.spROld = spR[o].p; d.spTOld = spT[o].p;
+        }
+        d.pF = pF.p; d.pTB = pTB.p; d.rcnt = rcnt.p; d.rslot = rslot.p;
+        d.bab = bab.p; d.bok = bok.p; d.bpoint = bpoint.p; d.bnormal = bnormal.p; d.bFs = bFs.p; d.bTb = bTb.p;
+        d.bFn = bFn.p; d.bTt = bTt.p; d.bsmax = bsmax.p; d.btmax = btmax.p; d.bF = bF.p; d.bTA = bTA.p; d.bTB = bTB.p;
+        d.bincStart = bincStart.p; d.binc = binc.p;
+        d.wpos = wpos.p; d.wvel = wvel.p; d.wangv = wangv.p; d.wq = wq.p; d.wmat = wmat.p;
+        d.vlocal = vlocal.p; d.vglobal = vglobal.p; d.vwall = vwall.p; d.tris = tris.p; d.tcenter = tcenter.p;
+        d.triOrder = triCells.sorted.p; d.triCellStart = triCells.start.p;
+        int wo = wcur ^ 1;
+        d.wtj = wtj[wcur].p; d.wcnt = wcnt[wcur].p; d.wS = wS[wcur].p; d.wR = wR[wcur].p; d.wT = wT[wcur].p;
+        if (haveWallRows) {
+            d.wtjOld = wtj[wo].p; d.wcntOld = wcnt[wo].p; d.wSOld = wS[wo].p; d.wROld = wR[wo].p; d.wTOld = wT[wo].p;
+        }
+        d.cpos = cpos.p; d.cvel = cvel.p; d.cangv = cangv.p; d.cforce = cforce.p; d.ctorque = ctorque.p; d.cq = cq.p;
+        d.cinvIa = cinvIa.p; d.cinvIb = cinvIb.p; d.cinvm = cinvm.p; d.cpeb = cpeb.p;
+        d.fconst = hFconst.empty() ? nullptr : fconst.p;
+        d.framp = framp; d.damp = damp; d.buoy = buoy; d.brho = brho; d.bcd = bcd; d.blevel = blevel;
+        d.bg3 = bg3; d.bu = bu; d.gravity = gravity;
+        d.status = status.p;
+        return d;
+    }
+
+    // ------------------------------------------------------- set-up ------
+    void build_materials() {
+        int mx = -1;
+        for (auto& r : rows.h) mx = std::max(mx, std::max(r.a, r.b));
+        for (auto& r : rows.l) mx = std::max(mx, std::max(r.a, r.b));
+        for (auto& r : rows.bd) mx = std::max(mx, std::max(r.a, r.b));
+        nMat = mx < 0 ? 0 : mx + 1;
+        cap = nMat > 0 ? nMat * (nMat + 1) / 2 + 1 : 0;
+        // defaults of buildFromTables (contactKernel.cu:18-31)
+        MatPair def{};
+        def.linear = 0; def.D = 0.0;  // e = 1 -> ln e = 0
+        def.gamma = 1.0; def.knks = 1.0;
+        std::vector<MatPair> tab(std::max(cap, 1), def);
+        std::vector<double> res(std::max(cap, 1), 1.0);
+        for (auto& r : rows.h) {
+            int ip = pair_param_index(r.a, r.b, nMat, cap);
+            MatPair& m = tab[ip];
+            m.E = r.v[0]; m.G = r.v[1]; res[ip] = r.v[2]; m.krks = r.v[3]; m.ktks = r.v[4];
+        }
+        std::vector<std::array<double, 3>> hmu(std::max(cap, 1), {0, 0, 0});
+        for (auto& r : rows.h) {
+            int ip = pair_param_index(r.a, r.b, nMat, cap);
+            hmu[ip] = {r.v[5], r.v[6], r.v[7]};
+        }
+        std::vector<std::array<double, 11>> lin(std::max(cap, 1));
+        for (auto& x : lin) x.fill(0.0);
+        for (auto& r : rows.l) {
+            int ip = pair_param_index(r.a, r.b, nMat, cap);
+            for (int k = 0; k < 11; k++) lin[ip][k] = r.v[k];
+        }
+        for (auto& r : rows.bd) {
+            int ip = pair_param_index(r.a, r.b, nMat, cap);
+            MatPair& m = tab[ip];
+            m.gamma = r.v[0]; m.Eb = r.v[1]; m.knks = r.v[2]; m.sigma = r.v[3]; m.C = r.v[4]; m.mu = r.v[5];
+        }
+        roll = tors = 0;
+        for (int ip = 0; ip < (int)tab.size(); ip++) {
+            MatPair& m = tab[ip];
+            double logR = std::log(res[ip]);
+            m.D = -logR / std::sqrt(logR * logR + kPi * kPi);
+            if (lin[ip][0] > 1.e-20) {
+                m.linear = 1;
+                m.kn = lin[ip][0]; m.ks = lin[ip][1]; m.kr = lin[ip][2]; m.kt = lin[ip][3];
+                m.dn = lin[ip][4]; m.ds = lin[ip][5]; m.dr = lin[ip][6]; m.dt = lin[ip][7];
+                m.mus = lin[ip][8]; m.mur = lin[ip][9]; m.mut = lin[ip][10];
+                if (m.kr > 0) roll = 1;
+                if (m.kt > 0) tors = 1;
+            } else {
+                m.linear = 0;
+                m.mus = hmu[ip][0]; m.mur = hmu[ip][1]; m.mut = hmu[ip][2];
+                if (m.krks > 0 && m.G > 0) roll = 1;
+                if (m.ktks > 0 && m.G > 0) tors = 1;
+            }
+        }
+        std::vector<MatPair> v(tab.begin(), tab.end());
+        mats.upload(v, s);
+    }
+
+    void upload_bonds() {
+        int nb = (int)hBab.size();
+        std::vector<int> ok(nb, 1);
+        std::vector<double> zero(nb, 0.0);
+        std::vector<double4> z4(nb, make_double4(0, 0, 0, 0));
+        bab.upload(hBab, s);
+        bok.upload(ok, s);
+        bpoint.upload(hBpoint, s);
+        bnormal.upload(hBnormal, s);
+        bFs.upload(z4, s); bTb.upload(z4, s); bF.upload(z4, s); bTA.upload(z4, s); bTB.upload(z4, s);
+        bFn.upload(zero, s); bTt.upload(zero, s); bsmax.upload(zero, s); btmax.upload(zero, s);
+        // static incidence list per ball, bonds in order (deterministic sum)
+        std::vector<int> cnt(N() + 1, 0);
+        for (auto& e : hBab) { cnt[e.x + 1]++; cnt[e.y + 1]++; }
+        for (int i = 0; i < N(); i++) cnt[i + 1] += cnt[i];
+        std::vector<int> inc(std::max(2 * nb, 1)), fill(cnt.begin(), cnt.end() - 1);
+        for (int b = 0; b < nb; b++) {
+            inc[fill[hBab[b].x]++] = 2 * b;
+            inc[fill[hBab[b].y]++] = 2 * b + 1;
+        }
+        bincStart.upload(cnt, s);
+        binc.upload(inc, s);
+    }
+
+    void alloc_pairs() {
+        size_t n = (size_t)N();
+        for (int b = 0; b < 2; b++) {
+            pj[b].alloc(n * K, s, true);
+            pcnt[b].alloc(n, s, true);
+            spS[b].alloc(n * K, s, true);
+            spR[b].alloc(roll ? n * K : 1, s, true);
+            spT[b].alloc(tors ? n * K : 1, s, true);
+        }
+        pF.alloc(n * K, s, true);
+        pTB.alloc(n * K, s, true);
+        rcnt.alloc(n, s, true);
+        rslot.alloc(n * KR, s, true);
+    }
+    void alloc_wall_rows() {
+        size_t n = (size_t)N();
+        for (int b = 0; b < 2; b++) {
+            wtj[b].alloc(n * KT, s, true);
+            wcnt[b].alloc(n, s, true);
+            wS[b].alloc(n * KT, s, true);
+            wR[b].alloc(roll ? n * KT : 1, s, true);
+            wT[b].alloc(tors ? n * KT : 1, s, true);
+        }
+    }
+    // Capacity growth keeps the k*N + A layout, so the first planes stay valid.
+    void grow(int needPairs, int needRev, int needTri) {
+        size_t n = (size_t)N();
+        if (needPairs > K) {
+            int nk = needPairs + needPairs / 4 + 1;
+            for (int b = 0; b < 2; b++) {
+                pj[b].grow(n * nk, s);
+                spS[b].grow(n * nk, s);
+                if (roll) spR[b].grow(n * nk, s);
+                if (tors) spT[b].grow(n * nk, s);
+            }
+            pF.alloc(n * nk, s, true);
+            pTB.alloc(n * nk, s, true);
+            K = nk;
+        }
+        if (needRev > KR) {
+            int nk = needRev + needRev / 4 + 1;
+            rslot.alloc(n * nk, s, true);
+            KR = nk;
+        }
+        if (needTri > KT) {
+            int nk = std::min(needTri + needTri / 4 + 1, kMaxTriPerBall);
+            if (needTri > kMaxTriPerBall)
+                throw Status(DEMSPH_ERR_OVERFLOW, "a ball touches more than 32 candidate triangles");
+            for (int b = 0; b < 2; b++) {
+                wtj[b].grow(n * nk, s);
+                wS[b].grow(n * nk, s);
+                if (roll) wR[b].grow(n * nk, s);
+                if (tors) wT[b].grow(n * nk, s);
+            }
+            KT = nk;
+        }
+    }
+
+    void launch_count(int k) { g_launches += k; }
+
+    // ------------------------------------------------------- pieces ------
+    void neighbor_search() {
+        ballCells.build(pos.p, N(), s);
+        launch_count(ballCells.launches);
+        cur ^= 1;
+        DemDev d = dev(true);
+        k_dem_build_pairs<<<grid_for(N(), 128), 128, 0, s>>>(d);
+        DEMSPH_CUDA(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * N(), s));
+        k_dem_reverse<<<grid_for(N(), 256), 256, 0, s>>>(d);
+        k_dem_reverse_order<<<grid_for(N(), 256), 256, 0, s>>>(d);
+        launch_count(3);
+        DEMSPH_LAUNCH_CHECK();
+        havePairs = true;
+    }
+    void tri_grid() {
+        if (hTris.empty()) return;
+        triCells.build(tcenter.p, (int)hTris.size(), s);
+        launch_count(triCells.launches);
+    }
+    // calculateBallContactForceTorque(dt) [+ addTriangleContactForceTorque(dtWall)]
+    // [+ external hook at extTime] [+ half-step integration]
+    void force_eval(double dt, bool walls, double dtWall, bool ext, double extTime, int integ, double hdt) {
+        DemDev d = dev(false);
+        const int n = N();
+        if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 256), 256, 0, s>>>(d, dt);
+        else k_dem_pair_forces<float><<<grid_for(n, 256), 256, 0, s>>>(d, dt);
+        launch_count(1);
+        if (d.nBond) {
+            k_dem_bonds<<<grid_for(d.nBond, 128), 128, 0, s>>>(d, dt);
+            launch_count(1);
+        }
+        bool doWalls = walls && !hTris.empty();
+        if (doWalls) {
+            if (wallsMove || !haveWallRows) tri_grid();
+            wcur ^= 1;
+            d = dev(false);
+        } else {
+            d.nTri = 0;
+        }
+        bool clumps = !hCpos.empty();
+        int fin = clumps ? 0 : integ;
+        if (precision == DEMSPH_PRECISION_FP64)
+            k_dem_finalize<double><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall, extTime, ext ? 1 : 0, fin, hdt);
+        else
+            k_dem_finalize<float><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall, extTime, ext ? 1 : 0, fin, hdt);
+        launch_count(1);
+        if (doWalls) {
+            haveWallRows = true;
+            if (wallsMove) {
+                k_dem_wall_move<<<grid_for(d.nWall, 64), 64, 0, s>>>(d, dtWall);
+                k_dem_vertices<<<grid_for(d.nVert, 256), 256, 0, s>>>(d);
+                k_dem_circumcenters<<<grid_for(d.nTri, 256), 256, 0, s>>>(d);
+                launch_count(3);
+            }
+        }
+        if (clumps && integ) {
+            k_dem_clumps<<<grid_for(d.nClump, 128), 128, 0, s>>>(d, hdt, integ == 1);
+            k_dem_pebbles<<<grid_for(n, 256), 256, 0, s>>>(d);
+            k_dem_integrate<<<grid_for(n, 256), 256, 0, s>>>(d, hdt, integ == 1);
+            launch_count(3);
+        }
+        DEMSPH_LAUNCH_CHECK();
+    }
+    // One pass of loop_ball / loop_ball_wall (DEMSolver.h:1376-1485).
+    void step_once() {
+        const double hdt = 0.5 * dt;
+        iStep++;
+        time += dt;
+        if (iStep % 5 == 0) neighbor_search();
+        bool walls = !hTris.empty();
+        force_eval(hdt, walls, dt, true, time - hdt, 1, hdt);
+        force_eval(hdt, walls, dt, true, time, 2, hdt);
+    }
+
+    DevStatus read_status() {
+        DevStatus h{};
+        DEMSPH_CUDA(cudaMemcpyAsync(&h, status.p, sizeof h, cudaMemcpyDeviceToHost, s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+        return h;
+    }
+    void clear_status() { DEMSPH_CUDA(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), s)); }
+
+    // ---------------------------------------------------- snapshots ------
+    // Dynamic state copied before a batch of steps so that a capacity
+    // overflow can be undone, the lists regrown and the steps replayed.
+    struct Snap {
+        std::vector<std::pair<void*, std::vector<char>>> dev;  // unused on the fast path
+        std::vector<std::unique_ptr<DBuf<char>>> bufs;
+        std::vector<std::pair<void*, size_t>> src;
+        long iStep;
+        double time;
+        int cur, wcur;
+        bool havePairs, haveWallRows;
+        int K, KT;
+    };
+    template <class T>
+    void snap_add(Snap& sn, DBuf<T>& b) {
+        if (!b.p || b.n == 0) return;
+        auto c = std::make_unique<DBuf<char>>();
+        c->alloc(b.bytes(), s, false);
+        DEMSPH_CUDA(cudaMemcpyAsync(c->p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
+        sn.src.push_back({(void*)&b, b.bytes()});
+        sn.bufs.push_back(std::move(c));
+    }
+    void take(Snap& sn) {
+        sn.iStep = iStep; sn.time = time; sn.cur = cur; sn.wcur = wcur; sn.havePairs = havePairs;
+        sn.haveWallRows = haveWallRows; sn.K = K; sn.KT = KT;
+        snap_add(sn, pos); snap_add(sn, vel); snap_add(sn, angv); snap_add(sn, force); snap_add(sn, torque);
+        for (int b = 0; b < 2; b++) {
+            snap_add(sn, pj[b]); snap_add(sn, pcnt[b]); snap_add(sn, spS[b]);
+            if (roll) snap_add(sn, spR[b]);
+            if (tors) snap_add(sn, spT[b]);
+            snap_add(sn, wtj[b]); snap_add(sn, wcnt[b]); snap_add(sn, wS[b]);
+            if (roll) snap_add(sn, wR[b]);
+            if (tors) snap_add(sn, wT[b]);
+        }
+        snap_add(sn, ballCells.sorted); snap_add(sn, ballCells.start);
+        snap_add(sn, rcnt); snap_add(sn, rslot);
+        snap_add(sn, bok); snap_add(sn, bpoint); snap_add(sn, bnormal); snap_add(sn, bFs); snap_add(sn, bTb);
+        snap_add(sn, bFn); snap_add(sn, bTt); snap_add(sn, bsmax); snap_add(sn, btmax);
+        snap_add(sn, wpos); snap_add(sn, wq); snap_add(sn, vglobal); snap_add(sn, tcenter);
+        snap_add(sn, cpos); snap_add(sn, cvel); snap_add(sn, cangv); snap_add(sn, cq);
+    }
+    void restore(Snap& sn) {
+        // pair / reverse rows were regrown in place (layout k*N + A), so the
+        // saved prefix is copied back into the start of each buffer.
+        for (size_t k = 0; k < sn.src.size(); k++) {
+            DBuf<char>* dst = (DBuf<char>*)sn.src[k].first;
+            DEMSPH_CUDA(cudaMemcpyAsync(dst->p, sn.bufs[k]->p, sn.src[k].second, cudaMemcpyDeviceToDevice, s));
+        }
+        iStep = sn.iStep; time = sn.time; cur = sn.cur; wcur = sn.wcur; havePairs = sn.havePairs;
+        haveWallRows = sn.haveWallRows;
+    }
+
+    void run(long n) {
+        if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (n <= 0) return;
+        for (int attempt = 0; attempt < 8; attempt++) {
+            Snap sn;
+            take(sn);
+            clear_status();
+            for (long k = 0; k < n; k++) step_once();
+            DevStatus st = read_status();
+            if (!st.overflow) return;
+            grow(st.need_pairs, st.need_rev, st.need_aux);
+            restore(sn);
+            // rows past the old capacity hold stale data; the rebuild rewrites them.
+        }
+        throw Status(DEMSPH_ERR_OVERFLOW, "pair lists kept overflowing after regrowth");
+    }
+
+    void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
+        if (hPos.empty()) throw Status(DEMSPH_ERR_SCENE, "the number of particles is equal to 0");
+        if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
+        for (auto& p : hPos) {
+            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
+                throw Status(DEMSPH_ERR_SCENE, "ball with non-finite position or non-positive radius");
+        }
+        precision = prec;
+        gmin = mn; gmax = mx; gravity = g; dt = timeStep;
+        build_materials();
+        int n = N();
+        pos.upload(hPos, s); vel.upload(hVel, s); angv.upload(hAngv, s);
+        std::vector<double4> z(n, make_double4(0, 0, 0, 0));
+        force.upload(z, s); torque.upload(z, s); forceA.upload(z, s); torqueA.upload(z, s);
+        mat.upload(hMat, s); clump.upload(hClump, s);
+        status.alloc(1, s, true);
+        // grids (DEMSolver.h:245-263)
+        double cell = 0;
+        for (auto& p : hPos) cell = std::max(cell, p.w * 2.0);
+        GridDesc bg{};
+        if (!grid_set(bg, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
+        ballCells.setup(bg, n, s);
+        double tcell = cell;
+        std::vector<double4> cent(hTris.size());
+        for (size_t t = 0; t < hTris.size(); t++) {
+            double3 a = xyz(hVlocal[hTris[t].x]), b = xyz(hVlocal[hTris[t].y]), c = xyz(hVlocal[hTris[t].z]);
+            double3 cc = circumcenter(a, b, c);
+            tcell = std::max(tcell, 2.0 * len(a - cc));
+            tcell = std::max(tcell, 2.0 * len(b - cc));
+            tcell = std::max(tcell, 2.0 * len(c - cc));
+            int w = hTris[t].w;
+            double3 o = xyz(hWpos[w]);
+            cent[t] = d4(circumcenter(a + o, b + o, c + o), 0);
+        }
+        GridDesc tg{};
+        grid_set(tg, mn, mx, tcell);
+        if (!hTris.empty()) triCells.setup(tg, (int)hTris.size(), s);
+        else triCells.g = tg;
+        // bodies
+        clump_upload();
+        wpos.upload(hWpos, s); wvel.upload(hWvel, s); wangv.upload(hWangv, s); wq.upload(hWq, s);
+        wmat.upload(hWmat, s);
+        vlocal.upload(hVlocal, s);
+        std::vector<double4> vg(hVlocal.size());
+        for (size_t v = 0; v < hVlocal.size(); v++) vg[v] = d4(xyz(hVlocal[v]) + xyz(hWpos[hVwall[v]]), 0);
+        vglobal.upload(vg, s);
+        vwall.upload(hVwall, s);
+        tris.upload(hTris, s);
+        tcenter.upload(cent, s);
+        wallsMove = false;
+        for (size_t w = 0; w < hWpos.size(); w++)
+            if (len2(xyz(hWvel[w])) > 0 || len2(xyz(hWangv[w])) > 0) wallsMove = true;
+        fconst.upload(hFconst, s);
+        upload_bonds();
+        // lists
+        alloc_pairs();
+        alloc_wall_rows();
+        cur = 0; wcur = 0; havePairs = false; haveWallRows = false;
+        // neighbour search + one dt = 0 force evaluation (DEMSolver.h:1995-1997);
+        // grow and redo when a first guess of a capacity was too small.
+        for (int attempt = 0; attempt < 8; attempt++) {
+            clear_status();
+            neighbor_search();
+            force_eval(0.0, !hTris.empty(), 0.0, false, 0.0, 0, 0.0);
+            DevStatus st = read_status();
+            if (!st.overflow) break;
+            grow(st.need_pairs, st.need_rev, st.need_aux);
+            havePairs = false;
+            haveWallRows = false;
+            if (attempt == 7) throw Status(DEMSPH_ERR_OVERFLOW, "initial pair lists overflow");
+        }
+        iStep = 0;
+        time = 0;
+        ready = true;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    }
+    void clump_upload() {
+        cpos.upload(hCpos, s); cvel.upload(hCvel, s); cangv.upload(hCangv, s); cq.upload(hCq, s);
+        cinvIa.upload(hCinvIa, s); cinvIb.upload(hCinvIb, s); cinvm.upload(hCinvm, s); cpeb.upload(hCpeb, s);
+        std::vector<double4> z(hCpos.size(), make_double4(0, 0, 0, 0));
+        cforce.upload(z, s); ctorque.upload(z, s);
+    }
+};
+
+}  // namespace demsph
+
+// ================================================================ C ABI ====
+using namespace demsph;
+
+struct demsph_dem_scene {
+    DemScene sc;
+};
+
+static inline double3 ld3(const double* a, long i) { return mk3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
+static inline void st3(double* a, long i, double3 v) { a[3 * i] = v.x; a[3 * i + 1] = v.y; a[3 * i + 2] = v.z; }
+
+#define SCENE_CHECK(h) \
+    if (!(h)) throw Status(DEMSPH_ERR_INVALID, "null scene handle")
+
+extern "C" {
+
+int demsph_dem_create(demsph_dem_t* out, void* stream) {
+    return guarded([&] {
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        auto* h = new demsph_dem_scene();
+        h->sc.s = (cudaStream_t)stream;
+        *out = h;
+    });
+}
+int demsph_dem_destroy(demsph_dem_t h) {
+    return guarded([&] {
+        if (!h) return;
+        cudaStream_t s = h->sc.s;
+        delete h;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int demsph_dem_set_hertzian_pair(demsph_dem_t h, int a, int b, double E, double G, double e, double krks, double ktks,
+                                 double mus, double mur, double mut) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.rows.h.push_back({a, b, {E, G, e, krks, ktks, mus, mur, mut, 0, 0, 0}});
+    });
+}
+int demsph_dem_set_linear_pair(demsph_dem_t h, int a, int b, double kn, double ks, double kr, double kt, double dn,
+                               double ds, double dr, double dtt, double mus, double mur, double mut) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.rows.l.push_back({a, b, {kn, ks, kr, kt, dn, ds, dr, dtt, mus, mur, mut}});
+    });
+}
+int demsph_dem_set_bonded_pair(demsph_dem_t h, int a, int b, double gamma, double Eb, double knks, double sigma,
+                               double C, double mu) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.rows.bd.push_back({a, b, {gamma, Eb, knks, sigma, C, mu, 0, 0, 0, 0, 0}});
+    });
+}
+int demsph_dem_add_balls(demsph_dem_t h, long n, const double* pos, const double* vel, const double* w,
+                         const double* rad, const double* dens, const int* mat, const int* clump, int fixed) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "balls must be added before initialisation");
+        if (n < 0 || (n > 0 && (!pos || !rad || !mat))) throw Status(DEMSPH_ERR_INVALID, "missing ball arrays");
+        for (long i = 0; i < n; i++) {
+            double r = rad[i];
+            double im = 0.0;
+            if (!fixed) {
+                double mass = 4. / 3. * r * r * r * kPi * (dens ? dens[i] : 0.0);
+                if (mass > 0.0) im = 1.0 / mass;
+            }
+            s.hPos.push_back(d4(ld3(pos, i), r));
+            s.hVel.push_back(d4(fixed || !vel ? mk3(0, 0, 0) : ld3(vel, i), im));
+            s.hAngv.push_back(d4(fixed || !w ? mk3(0, 0, 0) : ld3(w, i), 0));
+            s.hMat.push_back(mat[i]);
+            s.hClump.push_back(clump ? clump[i] : -1);
+        }
+    });
+}
+int demsph_dem_add_clump(demsph_dem_t h, long np, const double* pts, const double* rad, const double* centroid,
+                         const double* vel, const double* w, double mass, const double* I6, int mat) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "clumps must be added before initialisation");
+        int cid = (int)s.hCpos.size();
+        int ps = s.N(), pe = ps + (int)np;
+        double3 c = ld3(centroid, 0), v = ld3(vel, 0), ww = ld3(w, 0);
+        std::vector<double3> pv(np, v);
+        double vol = 0., im = 0.;
+        if (mass > 1.e-20) {
+            im = 1.0 / mass;
+            for (long i = 0; i < np; i++) {
+                vol += 4.0 / 3.0 * kPi * std::pow(rad[i], 3.0);
+                pv[i] += cross(ww, ld3(pts, i) - c);
+            }
+        }
+        double dave = vol > 0. ? mass / vol : 0.;
+        for (long i = 0; i < np; i++) {
+            double r = rad[i];
+            double m = 4. / 3. * r * r * r * kPi * dave;
+            double pim = m > 0.0 ? 1.0 / m : 0.0;
+            s.hPos.push_back(d4(ld3(pts, i), r));
+            s.hVel.push_back(d4(pv[i], pim));
+            s.hAngv.push_back(d4(ww, 0));
+            s.hMat.push_back(mat);
+            s.hClump.push_back(cid);
+        }
+        // inverse (myMat.h:163-179)
+        double xx = I6[0], yy = I6[1], zz = I6[2], xy = I6[3], xz = I6[4], yz = I6[5];
+        double di = 1.0 / (xx * (yy * zz - yz * yz) + xy * (yz * xz - xy * zz) + xz * (xy * yz - yy * xz));
+        double ixx = (yy * zz - yz * yz) * di, iyy = (xx * zz - xz * xz) * di, izz = (xx * yy - xy * xy) * di;
+        double ixy = -(xy * zz - xz * yz) * di, ixz = (xy * yz - xz * yy) * di, iyz = -(xx * yz - xz * xy) * di;
+        s.hCpos.push_back(d4(c, 0));
+        s.hCvel.push_back(d4(v, 0));
+        s.hCangv.push_back(d4(ww, 0));
+        s.hCq.push_back(make_double4(1, 0, 0, 0));
+        s.hCinvIa.push_back(make_double4(ixx, iyy, izz, ixy));
+        s.hCinvIb.push_back(make_double4(ixz, iyz, 0, 0));
+        s.hCinvm.push_back(im);
+        s.hCpeb.push_back(make_int2(ps, pe));
+    });
+}
+int demsph_dem_add_mesh_wall(demsph_dem_t h, long nv, const double* verts, long nt, const int* i0, const int* i1,
+                             const int* i2, const double* position, int mat) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "walls must be added before initialisation");
+        int mxi = -1;
+        for (long t = 0; t < nt; t++) mxi = std::max(mxi, std::max(i0[t], std::max(i1[t], i2[t])));
+        if (mxi >= nv) return;  // the reference returns silently (DEMSolver.h:1897)
+        int vs = (int)s.hVlocal.size();
+        int wi = (int)s.hWpos.size();
+        double3 p = ld3(position, 0);
+        s.hWpos.push_back(d4(p, 0));
+        s.hWvel.push_back(make_double4(0, 0, 0, 0));
+        s.hWangv.push_back(make_double4(0, 0, 0, 0));
+        s.hWq.push_back(make_double4(1, 0, 0, 0));
+        s.hWmat.push_back(mat);
+        for (long v = 0; v < nv; v++) {
+            s.hVlocal.push_back(d4(ld3(verts, v), 0));
+            s.hVwall.push_back(wi);
+        }
+        for (long t = 0; t < nt; t++) s.hTris.push_back(make_int4(vs + i0[t], vs + i1[t], vs + i2[t], wi));
+    });
+}
+int demsph_dem_set_wall_motion(demsph_dem_t h, int wall, const double* vel, const double* w) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (wall < 0 || wall >= (int)s.hWpos.size()) throw Status(DEMSPH_ERR_INVALID, "wall index out of range");
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "wall motion must be set before initialisation");
+        s.hWvel[wall] = d4(ld3(vel, 0), 0);
+        s.hWangv[wall] = d4(ld3(w, 0), 0);
+    });
+}
+int demsph_dem_add_bonds(demsph_dem_t h, long n, const int* a0, const int* b0, const double* posHost, long npos) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        std::map<std::pair<int, int>, int> have;
+        for (auto& e : s.hBab) have[{e.x, e.y}] = 1;
+        for (long k = 0; k < n; k++) {
+            int i0 = a0[k], i1 = b0[k];
+            if (i0 < 0 || i1 < 0 || i0 >= npos || i1 >= npos || i0 == i1) continue;
+            int a = std::min(i0, i1), b = std::max(i0, i1);
+            if (have.count({a, b})) continue;
+            have[{a, b}] = 1;
+            double3 pa = ld3(posHost, a), pb = ld3(posHost, b);
+            s.hBab.push_back(make_int2(a, b));
+            s.hBpoint.push_back(d4(0.5 * (pa + pb), 0));
+            s.hBnormal.push_back(d4(normalize(pa - pb), 0));
+        }
+        if (s.ready) {
+            // the reference re-runs initialize() after addInitialCondition (DEMSolver.h:1998)
+            s.upload_bonds();
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        }
+    });
+}
+int demsph_dem_set_constant_force(demsph_dem_t h, long n, const double* f, double ramp) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        s.hFconst.assign(std::max<long>(n, 0), make_double4(0, 0, 0, 0));
+        for (long i = 0; i < n; i++) s.hFconst[i] = d4(ld3(f, i), 0);
+        if (s.ready) {
+            s.hFconst.resize(s.N(), make_double4(0, 0, 0, 0));
+            s.fconst.upload(s.hFconst, s.s);
+        }
+        s.framp = ramp;
+    });
+}
+int demsph_dem_set_global_damping(demsph_dem_t h, double c) {
+    return guarded([&] { SCENE_CHECK(h); h->sc.damp = c; });
+}
+int demsph_dem_set_buoyancy_drag(demsph_dem_t h, double rho, double cd, const double* g, const double* u, double lvl) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        s.buoy = 1; s.brho = rho; s.bcd = cd; s.bg3 = ld3(g, 0); s.bu = ld3(u, 0); s.blevel = lvl;
+    });
+}
+int demsph_dem_initialize(demsph_dem_t h, const double* mn, const double* mx, const double* g, double dt, int prec) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (prec != DEMSPH_PRECISION_FP64 && prec != DEMSPH_PRECISION_MIXED)
+            throw Status(DEMSPH_ERR_INVALID, "unknown precision mode");
+        DemScene& s = h->sc;
+        if (!s.hFconst.empty()) s.hFconst.resize(s.N(), make_double4(0, 0, 0, 0));
+        s.initialize(ld3(mn, 0), ld3(mx, 0), ld3(g, 0), dt, prec);
+    });
+}
+int demsph_dem_step(demsph_dem_t h, long n) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.run(n);
+    });
+}
+int demsph_dem_neighbor_search(demsph_dem_t h) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        s.clear_status();
+        s.neighbor_search();
+        DevStatus st = s.read_status();
+        if (st.overflow) {
+            s.grow(st.need_pairs, st.need_rev, 0);
+            s.cur ^= 1;  // rebuild from the same previous list
+            s.neighbor_search();
+        }
+    });
+}
+int demsph_dem_eval_forces(demsph_dem_t h, double dt, int walls, double dtWall) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        s.force_eval(dt, walls != 0, dtWall, false, 0.0, 0, 0.0);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_dem_num_balls(demsph_dem_t h, long* n) {
+    return guarded([&] { SCENE_CHECK(h); *n = h->sc.N(); });
+}
+int demsph_dem_num_bonds(demsph_dem_t h, long* n) {
+    return guarded([&] { SCENE_CHECK(h); *n = (long)h->sc.hBab.size(); });
+}
+int demsph_dem_num_clumps(demsph_dem_t h, long* n) {
+    return guarded([&] { SCENE_CHECK(h); *n = (long)h->sc.hCpos.size(); });
+}
+int demsph_dem_step_index(demsph_dem_t h, long* step, double* time) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (step) *step = h->sc.iStep;
+        if (time) *time = h->sc.time;
+    });
+}
+int demsph_dem_get_balls(demsph_dem_t h, double* pos, double* vel, double* w, double* force, double* torque) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) {
+            for (int i = 0; i < s.N(); i++) {
+                if (pos) st3(pos, i, xyz(s.hPos[i]));
+                if (vel) st3(vel, i, xyz(s.hVel[i]));
+                if (w) st3(w, i, xyz(s.hAngv[i]));
+                if (force) st3(force, i, mk3(0, 0, 0));
+                if (torque) st3(torque, i, mk3(0, 0, 0));
+            }
+            return;
+        }
+        std::vector<double4> a;
+        auto get = [&](DBuf<double4>& b, double* o) {
+            if (!o) return;
+            b.download(a, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            for (int i = 0; i < s.N(); i++) st3(o, i, xyz(a[i]));
+        };
+        get(s.pos, pos); get(s.vel, vel); get(s.angv, w); get(s.force, force); get(s.torque, torque);
+    });
+}
+int demsph_dem_set_balls(demsph_dem_t h, const double* pos, const double* vel, const double* w) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        for (int i = 0; i < s.N(); i++) {
+            if (pos) { double3 p = ld3(pos, i); s.hPos[i].x = p.x; s.hPos[i].y = p.y; s.hPos[i].z = p.z; }
+            if (vel) { double3 p = ld3(vel, i); s.hVel[i].x = p.x; s.hVel[i].y = p.y; s.hVel[i].z = p.z; }
+            if (w) { double3 p = ld3(w, i); s.hAngv[i].x = p.x; s.hAngv[i].y = p.y; s.hAngv[i].z = p.z; }
+        }
+        if (s.ready) {
+            if (pos) s.pos.upload(s.hPos, s.s);
+            if (vel) s.vel.upload(s.hVel, s.s);
+            if (w) s.angv.upload(s.hAngv, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        }
+    });
+}
+
+// Pair rows flattened into the reference's CSR order.
+static void collect_rows(DemScene& s, int which, std::vector<int>& A, std::vector<int>& B, std::vector<size_t>& slot) {
+    int n = s.N();
+    std::vector<int> cnt, ids;
+    if (which == 0) {
+        if (!s.havePairs) return;
+        s.pcnt[s.cur].download(cnt, s.s);
+        s.pj[s.cur].download(ids, s.s);
+    } else {
+        if (!s.haveWallRows) return;
+        s.wcnt[s.wcur].download(cnt, s.s);
+        s.wtj[s.wcur].download(ids, s.s);
+    }
+    DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    for (int a = 0; a < n; a++)
+        for (int k = 0; k < cnt[a]; k++) {
+            size_t sl = (size_t)k * n + a;
+            A.push_back(a);
+            B.push_back(ids[sl]);
+            slot.push_back(sl);
+        }
+}
+int demsph_dem_num_pairs(demsph_dem_t h, int which, long* n) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        std::vector<int> A, B;
+        std::vector<size_t> sl;
+        collect_rows(h->sc, which, A, B, sl);
+        *n = (long)A.size();
+    });
+}
+int demsph_dem_get_pairs(demsph_dem_t h, int which, int* a, int* b, double* sliding, double* rolling, double* torsion,
+                         double* force, double* torque) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        std::vector<int> A, B;
+        std::vector<size_t> sl;
+        collect_rows(s, which, A, B, sl);
+        std::vector<double4> S, Rr, T, F, TB;
+        int c = which == 0 ? s.cur : s.wcur;
+        if (sliding) (which == 0 ? s.spS[c] : s.wS[c]).download(S, s.s);
+        if (rolling && s.roll) (which == 0 ? s.spR[c] : s.wR[c]).download(Rr, s.s);
+        if (torsion && s.tors) (which == 0 ? s.spT[c] : s.wT[c]).download(T, s.s);
+        if (which == 0 && force) s.pF.download(F, s.s);
+        if (which == 0 && torque) s.pTB.download(TB, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        std::vector<double4> P;
+        if (which == 0 && torque) s.pos.download(P, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (size_t k = 0; k < A.size(); k++) {
+            if (a) a[k] = A[k];
+            if (b) b[k] = B[k];
+            if (sliding) st3(sliding, k, xyz(S[sl[k]]));
+            if (rolling) st3(rolling, k, s.roll ? xyz(Rr[sl[k]]) : mk3(0, 0, 0));
+            if (torsion) st3(torsion, k, s.tors ? xyz(T[sl[k]]) : mk3(0, 0, 0));
+            if (force) st3(force, k, which == 0 ? xyz(F[sl[k]]) : mk3(0, 0, 0));
+            if (torque) st3(torque, k, which == 0 ? xyz(TB[sl[k]]) : mk3(0, 0, 0));
+        }
+    });
+}
+int demsph_dem_import_springs(demsph_dem_t h, long n, const int* a, const int* b, const double* sl, const double* ro,
+                              const double* to) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "no pair list");
+        std::map<std::pair<int, int>, long> idx;
+        for (long k = 0; k < n; k++) idx[{a[k], b[k]}] = k;
+        int N = s.N();
+        std::vector<int> cnt, ids;
+        std::vector<double4> S, Rr, T;
+        s.pcnt[s.cur].download(cnt, s.s);
+        s.pj[s.cur].download(ids, s.s);
+        s.spS[s.cur].download(S, s.s);
+        if (s.roll) s.spR[s.cur].download(Rr, s.s);
+        if (s.tors) s.spT[s.cur].download(T, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (int A = 0; A < N; A++)
+            for (int k = 0; k < cnt[A]; k++) {
+                size_t slot = (size_t)k * N + A;
+                auto it = idx.find({A, ids[slot]});
+                if (it == idx.end()) continue;
+                S[slot] = d4(ld3(sl, it->second), 0);
+                if (s.roll) Rr[slot] = d4(ld3(ro, it->second), 0);
+                if (s.tors) T[slot] = d4(ld3(to, it->second), 0);
+            }
+        DEMSPH_CUDA(cudaMemcpyAsync(s.spS[s.cur].p, S.data(), S.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        if (s.roll) DEMSPH_CUDA(cudaMemcpyAsync(s.spR[s.cur].p, Rr.data(), Rr.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        if (s.tors) DEMSPH_CUDA(cudaMemcpyAsync(s.spT[s.cur].p, T.data(), T.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_dem_get_bonds(demsph_dem_t h, int* a, int* b, int* ok, double* fn, double* tt, double* fs, double* tb,
+                         double* normal, double* point) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        int nb = (int)s.hBab.size();
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        std::vector<int> OK;
+        std::vector<double> FN, TT;
+        std::vector<double4> FS, TB, NO, PO;
+        s.bok.download(OK, s.s); s.bFn.download(FN, s.s); s.bTt.download(TT, s.s); s.bFs.download(FS, s.s);
+        s.bTb.download(TB, s.s); s.bnormal.download(NO, s.s); s.bpoint.download(PO, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (int k = 0; k < nb; k++) {
+            if (a) a[k] = s.hBab[k].x;
+            if (b) b[k] = s.hBab[k].y;
+            if (ok) ok[k] = OK[k];
+            if (fn) fn[k] = FN[k];
+            if (tt) tt[k] = TT[k];
+            if (fs) st3(fs, k, xyz(FS[k]));
+            if (tb) st3(tb, k, xyz(TB[k]));
+            if (normal) st3(normal, k, xyz(NO[k]));
+            if (point) st3(point, k, xyz(PO[k]));
+        }
+    });
+}
+int demsph_dem_get_clumps(demsph_dem_t h, double* pos, double* vel, double* w, double* q) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        std::vector<double4> P, Vv, W, Q;
+        s.cpos.download(P, s.s); s.cvel.download(Vv, s.s); s.cangv.download(W, s.s); s.cq.download(Q, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (size_t c = 0; c < P.size(); c++) {
+            if (pos) st3(pos, c, xyz(P[c]));
+            if (vel) st3(vel, c, xyz(Vv[c]));
+            if (w) st3(w, c, xyz(W[c]));
+            if (q) { q[4 * c] = Q[c].x; q[4 * c + 1] = Q[c].y; q[4 * c + 2] = Q[c].z; q[4 * c + 3] = Q[c].w; }
+        }
+    });
+}
+int demsph_dem_get_walls(demsph_dem_t h, double* pos, double* q, double* vglobal) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        std::vector<double4> P, Q, VG;
+        s.wpos.download(P, s.s); s.wq.download(Q, s.s); s.vglobal.download(VG, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (size_t c = 0; c < P.size(); c++) {
+            if (pos) st3(pos, c, xyz(P[c]));
+            if (q) { q[4 * c] = Q[c].x; q[4 * c + 1] = Q[c].y; q[4 * c + 2] = Q[c].z; q[4 * c + 3] = Q[c].w; }
+        }
+        if (vglobal) for (size_t v = 0; v < VG.size(); v++) st3(vglobal, v, xyz(VG[v]));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,830 @@
+// WCSPH path of the DEMSPH B200 library: per-step cell sort with physical
+// reordering of the fluid state, fluid-fluid and fluid-dummy neighbour lists,
+// Riemann momentum and continuity (Wendland C2), the linear equation of
+// state, and the scene runtime behind the demsph_sph_* C ABI.
+//
+// Layout in HBM (one scene):
+//   fluid  pos (x,y,z,h) | vel (vx,vy,vz,m) | st (rho,p,c,nu) : double4,
+//          rho0, drho : double, id : int (caller's index).  Every step the
+//          fluid is counting-sorted into cells and the arrays are permuted into
+//          cell order (double-buffered), so a cell's particles are contiguous
+//          and neighbour gathers stay in L1/L2.
+//   dummy  pos | vel | st (c,nu,rho0,-) | normal : double4, sorted once.
+//   lists  ELL, column-major: nb[k*N + i] = k-th neighbour of fluid i.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <memory>
+
+#include "cells.cuh"
+
+namespace demsph {
+
+extern std::atomic<long long> g_launches;
+
+struct SphDev {
+    int N, ND, KF, KD;
+    GridDesc g;
+    const int* fStart;   // fluid cell start (new order)
+    const int* dStart;   // dummy cell start (dummies stored in cell order)
+    const double4* pos;  // current fluid pos
+    const double4* vel;
+    const double4* st;
+    const double* rho0;
+    double* drho;
+    double4* posOut;
+    double4* velOut;
+    double4* stOut;
+    double4* acc;
+    const double4* dpos;
+    const double4* dvel;
+    const double4* dst;
+    const double4* dnorm;
+    int* nbF;
+    int* cntF;
+    int* nbD;
+    int* cntD;
+    double3 gravity;
+    DevStatus* status;
+};
+
+// Wendland C2 kernel gradient (WCSPHIntegrationKernel.cuh:15-32), with the
+// powers written as products.  Returns the factor f with gradW = f * r_ij.
+template <class R>
+__device__ __forceinline__ R gradw_factor(R r, R h) {
+    if (r < (R)1.e-20 || r >= (R)2.0 * h) return (R)0;
+    R q = r / h;
+    R sigma = (R)21.0 / ((R)16.0 * (R)kPi * h * h * h);
+    R t = (R)1.0 - (R)0.5 * q;
+    R t2 = t * t;
+    R t3 = t2 * t;
+    R dq = -(R)2.0 * t3 * ((R)1.0 + (R)2.0 * q) + (R)2.0 * (t3 * t);
+    R dWdr = sigma * dq / h;
+    return dWdr / r;
+}
+
+// Permutes the fluid into this step's cell order.
+__global__ void k_sph_permute(int n, const int* __restrict__ sorted, const double4* __restrict__ pos,
+                              const double4* __restrict__ vel, const double4* __restrict__ st,
+                              const double* __restrict__ rho0, const double* __restrict__ drho,
+                              const int* __restrict__ id, double4* __restrict__ pos2, double4* __restrict__ vel2,
+                              double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
+                              int* __restrict__ id2) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int o = sorted[t];
+    pos2[t] = pos[o];
+    vel2[t] = vel[o];
+    st2[t] = st[o];
+    rho02[t] = rho0[o];
+    drho2[t] = drho[o];
+    id2[t] = id[o];
+}
+
+// countSPHInteractionsKernel / writeSPHInteractionsKernel and the dummy pair
+// (SPHNeighborSearchKernel.cu:6-228) in one pass per fluid particle:
+// j != i, |r_ij| <= 2 max(h_i, h_j); rows in the reference's stencil order.
+__global__ void __launch_bounds__(128) k_sph_lists(SphDev d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const double4 pi = d.pos[i];
+    const double3 ri = xyz(pi);
+    Stencil st = stencil_of(ri, d.g);
+    int c = 0;
+    for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
+        for (int j = b; j < e; j++) {
+            if (j == i) continue;
+            double4 pj = d.pos[j];
+            double cut = 2.0 * fmax(pi.w, pj.w);
+            double3 r = ri - xyz(pj);
+            if ((cut * cut - dot(r, r)) >= 0.) {
+                if (c < d.KF) d.nbF[(size_t)c * d.N + i] = j;
+                c++;
+            }
+        }
+    });
+    if (c > d.KF) {
+        atomicMax(&d.status->need_pairs, c);
+        atomicExch(&d.status->overflow, 1);
+        c = d.KF;
+    }
+    d.cntF[i] = c;
+    if (d.ND == 0) { d.cntD[i] = 0; return; }
+    int cd = 0;
+    for_stencil_rows(st, d.g, d.dStart, [&](int b, int e) {
+        for (int j = b; j < e; j++) {
+            double4 pj = d.dpos[j];
+            double cut = 2.0 * fmax(pi.w, pj.w);
+            double3 r = ri - xyz(pj);
+            if ((cut * cut - dot(r, r)) >= 0.) {
+                if (cd < d.KD) d.nbD[(size_t)cd * d.N + i] = j;
+                cd++;
+            }
+        }
+    });
+    if (cd > d.KD) {
+        atomicMax(&d.status->need_aux, cd);
+        atomicExch(&d.status->overflow, 1);
+        cd = d.KD;
+    }
+    d.cntD[i] = cd;
+}
+
+// updateWCSPHAccelerationKernel (WCSPHIntegrationKernel.cu:42-148) fused with
+// the half kick (SPHVelocityIntegrationKernel, :150-159) and, in the first
+// half, the drift (SPHPositionIntegrationKernel, :161-170).  Reads the state
+// arrays and writes the integrated particle into separate output arrays, so
+// no thread sees a neighbour's updated state.
+template <class R>
+__global__ void __launch_bounds__(128) k_sph_accel(SphDev d, double hdt, double dt, int first) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    using VR = V<R>;
+    const double4 pi4 = d.pos[i];
+    const double3 ri = xyz(pi4);
+    const double4 vi4 = d.vel[i];
+    const VR vi = cvt<R>(xyz(vi4));
+    const double4 s4 = d.st[i];
+    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, nui = (R)s4.w, hi = (R)pi4.w;
+    VR acc = v3r<R>(0, 0, 0);
+    const int cf = d.cntF[i];
+    for (int k = 0; k < cf; k++) {
+        int j = d.nbF[(size_t)k * d.N + i];
+        double4 pj4 = d.pos[j];
+        double4 vj4 = d.vel[j];
+        double4 sj = d.st[j];
+        VR rij = cvt<R>(ri - xyz(pj4));
+        VR vj = cvt<R>(xyz(vj4));
+        R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, nuj = (R)sj.w, mj = (R)vj4.w;
+        R r = rlen(rij);
+        VR e = v3r<R>(0, 0, 0);
+        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R UL = dot(vi, e), UR = dot(vj, e);
+        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
+        VR dW = f * rij;
+        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
+        R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
+        R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
+        acc -= (R)2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
+        R nuij = (R)0.5 * (nui + nuj);
+        // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
+        acc += (R)2.0 * nuij * dot(-e, dW) * (vi - vj) * mj * ((R)1.0 / (rhoi * rhoj));
+    }
+    const int cd = d.cntD[i];
+    const VR g = cvt<R>(d.gravity);
+    for (int k = 0; k < cd; k++) {
+        int j = d.nbD[(size_t)k * d.N + i];
+        double4 pj4 = d.dpos[j];
+        double4 vj4 = d.dvel[j];
+        double4 sj = d.dst[j];
+        VR nw = cvt<R>(xyz(d.dnorm[j]));
+        VR vj = cvt<R>(xyz(vj4));
+        R cj = (R)sj.x, nuj = (R)sj.y, rho0j = (R)sj.z, mj = (R)vj4.w;
+        R UL = dot(-nw, vi);
+        R UR = -UL + (R)2.0 * dot(-nw, vj);
+        VR rji = cvt<R>(xyz(pj4) - ri);
+        R grj = dot(g, rji);
+        if (grj < (R)0.) grj = (R)0.;
+        R PR = PL + rhoi * grj;
+        R rhoj = PR / (cj * cj) + rho0j;
+        VR rij = cvt<R>(ri - xyz(pj4));
+        R r = rlen(rij);
+        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
+        VR dW = f * rij;
+        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
+        R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
+        R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
+        acc -= (R)2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
+        R nuij = (R)0.5 * (nui + nuj);
+        VR rh = v3r<R>(0, 0, 0);
+        if (r * r >= (R)1.0e-20) rh = rij * ((R)1.0 / r);
+        acc += (R)2.0 * nuij * dot(rh, dW) * (vi - vj) * mj * ((R)1.0 / (rhoi * rhoj));
+    }
+    double3 a = up(acc) + d.gravity;
+    d.acc[i] = d4(a, 0);
+    double3 v = xyz(vi4) + hdt * a;
+    d.velOut[i] = d4(v, vi4.w);
+    if (first) d.posOut[i] = d4(ri + dt * v, pi4.w);
+}
+
+// updateWCSPHDensityChangeKernel + SPHDensityPressureIntegrationKernel
+// (WCSPHIntegrationKernel.cu:172-282): drho += dt * 2 rho_i sum m_j/rho_j
+// (v_i - v*) . gradW; clamp drho >= -0.1 rho0; rho = rho0 + drho; p = c^2 drho.
+template <class R>
+__global__ void __launch_bounds__(128) k_sph_density(SphDev d, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    using VR = V<R>;
+    const double4 pi4 = d.pos[i];
+    const double3 ri = xyz(pi4);
+    const VR vi = cvt<R>(xyz(d.vel[i]));
+    const double4 s4 = d.st[i];
+    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, hi = (R)pi4.w;
+    R dRho = (R)0;
+    const int cf = d.cntF[i];
+    for (int k = 0; k < cf; k++) {
+        int j = d.nbF[(size_t)k * d.N + i];
+        double4 pj4 = d.pos[j];
+        double4 vj4 = d.vel[j];
+        double4 sj = d.st[j];
+        VR rij = cvt<R>(ri - xyz(pj4));
+        VR vj = cvt<R>(xyz(vj4));
+        R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, mj = (R)vj4.w;
+        R r = rlen(rij);
+        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
+        VR dW = f * rij;
+        VR e = v3r<R>(0, 0, 0);
+        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
+        VR vs = (R)0.5 * (vi + vj);
+        vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
+        dRho += mj / rhoj * dot(vi - vs, dW);
+    }
+    const int cd = d.cntD[i];
+    const VR g = cvt<R>(d.gravity);
+    for (int k = 0; k < cd; k++) {
+        int j = d.nbD[(size_t)k * d.N + i];
+        double4 pj4 = d.dpos[j];
+        double4 vj4 = d.dvel[j];
+        double4 sj = d.dst[j];
+        VR vj = cvt<R>(xyz(vj4));
+        R cj = (R)sj.x, rho0j = (R)sj.z, mj = (R)vj4.w;
+        VR rji = cvt<R>(xyz(pj4) - ri);
+        R grj = dot(g, rji);
+        if (grj < (R)0.) grj = (R)0.;
+        R PR = PL + rhoi * grj;
+        R rhoj = PR / (cj * cj) + rho0j;
+        VR rij = cvt<R>(ri - xyz(pj4));
+        R r = rlen(rij);
+        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
+        VR dW = f * rij;
+        VR e = v3r<R>(0, 0, 0);
+        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
+        VR vs = (R)0.5 * (vi + vj);
+        vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
+        dRho += mj / rhoj * dot(vi - vs, dW);
+    }
+    double dr = (double)(dRho * ((R)2.0 * rhoi));
+    double ch = d.drho[i] + dr * dt;
+    d.drho[i] = ch;
+    double r0 = d.rho0[i];
+    if (ch < -0.1 * r0) ch = -0.1 * r0;
+    d.stOut[i] = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
+}
+
+// calDummyParticleNormalKernel (WCSPHIntegrationKernel.cu:4-40) over the
+// dummy-dummy pairs (j != i within 2 max(h)), walked in stencil order; the
+// pairs are also written out as an ELL list for inspection.
+__global__ void k_sph_dummy_normals(int nd, GridDesc g, const int* __restrict__ dStart, const double4* __restrict__ dpos,
+                                    const double4* __restrict__ dvel, const double* __restrict__ drho,
+                                    double4* __restrict__ dnorm, int K, int* __restrict__ nb, int* __restrict__ cnt,
+                                    DevStatus* status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    double4 pi = dpos[i];
+    double3 ri = xyz(pi);
+    double3 th = mk3(0, 0, 0);
+    int c = 0;
+    Stencil st = stencil_of(ri, g);
+    for_stencil_rows(st, g, dStart, [&](int b, int e) {
+        for (int j = b; j < e; j++) {
+            if (j == i) continue;
+            double4 pj = dpos[j];
+            double cut = 2.0 * fmax(pi.w, pj.w);
+            double3 r = ri - xyz(pj);
+            if ((cut * cut - dot(r, r)) >= 0.) {
+                if (c < K) nb[(size_t)c * nd + i] = j;
+                c++;
+                double rl = len(r);
+                double f = gradw_factor<double>(rl, 0.5 * (pi.w + pj.w));
+                th -= dvel[j].w / drho[j] * (f * r);
+            }
+        }
+    });
+    if (c > K) {
+        atomicMax(&status->need_rev, c);
+        atomicExch(&status->overflow, 1);
+        c = K;
+    }
+    cnt[i] = c;
+    dnorm[i] = (len2(th) > 1.e-10) ? d4(th / len(th), 0) : make_double4(0, 0, 0, 0);
+}
+
+// ================================================================ host =====
+struct SphScene {
+    cudaStream_t s = 0;
+    int precision = DEMSPH_PRECISION_FP64;
+    bool ready = false;
+    // host staging: fluid and dummy particles in caller order
+    struct HostSet {
+        std::vector<double4> pos, vel, st;  // st = (rho, p, c, nu)
+        std::vector<double> rho0, drho;
+        size_t size() const { return pos.size(); }
+    } hf, hd;
+    double3 gravity{0, 0, 0};
+    double dt = 0;
+    long iStep = 0;
+    double time = 0;
+    int KF = 96, KD = 64, KDD = 96;
+    CellTable fCells, dCells;
+    DBuf<double4> pos[2], vel[2], st[2];
+    DBuf<double> rho0[2], drho[2];
+    DBuf<int> id[2];
+    DBuf<double4> acc;
+    int P = 0, Vv = 0, S = 0, R0 = 0, D = 0, ID = 0;
+    DBuf<double4> dpos, dvel, dst, dnorm;
+    DBuf<double> drhoD;  // dummy densities (normals only)
+    DBuf<int> did;
+    DBuf<int> nbF, cntF, nbD, cntD, nbDD, cntDD;
+    DBuf<DevStatus> status;
+    bool haveLists = false;
+
+    int N() const { return (int)hf.size(); }
+    int ND() const { return (int)hd.size(); }
+
+    SphDev dev() {
+        SphDev d{};
+        d.N = N(); d.ND = ND(); d.KF = KF; d.KD = KD;
+        d.g = fCells.g;
+        d.fStart = fCells.start.p;
+        d.dStart = dCells.start.p;
+        d.pos = pos[P].p; d.vel = vel[Vv].p; d.st = st[S].p; d.rho0 = rho0[R0].p; d.drho = drho[D].p;
+        d.acc = acc.p;
+        d.dpos = dpos.p; d.dvel = dvel.p; d.dst = dst.p; d.dnorm = dnorm.p;
+        d.nbF = nbF.p; d.cntF = cntF.p; d.nbD = nbD.p; d.cntD = cntD.p;
+        d.gravity = gravity;
+        d.status = status.p;
+        return d;
+    }
+
+    void alloc_lists() {
+        size_t n = (size_t)N();
+        nbF.alloc(n * KF, s, false);
+        cntF.alloc(n, s, true);
+        nbD.alloc(n * std::max(KD, 1), s, false);
+        cntD.alloc(n, s, true);
+    }
+
+    // WCSPHSolver::neighborSearch (WCSPHSolver.h:150-285): fluid cell sort,
+    // reorder, neighbour lists.
+    void neighbor_search() {
+        const int n = N();
+        fCells.build(pos[P].p, n, s, id[ID].p);
+        g_launches += fCells.launches;
+        k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
+                                                       drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
+                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p);
+        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        SphDev d = dev();
+        k_sph_lists<<<grid_for(n, 128), 128, 0, s>>>(d);
+        g_launches += 2;
+        DEMSPH_LAUNCH_CHECK();
+        haveLists = true;
+    }
+    void accel(int first) {
+        SphDev d = dev();
+        const int n = N();
+        d.posOut = pos[P ^ 1].p;
+        d.velOut = vel[Vv ^ 1].p;
+        if (precision == DEMSPH_PRECISION_FP64)
+            k_sph_accel<double><<<grid_for(n, 128), 128, 0, s>>>(d, 0.5 * dt, dt, first);
+        else
+            k_sph_accel<float><<<grid_for(n, 128), 128, 0, s>>>(d, 0.5 * dt, dt, first);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        if (first) P ^= 1;
+        Vv ^= 1;
+    }
+    void density() {
+        SphDev d = dev();
+        const int n = N();
+        d.stOut = st[S ^ 1].p;
+        if (precision == DEMSPH_PRECISION_FP64) k_sph_density<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        else k_sph_density<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        S ^= 1;
+    }
+    // One pass of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621).
+    void step_once() {
+        iStep++;
+        time += dt;
+        neighbor_search();
+        accel(1);
+        density();
+        accel(0);
+    }
+
+    DevStatus read_status() {
+        DevStatus h{};
+        DEMSPH_CUDA(cudaMemcpyAsync(&h, status.p, sizeof h, cudaMemcpyDeviceToHost, s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+        return h;
+    }
+    void clear_status() { DEMSPH_CUDA(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), s)); }
+    void grow(const DevStatus& st2) {
+        if (st2.need_pairs > KF) KF = st2.need_pairs + st2.need_pairs / 4 + 1;
+        if (st2.need_aux > KD) KD = st2.need_aux + st2.need_aux / 4 + 1;
+        alloc_lists();
+    }
+
+    // Saved dynamic state for overflow replay.
+    struct Snap {
+        std::vector<std::unique_ptr<DBuf<char>>> bufs;
+        std::vector<void*> dst;
+        std::vector<size_t> bytes;
+        long iStep;
+        double time;
+        int P, Vv, S, R0, D, ID;
+    };
+    template <class T>
+    void snap_add(Snap& sn, DBuf<T>& b) {
+        if (!b.p || b.n == 0) return;
+        auto c = std::make_unique<DBuf<char>>();
+        c->alloc(b.bytes(), s, false);
+        DEMSPH_CUDA(cudaMemcpyAsync(c->p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
+        sn.dst.push_back((void*)b.p);
+        sn.bytes.push_back(b.bytes());
+        sn.bufs.push_back(std::move(c));
+    }
+    void take(Snap& sn) {
+        sn.iStep = iStep; sn.time = time; sn.P = P; sn.Vv = Vv; sn.S = S; sn.R0 = R0; sn.D = D; sn.ID = ID;
+        snap_add(sn, pos[P]); snap_add(sn, vel[Vv]); snap_add(sn, st[S]); snap_add(sn, rho0[R0]);
+        snap_add(sn, drho[D]); snap_add(sn, id[ID]);
+    }
+    void restore(Snap& sn) {
+        for (size_t k = 0; k < sn.bufs.size(); k++)
+            DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
+        iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID;
+    }
+    void run(long n) {
+        if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (n <= 0) return;
+        for (int attempt = 0; attempt < 8; attempt++) {
+            Snap sn;
+            take(sn);
+            clear_status();
+            for (long k = 0; k < n; k++) step_once();
+            DevStatus st2 = read_status();
+            if (!st2.overflow) return;
+            grow(st2);
+            restore(sn);
+        }
+        throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists kept overflowing after regrowth");
+    }
+
+    void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
+        if (hf.size() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
+        if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
+        for (auto& p : hf.pos)
+            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
+                throw Status(DEMSPH_ERR_SCENE, "fluid particle with non-finite position or non-positive h");
+        precision = prec;
+        gravity = g;
+        dt = timeStep;
+        double cell = 0;
+        for (auto& p : hf.pos) cell = std::max(cell, p.w * 2.0);
+        for (auto& p : hd.pos) cell = std::max(cell, p.w * 2.0);
+        GridDesc gd{};
+        if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
+        status.alloc(1, s, true);
+        const int n = N(), nd = ND();
+        fCells.setup(gd, n, s);
+        dCells.setup(gd, std::max(nd, 1), s);
+        std::vector<int> ids(n);
+        for (int i = 0; i < n; i++) ids[i] = i;
+        for (int b = 0; b < 2; b++) {
+            pos[b].alloc(n, s, false); vel[b].alloc(n, s, false); st[b].alloc(n, s, false);
+            rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
+        }
+        P = Vv = S = R0 = D = ID = 0;
+        auto up4 = [&](DBuf<double4>& b, const std::vector<double4>& h) {
+            DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
+        };
+        up4(pos[0], hf.pos); up4(vel[0], hf.vel); up4(st[0], hf.st);
+        DEMSPH_CUDA(cudaMemcpyAsync(rho0[0].p, hf.rho0.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+        DEMSPH_CUDA(cudaMemcpyAsync(drho[0].p, hf.drho.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+        DEMSPH_CUDA(cudaMemcpyAsync(id[0].p, ids.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        acc.alloc(n, s, true);
+        // dummies: sort once into cell order (initializeBoundaryCondition, WCSPHSolver.h:29-110)
+        if (nd > 0) {
+            DBuf<double4> tp, tv, ts;
+            tp.upload(hd.pos, s); tv.upload(hd.vel, s);
+            std::vector<double4> dst4(nd);
+            std::vector<double> rh(nd);
+            for (int i = 0; i < nd; i++) {
+                dst4[i] = make_double4(hd.st[i].z, hd.st[i].w, hd.rho0[i], 0);
+                rh[i] = hd.st[i].x;
+            }
+            ts.upload(dst4, s);
+            DBuf<double> trh;
+            trh.upload(rh, s);
+            dCells.build(tp.p, nd, s);
+            g_launches += dCells.launches;
+            std::vector<int> order(nd);
+            DEMSPH_CUDA(cudaMemcpyAsync(order.data(), dCells.sorted.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s));
+            DEMSPH_CUDA(cudaStreamSynchronize(s));
+            std::vector<double4> sp(nd), sv(nd), ss(nd);
+            std::vector<double> sr(nd);
+            for (int t = 0; t < nd; t++) {
+                int o = order[t];
+                sp[t] = hd.pos[o]; sv[t] = hd.vel[o]; ss[t] = dst4[o]; sr[t] = rh[o];
+            }
+            dpos.upload(sp, s); dvel.upload(sv, s); dst.upload(ss, s); drhoD.upload(sr, s);
+            did.upload(order, s);
+            dnorm.alloc(nd, s, true);
+            for (int attempt = 0; attempt < 8; attempt++) {
+                nbDD.alloc((size_t)nd * KDD, s, false);
+                cntDD.alloc(nd, s, true);
+                clear_status();
+                k_sph_dummy_normals<<<grid_for(nd, 128), 128, 0, s>>>(nd, gd, dCells.start.p, dpos.p, dvel.p, drhoD.p,
+                                                                      dnorm.p, KDD, nbDD.p, cntDD.p, status.p);
+                g_launches += 1;
+                DEMSPH_LAUNCH_CHECK();
+                DevStatus st2 = read_status();
+                if (!st2.overflow) break;
+                KDD = st2.need_rev + st2.need_rev / 4 + 1;
+            }
+        } else {
+            dCells.build(nullptr, 0, s);
+            g_launches += dCells.launches;
+        }
+        // size the neighbour lists on the initial configuration (sorting the
+        // fluid into cell order, which any later step does anyway)
+        alloc_lists();
+        for (int attempt = 0; attempt < 8; attempt++) {
+            clear_status();
+            neighbor_search();
+            DevStatus st2 = read_status();
+            if (!st2.overflow) break;
+            grow(st2);
+        }
+        // a little headroom for compression during the run
+        KF = KF + KF / 8;
+        KD = KD + KD / 8;
+        alloc_lists();
+        haveLists = false;
+        iStep = 0;
+        time = 0;
+        ready = true;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    }
+};
+
+}  // namespace demsph
+
+// ================================================================ C ABI ====
+using namespace demsph;
+
+struct demsph_sph_scene {
+    SphScene sc;
+};
+
+static inline double3 sld3(const double* a, long i) { return mk3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
+static inline void sst3(double* a, long i, double3 v) { a[3 * i] = v.x; a[3 * i + 1] = v.y; a[3 * i + 2] = v.z; }
+
+#define SPH_CHECK(h) \
+    if (!(h)) throw Status(DEMSPH_ERR_INVALID, "null scene handle")
+
+extern "C" {
+
+int demsph_sph_create(demsph_sph_t* out, void* stream) {
+    return guarded([&] {
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        auto* h = new demsph_sph_scene();
+        h->sc.s = (cudaStream_t)stream;
+        *out = h;
+    });
+}
+int demsph_sph_destroy(demsph_sph_t h) {
+    return guarded([&] {
+        if (!h) return;
+        cudaStream_t s = h->sc.s;
+        delete h;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int demsph_sph_add(demsph_sph_t h, int dummy, long n, const double* pos, const double* vel, const double* c,
+                   const double* spacing, const double* dens, const double* visc) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "particles must be added before initialisation");
+        SphScene::HostSet& t = dummy ? s.hd : s.hf;
+        for (long i = 0; i < n; i++) {
+            double rho = dens[i], cc = c[i], sp = spacing[i];
+            if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
+            double m = sp * sp * sp * rho;
+            t.pos.push_back(d4(sld3(pos, i), 1.3 * sp));
+            t.vel.push_back(d4(vel ? sld3(vel, i) : mk3(0, 0, 0), m));
+            t.st.push_back(make_double4(rho, 0.0, cc, visc[i]));
+            t.rho0.push_back(rho);
+            t.drho.push_back(0.0);
+        }
+    });
+}
+int demsph_sph_initialize(demsph_sph_t h, const double* mn, const double* mx, const double* g, double dt, int prec) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (prec != DEMSPH_PRECISION_FP64 && prec != DEMSPH_PRECISION_MIXED)
+            throw Status(DEMSPH_ERR_INVALID, "unknown precision mode");
+        h->sc.initialize(sld3(mn, 0), sld3(mx, 0), sld3(g, 0), dt, prec);
+    });
+}
+int demsph_sph_step(demsph_sph_t h, long n) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        h->sc.run(n);
+    });
+}
+int demsph_sph_neighbor_search(demsph_sph_t h) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        for (int attempt = 0; attempt < 8; attempt++) {
+            SphScene::Snap sn;
+            s.take(sn);
+            s.clear_status();
+            s.neighbor_search();
+            DevStatus st2 = s.read_status();
+            if (!st2.overflow) return;
+            s.grow(st2);
+            s.restore(sn);
+        }
+        throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists overflow");
+    });
+}
+int demsph_sph_eval_accel(demsph_sph_t h) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready || !s.haveLists) throw Status(DEMSPH_ERR_NOT_READY, "no neighbour lists");
+        // acceleration only: kick / drift go to the scratch buffers, the state is unchanged
+        SphDev d = s.dev();
+        d.posOut = s.pos[s.P ^ 1].p;
+        d.velOut = s.vel[s.Vv ^ 1].p;
+        if (s.precision == DEMSPH_PRECISION_FP64)
+            k_sph_accel<double><<<grid_for(s.N(), 128), 128, 0, s.s>>>(d, 0.0, 0.0, 0);
+        else
+            k_sph_accel<float><<<grid_for(s.N(), 128), 128, 0, s.s>>>(d, 0.0, 0.0, 0);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_sph_num(demsph_sph_t h, int dummy, long* n) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        *n = dummy ? h->sc.ND() : h->sc.N();
+    });
+}
+int demsph_sph_step_index(demsph_sph_t h, long* step, double* time) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (step) *step = h->sc.iStep;
+        if (time) *time = h->sc.time;
+    });
+}
+int demsph_sph_get(demsph_sph_t h, int dummy, double* pos, double* vel, double* accel, double* rho, double* p,
+                   double* drho, double* normal) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (dummy) {
+            int nd = s.ND();
+            if (nd == 0) return;
+            std::vector<double4> P4, V4, S4, N4;
+            std::vector<int> ID;
+            std::vector<double> RH;
+            s.dpos.download(P4, s.s); s.dvel.download(V4, s.s); s.dnorm.download(N4, s.s); s.did.download(ID, s.s);
+            s.drhoD.download(RH, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            for (int t = 0; t < nd; t++) {
+                int o = ID[t];
+                if (pos) sst3(pos, o, xyz(P4[t]));
+                if (vel) sst3(vel, o, xyz(V4[t]));
+                if (accel) sst3(accel, o, mk3(0, 0, 0));
+                if (rho) rho[o] = RH[t];
+                if (p) p[o] = 0.0;
+                if (drho) drho[o] = 0.0;
+                if (normal) sst3(normal, o, xyz(N4[t]));
+            }
+            return;
+        }
+        int n = s.N();
+        std::vector<double4> P4, V4, S4, A4;
+        std::vector<double> DR;
+        std::vector<int> IDp, IDv, IDs, IDd;
+        s.pos[s.P].download(P4, s.s); s.vel[s.Vv].download(V4, s.s); s.st[s.S].download(S4, s.s);
+        s.drho[s.D].download(DR, s.s); s.acc.download(A4, s.s);
+        s.id[s.ID].download(IDp, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        // all fields share the order of the last permutation
+        for (int t = 0; t < n; t++) {
+            int o = IDp[t];
+            if (pos) sst3(pos, o, xyz(P4[t]));
+            if (vel) sst3(vel, o, xyz(V4[t]));
+            if (accel) sst3(accel, o, xyz(A4[t]));
+            if (rho) rho[o] = S4[t].x;
+            if (p) p[o] = S4[t].y;
+            if (drho) drho[o] = DR[t];
+            if (normal) sst3(normal, o, mk3(0, 0, 0));
+        }
+    });
+}
+int demsph_sph_set(demsph_sph_t h, const double* pos, const double* vel, const double* rho, const double* p,
+                   const double* drho) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        int n = s.N();
+        if (!s.ready) {
+            for (int i = 0; i < n; i++) {
+                if (pos) { double3 q = sld3(pos, i); s.hf.pos[i].x = q.x; s.hf.pos[i].y = q.y; s.hf.pos[i].z = q.z; }
+                if (vel) { double3 q = sld3(vel, i); s.hf.vel[i].x = q.x; s.hf.vel[i].y = q.y; s.hf.vel[i].z = q.z; }
+                if (rho) s.hf.st[i].x = rho[i];
+                if (p) s.hf.st[i].y = p[i];
+                if (drho) s.hf.drho[i] = drho[i];
+            }
+            return;
+        }
+        std::vector<double4> P4, V4, S4;
+        std::vector<double> DR;
+        std::vector<int> ID;
+        s.pos[s.P].download(P4, s.s); s.vel[s.Vv].download(V4, s.s); s.st[s.S].download(S4, s.s);
+        s.drho[s.D].download(DR, s.s); s.id[s.ID].download(ID, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (int t = 0; t < n; t++) {
+            int o = ID[t];
+            if (pos) { double3 q = sld3(pos, o); P4[t].x = q.x; P4[t].y = q.y; P4[t].z = q.z; }
+            if (vel) { double3 q = sld3(vel, o); V4[t].x = q.x; V4[t].y = q.y; V4[t].z = q.z; }
+            if (rho) S4[t].x = rho[o];
+            if (p) S4[t].y = p[o];
+            if (drho) DR[t] = drho[o];
+        }
+        DEMSPH_CUDA(cudaMemcpyAsync(s.pos[s.P].p, P4.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        DEMSPH_CUDA(cudaMemcpyAsync(s.vel[s.Vv].p, V4.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        DEMSPH_CUDA(cudaMemcpyAsync(s.st[s.S].p, S4.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        DEMSPH_CUDA(cudaMemcpyAsync(s.drho[s.D].p, DR.data(), n * sizeof(double), cudaMemcpyHostToDevice, s.s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        s.haveLists = false;
+    });
+}
+int demsph_sph_num_pairs(demsph_sph_t h, int which, long* n) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        std::vector<int> cnt;
+        if (which == 2) s.cntDD.download(cnt, s.s);
+        else {
+            if (!s.haveLists) throw Status(DEMSPH_ERR_NOT_READY, "no neighbour lists");
+            (which == 0 ? s.cntF : s.cntD).download(cnt, s.s);
+        }
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        long t = 0;
+        for (int c : cnt) t += c;
+        *n = t;
+    });
+}
+int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        std::vector<int> cnt, nb, rowId, colId;
+        int rows, K = 0;
+        if (which == 2) {
+            s.cntDD.download(cnt, s.s); s.nbDD.download(nb, s.s);
+            s.did.download(rowId, s.s);
+            colId = std::vector<int>();
+            rows = s.ND(); K = s.KDD;
+        } else {
+            if (!s.haveLists) throw Status(DEMSPH_ERR_NOT_READY, "no neighbour lists");
+            (which == 0 ? s.cntF : s.cntD).download(cnt, s.s);
+            (which == 0 ? s.nbF : s.nbD).download(nb, s.s);
+            s.id[s.ID].download(rowId, s.s);
+            rows = s.N(); K = which == 0 ? s.KF : s.KD;
+        }
+        std::vector<int> didv;
+        s.did.download(didv, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        (void)K;
+        const std::vector<int>& col = (which == 0) ? rowId : didv;
+        // rows emitted in the caller's original order
+        std::vector<int> rowOf(rows);
+        for (int t = 0; t < rows; t++) rowOf[rowId[t]] = t;
+        long w = 0;
+        for (int o = 0; o < rows; o++) {
+            int t = rowOf[o];
+            for (int k = 0; k < cnt[t]; k++) {
+                a[w] = o;
+                b[w] = col[nb[(size_t)k * rows + t]];
+                w++;
+            }
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,253 @@
+"""Scene descriptions: the reference's example scenes and seeded synthetic
+workloads with the sizes of the benchmark configurations.
+
+A scene is plain data (numpy arrays + parameters); ``build_dem`` /
+``build_sph`` load it into the solvers.  Generators take explicit seeds.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def uniform_point_cloud(mn, mx, dx):
+    """Inclusive-endpoint lattice of generateUniformPointCloud
+    (DEMSPH/pointCloudGeneration.h:7-58): floor(L/dx + 1e-12) + 1 points per
+    axis from the low corner, x fastest, then y, then z."""
+    eps = 1e-12
+    lo = np.minimum(mn, mx).astype(float)
+    hi = np.maximum(mn, mx).astype(float)
+    n = [max(0, int(math.floor((b - a) / dx + eps)) + 1) for a, b in zip(lo, hi)]
+    axes = []
+    for k in range(3):
+        v = lo[k] + np.arange(n[k]) * dx
+        axes.append(v[v <= hi[k] + eps])
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+
+
+@dataclass
+class DEMScene:
+    name: str
+    position: np.ndarray
+    radius: np.ndarray
+    density: np.ndarray
+    material: np.ndarray
+    velocity: np.ndarray = None
+    fixed: np.ndarray = None          # bool per ball (addFixedBall)
+    hertz: list = field(default_factory=list)    # rows of setHertzianPair args
+    linear: list = field(default_factory=list)   # rows of setLinearPair args
+    bonded: list = field(default_factory=list)   # rows of setBondedPair args
+    walls: list = field(default_factory=list)    # dicts: vertices, tri0, tri1, tri2, position, material
+    clumps: list = field(default_factory=list)   # dicts of addClump args
+    bond_initial_contacts: bool = False          # the addInitialCondition hook of the bonded scenes
+    buoyancy: tuple = None                       # (rho, Cd, g, u, level)
+    minb: tuple = (0, 0, 0)
+    maxb: tuple = (1, 1, 1)
+    gravity: tuple = (0, 0, -9.81)
+    dt: float = 1e-5
+    steps: int = 1000
+
+    @property
+    def num_moving(self):
+        nf = 0 if self.fixed is None else int(np.count_nonzero(self.fixed))
+        npeb = sum(len(c["radius"]) for c in self.clumps)
+        return self.position.shape[0] - nf + npeb
+
+
+@dataclass
+class SPHScene:
+    name: str
+    fluid: np.ndarray
+    dummy: np.ndarray
+    spacing: float
+    sound_speed: float
+    density: float = 1000.0
+    viscosity: float = 1e-3
+    minb: tuple = (0, 0, 0)
+    maxb: tuple = (1, 1, 1)
+    gravity: tuple = (0, 0, -9.81)
+    dt: float = 1e-4
+    steps: int = 1000
+
+
+# ---------------------------------------------------------------------------
+# Reference example scenes
+# ---------------------------------------------------------------------------
+def elastic_bounce():
+    """DEMSPH/elasticBounce.cpp: one sphere (r 0.01, rho 2000) dropped from
+    z = 0 onto a 2-triangle wall at z = -1, undamped linear spring with
+    contact time 5 ms, dt = t_c / 50."""
+    r, tc = 0.01, 0.005
+    m = 4.0 / 3.0 * r ** 3 * math.pi * 2000
+    verts = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1]], float)
+    s = DEMScene(
+        name="elastic_bounce",
+        position=np.zeros((1, 3)), radius=np.array([r]), density=np.array([2000.0]), material=np.array([0]),
+        linear=[(0, 0, 0.5 * m * math.pi ** 2 / tc / tc, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)],
+        walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0), material=0)],
+        minb=(-1, -1, -1), maxb=(1, 1, 1), gravity=(0, 0, -9.81), dt=tc / 50, steps=20000)
+    return s
+
+
+def dam_break_reference():
+    """DEMSPH/damBreak.cpp: 21 x 41 x 21 fluid lattice at dx = 0.005 in a
+    5H x 2H x 3H tank (H = 0.1) with three dummy layers, open top."""
+    H, sp = 0.1, 0.005
+    n = int(H / sp)
+    sp = H / n
+    fluid = uniform_point_cloud(np.array([0.0, 0, 0]), np.array([H, 2 * H, H]), sp)
+    tw = 3 * sp
+    lo = np.array([0.0, 0, 0]) - tw
+    hi = np.array([5 * H, 2 * H, 3 * H]) + tw
+    d0 = uniform_point_cloud(lo, hi, sp)
+    keep = (d0[:, 0] < 0) | (d0[:, 1] < 0) | (d0[:, 2] < 0) | (d0[:, 0] > 5 * H) | (d0[:, 1] > 2 * H)
+    c = 20.0 * math.sqrt(9.81 * H)
+    dt = 0.25 * 1.3 * sp / (c + 2.0 * math.sqrt(9.81 * H))
+    return SPHScene(name="dam_break_reference", fluid=fluid, dummy=d0[keep], spacing=sp, sound_speed=c,
+                    minb=tuple(lo), maxb=tuple(hi), dt=dt, steps=670)
+
+
+# ---------------------------------------------------------------------------
+# Benchmark-sized synthetic scenes
+# ---------------------------------------------------------------------------
+def hertz_params(E, nu):
+    """Effective moduli for like materials: E* = E / (2 (1 - nu^2)),
+    G* = E / (4 (2 - nu)(1 + nu))."""
+    return E / (2 * (1 - nu * nu)), E / (4 * (2 - nu) * (1 + nu))
+
+
+def dem_drop(n_side=16, spacing=0.012, radius=0.005, density=2500.0, jitter=0.0005, seed=1, plane_gap=0.001,
+             E=1e8, nu=0.3, restitution=0.8, mu=0.3, dt=1e-5, steps=1000):
+    """n_side^3 Hertz-Mindlin spheres on a jittered lattice dropped onto a
+    2-triangle plane wall (the plain DEM bounce workload: 4,096 spheres,
+    r 5 mm, rho 2500, 12 mm lattice, +-0.5 mm seeded jitter)."""
+    rng = np.random.default_rng(seed)
+    g = (np.arange(n_side) + 0.5) * spacing
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    p += rng.uniform(-jitter, jitter, size=p.shape)
+    n = p.shape[0]
+    Es, Gs = hertz_params(E, nu)
+    zmin = p[:, 2].min() - radius - plane_gap
+    L = n_side * spacing
+    cell = 2 * radius
+    lo = np.array([-2 * cell, -2 * cell, zmin - 2 * cell])
+    hi = np.array([L + 2 * cell, L + 2 * cell, p[:, 2].max() + radius + 2 * cell])
+    verts = np.array([[lo[0], lo[1], zmin], [hi[0], lo[1], zmin], [hi[0], hi[1], zmin], [lo[0], hi[1], zmin]])
+    return DEMScene(
+        name="dem_drop", position=p, radius=np.full(n, radius), density=np.full(n, density),
+        material=np.zeros(n, np.int32),
+        hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)],
+        walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0), material=0)],
+        minb=tuple(lo), maxb=tuple(hi), dt=dt, steps=steps)
+
+
+def dem_pack(n_side=16, radius=0.005, density=2500.0, overlap=0.02, seed=3, E=1e8, nu=0.3, restitution=0.8,
+             mu=0.3, vel=0.05, dt=1e-5):
+    """A dense, touching lattice pack with seeded random velocities and
+    spins: every ball starts in contact with its face neighbours, so pair
+    forces, friction springs and rolling all act from the first step."""
+    rng = np.random.default_rng(seed)
+    sp = 2 * radius * (1 - overlap)
+    g = (np.arange(n_side) + 0.5) * sp
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    p += rng.uniform(-0.02 * radius, 0.02 * radius, size=p.shape)
+    n = p.shape[0]
+    Es, Gs = hertz_params(E, nu)
+    L = n_side * sp
+    cell = 2 * radius
+    lo = np.array([-2 * cell] * 3)
+    hi = np.array([L + 2 * cell] * 3)
+    s = DEMScene(
+        name="dem_pack", position=p, radius=np.full(n, radius), density=np.full(n, density),
+        material=np.zeros(n, np.int32),
+        hertz=[(0, 0, Es, Gs, restitution, 0.2, 0.1, mu, 0.05, 0.05)],
+        minb=tuple(lo), maxb=tuple(hi), gravity=(0, 0, -9.81), dt=dt, steps=100)
+    s.velocity = rng.normal(0, vel, size=p.shape)
+    s.angvel = rng.normal(0, vel / radius, size=p.shape)
+    return s
+
+
+def sph_dam_break(nx=40, ny=40, nz=80, dx=0.01, tank=(1.6, 0.4, 1.0), layers=3, column_height=0.8, steps=2000):
+    """WCSPH dam break with nx*ny*nz fluid particles (default 40x40x80 =
+    128,000 at dx = 0.01 in a 0.4 x 0.4 x 0.8 column) inside a tank with
+    `layers` dummy layers on the floor and side walls (open top, the rule of
+    DEMSPH/damBreak.cpp:25-34); h = 1.3 dx, c0 = 10 sqrt(2 g H),
+    dt = 0.25 h / (c0 + 2 sqrt(g H))."""
+    gx = (np.arange(nx) + 0.5) * dx
+    gy = (np.arange(ny) + 0.5) * dx
+    gz = (np.arange(nz) + 0.5) * dx
+    z, y, x = np.meshgrid(gz, gy, gx, indexing="ij")
+    fluid = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    tw = layers * dx
+    lo = np.array([0.0, 0, 0]) - tw
+    hi = np.array(tank, float) + tw
+    ax = [np.arange(-layers, int(round(t / dx)) + layers) * dx + 0.5 * dx for t in tank]
+    zz, yy, xx = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    d0 = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    keep = (d0[:, 0] < 0) | (d0[:, 1] < 0) | (d0[:, 2] < 0) | (d0[:, 0] > tank[0]) | (d0[:, 1] > tank[1])
+    g = 9.81
+    c0 = 10.0 * math.sqrt(2 * g * column_height)
+    h = 1.3 * dx
+    dt = 0.25 * h / (c0 + 2.0 * math.sqrt(g * column_height))
+    return SPHScene(name="sph_dam_break", fluid=fluid, dummy=d0[keep], spacing=dx, sound_speed=c0,
+                    minb=tuple(lo), maxb=tuple(hi), dt=dt, steps=steps)
+
+
+# ---------------------------------------------------------------------------
+# Loading into the solvers
+# ---------------------------------------------------------------------------
+def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
+    from .solvers import DEMSolver
+
+    s = DEMSolver(stream)
+    for row in scene.hertz:
+        s.setHertzianPair(*row)
+    for row in scene.linear:
+        s.setLinearPair(*row)
+    for row in scene.bonded:
+        s.setBondedPair(*row)
+    fixed = np.zeros(scene.position.shape[0], bool) if scene.fixed is None else scene.fixed
+    # keep the caller's ball order: add runs of moving / fixed balls in sequence
+    idx = np.arange(scene.position.shape[0])
+    starts = np.flatnonzero(np.diff(np.r_[-1, fixed.astype(int)]) != 0)
+    bounds = list(starts) + [len(idx)]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        sl = slice(a, b)
+        if fixed[a]:
+            s.addFixedBalls(scene.position[sl], scene.radius[sl], scene.material[sl])
+        else:
+            vel = None if scene.velocity is None else scene.velocity[sl]
+            w = getattr(scene, "angvel", None)
+            s.addBalls(scene.position[sl], vel, None if w is None else w[sl], scene.radius[sl], scene.density[sl],
+                       scene.material[sl])
+    for c in scene.clumps:
+        s.addClump(c["point"], c["radius"], c["centroid"], c["velocity"], c["angularVelocity"], c["mass"],
+                   c["inertia"], c["material"])
+    for k, w in enumerate(scene.walls):
+        s.addMeshWall(w["vertices"], w["tri0"], w["tri1"], w["tri2"], w["position"], materialID=w["material"])
+        if "velocity" in w:
+            s.setMeshWallMotion(k, w["velocity"], w.get("angularVelocity", (0, 0, 0)))
+    if scene.buoyancy is not None:
+        s.setBuoyancyDrag(*scene.buoyancy)
+    if initialize:
+        s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
+        if scene.bond_initial_contacts:
+            p = s.getPairs(0)
+            s.addBondedInteraction(p["objectPointed"], p["objectPointing"], scene.position)
+    return s
+
+
+def build_sph(scene: SPHScene, precision="fp64", stream=None, initialize=True):
+    from .solvers import WCSPHSolver
+
+    s = WCSPHSolver(stream)
+    s.addSPHs(scene.fluid, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
+    s.addDummies(scene.dummy, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
+    if initialize:
+        s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
+    return s

@@ -1,0 +1,359 @@
+"""Python mirror of the reference's solver classes over the C ABI.
+
+``DEMSolver`` follows DEMSPH/kernel/DEMSolver.h (scene setup :1633-1959,
+solve :1961-2049, step pieces :278-906, getters :1541-1631) and
+``WCSPHSolver`` follows DEMSPH/kernel/WCSPHSolver.h (:522-624), with the same
+method names and argument meaning.  ``solve`` runs the reference's step loop
+without the VTU output; ``initialize`` + ``step`` split it for callers that
+step incrementally.  Bulk adders (``addBalls`` ...) take arrays.
+
+Errors: every native failure raises ``DemsphError`` carrying the status code.
+The reference instead returns silently or exits (DEMSolver.h:1974-2004).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import call
+
+_d = C.POINTER(C.c_double)
+_i = C.POINTER(C.c_int)
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return a.reshape(shape) if shape is not None else a
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_d)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_i)
+
+
+def _v3(x):
+    return _f64(x, (3,))
+
+
+def _stream_ptr(stream):
+    if stream is None or stream == 0:
+        return None
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+def num_steps(timeStep, maximumTime):
+    """Step count of solve(): size_t(maximumTime / timeStep) + 1 iterations of
+    ``while (iStep <= numStep)`` (DEMSolver.h:1988,1380), i.e. numStep + 1."""
+    return int(maximumTime / timeStep) + 1 + 1
+
+
+class DEMSolver:
+    """Spheres, clumps, triangle-mesh walls, linear / Hertz-Mindlin / bonded contact."""
+
+    def __init__(self, stream=None):
+        self._h = C.c_void_p()
+        call("demsph_dem_create", C.byref(self._h), _stream_ptr(stream))
+        self._nvert = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().demsph_dem_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ---------------------------------------------------------- materials --
+    def setHertzianPair(self, materialIndexA, materialIndexB, effectiveYoungsModulus, effectiveShearModulus,
+                        restitutionCoefficient, rollingStiffnessToShearStiffnessRatio=0.0,
+                        torsionStiffnessToShearStiffnessRatio=0.0, slidingFrictionCoefficient=0.0,
+                        rollingFrictionCoefficient=0.0, torsionFrictionCoefficient=0.0):
+        call("demsph_dem_set_hertzian_pair", self._h, materialIndexA, materialIndexB, effectiveYoungsModulus,
+             effectiveShearModulus, restitutionCoefficient, rollingStiffnessToShearStiffnessRatio,
+             torsionStiffnessToShearStiffnessRatio, slidingFrictionCoefficient, rollingFrictionCoefficient,
+             torsionFrictionCoefficient)
+
+    def setLinearPair(self, materialIndexA, materialIndexB, normalStiffness, slidingStiffness, rollingStiffness,
+                      torsionStiffness, normalDissipation, slidingDissipation, rollingDissipation, torsionDissipation,
+                      slidingFrictionCoefficient, rollingFrictionCoefficient, torsionFrictionCoefficient):
+        call("demsph_dem_set_linear_pair", self._h, materialIndexA, materialIndexB, normalStiffness,
+             slidingStiffness, rollingStiffness, torsionStiffness, normalDissipation, slidingDissipation,
+             rollingDissipation, torsionDissipation, slidingFrictionCoefficient, rollingFrictionCoefficient,
+             torsionFrictionCoefficient)
+
+    def setBondedPair(self, materialIndexA, materialIndexB, bondRadiusMultiplier, bondYoungsModulus,
+                      normalToShearStiffnessRatio, tensileStrength, cohesion, frictionCoefficient):
+        call("demsph_dem_set_bonded_pair", self._h, materialIndexA, materialIndexB, bondRadiusMultiplier,
+             bondYoungsModulus, normalToShearStiffnessRatio, tensileStrength, cohesion, frictionCoefficient)
+
+    # ------------------------------------------------------------- bodies --
+    def addBalls(self, position, velocity, angularVelocity, radius, density, materialID, clumpID=None):
+        p = _f64(position, (-1, 3))
+        n = p.shape[0]
+        v = _f64(np.zeros((n, 3)) if velocity is None else velocity, (n, 3))
+        w = _f64(np.zeros((n, 3)) if angularVelocity is None else angularVelocity, (n, 3))
+        r = _f64(np.broadcast_to(radius, (n,)))
+        d = _f64(np.broadcast_to(density, (n,)))
+        m = _i32(np.broadcast_to(materialID, (n,)))
+        c = None if clumpID is None else _i32(np.broadcast_to(clumpID, (n,)))
+        call("demsph_dem_add_balls", self._h, n, _dp(p), _dp(v), _dp(w), _dp(r), _dp(d), _ip(m), _ip(c), 0)
+
+    def addBall(self, position, velocity, angularVelocity, radius, density, materialID, clumpID=-1):
+        self.addBalls([position], [velocity], [angularVelocity], radius, density, materialID, clumpID)
+
+    def addFixedBalls(self, position, radius, materialID, clumpID=None):
+        p = _f64(position, (-1, 3))
+        n = p.shape[0]
+        r = _f64(np.broadcast_to(radius, (n,)))
+        m = _i32(np.broadcast_to(materialID, (n,)))
+        c = None if clumpID is None else _i32(np.broadcast_to(clumpID, (n,)))
+        call("demsph_dem_add_balls", self._h, n, _dp(p), None, None, _dp(r), None, _ip(m), _ip(c), 1)
+
+    def addFixedBall(self, position, radius, materialID, clumpID=-1):
+        self.addFixedBalls([position], radius, materialID, clumpID)
+
+    def addClump(self, point, radius, centroidPosition, velocity, angularVelocity, mass, inertiaTensor,
+                 materialID):
+        p = _f64(point, (-1, 3))
+        call("demsph_dem_add_clump", self._h, p.shape[0], _dp(p), _dp(_f64(radius)), _dp(_v3(centroidPosition)),
+             _dp(_v3(velocity)), _dp(_v3(angularVelocity)), float(mass), _dp(_f64(inertiaTensor, (6,))),
+             int(materialID))
+
+    def addMeshWall(self, vertexPosition, triIndex0, triIndex1, triIndex2, position, velocity=None,
+                    angularVelocity=None, materialID=0):
+        """Like the reference, velocity / angularVelocity are not applied
+        (DEMSolver.h:1901-1911); use setMeshWallMotion."""
+        v = _f64(vertexPosition, (-1, 3))
+        t0, t1, t2 = _i32(triIndex0), _i32(triIndex1), _i32(triIndex2)
+        call("demsph_dem_add_mesh_wall", self._h, v.shape[0], _dp(v), t0.shape[0], _ip(t0), _ip(t1), _ip(t2),
+             _dp(_v3(position)), int(materialID))
+        self._nvert += v.shape[0]
+
+    def setMeshWallMotion(self, wall, velocity, angularVelocity):
+        call("demsph_dem_set_wall_motion", self._h, int(wall), _dp(_v3(velocity)), _dp(_v3(angularVelocity)))
+
+    def addBondedInteraction(self, objectPointed, objectPointing, ballPosition):
+        a, b = _i32(objectPointed), _i32(objectPointing)
+        p = _f64(ballPosition, (-1, 3))
+        call("demsph_dem_add_bonds", self._h, a.shape[0], _ip(a), _ip(b), _dp(p), p.shape[0])
+
+    def setPeriodicBoundary(self, X, Y, Z):
+        if X or Y or Z:
+            raise NotImplementedError("periodic boundaries are not built in this library yet")
+
+    # ------------------------------------------------ external force hook --
+    def setConstantForce(self, force, rampTime=0.0):
+        f = _f64(force, (-1, 3))
+        call("demsph_dem_set_constant_force", self._h, f.shape[0], _dp(f), float(rampTime))
+
+    def setGlobalDamping(self, dampCoeff):
+        call("demsph_dem_set_global_damping", self._h, float(dampCoeff))
+
+    def setBuoyancyDrag(self, rhoFluid, Cd, gravity, fluidVelocity, waterLevel):
+        call("demsph_dem_set_buoyancy_drag", self._h, float(rhoFluid), float(Cd), _dp(_v3(gravity)),
+             _dp(_v3(fluidVelocity)), float(waterLevel))
+
+    # ---------------------------------------------------------------- run --
+    def initialize(self, minBoundary, maxBoundary, gravity, timeStep, precision="mixed"):
+        prec = _lib.PRECISION_FP64 if precision in ("fp64", _lib.PRECISION_FP64) else _lib.PRECISION_MIXED
+        call("demsph_dem_initialize", self._h, _dp(_v3(minBoundary)), _dp(_v3(maxBoundary)), _dp(_v3(gravity)),
+             float(timeStep), prec)
+
+    def step(self, numSteps=1):
+        call("demsph_dem_step", self._h, int(numSteps))
+
+    def solve(self, minBoundary, maxBoundary, gravity, timeStep, maximumTime, numFrame=0, dir=None,
+              deviceID=0, maximumThread=256, precision="mixed"):
+        self.initialize(minBoundary, maxBoundary, gravity, timeStep, precision)
+        self.step(num_steps(timeStep, maximumTime))
+
+    def neighborSearch(self):
+        call("demsph_dem_neighbor_search", self._h)
+
+    def calculateBallContactForceTorque(self, timeStep):
+        call("demsph_dem_eval_forces", self._h, float(timeStep), 0, 0.0)
+
+    def evalForces(self, timeStep, walls=False, wallTimeStep=0.0):
+        call("demsph_dem_eval_forces", self._h, float(timeStep), int(bool(walls)), float(wallTimeStep))
+
+    # ------------------------------------------------------------ getters --
+    def _n(self, fn, *a):
+        n = C.c_long()
+        call(fn, self._h, *a, C.byref(n))
+        return n.value
+
+    @property
+    def numBalls(self):
+        return self._n("demsph_dem_num_balls")
+
+    def stepIndex(self):
+        s, t = C.c_long(), C.c_double()
+        call("demsph_dem_step_index", self._h, C.byref(s), C.byref(t))
+        return s.value, t.value
+
+    def getBall(self):
+        n = self.numBalls
+        out = {k: np.zeros((n, 3)) for k in ("position", "velocity", "angularVelocity", "force", "torque")}
+        call("demsph_dem_get_balls", self._h, _dp(out["position"]), _dp(out["velocity"]),
+             _dp(out["angularVelocity"]), _dp(out["force"]), _dp(out["torque"]))
+        return out
+
+    def setBall(self, position=None, velocity=None, angularVelocity=None):
+        n = self.numBalls
+        f = lambda x: None if x is None else _f64(x, (n, 3))
+        call("demsph_dem_set_balls", self._h, _dp(f(position)), _dp(f(velocity)), _dp(f(angularVelocity)))
+
+    def getPairs(self, which=0):
+        """which = 0: ball-ball (getBallPair*), 1: ball-triangle (getBallTrianglePair*)."""
+        n = self._n("demsph_dem_num_pairs", which)
+        out = {"objectPointed": np.zeros(n, np.int32), "objectPointing": np.zeros(n, np.int32)}
+        for k in ("sliding", "rolling", "torsion", "force", "torqueB"):
+            out[k] = np.zeros((n, 3))
+        call("demsph_dem_get_pairs", self._h, which, _ip(out["objectPointed"]), _ip(out["objectPointing"]),
+             _dp(out["sliding"]), _dp(out["rolling"]), _dp(out["torsion"]), _dp(out["force"]), _dp(out["torqueB"]))
+        return out
+
+    def getBallPairPointed(self):
+        return self.getPairs(0)["objectPointed"]
+
+    def getBallPairPointing(self):
+        return self.getPairs(0)["objectPointing"]
+
+    def importSprings(self, objectPointed, objectPointing, sliding, rolling, torsion):
+        a, b = _i32(objectPointed), _i32(objectPointing)
+        call("demsph_dem_import_springs", self._h, a.shape[0], _ip(a), _ip(b), _dp(_f64(sliding, (-1, 3))),
+             _dp(_f64(rolling, (-1, 3))), _dp(_f64(torsion, (-1, 3))))
+
+    def getBondedInteraction(self):
+        n = self._n("demsph_dem_num_bonds")
+        out = {"objectPointed": np.zeros(n, np.int32), "objectPointing": np.zeros(n, np.int32),
+               "isBonded": np.zeros(n, np.int32), "normalForce": np.zeros(n), "torsionTorque": np.zeros(n)}
+        for k in ("shearForce", "bendingTorque", "normal", "point"):
+            out[k] = np.zeros((n, 3))
+        call("demsph_dem_get_bonds", self._h, _ip(out["objectPointed"]), _ip(out["objectPointing"]),
+             _ip(out["isBonded"]), _dp(out["normalForce"]), _dp(out["torsionTorque"]), _dp(out["shearForce"]),
+             _dp(out["bendingTorque"]), _dp(out["normal"]), _dp(out["point"]))
+        return out
+
+    def getClump(self):
+        n = self._n("demsph_dem_num_clumps")
+        out = {"position": np.zeros((n, 3)), "velocity": np.zeros((n, 3)), "angularVelocity": np.zeros((n, 3)),
+               "orientation": np.zeros((n, 4))}
+        if n:
+            call("demsph_dem_get_clumps", self._h, _dp(out["position"]), _dp(out["velocity"]),
+                 _dp(out["angularVelocity"]), _dp(out["orientation"]))
+        return out
+
+    def getMeshWall(self, numWalls=1):
+        out = {"position": np.zeros((numWalls, 3)), "orientation": np.zeros((numWalls, 4)),
+               "vertexGlobal": np.zeros((self._nvert, 3))}
+        call("demsph_dem_get_walls", self._h, _dp(out["position"]), _dp(out["orientation"]),
+             _dp(out["vertexGlobal"]))
+        return out
+
+
+class WCSPHSolver:
+    """Weakly compressible SPH with fixed dummy wall particles."""
+
+    def __init__(self, stream=None):
+        self._h = C.c_void_p()
+        call("demsph_sph_create", C.byref(self._h), _stream_ptr(stream))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().demsph_sph_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _add(self, dummy, position, velocity, soundSpeed, spacing, density, viscosity):
+        p = _f64(position, (-1, 3))
+        n = p.shape[0]
+        v = _f64(np.zeros((n, 3)) if velocity is None else velocity, (n, 3))
+        b = lambda x: _f64(np.broadcast_to(x, (n,)))
+        call("demsph_sph_add", self._h, int(dummy), n, _dp(p), _dp(v), _dp(b(soundSpeed)), _dp(b(spacing)),
+             _dp(b(density)), _dp(b(viscosity)))
+
+    def addSPHs(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(0, position, velocity, soundSpeed, spacing, density, viscosity)
+
+    def addDummies(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(1, position, velocity, soundSpeed, spacing, density, viscosity)
+
+    def addSPH(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(0, [position], [velocity], soundSpeed, spacing, density, viscosity)
+
+    def addDummy(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(1, [position], [velocity], soundSpeed, spacing, density, viscosity)
+
+    def initialize(self, minBoundary, maxBoundary, gravity, timeStep, precision="fp64"):
+        prec = _lib.PRECISION_MIXED if precision in ("mixed", _lib.PRECISION_MIXED) else _lib.PRECISION_FP64
+        call("demsph_sph_initialize", self._h, _dp(_v3(minBoundary)), _dp(_v3(maxBoundary)), _dp(_v3(gravity)),
+             float(timeStep), prec)
+
+    def step(self, numSteps=1):
+        call("demsph_sph_step", self._h, int(numSteps))
+
+    def solve(self, minBoundary, maxBoundary, gravity, timeStep, maximumTime, numFrame=0, dir=None, deviceID=0,
+              maximumThread=256, precision="fp64"):
+        self.initialize(minBoundary, maxBoundary, gravity, timeStep, precision)
+        self.step(num_steps(timeStep, maximumTime))
+
+    def neighborSearch(self):
+        call("demsph_sph_neighbor_search", self._h)
+
+    def evalAcceleration(self):
+        call("demsph_sph_eval_accel", self._h)
+
+    def num(self, dummy=False):
+        n = C.c_long()
+        call("demsph_sph_num", self._h, int(dummy), C.byref(n))
+        return n.value
+
+    def stepIndex(self):
+        s, t = C.c_long(), C.c_double()
+        call("demsph_sph_step_index", self._h, C.byref(s), C.byref(t))
+        return s.value, t.value
+
+    def _get(self, dummy):
+        n = self.num(dummy)
+        out = {"position": np.zeros((n, 3)), "velocity": np.zeros((n, 3)), "acceleration": np.zeros((n, 3)),
+               "density": np.zeros(n), "pressure": np.zeros(n), "densityChange": np.zeros(n),
+               "normal": np.zeros((n, 3))}
+        call("demsph_sph_get", self._h, int(dummy), _dp(out["position"]), _dp(out["velocity"]),
+             _dp(out["acceleration"]), _dp(out["density"]), _dp(out["pressure"]), _dp(out["densityChange"]),
+             _dp(out["normal"]))
+        return out
+
+    def getSPH(self):
+        return self._get(False)
+
+    def getDummy(self):
+        return self._get(True)
+
+    def setSPH(self, position=None, velocity=None, density=None, pressure=None, densityChange=None):
+        n = self.num()
+        f = lambda x, s: None if x is None else _f64(x, s)
+        call("demsph_sph_set", self._h, _dp(f(position, (n, 3))), _dp(f(velocity, (n, 3))), _dp(f(density, (n,))),
+             _dp(f(pressure, (n,))), _dp(f(densityChange, (n,))))
+
+    def getPairs(self, which=0):
+        """which = 0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy; original indices, CSR order."""
+        n = C.c_long()
+        call("demsph_sph_num_pairs", self._h, int(which), C.byref(n))
+        a, b = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32)
+        call("demsph_sph_get_pairs", self._h, int(which), _ip(a), _ip(b))
+        return a, b
