@@ -1,0 +1,294 @@
+"""Benchmark of the DEMSPH particle-interaction path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload: the plain 3-D WCSPH dam break -- 128,000 fluid particles
+(40 x 40 x 80 at dx = 0.01 m in a 0.4 x 0.4 x 0.8 m column) in a 1.6 x 0.4 x
+1.0 m tank with 3 layers of dummy wall particles (150,216), Wendland C2 with
+h = 1.3 dx, c0 = 10 sqrt(2 g 0.8), dt = 0.25 h / (c0 + 2 sqrt(0.8 g)).  One
+step = the reference's WCSPH step: cell sort + neighbour lists, momentum,
+kick, drift, continuity + EOS, momentum, kick.  Metric: particle-steps/s
+(fluid particles x steps / second).
+
+* value: K steps through the native C ABI with the state resident in HBM,
+  each step bracketed by CUDA events on the launching stream; L2 (126 MB) is
+  flushed by writing a 256 MB buffer between timed steps, outside the events.
+* e2e: the same metric through the public solver API as a user runs it:
+  scene upload from host memory, K steps, final state read back, all timed.
+* roofline: the momentum kernel (the dominant one), timed live per launch.
+* cpu_baseline: the FP64 C++ oracle on the host cores over a short sample.
+* --impl reference: the reference's step restated as the FP64 C++ oracle
+  (the reference has no CPU path; its CUDA build cannot be installed as a
+  package) on all host cores, same workload and metric.
+
+Multi-GPU: replicas only (one independent scene per rank, no collective on
+the data path); value = all ranks' particle-steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+WORKLOAD = "wcsph_dam_break_128k"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        mhz = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k] == "Active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ workload ----
+def workload():
+    from this_studio_b200 import scenes
+
+    return scenes.sph_dam_break()
+
+
+def algorithmic_bytes_momentum(nf, nd, first):
+    """Compulsory HBM bytes of one momentum launch: read each fluid particle's
+    pos, vel, (rho, p, c, nu) once (3 x 32 B) and its list row count (4 B),
+    each dummy's pos, vel, (c, nu, rho0), normal once (4 x 32 B); write the
+    acceleration and the kicked velocity (2 x 32 B) and, in the first half,
+    the drifted position (32 B).  Neighbour lists are an implementation aid
+    and neighbour re-reads are cache traffic, so neither is counted."""
+    return nf * (96 + 4 + 64 + (32 if first else 0)) + nd * 128
+
+
+def native(args, rank, world, dist):
+    import torch
+
+    import this_studio_b200 as tsb
+    from this_studio_b200 import _lib
+    from this_studio_b200.scenes import build_sph
+
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sc = workload()
+    nf, nd = sc.fluid.shape[0], sc.dummy.shape[0]
+    solver = build_sph(sc, args.precision)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # warm-up
+    solver.step(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    launches0 = tsb.kernel_launches()
+    times = []
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.step(1)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = tsb.kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = float(sum(times))
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = nf * args.steps * world / (total_ms / 1e3)
+
+    # per-kernel live timing for the roofline (same stream, events per phase)
+    import ctypes as C
+
+    phases = (C.c_double * 5)()
+    nprof = min(args.steps, 20)
+    _lib.call("demsph_sph_profile_steps", solver._h, nprof, phases)
+    ph = list(phases)
+    mom_ms = 0.5 * (ph[2] + ph[4])
+    mom_bytes = 0.5 * (algorithmic_bytes_momentum(nf, nd, True) + algorithmic_bytes_momentum(nf, nd, False))
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = mom_bytes / (mom_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("k_sph_accel_bytes_per_launch")
+
+    # end to end through the public API: upload, K steps, read back
+    torch.cuda.synchronize()
+    h0 = time.perf_counter()
+    s2 = build_sph(sc, args.precision)
+    s2.step(args.steps)
+    out = s2.getSPH()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - h0
+    h2d = (nf + nd) * (3 * 8 * 2 + 4 * 8)  # positions, velocities, 4 scalars per particle
+    d2h = sum(v.nbytes for v in out.values()) + 16 * args.steps  # final state + per-step status word
+    del s2
+    e2e = nf * args.steps * world / e2e_s
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64",
+        "data": "synthetic (seeded lattice dam break, no dataset)",
+        "config": {"workload": WORKLOAD, "fluid_particles": nf, "dummy_particles": nd, "h": 1.3 * sc.spacing,
+                   "dt": sc.dt, "precision": args.precision, "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps,
+                "what": "build scene from host arrays, initialise, K steps, read state back"},
+        "roofline": {"bound": "hbm", "kernel": "k_sph_accel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": mom_bytes, "ms_per_launch": mom_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s"},
+        "phase_ms": {"cell_sort": ph[0], "reorder_lists": ph[1], "momentum_1": ph[2], "continuity_eos": ph[3],
+                     "momentum_2": ph[4]},
+    }
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline(sc)
+    return line
+
+
+def cpu_baseline(sc, steps=2):
+    """The FP64 C++ oracle (the reference's step restated; OpenMP) on the host
+    cores, a bounded sample of the same workload."""
+    from oracle import oracle
+
+    oracle.build()
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.OracleSPH()
+    o.add_sph(sc.fluid, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    o.add_dummy(sc.dummy, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    o.initialize(sc.minb, sc.maxb, sc.gravity, sc.dt)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": sc.fluid.shape[0] * steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the full {sc.fluid.shape[0]}-particle workload after 1 warm-up step"}
+
+
+def reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle
+
+    sc = workload()
+    oracle.build()
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.OracleSPH()
+    o.add_sph(sc.fluid, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    o.add_dummy(sc.dummy, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    o.initialize(sc.minb, sc.maxb, sc.gravity, sc.dt)
+    # each step of this arm is the full workload step; bound the sample so the
+    # run ends within minutes on a many-core host
+    steps = max(1, min(args.steps, 5))
+    warm = max(1, min(args.warmup, 1))
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    v = sc.fluid.shape[0] * steps / dt
+    return {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": world, "steps": steps,
+            "warmup": warm, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice dam break, no dataset)",
+            "config": {"workload": WORKLOAD, "fluid_particles": sc.fluid.shape[0],
+                       "dummy_particles": sc.dummy.shape[0]},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": f"{steps} full steps after {warm} warm-up step(s)"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            line = reference(args, rank, world)
+        else:
+            line = native(args, rank, world, dist)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -179,6 +179,13 @@ int demsph_sph_step(demsph_sph_t s, long numSteps);
 int demsph_sph_neighbor_search(demsph_sph_t s);
 int demsph_sph_eval_accel(demsph_sph_t s);
 
+/* Instrumentation (no counterpart in the reference, which has no timers):
+ * runs numSteps steps with a CUDA event after each phase on the scene stream
+ * and returns the mean milliseconds per step of the 5 phases: cell sort,
+ * reorder + neighbour lists, momentum + kick + drift, continuity + EOS,
+ * momentum + kick. */
+int demsph_sph_profile_steps(demsph_sph_t s, long numSteps, double* phaseMs);
+
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);
 int demsph_sph_step_index(demsph_sph_t s, long* step, double* time);

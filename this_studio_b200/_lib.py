@@ -72,6 +72,7 @@ SIGNATURES = {
     "demsph_sph_step": [_vp, _long],
     "demsph_sph_neighbor_search": [_vp],
     "demsph_sph_eval_accel": [_vp],
+    "demsph_sph_profile_steps": [_vp, _long, _d],
     "demsph_sph_num": [_vp, _int, _l],
     "demsph_sph_num_pairs": [_vp, _int, _l],
     "demsph_sph_step_index": [_vp, _l, _d],

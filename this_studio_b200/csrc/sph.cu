@@ -416,6 +416,43 @@ struct SphScene {
         accel(0);
     }
 
+    // One step with a CUDA event after every phase, on the scene stream:
+    // 0 cell sort, 1 permute + lists, 2 accel + kick + drift, 3 continuity + EOS,
+    // 4 accel + kick.  Adds each phase's milliseconds into ms[0..4].
+    void step_profiled(double* ms) {
+        cudaEvent_t ev[6];
+        for (auto& e : ev) DEMSPH_CUDA(cudaEventCreate(&e));
+        iStep++;
+        time += dt;
+        const int n = N();
+        DEMSPH_CUDA(cudaEventRecord(ev[0], s));
+        fCells.build(pos[P].p, n, s, id[ID].p);
+        g_launches += fCells.launches;
+        DEMSPH_CUDA(cudaEventRecord(ev[1], s));
+        k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
+                                                       drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
+                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p);
+        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        SphDev d = dev();
+        k_sph_lists<<<grid_for(n, 128), 128, 0, s>>>(d);
+        g_launches += 2;
+        haveLists = true;
+        DEMSPH_CUDA(cudaEventRecord(ev[2], s));
+        accel(1);
+        DEMSPH_CUDA(cudaEventRecord(ev[3], s));
+        density();
+        DEMSPH_CUDA(cudaEventRecord(ev[4], s));
+        accel(0);
+        DEMSPH_CUDA(cudaEventRecord(ev[5], s));
+        DEMSPH_CUDA(cudaEventSynchronize(ev[5]));
+        for (int k = 0; k < 5; k++) {
+            float t = 0;
+            DEMSPH_CUDA(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+            ms[k] += t;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+
     DevStatus read_status() {
         DevStatus h{};
         DEMSPH_CUDA(cudaMemcpyAsync(&h, status.p, sizeof h, cudaMemcpyDeviceToHost, s));
@@ -672,6 +709,19 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         g_launches += 1;
         DEMSPH_LAUNCH_CHECK();
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_sph_profile_steps(demsph_sph_t h, long n, double* phaseMs) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        for (int k = 0; k < 5; k++) phaseMs[k] = 0.0;
+        s.clear_status();
+        for (long k = 0; k < n; k++) s.step_profiled(phaseMs);
+        DevStatus st2 = s.read_status();
+        if (st2.overflow) throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists overflowed during profiling");
+        for (int k = 0; k < 5; k++) phaseMs[k] /= (double)(n > 0 ? n : 1);
     });
 }
 int demsph_sph_num(demsph_sph_t h, int dummy, long* n) {
