@@ -29,6 +29,8 @@
 #ifndef DEMSPH_H
 #define DEMSPH_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -197,6 +199,25 @@ int demsph_sph_set(demsph_sph_t s, const double* position, const double* velocit
 /* Pair lists in the reference's CSR order (countSPHInteractionsKernel and friends,
  * SPHNeighborSearchKernel.cu:6-228), indices in the caller's original order. */
 int demsph_sph_get_pairs(demsph_sph_t s, int which, int* objectPointed, int* objectPointing);
+
+/* ======================================================================= */
+/* Reference launcher compatibility                                          */
+/* ======================================================================= */
+/* The reference's sort / scan launchers with their exact signatures
+ * (DEMSPH/kernel/buildHashStartEnd.cuh:5-19; `struct CUstream_st*` is
+ * cudaStream_t).  They return void like the reference; a failure is
+ * recorded for demsph_last_error().  gridD / blockD are ignored.
+ *
+ * buildHashStartEnd: hashIndex[i] = i, stable sort of (hashValue, hashIndex)
+ * by hashValue in place (a hand-written LSD radix sort instead of
+ * thrust::sort_by_key), then start[h] / end[h] for every key 0 <= h <
+ * startEndSize that occurs (buildHashStartEnd.cu:6-83).  Scratch of about
+ * 3 * hashListSize ints is taken with cudaMallocAsync on the stream.
+ * buildPrefixSum: inclusive scan (buildHashStartEnd.cu:85-117), size <= 2^24. */
+void buildHashStartEnd(int* start, int* end, int* hashIndex, int* hashValue, const size_t startEndSize,
+                       const size_t hashListSize, const size_t gridD_GPU, const size_t blockD_GPU,
+                       struct CUstream_st* stream_GPU);
+void buildPrefixSum(int* prefixSum, int* count, const size_t size, struct CUstream_st* stream);
 
 #ifdef __cplusplus
 }

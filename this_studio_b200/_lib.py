@@ -79,11 +79,15 @@ SIGNATURES = {
     "demsph_sph_get": [_vp, _int, _d, _d, _d, _d, _d, _d, _d],
     "demsph_sph_set": [_vp, _d, _d, _d, _d, _d],
     "demsph_sph_get_pairs": [_vp, _int, _i, _i],
+    "buildHashStartEnd": [_vp, _vp, _vp, _vp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, _vp],
+    "buildPrefixSum": [_vp, _vp, C.c_size_t, _vp],
 }
 _RESTYPE = {
     "demsph_last_error": C.c_char_p,
     "demsph_version": C.c_char_p,
     "demsph_kernel_launches": C.c_longlong,
+    "buildHashStartEnd": None,
+    "buildPrefixSum": None,
 }
 
 _lib = None
