@@ -127,13 +127,11 @@ struct RadixScratch {
     int* scanOffs;    // tiles + 1
 };
 
-static inline int rx_tiles(int n) { return (n + kRxTile - 1) / kRxTile; }
+static constexpr inline int rx_tiles(int n) { return (n + kRxTile - 1) / kRxTile; }
 // Number of int-sized words of scratch a sort of n items needs.
-static inline size_t rx_scratch_words(int n) {
-    size_t t = (size_t)rx_tiles(n > 0 ? n : 1);
-    size_t h = 256 * t;
-    size_t st = (h + 4095) / 4096;
-    return 2 * (size_t)n + h + st + st + 1 + 64;
+static constexpr inline size_t rx_scratch_words(int n) {
+    return 2 * (size_t)n + 256 * (size_t)rx_tiles(n > 0 ? n : 1) +
+           2 * ((256 * (size_t)rx_tiles(n > 0 ? n : 1) + 4095) / 4096) + 1 + 64;
 }
 static inline RadixScratch rx_carve(int* base, int n) {
     RadixScratch s;
