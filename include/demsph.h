@@ -219,6 +219,23 @@ void buildHashStartEnd(int* start, int* end, int* hashIndex, int* hashValue, con
                        struct CUstream_st* stream_GPU);
 void buildPrefixSum(int* prefixSum, int* count, const size_t size, struct CUstream_st* stream);
 
+/* No counterpart in the reference.  The same sort and start / end table as
+ * buildHashStartEnd, for callers that cannot allocate device memory: a host
+ * loop that reserved its whole memory budget up front, or code issuing work
+ * where a cudaMalloc (which may synchronise the device, or fail under memory
+ * pressure) is not allowed.  It calls no allocator: its scratch is a fixed
+ * array inside the library, sized for DEMSPH_NOALLOC_MAX_KEYS keys (3.3 MB,
+ * held on every GPU that loads the library until the process exits).  The
+ * first call on a device looks up that array's device address; make that
+ * first call before any stream capture.  All calls share the one array, so
+ * calls that overlap on the GPU (other streams, other host threads) race;
+ * calls ordered on one stream are safe.  Returns DEMSPH_OK,
+ * DEMSPH_ERR_INVALID when hashListSize > DEMSPH_NOALLOC_MAX_KEYS (with a
+ * message in demsph_last_error), or DEMSPH_ERR_CUDA. */
+#define DEMSPH_NOALLOC_MAX_KEYS 262144
+int demsph_build_hash_start_end_noalloc(int* start, int* end, int* hashIndex, int* hashValue, size_t startEndSize,
+                                        size_t hashListSize, struct CUstream_st* stream);
+
 #ifdef __cplusplus
 }
 #endif

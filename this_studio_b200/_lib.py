@@ -81,6 +81,7 @@ SIGNATURES = {
     "demsph_sph_get_pairs": [_vp, _int, _i, _i],
     "buildHashStartEnd": [_vp, _vp, _vp, _vp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, _vp],
     "buildPrefixSum": [_vp, _vp, C.c_size_t, _vp],
+    "demsph_build_hash_start_end_noalloc": [_vp, _vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp],
 }
 _RESTYPE = {
     "demsph_last_error": C.c_char_p,

@@ -13,6 +13,8 @@
 // chosen here.  Like the reference these return void; a failure is recorded
 // for demsph_last_error().
 #include <atomic>
+#include <climits>
+#include <mutex>
 
 #include "radix.cuh"
 
@@ -44,7 +46,7 @@ static __global__ void k_hb_finish(const unsigned* __restrict__ keys, int n, int
 
 // Words of scratch buildHashStartEnd needs for n keys: the radix sort's plus
 // one key array.
-size_t hash_sort_scratch_words(int n) { return rx_scratch_words(n) + (size_t)n + 64; }
+static constexpr size_t hash_sort_scratch_words(int n) { return rx_scratch_words(n) + (size_t)n + 64; }
 
 // The sort behind buildHashStartEnd on caller-provided scratch (words from
 // hash_sort_scratch_words).
@@ -58,6 +60,33 @@ void hash_sort_start_end(int* start, int* end, int* hashIndex, int* hashValue, i
     k_hb_finish<<<grid_for(n, 256), 256, 0, s>>>(keys, n, startEndSize, hashValue, start, end);
     g_launches += launches;
     DEMSPH_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------ non-allocating variant --
+// Scratch for demsph_build_hash_start_end_noalloc: one fixed array in the
+// module image, sized for DEMSPH_NOALLOC_MAX_KEYS keys (3.3 MB).  Each GPU that
+// loads the library holds it until the process exits.  Every word a call
+// reads is written earlier in the same call (histograms, scan tiles and key
+// buffers are fully overwritten), so nothing needs clearing between calls;
+// calls that overlap on the GPU share it and race.
+static __device__ __align__(256) int g_hash_sort_scratch[hash_sort_scratch_words(DEMSPH_NOALLOC_MAX_KEYS)];
+
+// Device address of the array for the current device, looked up once per
+// device on the first call (host code cannot use the symbol itself).
+static int* noalloc_scratch() {
+    static std::mutex mu;
+    static int* ptr[64] = {};
+    int dev = 0;
+    DEMSPH_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Status(DEMSPH_ERR_INVALID, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_hash_sort_scratch);
+        if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress of the sort scratch array failed");
+        ptr[dev] = (int*)p;
+    }
+    return ptr[dev];
 }
 
 }  // namespace demsph
@@ -80,6 +109,20 @@ void buildHashStartEnd(int* start, int* end, int* hashIndex, int* hashValue, con
         DEMSPH_CUDA(cudaMallocAsync((void**)&scratch, hash_sort_scratch_words(n) * sizeof(int), stream_GPU));
         hash_sort_start_end(start, end, hashIndex, hashValue, (int)startEndSize, n, scratch, stream_GPU);
         DEMSPH_CUDA(cudaFreeAsync(scratch, stream_GPU));
+    });
+}
+
+int demsph_build_hash_start_end_noalloc(int* start, int* end, int* hashIndex, int* hashValue, size_t startEndSize,
+                                        size_t hashListSize, cudaStream_t stream) {
+    return guarded([&] {
+        if (hashListSize == 0) return;
+        if (hashListSize > (size_t)DEMSPH_NOALLOC_MAX_KEYS)
+            throw Status(DEMSPH_ERR_INVALID, "demsph_build_hash_start_end_noalloc: " + std::to_string(hashListSize) +
+                                                 " keys exceed the fixed scratch for " +
+                                                 std::to_string(DEMSPH_NOALLOC_MAX_KEYS) + " keys");
+        if (startEndSize > (size_t)INT_MAX) throw Status(DEMSPH_ERR_INVALID, "startEndSize exceeds the int32 range");
+        int* scratch = noalloc_scratch();
+        hash_sort_start_end(start, end, hashIndex, hashValue, (int)startEndSize, (int)hashListSize, scratch, stream);
     });
 }
 
