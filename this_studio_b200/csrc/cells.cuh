@@ -4,9 +4,9 @@
 //
 // The number of cells is known, so a histogram + exclusive scan + scatter
 // gives the sorted index list and every cell's [start, start+1) range in
-// O(N + C) with no comparison sort.  The scatter uses atomics, so a short
-// per-cell insertion sort restores the reference's stable (key, index) order
-// and makes the result deterministic.
+// O(N + C) with no comparison sort.  The scatter uses atomics, so a ranking
+// pass inside each cell restores the reference's stable (key, index) order and
+// makes the result deterministic.
 #pragma once
 #include "common.cuh"
 
@@ -83,34 +83,33 @@ static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const 
     sorted[slot] = i;
 }
 
-// Restores ascending order inside each cell, by orderKey[value] (or by the
-// value itself when orderKey is null): the stable order of the reference sort.
-static __global__ void k_cell_order(int ncell, const int* __restrict__ start, int* __restrict__ sorted,
-                             const int* __restrict__ orderKey) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
+// Restores ascending order inside each cell by orderKey[value] (by the value
+// itself when orderKey is null): the stable order of the reference sort.  One
+// thread per object counts the cell members that precede it, so a crowded
+// cell costs O(members) per thread instead of a serial insertion sort.
+static __global__ void k_cell_rank(int n, const int* __restrict__ key, const int* __restrict__ start,
+                                   const int* __restrict__ unordered, int* __restrict__ sorted,
+                                   const int* __restrict__ orderKey) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int v = unordered[s];
+    int c = key[v];
     int b = start[c], e = start[c + 1];
-    if (e - b < 2) return;
-    for (int i = b + 1; i < e; i++) {
-        int v = sorted[i];
-        int kv = orderKey ? orderKey[v] : v;
-        int j = i - 1;
-        while (j >= b) {
-            int u = sorted[j];
-            int ku = orderKey ? orderKey[u] : u;
-            if (ku <= kv) break;
-            sorted[j + 1] = u;
-            j--;
-        }
-        sorted[j + 1] = v;
+    int kv = orderKey ? orderKey[v] : v;
+    int r = 0;
+    for (int q = b; q < e; q++) {
+        int u = unordered[q];
+        int ku = orderKey ? orderKey[u] : u;
+        r += ku < kv;
     }
+    sorted[b + r] = v;
 }
 
 // Host side: owns the cell arrays of one grid and builds them on a stream.
 struct CellTable {
     GridDesc g{};
     int ncell = 0;
-    DBuf<int> key, cnt, start, sorted;
+    DBuf<int> key, cnt, start, sorted, unordered;
     std::vector<DBuf<int>*> scanTmp;  // per-level tile sums / offsets
     int launches = 0;                 // kernels issued by the last build
 
@@ -122,6 +121,7 @@ struct CellTable {
         ncell = g.ncell();
         key.alloc(nobj > 0 ? nobj : 1, s, false);
         sorted.alloc(nobj > 0 ? nobj : 1, s, false);
+        unordered.alloc(nobj > 0 ? nobj : 1, s, false);
         cnt.alloc(ncell, s, true);
         start.alloc((size_t)ncell + 1, s, true);
         for (auto* b : scanTmp) delete b;
@@ -163,8 +163,8 @@ struct CellTable {
         }
         scan(cnt.p, start.p, ncell, 0, s);
         if (n > 0) {
-            k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, sorted.p);
-            k_cell_order<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, start.p, sorted.p, orderKey);
+            k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, unordered.p);
+            k_cell_rank<<<grid_for(n, 256), 256, 0, s>>>(n, key.p, start.p, unordered.p, sorted.p, orderKey);
             launches += 2;
         }
         DEMSPH_LAUNCH_CHECK();

@@ -40,6 +40,9 @@ struct SphDev {
     const double4* dvel;
     const double4* dst;
     const double4* dnorm;
+    const float4* posf;   // fluid (x, y, z) - grid min and h, FP32, this step's order
+    const float4* dposf;  // dummies, same form
+    float eps;            // bound on |float coordinate - exact coordinate|
     int* nbF;
     int* cntF;
     int* nbD;
@@ -56,11 +59,50 @@ __device__ __forceinline__ R gradw_factor(R r, R h) {
     R q = r / h;
     R sigma = (R)21.0 / ((R)16.0 * (R)kPi * h * h * h);
     R t = (R)1.0 - (R)0.5 * q;
-    R t2 = t * t;
-    R t3 = t2 * t;
+    R t3 = t * t * t;
     R dq = -(R)2.0 * t3 * ((R)1.0 + (R)2.0 * q) + (R)2.0 * (t3 * t);
     R dWdr = sigma * dq / h;
     return dWdr / r;
+}
+
+// The same factor with the per-particle constants of h hoisted out of the
+// pair loop: invh = 1/h, sig = 21 / (16 pi h^3) and the pair's 1/r.  Only when
+// the neighbour's h differs from the particle's are they formed per pair.
+template <class R>
+struct HConst {
+    R h, invh, sig;
+};
+template <class R>
+__device__ __forceinline__ HConst<R> hconst(R h) {
+    return HConst<R>{h, (R)1.0 / h, (R)21.0 / ((R)16.0 * (R)kPi * h * h * h)};
+}
+template <class R>
+__device__ __forceinline__ R gradw_fast(R r, R inv_r, const HConst<R>& hi, R hj) {
+    HConst<R> k = hi;
+    if (hj != hi.h) k = hconst<R>((R)0.5 * (hi.h + hj));
+    if (r < (R)1.e-20 || r >= (R)2.0 * k.h) return (R)0;
+    R q = r * k.invh;
+    R t = (R)1.0 - (R)0.5 * q;
+    R t3 = t * t * t;
+    R dq = -(R)2.0 * t3 * ((R)1.0 + (R)2.0 * q) + (R)2.0 * (t3 * t);
+    return k.sig * dq * k.invh * inv_r;
+}
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+
+// Four lanes cooperate on one fluid particle: neighbour loops are split
+// across the lane quad and the partial sums are combined with shuffles, so a
+// 128-thread block holds 32 particles and four times as many gathers are in
+// flight per particle as with one thread each.
+constexpr int kQuad = 4;
+constexpr int kSphBlock = 128;
+constexpr int kSphPerBlock = kSphBlock / kQuad;
+__device__ __forceinline__ unsigned quad_mask() { return 0xFu << ((threadIdx.x & 31) & ~3u); }
+template <class T>
+__device__ __forceinline__ T quad_sum(T v, unsigned m) {
+    v += __shfl_xor_sync(m, v, 1);
+    v += __shfl_xor_sync(m, v, 2);
+    return v;
 }
 
 // Permutes the fluid into this step's cell order.
@@ -69,11 +111,13 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
                               const double* __restrict__ rho0, const double* __restrict__ drho,
                               const int* __restrict__ id, double4* __restrict__ pos2, double4* __restrict__ vel2,
                               double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
-                              int* __restrict__ id2) {
+                              int* __restrict__ id2, float4* __restrict__ posf, double3 origin) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     int o = sorted[t];
-    pos2[t] = pos[o];
+    double4 p = pos[o];
+    pos2[t] = p;
+    posf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
     vel2[t] = vel[o];
     st2[t] = st[o];
     rho02[t] = rho0[o];
@@ -82,52 +126,116 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
 }
 
 // countSPHInteractionsKernel / writeSPHInteractionsKernel and the dummy pair
-// (SPHNeighborSearchKernel.cu:6-228) in one pass per fluid particle:
-// j != i, |r_ij| <= 2 max(h_i, h_j); rows in the reference's stencil order.
-__global__ void __launch_bounds__(128) k_sph_lists(SphDev d) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    const double4 pi = d.pos[i];
+// kernels (SPHNeighborSearchKernel.cu:6-228) in one pass: j != i,
+// |r_ij| <= 2 max(h_i, h_j), rows in the reference's stencil order.
+// Built one warp per cell.  All particles of a cell share
+// the cell's 27-cell stencil (the reference clamps positions and cell indices
+// the same way for every particle of a cell), so the warp loads each stencil
+// row's candidates once, 32 at a time, into shared memory with coalesced
+// loads, and every lane tests them against its own particle in row order,
+// appending hits to its ELL row.  The rows come out in the reference's order.
+constexpr int kListWarps = 4;
+__device__ __forceinline__ void cell_collect(int ps, int pe, const Stencil& st, const GridDesc& g,
+                                             const int* __restrict__ cellStart, const double4* __restrict__ own,
+                                             const float4* __restrict__ ownf, const double4* __restrict__ other,
+                                             const float4* __restrict__ otherf, float eps, bool same, int K, int N,
+                                             int* __restrict__ nb, int* __restrict__ cnt, int* needMax, int* overflow,
+                                             float4* cand) {
+    const int lane = threadIdx.x & 31;
+    for (int g0 = ps; g0 < pe; g0 += 32) {
+        const int i = g0 + lane;
+        const bool mine = i < pe;
+        const float4 pf = mine ? ownf[i] : make_float4(0, 0, 0, 0);
+        int c = 0;
+        for_stencil_rows(st, g, cellStart, [&](int b, int e) {
+            for (int base = b; base < e; base += 32) {
+                __syncwarp();
+                if (base + lane < e) cand[lane] = otherf[base + lane];
+                __syncwarp();
+                const int m = min(32, e - base);
+                if (mine) {
+                    for (int t = 0; t < m; t++) {
+                        const int j = base + t;
+                        if (same && j == i) continue;
+                        const float4 q = cand[t];
+                        // FP32 distance on domain-relative coordinates.  Each
+                        // coordinate is within eps of exact, so d2 is within
+                        // band of the exact value; only candidates inside that
+                        // band need the reference's FP64 test.
+                        const float cut = 2.0f * fmaxf(pf.w, q.w);
+                        const float dx = pf.x - q.x, dy = pf.y - q.y, dz = pf.z - q.z;
+                        const float d2 = dx * dx + dy * dy + dz * dz;
+                        const float c2 = cut * cut;
+                        const float band = 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * c2;
+                        bool hit;
+                        if (d2 < c2 - band) hit = true;
+                        else if (d2 > c2 + band) hit = false;
+                        else {
+                            const double4 pi = own[i], pj = other[j];
+                            double cd = 2.0 * fmax(pi.w, pj.w);
+                            double3 r = xyz(pi) - xyz(pj);
+                            hit = (cd * cd - dot(r, r)) >= 0.;
+                        }
+                        if (hit) {
+                            if (c < K) nb[(size_t)c * N + i] = j;
+                            c++;
+                        }
+                    }
+                }
+            }
+        });
+        if (mine) {
+            if (c > K) {  // the passes walk this particle's stencil instead
+                atomicMax(needMax, c);
+                atomicExch(overflow, 1);
+                c = -1;
+            }
+            cnt[i] = c;
+        }
+    }
+}
+__global__ void __launch_bounds__(32 * kListWarps) k_sph_lists_cell(SphDev d, int ncell) {
+    __shared__ float4 cand[kListWarps][32];
+    const int w = threadIdx.x >> 5;
+    const int cell = blockIdx.x * kListWarps + w;
+    if (cell >= ncell) return;
+    const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
+    if (ps == pe) return;
+    // stencil of the cell: the one every particle of the cell computes
+    const double4 p0 = d.pos[ps];
+    Stencil st = stencil_of(xyz(p0), d.g);
+    cell_collect(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N, d.nbF, d.cntF,
+                 &d.status->need_pairs, &d.status->overflow, cand[w]);
+    if (d.ND > 0)
+        cell_collect(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false, d.KD, d.N, d.nbD,
+                     d.cntD, &d.status->need_aux, &d.status->overflow, cand[w]);
+    else if ((threadIdx.x & 31) == 0)
+        for (int i = ps; i < pe; i++) d.cntD[i] = 0;
+}
+
+// Calls f(j) for this lane's share of particle i's neighbours: from the ELL
+// row when it fitted (cnt >= 0), otherwise by walking the cell stencil with
+// the list's cutoff test (a row that overflowed its capacity).
+template <class F>
+__device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ nb, int N, int i, int self,
+                                               double4 pi, const GridDesc& g, const int* __restrict__ cellStart,
+                                               const double4* __restrict__ other, F&& f) {
+    const int sub = threadIdx.x & 3;
+    if (cnt >= 0) {
+        for (int k = sub; k < cnt; k += kQuad) f(nb[(size_t)k * N + i]);
+        return;
+    }
     const double3 ri = xyz(pi);
-    Stencil st = stencil_of(ri, d.g);
-    int c = 0;
-    for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
-        for (int j = b; j < e; j++) {
-            if (j == i) continue;
-            double4 pj = d.pos[j];
+    Stencil st = stencil_of(ri, g);
+    for_stencil_rows(st, g, cellStart, [&](int b, int e) {
+        for (int j = b + sub; j < e; j += kQuad) {
+            if (j == self) continue;
+            double4 pj = other[j];
             double cut = 2.0 * fmax(pi.w, pj.w);
             double3 r = ri - xyz(pj);
-            if ((cut * cut - dot(r, r)) >= 0.) {
-                if (c < d.KF) d.nbF[(size_t)c * d.N + i] = j;
-                c++;
-            }
+            if ((cut * cut - dot(r, r)) >= 0.) f(j);
         }
     });
-    if (c > d.KF) {
-        atomicMax(&d.status->need_pairs, c);
-        atomicExch(&d.status->overflow, 1);
-        c = d.KF;
-    }
-    d.cntF[i] = c;
-    if (d.ND == 0) { d.cntD[i] = 0; return; }
-    int cd = 0;
-    for_stencil_rows(st, d.g, d.dStart, [&](int b, int e) {
-        for (int j = b; j < e; j++) {
-            double4 pj = d.dpos[j];
-            double cut = 2.0 * fmax(pi.w, pj.w);
-            double3 r = ri - xyz(pj);
-            if ((cut * cut - dot(r, r)) >= 0.) {
-                if (cd < d.KD) d.nbD[(size_t)cd * d.N + i] = j;
-                cd++;
-            }
-        }
-    });
-    if (cd > d.KD) {
-        atomicMax(&d.status->need_aux, cd);
-        atomicExch(&d.status->overflow, 1);
-        cd = d.KD;
-    }
-    d.cntD[i] = cd;
 }
 
 // updateWCSPHAccelerationKernel (WCSPHIntegrationKernel.cu:42-148) fused with
@@ -136,44 +244,46 @@ __global__ void __launch_bounds__(128) k_sph_lists(SphDev d) {
 // arrays and writes the integrated particle into separate output arrays, so
 // no thread sees a neighbour's updated state.
 template <class R>
-__global__ void __launch_bounds__(128) k_sph_accel(SphDev d, double hdt, double dt, int first) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, double dt, int first) {
+    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
     const double3 ri = xyz(pi4);
     const double4 vi4 = d.vel[i];
     const VR vi = cvt<R>(xyz(vi4));
     const double4 s4 = d.st[i];
-    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, nui = (R)s4.w, hi = (R)pi4.w;
+    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, nui = (R)s4.w;
+    const HConst<R> hk = hconst<R>((R)pi4.w);
     VR acc = v3r<R>(0, 0, 0);
-    const int cf = d.cntF[i];
-    for (int k = 0; k < cf; k++) {
-        int j = d.nbF[(size_t)k * d.N + i];
+    quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         double4 pj4 = d.pos[j];
         double4 vj4 = d.vel[j];
         double4 sj = d.st[j];
         VR rij = cvt<R>(ri - xyz(pj4));
         VR vj = cvt<R>(xyz(vj4));
         R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, nuj = (R)sj.w, mj = (R)vj4.w;
-        R r = rlen(rij);
-        VR e = v3r<R>(0, 0, 0);
-        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R r2 = dot(rij, rij);
+        // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
+        // reference's normalize does (myVec.h:112-128)
+        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+        R r = r2 * inv_r;
+        VR e = rij * (-inv_r);
         R UL = dot(vi, e), UR = dot(vj, e);
-        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
-        VR dW = f * rij;
+        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
         R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        acc -= (R)2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
+        R inv_rr = (R)1.0 / (rhoi * rhoj);
+        acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
         R nuij = (R)0.5 * (nui + nuj);
         // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
-        acc += (R)2.0 * nuij * dot(-e, dW) * (vi - vj) * mj * ((R)1.0 / (rhoi * rhoj));
-    }
-    const int cd = d.cntD[i];
+        acc += (R)2.0 * nuij * dot(-e, dW) * (vi - vj) * mj * inv_rr;
+    });
     const VR g = cvt<R>(d.gravity);
-    for (int k = 0; k < cd; k++) {
-        int j = d.nbD[(size_t)k * d.N + i];
+    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         double4 pj4 = d.dpos[j];
         double4 vj4 = d.dvel[j];
         double4 sj = d.dst[j];
@@ -182,25 +292,29 @@ __global__ void __launch_bounds__(128) k_sph_accel(SphDev d, double hdt, double 
         R cj = (R)sj.x, nuj = (R)sj.y, rho0j = (R)sj.z, mj = (R)vj4.w;
         R UL = dot(-nw, vi);
         R UR = -UL + (R)2.0 * dot(-nw, vj);
-        VR rji = cvt<R>(xyz(pj4) - ri);
-        R grj = dot(g, rji);
+        VR rij = cvt<R>(ri - xyz(pj4));
+        R grj = -dot(g, rij);
         if (grj < (R)0.) grj = (R)0.;
         R PR = PL + rhoi * grj;
         R rhoj = PR / (cj * cj) + rho0j;
-        VR rij = cvt<R>(ri - xyz(pj4));
-        R r = rlen(rij);
-        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
-        VR dW = f * rij;
+        R r2 = dot(rij, rij);
+        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+        R r = r2 * inv_r;
+        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
         R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        acc -= (R)2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
+        R inv_rr = (R)1.0 / (rhoi * rhoj);
+        acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
         R nuij = (R)0.5 * (nui + nuj);
-        VR rh = v3r<R>(0, 0, 0);
-        if (r * r >= (R)1.0e-20) rh = rij * ((R)1.0 / r);
-        acc += (R)2.0 * nuij * dot(rh, dW) * (vi - vj) * mj * ((R)1.0 / (rhoi * rhoj));
-    }
-    double3 a = up(acc) + d.gravity;
+        acc += (R)2.0 * nuij * dot(rij * inv_r, dW) * (vi - vj) * mj * inv_rr;
+    });
+    double3 a = up(acc);
+    a.x = quad_sum(a.x, gm);
+    a.y = quad_sum(a.y, gm);
+    a.z = quad_sum(a.z, gm);
+    if (sub != 0) return;
+    a += d.gravity;
     d.acc[i] = d4(a, 0);
     double3 v = xyz(vi4) + hdt * a;
     d.velOut[i] = d4(v, vi4.w);
@@ -211,61 +325,61 @@ __global__ void __launch_bounds__(128) k_sph_accel(SphDev d, double hdt, double 
 // (WCSPHIntegrationKernel.cu:172-282): drho += dt * 2 rho_i sum m_j/rho_j
 // (v_i - v*) . gradW; clamp drho >= -0.1 rho0; rho = rho0 + drho; p = c^2 drho.
 template <class R>
-__global__ void __launch_bounds__(128) k_sph_density(SphDev d, double dt) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) {
+    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
     const double3 ri = xyz(pi4);
     const VR vi = cvt<R>(xyz(d.vel[i]));
     const double4 s4 = d.st[i];
-    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, hi = (R)pi4.w;
+    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z;
+    const HConst<R> hk = hconst<R>((R)pi4.w);
     R dRho = (R)0;
-    const int cf = d.cntF[i];
-    for (int k = 0; k < cf; k++) {
-        int j = d.nbF[(size_t)k * d.N + i];
+    quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         double4 pj4 = d.pos[j];
         double4 vj4 = d.vel[j];
         double4 sj = d.st[j];
         VR rij = cvt<R>(ri - xyz(pj4));
         VR vj = cvt<R>(xyz(vj4));
         R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, mj = (R)vj4.w;
-        R r = rlen(rij);
-        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
-        VR dW = f * rij;
-        VR e = v3r<R>(0, 0, 0);
-        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R r2 = dot(rij, rij);
+        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+        R r = r2 * inv_r;
+        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR e = rij * (-inv_r);
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         VR vs = (R)0.5 * (vi + vj);
         vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
         dRho += mj / rhoj * dot(vi - vs, dW);
-    }
-    const int cd = d.cntD[i];
+    });
     const VR g = cvt<R>(d.gravity);
-    for (int k = 0; k < cd; k++) {
-        int j = d.nbD[(size_t)k * d.N + i];
+    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         double4 pj4 = d.dpos[j];
         double4 vj4 = d.dvel[j];
         double4 sj = d.dst[j];
         VR vj = cvt<R>(xyz(vj4));
         R cj = (R)sj.x, rho0j = (R)sj.z, mj = (R)vj4.w;
-        VR rji = cvt<R>(xyz(pj4) - ri);
-        R grj = dot(g, rji);
+        VR rij = cvt<R>(ri - xyz(pj4));
+        R grj = -dot(g, rij);
         if (grj < (R)0.) grj = (R)0.;
         R PR = PL + rhoi * grj;
         R rhoj = PR / (cj * cj) + rho0j;
-        VR rij = cvt<R>(ri - xyz(pj4));
-        R r = rlen(rij);
-        R f = gradw_factor<R>(r, (R)0.5 * (hi + (R)pj4.w));
-        VR dW = f * rij;
-        VR e = v3r<R>(0, 0, 0);
-        if (r * r >= (R)1.0e-20) e = rij * (-(R)1.0 / r);
+        R r2 = dot(rij, rij);
+        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+        R r = r2 * inv_r;
+        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR e = rij * (-inv_r);
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         VR vs = (R)0.5 * (vi + vj);
         vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
         dRho += mj / rhoj * dot(vi - vs, dW);
-    }
-    double dr = (double)(dRho * ((R)2.0 * rhoi));
+    });
+    double dsum = quad_sum((double)dRho, gm);
+    if (sub != 0) return;
+    double dr = dsum * (2.0 * (double)rhoi);
     double ch = d.drho[i] + dr * dt;
     d.drho[i] = ch;
     double r0 = d.rho0[i];
@@ -332,6 +446,8 @@ struct SphScene {
     DBuf<double> rho0[2], drho[2];
     DBuf<int> id[2];
     DBuf<double4> acc;
+    DBuf<float4> posf, dposf;
+    float eps = 0;
     int P = 0, Vv = 0, S = 0, R0 = 0, D = 0, ID = 0;
     DBuf<double4> dpos, dvel, dst, dnorm;
     DBuf<double> drhoD;  // dummy densities (normals only)
@@ -353,6 +469,7 @@ struct SphScene {
         d.acc = acc.p;
         d.dpos = dpos.p; d.dvel = dvel.p; d.dst = dst.p; d.dnorm = dnorm.p;
         d.nbF = nbF.p; d.cntF = cntF.p; d.nbD = nbD.p; d.cntD = cntD.p;
+        d.posf = posf.p; d.dposf = dposf.p; d.eps = eps;
         d.gravity = gravity;
         d.status = status.p;
         return d;
@@ -374,10 +491,10 @@ struct SphScene {
         g_launches += fCells.launches;
         k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
                                                        drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
-                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p);
+                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p, fCells.g.mn);
         P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
         SphDev d = dev();
-        k_sph_lists<<<grid_for(n, 128), 128, 0, s>>>(d);
+        k_sph_lists_cell<<<grid_for(fCells.ncell, kListWarps), 32 * kListWarps, 0, s>>>(d, fCells.ncell);
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
@@ -388,9 +505,9 @@ struct SphScene {
         d.posOut = pos[P ^ 1].p;
         d.velOut = vel[Vv ^ 1].p;
         if (precision == DEMSPH_PRECISION_FP64)
-            k_sph_accel<double><<<grid_for(n, 128), 128, 0, s>>>(d, 0.5 * dt, dt, first);
+            k_sph_accel<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
         else
-            k_sph_accel<float><<<grid_for(n, 128), 128, 0, s>>>(d, 0.5 * dt, dt, first);
+            k_sph_accel<float><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
         g_launches += 1;
         DEMSPH_LAUNCH_CHECK();
         if (first) P ^= 1;
@@ -400,8 +517,8 @@ struct SphScene {
         SphDev d = dev();
         const int n = N();
         d.stOut = st[S ^ 1].p;
-        if (precision == DEMSPH_PRECISION_FP64) k_sph_density<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
-        else k_sph_density<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        if (precision == DEMSPH_PRECISION_FP64) k_sph_density<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
+        else k_sph_density<float><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
         g_launches += 1;
         DEMSPH_LAUNCH_CHECK();
         S ^= 1;
@@ -431,10 +548,10 @@ struct SphScene {
         DEMSPH_CUDA(cudaEventRecord(ev[1], s));
         k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
                                                        drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
-                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p);
+                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p, fCells.g.mn);
         P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
         SphDev d = dev();
-        k_sph_lists<<<grid_for(n, 128), 128, 0, s>>>(d);
+        k_sph_lists_cell<<<grid_for(fCells.ncell, kListWarps), 32 * kListWarps, 0, s>>>(d, fCells.ncell);
         g_launches += 2;
         haveLists = true;
         DEMSPH_CUDA(cudaEventRecord(ev[2], s));
@@ -495,20 +612,16 @@ struct SphScene {
             DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
         iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID;
     }
+    // Steps without a state snapshot: a list row that overflows its capacity
+    // is walked from the cell table by the passes (same neighbours), so an
+    // overflow never changes results; the lists are regrown for later calls.
     void run(long n) {
         if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         if (n <= 0) return;
-        for (int attempt = 0; attempt < 8; attempt++) {
-            Snap sn;
-            take(sn);
-            clear_status();
-            for (long k = 0; k < n; k++) step_once();
-            DevStatus st2 = read_status();
-            if (!st2.overflow) return;
-            grow(st2);
-            restore(sn);
-        }
-        throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists kept overflowing after regrowth");
+        clear_status();
+        for (long k = 0; k < n; k++) step_once();
+        DevStatus st2 = read_status();
+        if (st2.overflow) grow(st2);
     }
 
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
@@ -544,6 +657,14 @@ struct SphScene {
         DEMSPH_CUDA(cudaMemcpyAsync(drho[0].p, hf.drho.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
         DEMSPH_CUDA(cudaMemcpyAsync(id[0].p, ids.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
         acc.alloc(n, s, true);
+        posf.alloc(n, s, true);
+        // FP32 prefilter bound: coordinates are stored relative to the grid
+        // minimum; a float within |x| <= L has error <= L * 2^-24.  Positions
+        // outside the domain by up to a domain length are still covered.
+        {
+            double L = std::max(gd.mx.x - gd.mn.x, std::max(gd.mx.y - gd.mn.y, gd.mx.z - gd.mn.z));
+            eps = (float)(2.0 * L * std::ldexp(1.0, -24));
+        }
         // dummies: sort once into cell order (initializeBoundaryCondition, WCSPHSolver.h:29-110)
         if (nd > 0) {
             DBuf<double4> tp, tv, ts;
@@ -569,6 +690,11 @@ struct SphScene {
                 sp[t] = hd.pos[o]; sv[t] = hd.vel[o]; ss[t] = dst4[o]; sr[t] = rh[o];
             }
             dpos.upload(sp, s); dvel.upload(sv, s); dst.upload(ss, s); drhoD.upload(sr, s);
+            std::vector<float4> spf(nd);
+            for (int t = 0; t < nd; t++)
+                spf[t] = make_float4((float)(sp[t].x - gd.mn.x), (float)(sp[t].y - gd.mn.y), (float)(sp[t].z - gd.mn.z),
+                                     (float)sp[t].w);
+            dposf.upload(spf, s);
             did.upload(order, s);
             dnorm.alloc(nd, s, true);
             for (int attempt = 0; attempt < 8; attempt++) {
@@ -680,17 +806,16 @@ int demsph_sph_neighbor_search(demsph_sph_t h) {
         SPH_CHECK(h);
         SphScene& s = h->sc;
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
-        for (int attempt = 0; attempt < 8; attempt++) {
-            SphScene::Snap sn;
-            s.take(sn);
-            s.clear_status();
-            s.neighbor_search();
-            DevStatus st2 = s.read_status();
-            if (!st2.overflow) return;
+        s.clear_status();
+        s.neighbor_search();
+        DevStatus st2 = s.read_status();
+        if (st2.overflow) {  // rebuild with room so that the lists are complete
             s.grow(st2);
-            s.restore(sn);
+            SphDev d = s.dev();
+            k_sph_lists_cell<<<grid_for(s.fCells.ncell, kListWarps), 32 * kListWarps, 0, s.s>>>(d, s.fCells.ncell);
+            g_launches += 1;
+            DEMSPH_LAUNCH_CHECK();
         }
-        throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists overflow");
     });
 }
 int demsph_sph_eval_accel(demsph_sph_t h) {
@@ -703,9 +828,9 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         d.posOut = s.pos[s.P ^ 1].p;
         d.velOut = s.vel[s.Vv ^ 1].p;
         if (s.precision == DEMSPH_PRECISION_FP64)
-            k_sph_accel<double><<<grid_for(s.N(), 128), 128, 0, s.s>>>(d, 0.0, 0.0, 0);
+            k_sph_accel<double><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
         else
-            k_sph_accel<float><<<grid_for(s.N(), 128), 128, 0, s.s>>>(d, 0.0, 0.0, 0);
+            k_sph_accel<float><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
         g_launches += 1;
         DEMSPH_LAUNCH_CHECK();
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
@@ -835,7 +960,10 @@ int demsph_sph_num_pairs(demsph_sph_t h, int which, long* n) {
         }
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         long t = 0;
-        for (int c : cnt) t += c;
+        for (int c : cnt) {
+            if (c < 0) throw Status(DEMSPH_ERR_OVERFLOW, "a list row overflowed; call neighborSearch to rebuild");
+            t += c;
+        }
         *n = t;
     });
 }
@@ -865,6 +993,8 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
         // rows emitted in the caller's original order
         std::vector<int> rowOf(rows);
         for (int t = 0; t < rows; t++) rowOf[rowId[t]] = t;
+        for (int c : cnt)
+            if (c < 0) throw Status(DEMSPH_ERR_OVERFLOW, "a list row overflowed; call neighborSearch to rebuild");
         long w = 0;
         for (int o = 0; o < rows; o++) {
             int t = rowOf[o];
