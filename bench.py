@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     return ap.parse_args()
 
 
@@ -116,6 +116,48 @@ def algorithmic_bytes_momentum(nf, nd, first):
     return nf * (96 + 4 + 64 + (32 if first else 0)) + nd * 128
 
 
+def timed_steps(torch, solver, steps, flush):
+    """Per-step CUDA-event times (ms) with an L2 flush before each step, outside
+    the events."""
+    times = []
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.step(1)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def dem_bounce(torch, steps, warmup, flush):
+    """The plain DEM bounce of BASELINE config 1: 4,096 Hertz-Mindlin spheres
+    (r 5 mm, rho 2500, 16^3 lattice at 12 mm, +-0.5 mm seeded jitter) dropping
+    onto a 2-triangle plane, dt = 1e-5, mixed precision."""
+    from this_studio_b200 import scenes
+
+    sc = scenes.dem_drop()
+    s = scenes.build_dem(sc, "mixed")
+    s.step(max(warmup, 3))
+    block = 10  # steps per timed call; the call's overflow bookkeeping amortises over them
+    times = []
+    torch.cuda.synchronize()
+    for _ in range(max(1, steps // block)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.step(block)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(sum(times)) / (len(times) * block)
+    return {"workload": "dem_bounce_4096", "value": sc.position.shape[0] / (ms / 1e3), "unit": METRIC,
+            "ms_per_step": ms, "precision": "mixed", "steps": steps,
+            "note": "4,096 spheres; launch-bound at this size (see DESIGN.md)"}
+
+
 def native(args, rank, world, dist):
     import torch
 
@@ -137,16 +179,7 @@ def native(args, rank, world, dist):
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     launches0 = tsb.kernel_launches()
-    times = []
-    torch.cuda.synchronize()
-    for _ in range(args.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        solver.step(1)
-        e1.record()
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    times = timed_steps(torch, solver, args.steps, flush)
     torch.cuda.synchronize()
     launches = tsb.kernel_launches() - launches0
     clk = clocks.stop()
@@ -190,14 +223,27 @@ def native(args, rank, world, dist):
     del s2
     e2e = nf * args.steps * world / e2e_s
 
+    # the other precision and the DEM workload, for reference next to the headline
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    s3 = build_sph(sc, other)
+    s3.step(3)
+    t3 = timed_steps(torch, s3, min(args.steps, 100), flush)
+    del s3
+    other_value = nf / (float(sum(t3)) / len(t3) / 1e3)
+    dem = dem_bounce(torch, min(args.steps, 200), args.warmup, flush)
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": "synthetic (seeded lattice dam break, no dataset)",
         "config": {"workload": WORKLOAD, "fluid_particles": nf, "dummy_particles": nd, "h": 1.3 * sc.spacing,
-                   "dt": sc.dt, "precision": args.precision, "l2": "flushed (256 MB write) between timed steps",
-                   "parallelism": f"replicas x{world}"},
+                   "dt": sc.dt, "precision": args.precision,
+                   "precision_note": "FP32 force arithmetic, FP64 positions / velocities / density accumulation"
+                   if args.precision == "mixed" else "FP64 throughout (the reference's arithmetic)",
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+        "value_" + other: other_value,
+        "dem": dem,
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,

@@ -150,6 +150,21 @@ int demsph_dem_get_pairs(demsph_dem_t s, int which, int* objectPointed, int* obj
  * writeBallInteractionsKernel, ballNeighborSearchKernel.cu:130-143). */
 int demsph_dem_import_springs(demsph_dem_t s, long n, const int* objectPointed, const int* objectPointing,
                               const double* sliding, const double* rolling, const double* torsion);
+/* Same for the ball-triangle contact rows, keyed by (ball, triangle).  No
+ * counterpart in the reference: used to carry wall contact history when a
+ * scene's state moves between device scenes (batching). */
+int demsph_dem_import_wall_springs(demsph_dem_t s, long n, const int* ball, const int* triangle,
+                                   const double* sliding, const double* rolling, const double* torsion);
+/* No counterpart in the reference (batching).  Copies the state of balls
+ * carried over from scene src into scene dst on the device: for destination
+ * ball a with srcOf[a] >= 0, its position (plus shift[3a..3a+2]), velocity,
+ * angular velocity, its pair row with partner indices plus ballDelta[a], and
+ * its ball-triangle row with triangle indices plus triDelta[a].  Arrays have
+ * one entry per destination ball.  Partners must move with the ball (one
+ * batch member's balls keep their relative order), and dst must have been
+ * initialised with the same material / spring configuration. */
+int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf, const int* ballDelta,
+                            const int* triDelta, const double* shift);
 /* getBondedInteraction (DEMSolver.h:1547) fields */
 int demsph_dem_get_bonds(demsph_dem_t s, int* objectPointed, int* objectPointing, int* isBonded, double* normalForce,
                          double* torsionTorque, double* shearForce, double* bendingTorque, double* normal,
@@ -187,6 +202,14 @@ int demsph_sph_eval_accel(demsph_sph_t s);
  * reorder + neighbour lists, momentum + kick + drift, continuity + EOS,
  * momentum + kick. */
 int demsph_sph_profile_steps(demsph_sph_t s, long numSteps, double* phaseMs);
+
+/* No counterpart in the reference (batching).  Copies the fluid state of
+ * particles carried over from scene src into scene dst on the device: source
+ * particle i (caller index) goes to destination particle dstOf[i] (-1: not
+ * carried) with its position shifted by shift[3*dstOf[i]..]; velocity,
+ * density, pressure and density change are copied.  shift has one entry per
+ * destination particle; dst's neighbour lists are rebuilt at its next step. */
+int demsph_sph_copy_members(demsph_sph_t dst, demsph_sph_t src, const int* dstOf, const double* shift);
 
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);

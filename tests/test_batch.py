@@ -1,0 +1,106 @@
+"""Batched and served forms.
+
+CPU: tile packing.  GPU: a scene gives the same result alone and inside a
+batch whose membership changes while it runs (the batched form's contract),
+and the server completes a small stream with the results of each scene equal
+to running it alone."""
+import numpy as np
+import pytest
+
+from this_studio_b200 import batch, scenes, serve
+
+from .helpers import rel_err
+
+
+def test_tiles_do_not_overlap():
+    rng = np.random.default_rng(0)
+    boxes = []
+    for _ in range(40):
+        lo = rng.uniform(-1, 1, 3)
+        boxes.append((lo, lo + rng.uniform(0.1, 0.5, 3)))
+    gap = 0.05
+    offs = batch.tile_offsets(boxes, gap)
+    placed = [(np.asarray(lo) + o, np.asarray(hi) + o) for (lo, hi), o in zip(boxes, offs)]
+    for i in range(len(placed)):
+        for j in range(i + 1, len(placed)):
+            a, b = placed[i], placed[j]
+            sep = np.maximum(a[0] - b[1], b[0] - a[1])[:2].max()
+            assert sep >= gap - 1e-12
+    assert all(o[2] == 0 for o in offs)
+
+
+def test_stream_is_seeded():
+    a = serve.make_stream(20, seed=3)
+    b = serve.make_stream(20, seed=3)
+    assert [(r.kind, r.n, r.arrival) for r in a] == [(r.kind, r.n, r.arrival) for r in b]
+    assert all(1000 <= r.n <= 200_000 for r in a)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_dem_member_same_alone_and_in_mix(gpu, prec, tol):
+    x = scenes.dem_drop_poly(1500, seed=1)
+    others = [scenes.dem_drop_poly(n, seed=s) for n, s in ((800, 2), (2500, 3), (1200, 4))]
+    alone = scenes.build_dem(x, prec)
+    alone.step(100)
+    pa = alone.getBall()["position"]
+    b = batch.DEMBatch(prec)
+    b.members = [batch.Member(0, x), batch.Member(1, others[0]), batch.Member(2, others[1])]
+    b.rebuild()
+    b.step(45)
+    # membership changes at a multiple of 5 steps: one leaves, one arrives
+    b.capture()
+    keep = {m.key: m for m in b.members}
+    b.members = [keep[0], keep[2], batch.Member(3, others[2])]
+    b.rebuild()
+    b.step(55)
+    b.capture()
+    pm = b.members[0].state["position"]
+    assert b.members[0].steps_done == 100
+    e = rel_err(pm - x.position, pa - x.position)
+    print(f"{prec}: DEM displacement alone vs in the mix {e:.2e}")
+    assert e < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_sph_member_same_alone_and_in_mix(gpu, prec, tol):
+    c0, dt = serve.stream_params(20000)
+    x = scenes.sph_column(8000, c0, dt)
+    others = [scenes.sph_column(n, c0, dt) for n in (3000, 12000)]
+    alone = scenes.build_sph(x, prec)
+    alone.step(60)
+    pa = alone.getSPH()["position"]
+    b = batch.SPHBatch(prec)
+    b.members = [batch.Member(0, others[0]), batch.Member(1, x)]
+    b.rebuild()
+    b.step(25)
+    b.capture()
+    keep = {m.key: m for m in b.members}
+    b.members = [keep[1], batch.Member(2, others[1])]
+    b.rebuild()
+    b.step(35)
+    b.capture()
+    pm = b.members[0].state["position"]
+    e = rel_err(pm - x.fluid, pa - x.fluid)
+    print(f"{prec}: SPH displacement alone vs in the mix {e:.2e}")
+    assert e < tol
+
+
+@pytest.mark.gpu
+def test_server_completes_stream_and_matches_alone(gpu):
+    reqs = serve.make_stream(10, seed=11, n_min=1000, n_max=8000, rate=400.0, steps=60)
+    srv = serve.SceneServer(hbm_budget=2e9, chunk=20, precision="fp64", keep_states=True)
+    m = srv.run(reqs)
+    assert all(r.done is not None and r.final is not None for r in reqs)
+    assert m["scene_step_latency_p99_ms"] >= m["scene_step_latency_p50_ms"] > 0
+    c0, dt = srv.sph_c0, srv.sph_dt
+    for r in reqs[:4]:
+        sc = r.build(c0, dt)
+        s = scenes.build_dem(sc, "fp64") if r.kind == "dem" else scenes.build_sph(sc, "fp64")
+        s.step(r.steps)
+        ref = s.getBall()["position"] if r.kind == "dem" else s.getSPH()["position"]
+        base = sc.position if r.kind == "dem" else sc.fluid
+        e = rel_err(r.final["position"] - base, ref - base)
+        print(f"request {r.key} ({r.kind}, {r.np_} particles): served vs alone {e:.2e}")
+        assert e < 1e-9

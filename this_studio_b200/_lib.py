@@ -62,6 +62,8 @@ SIGNATURES = {
     "demsph_dem_set_balls": [_vp, _d, _d, _d],
     "demsph_dem_get_pairs": [_vp, _int, _i, _i, _d, _d, _d, _d, _d],
     "demsph_dem_import_springs": [_vp, _long, _i, _i, _d, _d, _d],
+    "demsph_dem_import_wall_springs": [_vp, _long, _i, _i, _d, _d, _d],
+    "demsph_dem_copy_members": [_vp, _vp, _i, _i, _i, _d],
     "demsph_dem_get_bonds": [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d],
     "demsph_dem_get_clumps": [_vp, _d, _d, _d, _d],
     "demsph_dem_get_walls": [_vp, _d, _d, _d],
@@ -73,6 +75,7 @@ SIGNATURES = {
     "demsph_sph_neighbor_search": [_vp],
     "demsph_sph_eval_accel": [_vp],
     "demsph_sph_profile_steps": [_vp, _long, _d],
+    "demsph_sph_copy_members": [_vp, _vp, _i, _d],
     "demsph_sph_num": [_vp, _int, _l],
     "demsph_sph_num_pairs": [_vp, _int, _l],
     "demsph_sph_step_index": [_vp, _l, _d],

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <unordered_map>
 
 #include "cells.cuh"
 #include "dem_physics.cuh"
@@ -618,6 +619,54 @@ __global__ void k_dem_circumcenters(DemDev d) {
     if (t >= d.nTri) return;
     int4 tv = d.tris[t];
     d.tcenter[t] = d4(circumcenter(xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]), xyz(d.vglobal[tv.z])), 0);
+}
+
+// ------------------------------------------------------------ batching ----
+// Copies the state of continuing batch members from another scene: ball
+// kinematics (translated), pair rows with partner indices shifted by the
+// member's index offset, and ball-triangle rows with triangle indices
+// shifted.  srcOf[a] is the source ball of destination ball a (-1: new ball,
+// keeps its freshly initialised state).
+struct CopyMap {
+    const int* srcOf;
+    const int* ballDelta;  // destination index - source index, per destination ball
+    const int* triDelta;
+    const double4* shift;  // per destination ball
+};
+__global__ void k_dem_copy_members(DemDev dst, DemDev src, CopyMap cm) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= dst.N) return;
+    int s = cm.srcOf[a];
+    if (s < 0) return;
+    double4 p = src.pos[s];
+    double4 sh = cm.shift[a];
+    dst.pos[a] = make_double4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
+    dst.vel[a] = src.vel[s];
+    dst.angv[a] = src.angv[s];
+    dst.force[a] = src.force[s];
+    dst.torque[a] = src.torque[s];
+    int bd = cm.ballDelta[a];
+    int c = src.pcnt[s];
+    for (int k = 0; k < c; k++) {
+        size_t so = (size_t)k * src.N + s, dO = (size_t)k * dst.N + a;
+        dst.pj[dO] = src.pj[so] + bd;
+        dst.spS[dO] = src.spS[so];
+        if (dst.roll) dst.spR[dO] = src.spR[so];
+        if (dst.tors) dst.spT[dO] = src.spT[so];
+    }
+    dst.pcnt[a] = c;
+    if (dst.nTri && src.nTri && src.wcnt) {
+        int td = cm.triDelta[a];
+        int cw = src.wcnt[s];
+        for (int k = 0; k < cw; k++) {
+            size_t so = (size_t)k * src.N + s, dO = (size_t)k * dst.N + a;
+            dst.wtj[dO] = src.wtj[so] + td;
+            dst.wS[dO] = src.wS[so];
+            if (dst.roll) dst.wR[dO] = src.wR[so];
+            if (dst.tors) dst.wT[dO] = src.wT[so];
+        }
+        dst.wcnt[a] = cw;
+    }
 }
 
 // ================================================================ host =====
@@ -1462,36 +1511,108 @@ int demsph_dem_get_pairs(demsph_dem_t h, int which, int* a, int* b, double* slid
         }
     });
 }
+// Sets the springs of the current rows (which = 0: ball-ball pair list,
+// 1: ball-triangle candidate rows) from a list keyed by (ball, partner).
+static void import_rows(DemScene& s, int which, long n, const int* a, const int* b, const double* sl, const double* ro,
+                        const double* to) {
+    if (which == 0 && !s.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "no pair list");
+    if (which == 1 && !s.haveWallRows) throw Status(DEMSPH_ERR_NOT_READY, "no wall contact rows");
+    std::unordered_map<long long, long> idx;
+    idx.reserve((size_t)n * 2 + 1);
+    for (long k = 0; k < n; k++) idx[((long long)a[k] << 32) | (unsigned)b[k]] = k;
+    int N = s.N();
+    int c = which == 0 ? s.cur : s.wcur;
+    DBuf<int>& CNT = which == 0 ? s.pcnt[c] : s.wcnt[c];
+    DBuf<int>& IDS = which == 0 ? s.pj[c] : s.wtj[c];
+    DBuf<double4>& BS = which == 0 ? s.spS[c] : s.wS[c];
+    DBuf<double4>& BR = which == 0 ? s.spR[c] : s.wR[c];
+    DBuf<double4>& BT = which == 0 ? s.spT[c] : s.wT[c];
+    std::vector<int> cnt, ids;
+    std::vector<double4> S, Rr, T;
+    CNT.download(cnt, s.s);
+    IDS.download(ids, s.s);
+    BS.download(S, s.s);
+    if (s.roll) BR.download(Rr, s.s);
+    if (s.tors) BT.download(T, s.s);
+    DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    for (int A = 0; A < N; A++)
+        for (int k = 0; k < cnt[A]; k++) {
+            size_t slot = (size_t)k * N + A;
+            auto it = idx.find(((long long)A << 32) | (unsigned)ids[slot]);
+            if (it == idx.end()) continue;
+            S[slot] = d4(ld3(sl, it->second), 0);
+            if (s.roll && ro) Rr[slot] = d4(ld3(ro, it->second), 0);
+            if (s.tors && to) T[slot] = d4(ld3(to, it->second), 0);
+        }
+    DEMSPH_CUDA(cudaMemcpyAsync(BS.p, S.data(), S.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+    if (s.roll) DEMSPH_CUDA(cudaMemcpyAsync(BR.p, Rr.data(), Rr.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+    if (s.tors) DEMSPH_CUDA(cudaMemcpyAsync(BT.p, T.data(), T.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+    DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+}
 int demsph_dem_import_springs(demsph_dem_t h, long n, const int* a, const int* b, const double* sl, const double* ro,
                               const double* to) {
     return guarded([&] {
         SCENE_CHECK(h);
-        DemScene& s = h->sc;
-        if (!s.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "no pair list");
-        std::map<std::pair<int, int>, long> idx;
-        for (long k = 0; k < n; k++) idx[{a[k], b[k]}] = k;
-        int N = s.N();
-        std::vector<int> cnt, ids;
-        std::vector<double4> S, Rr, T;
-        s.pcnt[s.cur].download(cnt, s.s);
-        s.pj[s.cur].download(ids, s.s);
-        s.spS[s.cur].download(S, s.s);
-        if (s.roll) s.spR[s.cur].download(Rr, s.s);
-        if (s.tors) s.spT[s.cur].download(T, s.s);
+        import_rows(h->sc, 0, n, a, b, sl, ro, to);
+    });
+}
+int demsph_dem_import_wall_springs(demsph_dem_t h, long n, const int* ball, const int* tri, const double* sl,
+                                   const double* ro, const double* to) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        import_rows(h->sc, 1, n, ball, tri, sl, ro, to);
+    });
+}
+int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf, const int* ballDelta,
+                            const int* triDelta, const double* shift) {
+    return guarded([&] {
+        SCENE_CHECK(dst);
+        SCENE_CHECK(src);
+        DemScene& d = dst->sc;
+        DemScene& s = src->sc;
+        if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
+        if (!s.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "source has no pair list");
+        if (d.roll != s.roll || d.tors != s.tors)
+            throw Status(DEMSPH_ERR_INVALID, "source and destination differ in rolling / torsion springs");
+        const int n = d.N();
+        // the rows keep their counts, so give the destination at least the source's capacities
+        d.grow(s.K, 0, s.haveWallRows ? s.KT : 0);
+        std::vector<double4> sh(n);
+        for (int a = 0; a < n; a++) sh[a] = make_double4(shift[3 * a], shift[3 * a + 1], shift[3 * a + 2], 0);
+        DBuf<int> so, bd, td;
+        DBuf<double4> shd;
+        so.upload(std::vector<int>(srcOf, srcOf + n), d.s);
+        bd.upload(std::vector<int>(ballDelta, ballDelta + n), d.s);
+        td.upload(std::vector<int>(triDelta, triDelta + n), d.s);
+        shd.upload(sh, d.s);
+        // the source's work must be finished before the destination reads it
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
-        for (int A = 0; A < N; A++)
-            for (int k = 0; k < cnt[A]; k++) {
-                size_t slot = (size_t)k * N + A;
-                auto it = idx.find({A, ids[slot]});
-                if (it == idx.end()) continue;
-                S[slot] = d4(ld3(sl, it->second), 0);
-                if (s.roll) Rr[slot] = d4(ld3(ro, it->second), 0);
-                if (s.tors) T[slot] = d4(ld3(to, it->second), 0);
-            }
-        DEMSPH_CUDA(cudaMemcpyAsync(s.spS[s.cur].p, S.data(), S.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
-        if (s.roll) DEMSPH_CUDA(cudaMemcpyAsync(s.spR[s.cur].p, Rr.data(), Rr.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
-        if (s.tors) DEMSPH_CUDA(cudaMemcpyAsync(s.spT[s.cur].p, T.data(), T.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
-        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        if (!d.havePairs) d.cur ^= 1;
+        DemDev dd = d.dev(false);
+        if (!d.haveWallRows || d.hTris.empty()) dd.nTri = 0;
+        DemDev sd = s.dev(false);
+        if (!s.haveWallRows) sd.wcnt = nullptr;
+        k_dem_copy_members<<<grid_for(n, 128), 128, 0, d.s>>>(dd, sd, CopyMap{so.p, bd.p, td.p, shd.p});
+        d.launch_count(1);
+        DEMSPH_LAUNCH_CHECK();
+        d.havePairs = true;
+        // reverse lists for the copied rows
+        DEMSPH_CUDA(cudaMemsetAsync(d.rcnt.p, 0, sizeof(int) * n, d.s));
+        d.clear_status();
+        DemDev dr = d.dev(false);
+        k_dem_reverse<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
+        k_dem_reverse_order<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
+        d.launch_count(2);
+        DevStatus st = d.read_status();
+        if (st.overflow) {
+            d.grow(0, st.need_rev, 0);
+            DEMSPH_CUDA(cudaMemsetAsync(d.rcnt.p, 0, sizeof(int) * n, d.s));
+            dr = d.dev(false);
+            k_dem_reverse<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
+            k_dem_reverse_order<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
+            d.launch_count(2);
+        }
+        DEMSPH_CUDA(cudaStreamSynchronize(d.s));
     });
 }
 int demsph_dem_get_bonds(demsph_dem_t h, int* a, int* b, int* ok, double* fn, double* tt, double* fs, double* tb,

@@ -146,6 +146,9 @@ __device__ __forceinline__ void cell_collect(int ps, int pe, const Stencil& st, 
         const int i = g0 + lane;
         const bool mine = i < pe;
         const float4 pf = mine ? ownf[i] : make_float4(0, 0, 0, 0);
+        const float cutOwn = 2.0f * pf.w, c2Own = cutOwn * cutOwn;
+        const float bandOwn = 4.0f * eps * (cutOwn + 2.0f * eps) * 1.7321f + 4.0e-6f * c2Own;
+        const float loOwn = c2Own - bandOwn, hiOwn = c2Own + bandOwn;
         int c = 0;
         for_stencil_rows(st, g, cellStart, [&](int b, int e) {
             for (int base = b; base < e; base += 32) {
@@ -161,15 +164,21 @@ __device__ __forceinline__ void cell_collect(int ps, int pe, const Stencil& st, 
                         // FP32 distance on domain-relative coordinates.  Each
                         // coordinate is within eps of exact, so d2 is within
                         // band of the exact value; only candidates inside that
-                        // band need the reference's FP64 test.
-                        const float cut = 2.0f * fmaxf(pf.w, q.w);
+                        // band need the reference's FP64 test.  The thresholds
+                        // of the particle's own h are hoisted out of the loop.
+                        float lo = loOwn, hi = hiOwn;
+                        if (q.w > pf.w) {
+                            const float cut = 2.0f * q.w;
+                            const float c2 = cut * cut;
+                            const float band = 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * c2;
+                            lo = c2 - band;
+                            hi = c2 + band;
+                        }
                         const float dx = pf.x - q.x, dy = pf.y - q.y, dz = pf.z - q.z;
                         const float d2 = dx * dx + dy * dy + dz * dz;
-                        const float c2 = cut * cut;
-                        const float band = 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * c2;
                         bool hit;
-                        if (d2 < c2 - band) hit = true;
-                        else if (d2 > c2 + band) hit = false;
+                        if (d2 < lo) hit = true;
+                        else if (d2 > hi) hit = false;
                         else {
                             const double4 pi = own[i], pj = other[j];
                             double cd = 2.0 * fmax(pi.w, pj.w);
@@ -222,6 +231,7 @@ __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ 
                                                const double4* __restrict__ other, F&& f) {
     const int sub = threadIdx.x & 3;
     if (cnt >= 0) {
+#pragma unroll 2
         for (int k = sub; k < cnt; k += kQuad) f(nb[(size_t)k * N + i]);
         return;
     }
@@ -423,6 +433,33 @@ __global__ void k_sph_dummy_normals(int nd, GridDesc g, const int* __restrict__ 
     }
     cnt[i] = c;
     dnorm[i] = (len2(th) > 1.e-10) ? d4(th / len(th), 0) : make_double4(0, 0, 0, 0);
+}
+
+// Copies continuing batch members' fluid state from another scene.  For the
+// source particle at sorted slot t with caller id i, dstOf[i] is its caller id
+// in the destination (-1: retired); dstSlot maps destination ids to their
+// current sorted slot.  Positions are translated by the member's shift.
+__global__ void k_sph_copy_members(int nsrc, const int* __restrict__ srcId, const double4* __restrict__ spos,
+                                   const double4* __restrict__ svel, const double4* __restrict__ sst,
+                                   const double* __restrict__ sdrho, const int* __restrict__ dstOf,
+                                   const int* __restrict__ dstSlot, const double4* __restrict__ shift,
+                                   double4* __restrict__ dpos, double4* __restrict__ dvel, double4* __restrict__ dst,
+                                   double* __restrict__ ddrho) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nsrc) return;
+    int nid = dstOf[srcId[t]];
+    if (nid < 0) return;
+    int u = dstSlot[nid];
+    double4 p = spos[t];
+    double4 sh = shift[nid];
+    dpos[u] = make_double4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
+    dvel[u] = svel[t];
+    dst[u] = sst[t];
+    ddrho[u] = sdrho[t];
+}
+__global__ void k_sph_slot_of(int n, const int* __restrict__ id, int* __restrict__ slot) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) slot[id[t]] = t;
 }
 
 // ================================================================ host =====
@@ -847,6 +884,32 @@ int demsph_sph_profile_steps(demsph_sph_t h, long n, double* phaseMs) {
         DevStatus st2 = s.read_status();
         if (st2.overflow) throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists overflowed during profiling");
         for (int k = 0; k < 5; k++) phaseMs[k] /= (double)(n > 0 ? n : 1);
+    });
+}
+int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, const int* dstOf, const double* shift) {
+    return guarded([&] {
+        SPH_CHECK(dsth);
+        SPH_CHECK(srch);
+        SphScene& d = dsth->sc;
+        SphScene& s = srch->sc;
+        if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
+        const int ns = s.N(), nd = d.N();
+        std::vector<double4> sh(nd);
+        for (int a = 0; a < nd; a++) sh[a] = make_double4(shift[3 * a], shift[3 * a + 1], shift[3 * a + 2], 0);
+        DBuf<int> dOf, slot;
+        DBuf<double4> shd;
+        dOf.upload(std::vector<int>(dstOf, dstOf + ns), d.s);
+        slot.alloc(nd, d.s, false);
+        shd.upload(sh, d.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        k_sph_slot_of<<<grid_for(nd, 256), 256, 0, d.s>>>(nd, d.id[d.ID].p, slot.p);
+        k_sph_copy_members<<<grid_for(ns, 256), 256, 0, d.s>>>(ns, s.id[s.ID].p, s.pos[s.P].p, s.vel[s.Vv].p,
+                                                              s.st[s.S].p, s.drho[s.D].p, dOf.p, slot.p, shd.p,
+                                                              d.pos[d.P].p, d.vel[d.Vv].p, d.st[d.S].p, d.drho[d.D].p);
+        g_launches += 2;
+        DEMSPH_LAUNCH_CHECK();
+        DEMSPH_CUDA(cudaStreamSynchronize(d.s));
+        d.haveLists = false;
     });
 }
 int demsph_sph_num(demsph_sph_t h, int dummy, long* n) {

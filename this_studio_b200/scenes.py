@@ -198,6 +198,58 @@ def sph_dam_break(nx=40, ny=40, nz=80, dx=0.01, tank=(1.6, 0.4, 1.0), layers=3, 
                     minb=tuple(lo), maxb=tuple(hi), dt=dt, steps=steps)
 
 
+def dem_drop_poly(n, seed, sigma=0.2, ratio=3.0, r0=0.005, density=2500.0, E=1e8, nu=0.3, restitution=0.8,
+                  mu=0.3, dt=1e-5):
+    """About n Hertz-Mindlin spheres with log-normal radii (sigma, max/min <=
+    ratio) on a jittered lattice dropped onto a 2-triangle plane: the DEM drop
+    of the scene stream."""
+    rng = np.random.default_rng(seed)
+    side = max(2, int(round(n ** (1.0 / 3.0))))
+    rmax = r0 * math.sqrt(ratio)
+    rad = np.exp(np.log(r0) + sigma * rng.standard_normal(side ** 3)).clip(r0 / math.sqrt(ratio), rmax)
+    sp = 2.4 * rmax
+    g = (np.arange(side) + 0.5) * sp
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    p += rng.uniform(-0.1 * rmax, 0.1 * rmax, size=p.shape)
+    Es, Gs = hertz_params(E, nu)
+    zmin = (p[:, 2] - rad).min() - 0.1 * rmax
+    L = side * sp
+    cell = 2 * rmax
+    lo = np.array([-2 * cell, -2 * cell, zmin - 2 * cell])
+    hi = np.array([L + 2 * cell, L + 2 * cell, (p[:, 2] + rad).max() + 2 * cell])
+    verts = np.array([[lo[0], lo[1], zmin], [hi[0], lo[1], zmin], [hi[0], hi[1], zmin], [lo[0], hi[1], zmin]])
+    k = p.shape[0]
+    return DEMScene(name="dem_drop_poly", position=p, radius=rad, density=np.full(k, density),
+                    material=np.zeros(k, np.int32), hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)],
+                    walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0),
+                                material=0)],
+                    minb=tuple(lo), maxb=tuple(hi), dt=dt)
+
+
+def sph_column(n, sound_speed, dt, dx=0.01, layers=3):
+    """A dam break with about n fluid particles: a nx x nx x 2nx column at the
+    left end of a tank four columns long and 1.25 columns high, three dummy
+    layers, open top (the dam break of the scene stream).  Sound speed and dt
+    are given so that scenes of one stream share them."""
+    nx = max(2, int(round((n / 2.0) ** (1.0 / 3.0))))
+    nz = 2 * nx
+    tank = (4 * nx * dx, nx * dx, 1.25 * nz * dx)
+    gx = (np.arange(nx) + 0.5) * dx
+    gz = (np.arange(nz) + 0.5) * dx
+    z, y, x = np.meshgrid(gz, gx, gx, indexing="ij")
+    fluid = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    tw = layers * dx
+    lo = np.array([0.0, 0, 0]) - tw
+    hi = np.array(tank, float) + tw
+    ax = [np.arange(-layers, int(round(t / dx)) + layers) * dx + 0.5 * dx for t in tank]
+    zz, yy, xx = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    d0 = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    keep = (d0[:, 0] < 0) | (d0[:, 1] < 0) | (d0[:, 2] < 0) | (d0[:, 0] > tank[0]) | (d0[:, 1] > tank[1])
+    return SPHScene(name="sph_column", fluid=fluid, dummy=d0[keep], spacing=dx, sound_speed=sound_speed,
+                    minb=tuple(lo), maxb=tuple(hi), dt=dt)
+
+
 # ---------------------------------------------------------------------------
 # Loading into the solvers
 # ---------------------------------------------------------------------------

@@ -235,6 +235,11 @@ class DEMSolver:
         call("demsph_dem_import_springs", self._h, a.shape[0], _ip(a), _ip(b), _dp(_f64(sliding, (-1, 3))),
              _dp(_f64(rolling, (-1, 3))), _dp(_f64(torsion, (-1, 3))))
 
+    def importWallSprings(self, ball, triangle, sliding, rolling, torsion):
+        a, b = _i32(ball), _i32(triangle)
+        call("demsph_dem_import_wall_springs", self._h, a.shape[0], _ip(a), _ip(b), _dp(_f64(sliding, (-1, 3))),
+             _dp(_f64(rolling, (-1, 3))), _dp(_f64(torsion, (-1, 3))))
+
     def getBondedInteraction(self):
         n = self._n("demsph_dem_num_bonds")
         out = {"objectPointed": np.zeros(n, np.int32), "objectPointing": np.zeros(n, np.int32),
