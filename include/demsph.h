@@ -57,6 +57,13 @@ const char* demsph_last_error(void);
 const char* demsph_version(void);
 /* Number of CUDA kernels this library has launched since load (instrumentation). */
 long long demsph_kernel_launches(void);
+/* No counterpart in the reference.  Scene buffers come from the current
+ * device's default stream-ordered memory pool; by default the pool hands
+ * freed memory back to the driver at every synchronisation.  This keeps up to
+ * `bytes` of freed memory in this process's pool instead, so a loop that
+ * destroys and re-creates scenes (the batched and served forms) reuses it
+ * without re-mapping.  Affects only this process. */
+int demsph_retain_device_memory(unsigned long long bytes);
 
 /* ======================================================================= */
 /* DEM: spheres, clumps, triangle-mesh walls, contact + parallel bonds      */

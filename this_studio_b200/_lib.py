@@ -36,6 +36,7 @@ SIGNATURES = {
     "demsph_last_error": [],
     "demsph_version": [],
     "demsph_kernel_launches": [],
+    "demsph_retain_device_memory": [C.c_ulonglong],
     "demsph_dem_create": [_pvp, _vp],
     "demsph_dem_destroy": [_vp],
     "demsph_dem_set_hertzian_pair": [_vp, _int, _int] + [_dbl] * 8,
@@ -130,3 +131,8 @@ def call(name, *args):
 
 def kernel_launches() -> int:
     return int(lib().demsph_kernel_launches())
+
+
+def retain_device_memory(nbytes: int) -> None:
+    """Keeps up to nbytes of freed scene memory in this process's pool."""
+    call("demsph_retain_device_memory", int(nbytes))

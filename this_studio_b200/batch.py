@@ -8,12 +8,18 @@ interacting pair, so a member evolves as it does alone, up to rounding of the
 translated coordinates, while all members share one set of kernel launches
 per step (one cell sort, one pair pass, one reduction, ...).
 
-Membership changes (admission, retirement) rebuild the device scene at a
-step boundary and carry each continuing member's state across: positions,
-velocities and angular velocities, ball-ball and ball-wall springs (DEM), and
-density / pressure / density change (SPH).  DEM members change only at steps
-that are multiples of 5, the reference's re-sort cadence (DEMSolver.h:1384),
-so the pair list is rebuilt on the same steps as when the member runs alone.
+Membership changes (admission, retirement) replace the device scene at a
+step boundary in two parts.  `prepare(members)` builds and initialises the
+next device scene from the members' initial scenes (or host states), on the
+batch's other stream, and can run while the current scene is stepping.
+`commit(prepared)` then copies the continuing members' state from the
+current device scene into the new one with a device kernel (no host round
+trip): positions (re-translated), velocities and angular velocities, their
+pair rows and ball-triangle rows with the springs (DEM), and density /
+pressure / density change (SPH).  DEM members change only at steps that are
+multiples of 5, the reference's re-sort cadence (DEMSolver.h:1384), and their
+pair rows are copied as they are, so each member uses exactly the pair list it
+would use alone.
 
 Members keep the reference's domain-edge behaviour only while their particles
 stay inside their own domain box: a particle that leaves it is clamped into
@@ -22,6 +28,7 @@ the edge cells of the batch domain rather than of its own.
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -35,8 +42,23 @@ class Member:
     scene: object
     offset: np.ndarray = None
     steps_done: int = 0
-    # carried state (member-local coordinates / indices)
+    # host copy of the state (member-local coordinates / indices), filled by
+    # capture(); a member with a host state and no device home starts from it
     state: dict = field(default_factory=dict)
+    home: object = None        # the device scene holding the member's live state
+    range: tuple = None        # its particle index range there
+    tri_range: tuple = None    # its triangle index range there (DEM)
+
+
+@dataclass
+class Prepared:
+    """A device scene built for a member list, not yet holding their state."""
+    solver: object
+    members: list
+    ranges: list
+    tri_ranges: list
+    offsets: list
+    stream: int
 
 
 def tile_offsets(boxes, gap):
@@ -58,31 +80,64 @@ def tile_offsets(boxes, gap):
     return offs
 
 
-class DEMBatch:
-    """DEM members of one time step and gravity stepped together."""
+class _Batch:
+    """Member bookkeeping shared by the DEM and WCSPH batches."""
 
-    def __init__(self, precision="mixed", stream=None):
+    def __init__(self, precision="mixed", stream=None, streams=None):
         self.precision = precision
-        self.stream = stream
+        # two streams: the next scene is prepared on the one the current scene
+        # does not use
+        self.streams = list(streams) if streams is not None else [stream, stream]
+        self.cur_stream = 0
         self.members: list[Member] = []
         self.solver = None
         self.ranges = []
+        self.tri_ranges = []
+        # seconds spent preparing device scenes (build + initialise) and in
+        # the state carry, and how many scenes were committed
+        self.timing = {"initialize_s": 0.0, "carry_s": 0.0, "rebuilds": 0}
+
+    def _carried(self, prep):
+        old = self.solver
+        return [(m, k) for k, m in enumerate(prep.members) if old is not None and m.home is old]
+
+    def rebuild(self):
+        """prepare + commit of the current member list."""
+        if not self.members:
+            self.solver = None
+            return
+        self.commit(self.prepare(self.members))
+
+    def step(self, n):
+        if self.solver is not None and n > 0:
+            self.solver.step(n)
+            for m in self.members:
+                m.steps_done += n
+
+    def clear(self):
+        self.solver = None
+        self.members = []
+
+
+class DEMBatch(_Batch):
+    """DEM members of one time step and gravity stepped together."""
 
     @staticmethod
     def cell_of(scene):
         return 2.0 * float(np.max(scene.radius))
 
-    def _materials(self):
+    @staticmethod
+    def _materials(members):
         """One material id per distinct material row set; members that share
         parameters share ids."""
         sig = {}
         ids = []
         rows_h, rows_l, rows_b = [], [], []
-        for m in self.members:
+        for m in members:
             key = (tuple(map(tuple, m.scene.hertz)), tuple(map(tuple, m.scene.linear)),
                    tuple(map(tuple, m.scene.bonded)))
             if key not in sig:
-                mats = sorted({int(v) for v in m.scene.material} |
+                mats = sorted({int(v) for v in np.unique(m.scene.material)} |
                               {int(w["material"]) for w in m.scene.walls} |
                               {int(r[i]) for r in m.scene.hertz + m.scene.linear + m.scene.bonded for i in (0, 1)})
                 base = sum(len(v[1]) for v in sig.values())
@@ -97,29 +152,31 @@ class DEMBatch:
             ids.append(sig[key][0])
         return ids, rows_h, rows_l, rows_b
 
-    def rebuild(self):
-        """(Re)creates the device scene from the members' current states."""
+    def prepare(self, members):
+        """Builds and initialises the device scene for `members`: each from
+        its host state if it has one and lives in no device scene, else from
+        its initial scene."""
         from .scenes import DEMScene
 
-        self.solver = None
-        if not self.members:
-            return
-        cell = max(self.cell_of(m.scene) for m in self.members)
-        boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in self.members]
+        tic = time.perf_counter()
+        for m in members:
+            sc = m.scene
+            assert not sc.clumps and not sc.bonded and not sc.bond_initial_contacts, \
+                "batched DEM members are balls and mesh walls"
+        cell = max(self.cell_of(m.scene) for m in members)
+        boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in members]
         offs = tile_offsets(boxes, gap=2.0 * cell)
-        remaps, rows_h, rows_l, rows_b = self._materials()
+        remaps, rows_h, rows_l, rows_b = self._materials(members)
         pos, vel, w, rad, den, mat, fixed = [], [], [], [], [], [], []
         walls = []
         lo = np.full(3, np.inf)
         hi = np.full(3, -np.inf)
-        self.ranges = []
-        self.tri_ranges = []
+        ranges, tri_ranges = [], []
         start = 0
         tstart = 0
-        for m, off, remap in zip(self.members, offs, remaps):
+        for m, off, remap in zip(members, offs, remaps):
             sc = m.scene
-            m.offset = off
-            st = m.state
+            st = m.state if m.home is None else {}
             n = sc.position.shape[0]
             pos.append((st["position"] if "position" in st else sc.position) + off)
             v0 = sc.velocity if sc.velocity is not None else np.zeros((n, 3))
@@ -129,7 +186,9 @@ class DEMBatch:
             w.append(st.get("angularVelocity", w0))
             rad.append(sc.radius)
             den.append(sc.density)
-            mat.append(np.array([remap[int(x)] for x in sc.material], np.int32))
+            lut = np.zeros(max(remap) + 1, np.int32)
+            lut[list(remap)] = list(remap.values())
+            mat.append(lut[np.asarray(sc.material, np.int64)])
             fixed.append(np.zeros(n, bool) if sc.fixed is None else sc.fixed)
             for wl in sc.walls:
                 d = dict(wl)
@@ -137,24 +196,27 @@ class DEMBatch:
                 d["material"] = remap[int(wl["material"])]
                 walls.append(d)
             nt = sum(len(wl["tri0"]) for wl in sc.walls)
-            self.ranges.append((start, start + n))
-            self.tri_ranges.append((tstart, tstart + nt))
+            ranges.append((start, start + n))
+            tri_ranges.append((tstart, tstart + nt))
             start += n
             tstart += nt
             lo = np.minimum(lo, np.asarray(sc.minb) + off)
             hi = np.maximum(hi, np.asarray(sc.maxb) + off)
-        first = self.members[0].scene
+        first = members[0].scene
         big = DEMScene(name="batch", position=np.concatenate(pos), radius=np.concatenate(rad),
                        density=np.concatenate(den), material=np.concatenate(mat),
                        velocity=np.concatenate(vel), fixed=np.concatenate(fixed), hertz=rows_h, linear=rows_l,
                        bonded=rows_b, walls=walls, minb=tuple(lo), maxb=tuple(hi), gravity=first.gravity,
                        dt=first.dt)
         big.angvel = np.concatenate(w)
-        self.solver = S.build_dem(big, self.precision, self.stream)
-        # contact history of continuing members, renumbered into the batch
+        si = 1 - self.cur_stream
+        new = S.build_dem(big, self.precision, self.streams[si])
+        # members entering from a host state: their springs, renumbered
         A, B, SL, RO, TO = [], [], [], [], []
         WA, WT, WS, WR, WTo = [], [], [], [], []
-        for m, (b0, _), (t0, _) in zip(self.members, self.ranges, self.tri_ranges):
+        for m, (b0, _), (t0, _) in zip(members, ranges, tri_ranges):
+            if m.home is not None:
+                continue
             st = m.state
             if "pairs" in st:
                 p = st["pairs"]
@@ -165,20 +227,54 @@ class DEMBatch:
                 WA.append(p["a"] + b0); WT.append(p["b"] + t0)
                 WS.append(p["sliding"]); WR.append(p["rolling"]); WTo.append(p["torsion"])
         if A:
-            self.solver.importSprings(np.concatenate(A), np.concatenate(B), np.concatenate(SL), np.concatenate(RO),
-                                      np.concatenate(TO))
+            new.importSprings(np.concatenate(A), np.concatenate(B), np.concatenate(SL), np.concatenate(RO),
+                              np.concatenate(TO))
         if WA:
-            self.solver.importWallSprings(np.concatenate(WA), np.concatenate(WT), np.concatenate(WS),
-                                          np.concatenate(WR), np.concatenate(WTo))
+            new.importWallSprings(np.concatenate(WA), np.concatenate(WT), np.concatenate(WS),
+                                  np.concatenate(WR), np.concatenate(WTo))
+        self.timing["initialize_s"] += time.perf_counter() - tic
+        return Prepared(new, list(members), ranges, tri_ranges, offs, si)
 
-    def capture(self):
-        """Copies every member's state out of the device scene."""
+    def commit(self, prep):
+        """Carries the continuing members' state from the current device
+        scene into the prepared one and makes it current."""
+        tic = time.perf_counter()
+        old = self.solver
+        carried = self._carried(prep)
+        if carried:
+            n = prep.ranges[-1][1]
+            srcOf = np.full(n, -1, np.int32)
+            bdel = np.zeros(n, np.int32)
+            tdel = np.zeros(n, np.int32)
+            shift = np.zeros((n, 3))
+            for m, k in carried:
+                b0, b1 = prep.ranges[k]
+                s0 = m.range[0]
+                srcOf[b0:b1] = np.arange(s0, s0 + (b1 - b0), dtype=np.int32)
+                bdel[b0:b1] = b0 - s0
+                tdel[b0:b1] = prep.tri_ranges[k][0] - m.tri_range[0]
+                shift[b0:b1] = prep.offsets[k] - m.offset
+            prep.solver.copyMembers(old, srcOf, bdel, tdel, shift)
+        for m, r, t, off in zip(prep.members, prep.ranges, prep.tri_ranges, prep.offsets):
+            m.home, m.range, m.tri_range, m.offset = prep.solver, r, t, off
+        self.members = prep.members
+        self.ranges, self.tri_ranges = prep.ranges, prep.tri_ranges
+        self.solver = prep.solver
+        self.cur_stream = prep.stream
+        self.timing["carry_s"] += time.perf_counter() - tic
+        self.timing["rebuilds"] += 1
+
+    def capture(self, keys=None):
+        """Copies the state of the members (or of those in `keys`) out of the
+        device scene into their host state."""
         if self.solver is None:
             return
         b = self.solver.getBall()
         pp = self.solver.getPairs(0)
         wp = self.solver.getPairs(1)
         for m, (b0, b1), (t0, t1) in zip(self.members, self.ranges, self.tri_ranges):
+            if keys is not None and m.key not in keys:
+                continue
             st = m.state
             st["position"] = b["position"][b0:b1] - m.offset
             st["velocity"] = b["velocity"][b0:b1]
@@ -192,83 +288,93 @@ class DEMBatch:
                                 "sliding": wp["sliding"][sel], "rolling": wp["rolling"][sel],
                                 "torsion": wp["torsion"][sel]}
 
-    def step(self, n):
-        if self.solver is not None and n > 0:
-            self.solver.step(n)
-            for m in self.members:
-                m.steps_done += n
-
     def num_particles(self):
         return sum(m.scene.num_moving for m in self.members)
 
 
-class SPHBatch:
+class SPHBatch(_Batch):
     """WCSPH members of one time step and gravity stepped together."""
 
-    def __init__(self, precision="mixed", stream=None):
-        self.precision = precision
-        self.stream = stream
-        self.members: list[Member] = []
-        self.solver = None
-        self.ranges = []
-
-    def rebuild(self):
+    def prepare(self, members):
+        """Builds and initialises the device scene for `members` (see
+        DEMBatch.prepare)."""
         from .solvers import WCSPHSolver
 
-        self.solver = None
-        if not self.members:
-            return
-        cell = max(2.0 * 1.3 * m.scene.spacing for m in self.members)
-        boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in self.members]
+        tic = time.perf_counter()
+        cell = max(2.0 * 1.3 * m.scene.spacing for m in members)
+        boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in members]
         offs = tile_offsets(boxes, gap=2.0 * cell)
-        s = WCSPHSolver(self.stream)
+        si = 1 - self.cur_stream
+        s = WCSPHSolver(self.streams[si])
         lo = np.full(3, np.inf)
         hi = np.full(3, -np.inf)
-        self.ranges = []
+        ranges = []
         start = 0
-        for m, off in zip(self.members, offs):
+        for m, off in zip(members, offs):
             sc = m.scene
-            m.offset = off
             n = sc.fluid.shape[0]
-            s.addSPHs(m.state.get("position", sc.fluid) + off, m.state.get("velocity"), sc.sound_speed, sc.spacing,
+            st = m.state if m.home is None else {}
+            s.addSPHs(st.get("position", sc.fluid) + off, st.get("velocity"), sc.sound_speed, sc.spacing,
                       sc.density, sc.viscosity)
-            self.ranges.append((start, start + n))
+            ranges.append((start, start + n))
             start += n
             lo = np.minimum(lo, np.asarray(sc.minb) + off)
             hi = np.maximum(hi, np.asarray(sc.maxb) + off)
-        for m, off in zip(self.members, offs):
+        for m, off in zip(members, offs):
             sc = m.scene
             s.addDummies(sc.dummy + off, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
-        first = self.members[0].scene
+        first = members[0].scene
         s.initialize(tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
-        if any("density" in m.state for m in self.members):
-            n = start
-            rho = np.empty(n)
-            p = np.empty(n)
-            dr = np.empty(n)
-            for m, (a, b) in zip(self.members, self.ranges):
-                rho[a:b] = m.state.get("density", np.full(b - a, m.scene.density))
-                p[a:b] = m.state.get("pressure", np.zeros(b - a))
-                dr[a:b] = m.state.get("densityChange", np.zeros(b - a))
+        hosted = [m.home is None and "density" in m.state for m in members]
+        if any(hosted):
+            rho = np.empty(start)
+            p = np.empty(start)
+            dr = np.empty(start)
+            for m, h, (a, b) in zip(members, hosted, ranges):
+                st = m.state if h else {}
+                rho[a:b] = st.get("density", np.full(b - a, m.scene.density))
+                p[a:b] = st.get("pressure", np.zeros(b - a))
+                dr[a:b] = st.get("densityChange", np.zeros(b - a))
             s.setSPH(density=rho, pressure=p, densityChange=dr)
-        self.solver = s
+        self.timing["initialize_s"] += time.perf_counter() - tic
+        return Prepared(s, list(members), ranges, [None] * len(members), offs, si)
 
-    def capture(self):
+    def commit(self, prep):
+        """Carries the continuing members' fluid state into the prepared
+        scene and makes it current."""
+        tic = time.perf_counter()
+        old = self.solver
+        carried = self._carried(prep)
+        if carried:
+            dstOf = np.full(old.num(), -1, np.int32)
+            shift = np.zeros((prep.ranges[-1][1], 3))
+            for m, k in carried:
+                a, b = prep.ranges[k]
+                s0 = m.range[0]
+                dstOf[s0:s0 + (b - a)] = np.arange(a, b, dtype=np.int32)
+                shift[a:b] = prep.offsets[k] - m.offset
+            prep.solver.copyMembers(old, dstOf, shift)
+        for m, r, off in zip(prep.members, prep.ranges, prep.offsets):
+            m.home, m.range, m.offset = prep.solver, r, off
+        self.members = prep.members
+        self.ranges = prep.ranges
+        self.solver = prep.solver
+        self.cur_stream = prep.stream
+        self.timing["carry_s"] += time.perf_counter() - tic
+        self.timing["rebuilds"] += 1
+
+    def capture(self, keys=None):
         if self.solver is None:
             return
         st = self.solver.getSPH()
         for m, (a, b) in zip(self.members, self.ranges):
+            if keys is not None and m.key not in keys:
+                continue
             m.state["position"] = st["position"][a:b] - m.offset
             m.state["velocity"] = st["velocity"][a:b]
             m.state["density"] = st["density"][a:b]
             m.state["pressure"] = st["pressure"][a:b]
             m.state["densityChange"] = st["densityChange"][a:b]
-
-    def step(self, n):
-        if self.solver is not None and n > 0:
-            self.solver.step(n)
-            for m in self.members:
-                m.steps_done += n
 
     def num_particles(self):
         return sum(m.scene.fluid.shape[0] for m in self.members)

@@ -249,6 +249,7 @@ struct DevStatus {
     int need_pairs;    // largest per-row count seen for the ball/fluid list
     int need_rev;      // largest reverse-list count
     int need_aux;      // largest per-row count for the secondary list
+    int bad_index;     // nonzero: a remapped index fell outside its array
 };
 
 }  // namespace demsph

@@ -647,25 +647,39 @@ __global__ void k_dem_copy_members(DemDev dst, DemDev src, CopyMap cm) {
     dst.torque[a] = src.torque[s];
     int bd = cm.ballDelta[a];
     int c = src.pcnt[s];
+    int kept = 0;
     for (int k = 0; k < c; k++) {
-        size_t so = (size_t)k * src.N + s, dO = (size_t)k * dst.N + a;
-        dst.pj[dO] = src.pj[so] + bd;
+        size_t so = (size_t)k * src.N + s, dO = (size_t)kept * dst.N + a;
+        int j = src.pj[so] + bd;
+        if (j < 0 || j >= dst.N) {  // a partner outside the batch: the maps were inconsistent
+            atomicExch(&dst.status->bad_index, 1);
+            continue;
+        }
+        dst.pj[dO] = j;
         dst.spS[dO] = src.spS[so];
         if (dst.roll) dst.spR[dO] = src.spR[so];
         if (dst.tors) dst.spT[dO] = src.spT[so];
+        kept++;
     }
-    dst.pcnt[a] = c;
+    dst.pcnt[a] = kept;
     if (dst.nTri && src.nTri && src.wcnt) {
         int td = cm.triDelta[a];
         int cw = src.wcnt[s];
+        kept = 0;
         for (int k = 0; k < cw; k++) {
-            size_t so = (size_t)k * src.N + s, dO = (size_t)k * dst.N + a;
-            dst.wtj[dO] = src.wtj[so] + td;
+            size_t so = (size_t)k * src.N + s, dO = (size_t)kept * dst.N + a;
+            int t = src.wtj[so] + td;
+            if (t < 0 || t >= dst.nTri) {
+                atomicExch(&dst.status->bad_index, 1);
+                continue;
+            }
+            dst.wtj[dO] = t;
             dst.wS[dO] = src.wS[so];
             if (dst.roll) dst.wR[dO] = src.wR[so];
             if (dst.tors) dst.wT[dO] = src.wT[so];
+            kept++;
         }
-        dst.wcnt[a] = cw;
+        dst.wcnt[a] = kept;
     }
 }
 
@@ -1571,10 +1585,12 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf
         DemScene& d = dst->sc;
         DemScene& s = src->sc;
         if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
-        if (!s.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "source has no pair list");
+        if (!s.havePairs || !d.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "scene has no pair list");
         if (d.roll != s.roll || d.tors != s.tors)
             throw Status(DEMSPH_ERR_INVALID, "source and destination differ in rolling / torsion springs");
         const int n = d.N();
+        for (int a = 0; a < n; a++)
+            if (srcOf[a] < -1 || srcOf[a] >= s.N()) throw Status(DEMSPH_ERR_INVALID, "source ball index out of range");
         // the rows keep their counts, so give the destination at least the source's capacities
         d.grow(s.K, 0, s.haveWallRows ? s.KT : 0);
         std::vector<double4> sh(n);
@@ -1587,7 +1603,7 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf
         shd.upload(sh, d.s);
         // the source's work must be finished before the destination reads it
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
-        if (!d.havePairs) d.cur ^= 1;
+        d.clear_status();
         DemDev dd = d.dev(false);
         if (!d.haveWallRows || d.hTris.empty()) dd.nTri = 0;
         DemDev sd = s.dev(false);
@@ -1595,10 +1611,10 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf
         k_dem_copy_members<<<grid_for(n, 128), 128, 0, d.s>>>(dd, sd, CopyMap{so.p, bd.p, td.p, shd.p});
         d.launch_count(1);
         DEMSPH_LAUNCH_CHECK();
-        d.havePairs = true;
+        DevStatus cs = d.read_status();
+        if (cs.bad_index) throw Status(DEMSPH_ERR_INVALID, "a carried pair partner or triangle left the batch");
         // reverse lists for the copied rows
         DEMSPH_CUDA(cudaMemsetAsync(d.rcnt.p, 0, sizeof(int) * n, d.s));
-        d.clear_status();
         DemDev dr = d.dev(false);
         k_dem_reverse<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
         k_dem_reverse_order<<<grid_for(n, 256), 256, 0, d.s>>>(dr);

@@ -894,6 +894,15 @@ int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, const int* dst
         SphScene& s = srch->sc;
         if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
         const int ns = s.N(), nd = d.N();
+        std::vector<char> hit(nd, 0);
+        for (int i = 0; i < ns; i++) {
+            int t = dstOf[i];
+            if (t < -1 || t >= nd) throw Status(DEMSPH_ERR_INVALID, "destination particle index out of range");
+            if (t >= 0) {
+                if (hit[t]) throw Status(DEMSPH_ERR_INVALID, "two source particles map to one destination");
+                hit[t] = 1;
+            }
+        }
         std::vector<double4> sh(nd);
         for (int a = 0; a < nd; a++) sh[a] = make_double4(shift[3 * a], shift[3 * a + 1], shift[3 * a + 2], 0);
         DBuf<int> dOf, slot;

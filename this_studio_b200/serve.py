@@ -2,12 +2,13 @@
 run, by HBM budget, into the batched form (this_studio_b200/batch.py).
 
 Requests arrive over time (a seeded Poisson stream of DEM drops and WCSPH
-dam breaks of uneven size).  The server keeps one DEM batch and one WCSPH
-batch resident on the GPU, each on its own CUDA stream and host thread so the
-two overlap on the device.  Every chunk of steps (a multiple of 5 for DEM, the
-re-sort cadence) it retires finished members, admits waiting requests whose
-memory estimate fits the budget, and rebuilds the batch with the continuing
-members' state carried over.  Reported: aggregate particle-steps/s, p50 / p99
+dam breaks of uneven size); each carries its scene, generated before the
+clock starts, as a client would send it.  The server keeps one DEM batch and
+one WCSPH batch resident on the GPU, each on its own CUDA stream and host
+thread so the two overlap on the device.  Every chunk of steps (a multiple of
+5 for DEM, the re-sort cadence) a kind's worker retires finished members,
+admits waiting requests whose memory estimate fits the budget, and rebuilds
+its batch with the continuing members' state carried over on the device.  Reported: aggregate particle-steps/s, p50 / p99
 of scene latency (arrival to completion) and of scene-step latency (wall time
 of the chunk a scene-step ran in, divided by the chunk's steps), and admission
 waits.
@@ -104,99 +105,156 @@ class SceneServer:
         self.max_members = max_members
         self.keep_states = keep_states
         self.sph_c0, self.sph_dt = sph_c0, sph_dt
-        self.streams = {"dem": torch.cuda.Stream(), "sph": torch.cuda.Stream()}
-        self.batches = {"dem": DEMBatch(precision, self.streams["dem"]),
-                        "sph": SPHBatch(precision, self.streams["sph"])}
+        from . import _lib
+
+        # batches are re-created at membership changes: keep their memory pooled
+        _lib.retain_device_memory(int(2 * hbm_budget))
+        # two streams per kind: the next batch scene is prepared on one while
+        # the current scene steps on the other
+        self.streams = {k: [torch.cuda.Stream(), torch.cuda.Stream()] for k in ("dem", "sph")}
+        self.batches = {"dem": DEMBatch(precision, streams=self.streams["dem"]),
+                        "sph": SPHBatch(precision, streams=self.streams["sph"])}
 
     def run(self, requests, log=None):
+        """Serves the requests to completion; returns the stream's metrics.
+
+        One worker thread per kind owns that kind's batch.  Before each chunk
+        a worker retires the members that finished, commits the batch scene
+        prepared during the previous chunk (carrying the continuing members'
+        state on the device), and plans the membership after the coming
+        chunk: the members that will still be running plus arrived requests
+        of its kind (arrival order, first fit against the shared HBM budget).
+        If that differs from the current membership, the next batch scene is
+        built and initialised on a helper thread and the batch's other stream
+        while the chunk runs, so scene set-up overlaps the steps.  The
+        prepared and the running scene coexist, so the device holds up to
+        twice the budget at a boundary."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         if self.sph_c0 is None:
             self.sph_c0, self.sph_dt = stream_params(max(r.n for r in reqs))
-        waiting = list(reqs)
+        for r in reqs:
+            r.build(self.sph_c0, self.sph_dt)
+            r.np_ = r.particles()
+        by_key = {r.key: r for r in reqs}
+        lock = threading.Lock()
+        waiting = {"dem": [r for r in reqs if r.kind == "dem"], "sph": [r for r in reqs if r.kind == "sph"]}
         active = {"dem": {}, "sph": {}}
-        used = 0.0
+        used = [0.0]
+        stats = {k: {"busy": 0.0, "chunks": 0, "rebuild": 0.0} for k in ("dem", "sph")}
+        errors = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
-        busy = 0.0
-        chunks = 0
-        rebuild_s = 0.0
-        retired = {"dem": {}, "sph": {}}
-        while waiting or active["dem"] or active["sph"]:
-            t = now()
-            # retire
-            for kind in ("dem", "sph"):
-                b = self.batches[kind]
-                for m in b.members:
-                    if m.key in active[kind] and m.steps_done >= active[kind][m.key].steps:
-                        r = active[kind].pop(m.key)
-                        r.done = t
-                        used -= r.bytes()
-                        r.scene = None
-                        retired[kind][m.key] = r
-            # admit (arrival order, first fit by budget)
-            changed = {"dem": False, "sph": False}
-            keep = []
-            for r in waiting:
-                if r.arrival <= t and len(active[r.kind]) < self.max_members:
-                    r.build(self.sph_c0, self.sph_dt)
-                    r.np_ = r.particles()
-                    if used + r.bytes() <= self.budget or not (active["dem"] or active["sph"]):
-                        used += r.bytes()
-                        r.admitted = t
-                        active[r.kind][r.key] = r
-                        changed[r.kind] = True
-                        continue
-                keep.append(r)
-            waiting = keep
-            # rebuild batches whose membership changed, carrying state
-            tr = time.perf_counter()
-            for kind in ("dem", "sph"):
-                b = self.batches[kind]
-                cur = {m.key for m in b.members}
-                want = set(active[kind])
-                if cur != want or changed[kind]:
-                    b.capture()
-                    old = {m.key: m for m in b.members}
-                    for k in cur - want:
+
+        def worker(kind):
+            b = self.batches[kind]
+            st = stats[kind]
+            act = active[kind]
+            prep = None      # (Prepared or None for "no members", newly admitted requests)
+            try:
+                while True:
+                    # retire members that completed their steps
+                    t = now()
+                    gone = [m.key for m in b.members if m.steps_done >= by_key[m.key].steps]
+                    if gone:
                         if self.keep_states:
-                            retired[kind][k].final = old[k].state
-                        retired[kind].pop(k, None)
-                    b.members = [old[k] if k in old else Member(key=k, scene=active[kind][k].scene)
-                                 for k in sorted(want)]
-                    b.rebuild()
-            rebuild_s += time.perf_counter() - tr
-            if not (active["dem"] or active["sph"]):
-                if waiting:  # idle until the next arrival
-                    time.sleep(max(0.0, min(0.05, waiting[0].arrival - now())))
-                continue
-            # one chunk on both batches at once (separate streams and threads)
-            c0 = time.perf_counter()
-            lat = {}
+                            b.capture(keys=set(gone))
+                        with lock:
+                            for k in gone:
+                                r = by_key[k]
+                                r.done = t
+                                used[0] -= r.bytes()
+                                del act[k]
+                        for m in b.members:
+                            if m.key in gone:
+                                by_key[m.key].final = m.state if self.keep_states else None
+                                by_key[m.key].scene = None
+                    # commit the scene prepared during the last chunk
+                    if prep is not None:
+                        tr = time.perf_counter()
+                        pr, adm = prep
+                        prep = None
+                        if pr is None:
+                            b.clear()
+                        else:
+                            b.commit(pr)
+                        st["rebuild"] += time.perf_counter() - tr
+                        for r in adm:
+                            r.admitted = now()
+                    # plan the membership after the coming chunk
+                    with lock:
+                        surv = [m for m in b.members if m.steps_done + self.chunk < by_key[m.key].steps]
+                        adm, keep = [], []
+                        for r in waiting[kind]:
+                            if r.arrival <= t and len(surv) + len(adm) < self.max_members and (
+                                    used[0] + r.bytes() <= self.budget or not (active["dem"] or active["sph"])):
+                                used[0] += r.bytes()
+                                act[r.key] = r
+                                adm.append(r)
+                            else:
+                                keep.append(r)
+                        waiting[kind] = keep
+                        pending = list(keep)
+                    nxt = surv + [Member(key=r.key, scene=r.scene) for r in adm]
+                    if not b.members:
+                        if nxt:  # nothing running: set up now
+                            tr = time.perf_counter()
+                            b.commit(b.prepare(nxt))
+                            st["rebuild"] += time.perf_counter() - tr
+                            for r in adm:
+                                r.admitted = now()
+                            continue
+                        if not pending:
+                            return
+                        time.sleep(max(0.0, min(0.02, pending[0].arrival - now())))
+                        continue
+                    helper = None
+                    out = []
+                    if adm or len(surv) != len(b.members):
+                        if nxt:
+                            def build(ms=nxt):
+                                try:
+                                    out.append(b.prepare(ms))
+                                except BaseException as e:
+                                    out.append(e)
 
-            def run(kind):
-                b = self.batches[kind]
-                if b.members:
-                    s = time.perf_counter()
+                            helper = threading.Thread(target=build)
+                            helper.start()
+                        else:
+                            prep = (None, [])
+                    c = time.perf_counter()
                     b.step(self.chunk)
-                    lat[kind] = (time.perf_counter() - s) / self.chunk
+                    lat = (time.perf_counter() - c) / self.chunk
+                    st["busy"] += time.perf_counter() - c
+                    st["chunks"] += 1
+                    for m in b.members:
+                        by_key[m.key].step_lat.append(lat)
+                    if helper is not None:
+                        helper.join()
+                        if isinstance(out[0], BaseException):
+                            raise out[0]
+                        prep = (out[0], adm)
+                    if log:
+                        log(f"t={now():.2f}s {kind}: members={len(b.members)} next={len(nxt)} "
+                            f"waiting={len(pending)} lat={lat * 1e3:.3f} ms")
+            except BaseException as e:  # surfaced on the calling thread
+                errors.append(e)
 
-            th = [threading.Thread(target=run, args=(k,)) for k in ("dem", "sph")]
-            for x in th:
-                x.start()
-            for x in th:
-                x.join()
-            busy += time.perf_counter() - c0
-            chunks += 1
-            for kind, l in lat.items():
-                for r in active[kind].values():
-                    r.step_lat.append(l)
-            if log:
-                log(f"t={now():.2f}s active dem={len(active['dem'])} sph={len(active['sph'])} "
-                    f"waiting={len(waiting)} lat={lat}")
+        th = [threading.Thread(target=worker, args=(k,)) for k in ("dem", "sph")]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        if errors:
+            raise errors[0]
         makespan = now()
         for b in self.batches.values():
-            b.solver = None
-        return self._metrics(reqs, makespan, busy, chunks, rebuild_s)
+            b.clear()
+        busy = max(stats[k]["busy"] for k in stats)
+        m = self._metrics(reqs, makespan, busy, sum(stats[k]["chunks"] for k in stats),
+                          sum(stats[k]["rebuild"] for k in stats))
+        m["per_kind"] = {k: {"busy_s": stats[k]["busy"], "chunks": stats[k]["chunks"],
+                             "commit_s": stats[k]["rebuild"], **self.batches[k].timing} for k in stats}
+        return m
 
     def _metrics(self, reqs, makespan, busy, chunks, rebuild_s):
         ps = sum(r.np_ * r.steps for r in reqs)
@@ -224,14 +282,19 @@ def particle_steps(requests, sph_c0, sph_dt):
 
 
 def run_plain(requests, precision="mixed", sph_c0=None, sph_dt=None):
-    """Every request alone on the plain solver, one after another."""
+    """Every request alone on the plain solver, one after another.  Scenes
+    are generated before the clock starts, as for the server; the time covers
+    building each device scene (upload, initialisation) and its steps."""
     import torch
 
     if sph_c0 is None:
         sph_c0, sph_dt = stream_params(max(r.n for r in requests))
+    for r in requests:
+        r.build(sph_c0, sph_dt)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in requests:
-        sc = r.build(sph_c0, sph_dt)
+        sc = r.scene
         s = scenes.build_dem(sc, precision) if r.kind == "dem" else scenes.build_sph(sc, precision)
         s.step(r.steps)
         del s

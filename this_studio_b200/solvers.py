@@ -240,6 +240,14 @@ class DEMSolver:
         call("demsph_dem_import_wall_springs", self._h, a.shape[0], _ip(a), _ip(b), _dp(_f64(sliding, (-1, 3))),
              _dp(_f64(rolling, (-1, 3))), _dp(_f64(torsion, (-1, 3))))
 
+    def copyMembers(self, source, srcOf, ballDelta, triDelta, shift):
+        """Device-side carry of continuing batch members from `source` (a
+        DEMSolver): per destination ball, its source ball (-1: keep), the index
+        shifts of its pair partners and wall triangles, and its translation."""
+        n = self.numBalls
+        call("demsph_dem_copy_members", self._h, source._h, _ip(_i32(srcOf)), _ip(_i32(ballDelta)),
+             _ip(_i32(triDelta)), _dp(_f64(shift, (n, 3))))
+
     def getBondedInteraction(self):
         n = self._n("demsph_dem_num_bonds")
         out = {"objectPointed": np.zeros(n, np.int32), "objectPointing": np.zeros(n, np.int32),
@@ -354,6 +362,12 @@ class WCSPHSolver:
         f = lambda x, s: None if x is None else _f64(x, s)
         call("demsph_sph_set", self._h, _dp(f(position, (n, 3))), _dp(f(velocity, (n, 3))), _dp(f(density, (n,))),
              _dp(f(pressure, (n,))), _dp(f(densityChange, (n,))))
+
+    def copyMembers(self, source, dstOf, shift):
+        """Device-side carry of fluid state from `source` (a WCSPHSolver):
+        source particle i goes to particle dstOf[i] (-1: not carried),
+        translated by shift[dstOf[i]]."""
+        call("demsph_sph_copy_members", self._h, source._h, _ip(_i32(dstOf)), _dp(_f64(shift, (self.num(), 3))))
 
     def getPairs(self, which=0):
         """which = 0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy; original indices, CSR order."""
