@@ -16,6 +16,11 @@ kick, drift, continuity + EOS, momentum, kick.  Metric: particle-steps/s
 * e2e: the same metric through the public solver API as a user runs it:
   scene upload from host memory, K steps, final state read back, all timed.
 * roofline: the momentum kernel (the dominant one), timed live per launch.
+* stream: the serving / batching stream -- 64 seeded scenes (DEM drops and
+  WCSPH dam breaks, 1k-200k particles, 500 steps each, Poisson arrivals)
+  through the continuous-batching server in mixed precision, beside the same
+  scenes run one at a time on the plain solver (FP64 and mixed); wall clock,
+  with p50 / p99 scene-step and scene latency.
 * cpu_baseline: the FP64 C++ oracle on the host cores over a short sample.
 * --impl reference: the reference's step restated as the FP64 C++ oracle
   (the reference has no CPU path; its CUDA build cannot be installed as a
@@ -51,6 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--stream", type=int, default=64,
+                    help="scenes in the served-stream measurement (0: skip it)")
     return ap.parse_args()
 
 
@@ -158,6 +165,42 @@ def dem_bounce(torch, steps, warmup, flush):
             "note": "4,096 spheres; launch-bound at this size (see DESIGN.md)"}
 
 
+def served_stream(torch, num, seed=5, rate=30.0, steps=500, chunk=100):
+    """The serving / batching stream (seeded Poisson arrivals of DEM drops and
+    WCSPH dam breaks, particle counts log-uniform over 1k-200k, polydisperse
+    DEM radii, 500 steps each): the first `num` scenes served by the
+    continuous-batching server (mixed precision), then the same scenes run
+    one after another on the plain solver in FP64 and in mixed precision.
+    Wall-clock times; scenes are generated before each clock starts."""
+    from this_studio_b200 import serve
+
+    n_max = 200_000
+    c0, dt = serve.stream_params(n_max)
+    mk = lambda: serve.make_stream(num, seed=seed, n_min=1000, n_max=n_max, rate=rate, steps=steps)
+    # warm-up: module loads and memory pools
+    serve.SceneServer(hbm_budget=4e9, chunk=10, sph_c0=c0, sph_dt=dt).run(
+        serve.make_stream(4, seed=1, n_min=1000, n_max=4000, rate=1e4, steps=20))
+    reqs = mk()
+    ps = serve.particle_steps(reqs, c0, dt)
+    srv = serve.SceneServer(hbm_budget=60e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt)
+    torch.cuda.synchronize()
+    m = srv.run(reqs)
+    plain = {}
+    for prec in ("fp64", "mixed"):
+        plain[prec] = ps / serve.run_plain(mk(), prec, c0, dt)
+    return {"workload": f"served_stream_{num}", "scenes": num, "seed": seed, "arrival_rate_per_s": rate,
+            "steps_per_scene": steps, "chunk_steps": chunk, "particle_steps": ps,
+            "value": m["value"], "unit": METRIC, "makespan_s": m["makespan_s"],
+            "plain_fp64_value": plain["fp64"], "plain_mixed_value": plain["mixed"],
+            "speedup_vs_plain_fp64": m["value"] / plain["fp64"],
+            "speedup_vs_plain_mixed": m["value"] / plain["mixed"],
+            "scene_step_latency_p50_ms": m["scene_step_latency_p50_ms"],
+            "scene_step_latency_p99_ms": m["scene_step_latency_p99_ms"],
+            "scene_latency_p50_s": m["scene_latency_p50_s"], "scene_latency_p99_s": m["scene_latency_p99_s"],
+            "admission_wait_p50_s": m["admission_wait_p50_s"], "admission_wait_p99_s": m["admission_wait_p99_s"],
+            "per_kind": m["per_kind"]}
+
+
 def native(args, rank, world, dist):
     import torch
 
@@ -231,6 +274,8 @@ def native(args, rank, world, dist):
     del s3
     other_value = nf / (float(sum(t3)) / len(t3) / 1e3)
     dem = dem_bounce(torch, min(args.steps, 200), args.warmup, flush)
+    del flush
+    stream = served_stream(torch, args.stream) if (args.stream > 0 and rank == 0 and world == 1) else None
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -244,6 +289,7 @@ def native(args, rank, world, dist):
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "value_" + other: other_value,
         "dem": dem,
+        "stream": stream,
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,

@@ -209,6 +209,17 @@ int demsph_sph_eval_accel(demsph_sph_t s);
  * reorder + neighbour lists, momentum + kick + drift, continuity + EOS,
  * momentum + kick. */
 int demsph_sph_profile_steps(demsph_sph_t s, long numSteps, double* phaseMs);
+/* No counterpart in the reference (autotuner).  Rebuilds the neighbour lists
+ * of the current state `trials` times with each compiled block shape of the
+ * list build (warps per block x candidates staged per warp), times them with
+ * CUDA events on the scene's stream, and keeps the fastest for later steps.
+ * Writes the chosen shape to *chosen and each shape's milliseconds per build
+ * to msPerShape[0 .. demsph_sph_num_list_shapes()-1] (either may be NULL).
+ * The lists are unchanged by the choice (same pairs, same order). */
+int demsph_sph_tune(demsph_sph_t s, int trials, int* chosen, double* msPerShape);
+int demsph_sph_num_list_shapes(void);
+/* Selects a list-build block shape by index (what demsph_sph_tune picks). */
+int demsph_sph_set_list_shape(demsph_sph_t s, int shape);
 
 /* No counterpart in the reference (batching).  Copies the fluid state of
  * particles carried over from scene src into scene dst on the device: source

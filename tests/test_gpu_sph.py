@@ -82,3 +82,26 @@ def test_reference_frame1(gpu, dam):
     assert np.abs(s["velocity"][idx] - fx["velocity"]).max() < 1e-5
     assert np.abs(s["density"][idx] - fx["density"]).max() < 5e-5
     assert np.abs(s["pressure"][idx] - fx["pressure"]).max() < 2e-2
+
+
+def test_list_shapes_give_identical_lists(gpu, oracle_lib, dam):
+    """Every block shape the autotuner may pick builds the same pairs in the
+    same order as the oracle; tune() keeps one of them."""
+    o = oracle_sph(dam)
+    o.neighbor_search()
+    ref = [o.pairs(w) for w in (0, 1)]
+    g = build_sph(dam, "mixed")
+    from this_studio_b200 import _lib
+
+    for shape in range(_lib.lib().demsph_sph_num_list_shapes()):
+        g.setListShape(shape)
+        g.neighborSearch()
+        for w in (0, 1):
+            a, b = g.getPairs(w)
+            np.testing.assert_array_equal(a, ref[w][0])
+            np.testing.assert_array_equal(b, ref[w][1])
+    chosen, ms = g.tune(trials=3)
+    print(f"list build ms per shape {np.round(ms, 4)} -> {chosen}")
+    assert 0 <= chosen < len(ms) and np.all(ms > 0)
+    a, b = g.getPairs(0)
+    np.testing.assert_array_equal(a, ref[0][0])

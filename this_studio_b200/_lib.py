@@ -76,6 +76,9 @@ SIGNATURES = {
     "demsph_sph_neighbor_search": [_vp],
     "demsph_sph_eval_accel": [_vp],
     "demsph_sph_profile_steps": [_vp, _long, _d],
+    "demsph_sph_tune": [_vp, _int, _i, _d],
+    "demsph_sph_num_list_shapes": [],
+    "demsph_sph_set_list_shape": [_vp, _int],
     "demsph_sph_copy_members": [_vp, _vp, _i, _d],
     "demsph_sph_num": [_vp, _int, _l],
     "demsph_sph_num_pairs": [_vp, _int, _l],

@@ -15,6 +15,7 @@
 #include <atomic>
 #include <cmath>
 #include <memory>
+#include <type_traits>
 
 #include "cells.cuh"
 
@@ -40,6 +41,18 @@ struct SphDev {
     const double4* dvel;
     const double4* dst;
     const double4* dnorm;
+    // FP32 shadows of the fluid (v, m) and (rho, p, c, nu) records and of
+    // the dummies' (v, m), (c, nu, rho0, -) and normals: what the
+    // mixed-precision passes gather (the FP32 values those passes would
+    // round the FP64 records to anyway).  Each kernel that writes an FP64
+    // record writes its shadow too.
+    const float4* velf;
+    const float4* stf;
+    float4* velfOut;
+    float4* stfOut;
+    const float4* dvelf;
+    const float4* dstf;
+    const float4* dnormf;
     const float4* posf;   // fluid (x, y, z) - grid min and h, FP32, this step's order
     const float4* dposf;  // dummies, same form
     float eps;            // bound on |float coordinate - exact coordinate|
@@ -105,21 +118,38 @@ __device__ __forceinline__ T quad_sum(T v, unsigned m) {
     return v;
 }
 
+__device__ __forceinline__ float4 f4(double4 a) { return make_float4((float)a.x, (float)a.y, (float)a.z, (float)a.w); }
+
+// Rewrites the FP32 shadows from the FP64 records (after a host-side change).
+__global__ void k_sph_shadow(int n, const double4* __restrict__ a, const double4* __restrict__ b,
+                             const double4* __restrict__ c, float4* __restrict__ af, float4* __restrict__ bf,
+                             float4* __restrict__ cf) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    af[t] = f4(a[t]);
+    bf[t] = f4(b[t]);
+    if (c) cf[t] = f4(c[t]);
+}
+
 // Permutes the fluid into this step's cell order.
 __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const double4* __restrict__ pos,
                               const double4* __restrict__ vel, const double4* __restrict__ st,
                               const double* __restrict__ rho0, const double* __restrict__ drho,
                               const int* __restrict__ id, double4* __restrict__ pos2, double4* __restrict__ vel2,
                               double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
-                              int* __restrict__ id2, float4* __restrict__ posf, double3 origin) {
+                              int* __restrict__ id2, float4* __restrict__ posf, float4* __restrict__ velf2,
+                              float4* __restrict__ stf2, double3 origin) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     int o = sorted[t];
     double4 p = pos[o];
     pos2[t] = p;
     posf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
-    vel2[t] = vel[o];
-    st2[t] = st[o];
+    const double4 v = vel[o], q = st[o];
+    vel2[t] = v;
+    st2[t] = q;
+    velf2[t] = f4(v);
+    stf2[t] = f4(q);
     rho02[t] = rho0[o];
     drho2[t] = drho[o];
     id2[t] = id[o];
@@ -128,98 +158,184 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
 // countSPHInteractionsKernel / writeSPHInteractionsKernel and the dummy pair
 // kernels (SPHNeighborSearchKernel.cu:6-228) in one pass: j != i,
 // |r_ij| <= 2 max(h_i, h_j), rows in the reference's stencil order.
-// Built one warp per cell.  All particles of a cell share
-// the cell's 27-cell stencil (the reference clamps positions and cell indices
-// the same way for every particle of a cell), so the warp loads each stencil
-// row's candidates once, 32 at a time, into shared memory with coalesced
-// loads, and every lane tests them against its own particle in row order,
-// appending hits to its ELL row.  The rows come out in the reference's order.
-constexpr int kListWarps = 4;
-__device__ __forceinline__ void cell_collect(int ps, int pe, const Stencil& st, const GridDesc& g,
-                                             const int* __restrict__ cellStart, const double4* __restrict__ own,
-                                             const float4* __restrict__ ownf, const double4* __restrict__ other,
-                                             const float4* __restrict__ otherf, float eps, bool same, int K, int N,
-                                             int* __restrict__ nb, int* __restrict__ cnt, int* needMax, int* overflow,
-                                             float4* cand) {
+//
+// Built one warp per cell.  All particles of a cell share the cell's 27-cell
+// stencil (the reference clamps positions and cell indices the same way for
+// every particle of a cell), so the warp stages the stencil's candidates --
+// nine rows of three contiguous cells, in row order -- once in shared memory
+// (coalesced loads), then sweeps them for each of the cell's particles in
+// turn, one candidate per lane: a ballot of the hits and a popcount prefix
+// give every hit its slot, so the row keeps the candidates' order, which is
+// the reference's.  A stencil with more candidates than the stage holds is
+// swept in consecutive chunks with the running count carried over.
+//
+// The test runs on FP32 coordinates relative to the grid minimum.  Each is
+// within eps of the exact value, so |r|^2 is within `band` of the exact
+// |r|^2; only candidates inside that band take the reference's FP64 test, so
+// the pair set is the reference's exactly.
+// Block shapes of the list build the autotuner chooses from: warps per
+// block, candidates staged per warp (a multiple of 32), and the resident
+// blocks per SM the register budget is fitted to.
+struct ListShape {
+    int warps, stage, minBlocks;
+};
+constexpr ListShape kListShapes[] = {{4, 512, 6}, {4, 384, 8}, {8, 256, 4}, {2, 512, 12}};
+constexpr int kNumListShapes = 4;
+
+__device__ __forceinline__ float list_band(float cut, float eps) {
+    return 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * cut * cut;
+}
+
+// Staged candidate: (x, y, z) relative to the grid minimum and, when every
+// particle has the same h, the candidate's index in w (its bits); otherwise
+// w = h and the index is staged separately.  Padding entries sit far away.
+template <bool kUniformH>
+struct ListStage {
+    float4* pos;
+    int* idx;
+    __device__ __forceinline__ void put(int v, float4 q, int j) const {
+        if (kUniformH) q.w = __int_as_float(j);
+        else idx[v] = j;
+        pos[v] = q;
+    }
+    __device__ __forceinline__ void pad(int v) const {
+        pos[v] = make_float4(1.0e18f, 1.0e18f, 1.0e18f, kUniformH ? __int_as_float(-1) : 0.0f);
+        if (!kUniformH) idx[v] = -1;
+    }
+    __device__ __forceinline__ int index(int v, float4 q) const { return kUniformH ? __float_as_int(q.w) : idx[v]; }
+};
+
+// One own particle against one staged batch: hit / band flags for this lane.
+template <bool kUniformH>
+__device__ __forceinline__ void list_test(const float4& pf, const float4& q, float loI, float hiI, float eps,
+                                          bool& in, bool& band) {
+    float lo = loI, hi = hiI;
+    if (!kUniformH && q.w > pf.w) {
+        const float cut = 2.0f * q.w, c2 = cut * cut, bd = list_band(cut, eps);
+        lo = c2 - bd;
+        hi = c2 + bd;
+    }
+    const float dx = pf.x - q.x, dy = pf.y - q.y, dz = pf.z - q.z;
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    in = d2 < lo;
+    band = !in && d2 <= hi;
+}
+
+__device__ __forceinline__ bool list_exact(const double4* __restrict__ own, const double4* __restrict__ other, int i,
+                                           int j) {
+    const double4 pi = own[i], pj = other[j];
+    const double cd = 2.0 * fmax(pi.w, pj.w);
+    const double3 r = xyz(pi) - xyz(pj);
+    return (cd * cd - dot(r, r)) >= 0.;
+}
+
+template <bool kUniformH, int kStage>
+__device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, const GridDesc& g,
+                                           const int* __restrict__ cellStart, const double4* __restrict__ own,
+                                           const float4* __restrict__ ownf, const double4* __restrict__ other,
+                                           const float4* __restrict__ otherf, float eps, bool same, int K, int N,
+                                           int* __restrict__ nb, int* __restrict__ cnt, int* needMax, int* overflow,
+                                           const ListStage<kUniformH>& sg) {
     const int lane = threadIdx.x & 31;
-    for (int g0 = ps; g0 < pe; g0 += 32) {
-        const int i = g0 + lane;
-        const bool mine = i < pe;
-        const float4 pf = mine ? ownf[i] : make_float4(0, 0, 0, 0);
-        const float cutOwn = 2.0f * pf.w, c2Own = cutOwn * cutOwn;
-        const float bandOwn = 4.0f * eps * (cutOwn + 2.0f * eps) * 1.7321f + 4.0e-6f * c2Own;
-        const float loOwn = c2Own - bandOwn, hiOwn = c2Own + bandOwn;
-        int c = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    int total = 0;
+    for_stencil_rows(st, g, cellStart, [&](int b, int e) { total += e - b; });
+    if (total == 0) {
+        for (int i = ps + lane; i < pe; i += 32) cnt[i] = 0;
+        return;
+    }
+    const int nchunk = (total + kStage - 1) / kStage;
+    for (int ch = 0; ch < nchunk; ch++) {
+        const int c0 = ch * kStage, c1 = min(total, c0 + kStage);
+        const int m = c1 - c0, mp = (m + 31) & ~31;
+        __syncwarp();
+        int off = 0;
         for_stencil_rows(st, g, cellStart, [&](int b, int e) {
-            for (int base = b; base < e; base += 32) {
-                __syncwarp();
-                if (base + lane < e) cand[lane] = otherf[base + lane];
-                __syncwarp();
-                const int m = min(32, e - base);
-                if (mine) {
-                    for (int t = 0; t < m; t++) {
-                        const int j = base + t;
-                        if (same && j == i) continue;
-                        const float4 q = cand[t];
-                        // FP32 distance on domain-relative coordinates.  Each
-                        // coordinate is within eps of exact, so d2 is within
-                        // band of the exact value; only candidates inside that
-                        // band need the reference's FP64 test.  The thresholds
-                        // of the particle's own h are hoisted out of the loop.
-                        float lo = loOwn, hi = hiOwn;
-                        if (q.w > pf.w) {
-                            const float cut = 2.0f * q.w;
-                            const float c2 = cut * cut;
-                            const float band = 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * c2;
-                            lo = c2 - band;
-                            hi = c2 + band;
-                        }
-                        const float dx = pf.x - q.x, dy = pf.y - q.y, dz = pf.z - q.z;
-                        const float d2 = dx * dx + dy * dy + dz * dz;
-                        bool hit;
-                        if (d2 < lo) hit = true;
-                        else if (d2 > hi) hit = false;
-                        else {
-                            const double4 pi = own[i], pj = other[j];
-                            double cd = 2.0 * fmax(pi.w, pj.w);
-                            double3 r = xyz(pi) - xyz(pj);
-                            hit = (cd * cd - dot(r, r)) >= 0.;
-                        }
-                        if (hit) {
-                            if (c < K) nb[(size_t)c * N + i] = j;
-                            c++;
-                        }
-                    }
+            const int lo = max(b, b + (c0 - off)), hi = min(e, b + (c1 - off));
+            for (int j = lo + lane; j < hi; j += 32) sg.put(off + (j - b) - c0, otherf[j], j);
+            off += e - b;
+        });
+        if (m + lane < mp) sg.pad(m + lane);
+        __syncwarp();
+        // two own particles per sweep share each staged load
+        for (int i0 = ps; i0 < pe; i0 += 2) {
+            const int i1 = min(i0 + 1, pe - 1);
+            const bool two = i0 + 1 < pe;
+            const float4 pa = ownf[i0], pb = ownf[i1];
+            const float cA = 2.0f * pa.w, cB = 2.0f * pb.w;
+            const float bA = list_band(cA, eps), bB = list_band(cB, eps);
+            const float loA = cA * cA - bA, hiA = cA * cA + bA, loB = cB * cB - bB, hiB = cB * cB + bB;
+            int na = ch == 0 ? 0 : cnt[i0];
+            int nbc = (ch == 0 || !two) ? 0 : cnt[i1];
+            for (int v0 = 0; v0 < mp; v0 += 32) {
+                const int v = v0 + lane;
+                const float4 q = sg.pos[v];
+                const int j = sg.index(v, q);
+                bool inA, bandA, inB, bandB;
+                list_test<kUniformH>(pa, q, loA, hiA, eps, inA, bandA);
+                list_test<kUniformH>(pb, q, loB, hiB, eps, inB, bandB);
+                if (same) {
+                    if (j == i0) inA = bandA = false;
+                    if (j == i1) inB = bandB = false;
+                }
+                if (!two) inB = bandB = false;
+                if (__any_sync(0xffffffffu, bandA || bandB)) {
+                    if (bandA) inA = list_exact(own, other, i0, j);
+                    if (bandB) inB = list_exact(own, other, i1, j);
+                }
+                const unsigned hA = __ballot_sync(0xffffffffu, inA);
+                const unsigned hB = __ballot_sync(0xffffffffu, inB);
+                if (hA) {
+                    const int k = na + __popc(hA & lt);
+                    if (inA && k < K) nb[(size_t)k * N + i0] = j;
+                    na += __popc(hA);
+                }
+                if (hB) {
+                    const int k = nbc + __popc(hB & lt);
+                    if (inB && k < K) nb[(size_t)k * N + i1] = j;
+                    nbc += __popc(hB);
                 }
             }
-        });
-        if (mine) {
-            if (c > K) {  // the passes walk this particle's stencil instead
-                atomicMax(needMax, c);
-                atomicExch(overflow, 1);
-                c = -1;
+            if (lane < 2 && (lane == 0 || two)) {
+                const int i = lane == 0 ? i0 : i1;
+                const int c = lane == 0 ? na : nbc;
+                if (ch + 1 < nchunk) {
+                    cnt[i] = c;
+                } else if (c > K) {  // the passes walk this particle's stencil instead
+                    atomicMax(needMax, c);
+                    atomicExch(overflow, 1);
+                    cnt[i] = -1;
+                } else {
+                    cnt[i] = c;
+                }
             }
-            cnt[i] = c;
+            __syncwarp();
         }
     }
 }
-__global__ void __launch_bounds__(32 * kListWarps) k_sph_lists_cell(SphDev d, int ncell) {
-    __shared__ float4 cand[kListWarps][32];
+
+template <bool kUniformH, int kShape>
+__global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
+    k_sph_lists_cell(SphDev d, int ncell) {
+    constexpr int kListWarps = kListShapes[kShape].warps, kStage = kListShapes[kShape].stage;
+    __shared__ float4 sPos[kListWarps][kStage];
+    __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
     const int w = threadIdx.x >> 5;
     const int cell = blockIdx.x * kListWarps + w;
     if (cell >= ncell) return;
     const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
     if (ps == pe) return;
+    ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
     // stencil of the cell: the one every particle of the cell computes
     const double4 p0 = d.pos[ps];
     Stencil st = stencil_of(xyz(p0), d.g);
-    cell_collect(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N, d.nbF, d.cntF,
-                 &d.status->need_pairs, &d.status->overflow, cand[w]);
+    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N,
+                                  d.nbF, d.cntF, &d.status->need_pairs, &d.status->overflow, sg);
     if (d.ND > 0)
-        cell_collect(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false, d.KD, d.N, d.nbD,
-                     d.cntD, &d.status->need_aux, &d.status->overflow, cand[w]);
-    else if ((threadIdx.x & 31) == 0)
-        for (int i = ps; i < pe; i++) d.cntD[i] = 0;
+        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false, d.KD, d.N,
+                              d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg);
+    else
+        for (int i = ps + (threadIdx.x & 31); i < pe; i += 32) d.cntD[i] = 0;
 }
 
 // Calls f(j) for this lane's share of particle i's neighbours: from the ELL
@@ -253,6 +369,40 @@ __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ 
 // half, the drift (SPHPositionIntegrationKernel, :161-170).  Reads the state
 // arrays and writes the integrated particle into separate output arrays, so
 // no thread sees a neighbour's updated state.
+// Neighbour records in the precision of the pass: the FP64 records for the
+// FP64 passes, their FP32 shadows for the mixed-precision ones (the same
+// values those passes would compute by rounding the FP64 records).
+template <class R>
+__device__ __forceinline__ void load_fluid(const SphDev& d, int j, V<R>& vj, R& mj, R& rhoj, R& PR, R& cj, R& nuj) {
+    if constexpr (std::is_same<R, float>::value) {
+        const float4 v = d.velf[j], q = d.stf[j];
+        vj = make_float3(v.x, v.y, v.z);
+        mj = v.w;
+        rhoj = q.x; PR = q.y; cj = q.z; nuj = q.w;
+    } else {
+        const double4 v = d.vel[j], q = d.st[j];
+        vj = xyz(v);
+        mj = v.w;
+        rhoj = q.x; PR = q.y; cj = q.z; nuj = q.w;
+    }
+}
+template <class R>
+__device__ __forceinline__ void load_dummy(const SphDev& d, int j, V<R>& nw, V<R>& vj, R& mj, R& cj, R& nuj, R& rho0j) {
+    if constexpr (std::is_same<R, float>::value) {
+        const float4 n = d.dnormf[j], v = d.dvelf[j], q = d.dstf[j];
+        nw = make_float3(n.x, n.y, n.z);
+        vj = make_float3(v.x, v.y, v.z);
+        mj = v.w;
+        cj = q.x; nuj = q.y; rho0j = q.z;
+    } else {
+        const double4 n = d.dnorm[j], v = d.dvel[j], q = d.dst[j];
+        nw = xyz(n);
+        vj = xyz(v);
+        mj = v.w;
+        cj = q.x; nuj = q.y; rho0j = q.z;
+    }
+}
+
 template <class R>
 __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
@@ -270,11 +420,10 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     VR acc = v3r<R>(0, 0, 0);
     quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         double4 pj4 = d.pos[j];
-        double4 vj4 = d.vel[j];
-        double4 sj = d.st[j];
+        VR vj;
+        R rhoj, PR, cj, nuj, mj;
+        load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
         VR rij = cvt<R>(ri - xyz(pj4));
-        VR vj = cvt<R>(xyz(vj4));
-        R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, nuj = (R)sj.w, mj = (R)vj4.w;
         R r2 = dot(rij, rij);
         // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
         // reference's normalize does (myVec.h:112-128)
@@ -295,11 +444,9 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     const VR g = cvt<R>(d.gravity);
     if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         double4 pj4 = d.dpos[j];
-        double4 vj4 = d.dvel[j];
-        double4 sj = d.dst[j];
-        VR nw = cvt<R>(xyz(d.dnorm[j]));
-        VR vj = cvt<R>(xyz(vj4));
-        R cj = (R)sj.x, nuj = (R)sj.y, rho0j = (R)sj.z, mj = (R)vj4.w;
+        VR nw, vj;
+        R cj, nuj, rho0j, mj;
+        load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
         R UL = dot(-nw, vi);
         R UR = -UL + (R)2.0 * dot(-nw, vj);
         VR rij = cvt<R>(ri - xyz(pj4));
@@ -327,7 +474,9 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     a += d.gravity;
     d.acc[i] = d4(a, 0);
     double3 v = xyz(vi4) + hdt * a;
-    d.velOut[i] = d4(v, vi4.w);
+    const double4 v4 = d4(v, vi4.w);
+    d.velOut[i] = v4;
+    d.velfOut[i] = f4(v4);
     if (first) d.posOut[i] = d4(ri + dt * v, pi4.w);
 }
 
@@ -350,11 +499,10 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     R dRho = (R)0;
     quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         double4 pj4 = d.pos[j];
-        double4 vj4 = d.vel[j];
-        double4 sj = d.st[j];
+        VR vj;
+        R rhoj, PR, cj, nuj, mj;
+        load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
         VR rij = cvt<R>(ri - xyz(pj4));
-        VR vj = cvt<R>(xyz(vj4));
-        R rhoj = (R)sj.x, PR = (R)sj.y, cj = (R)sj.z, mj = (R)vj4.w;
         R r2 = dot(rij, rij);
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
@@ -368,10 +516,9 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     const VR g = cvt<R>(d.gravity);
     if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         double4 pj4 = d.dpos[j];
-        double4 vj4 = d.dvel[j];
-        double4 sj = d.dst[j];
-        VR vj = cvt<R>(xyz(vj4));
-        R cj = (R)sj.x, rho0j = (R)sj.z, mj = (R)vj4.w;
+        VR nw, vj;
+        R cj, nuj, rho0j, mj;
+        load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
         VR rij = cvt<R>(ri - xyz(pj4));
         R grj = -dot(g, rij);
         if (grj < (R)0.) grj = (R)0.;
@@ -394,7 +541,9 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     d.drho[i] = ch;
     double r0 = d.rho0[i];
     if (ch < -0.1 * r0) ch = -0.1 * r0;
-    d.stOut[i] = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
+    const double4 so = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
+    d.stOut[i] = so;
+    d.stfOut[i] = f4(so);
 }
 
 // calDummyParticleNormalKernel (WCSPHIntegrationKernel.cu:4-40) over the
@@ -484,6 +633,7 @@ struct SphScene {
     DBuf<int> id[2];
     DBuf<double4> acc;
     DBuf<float4> posf, dposf;
+    DBuf<float4> velf[2], stf[2], dvelf, dstf, dnormf;  // FP32 shadows
     float eps = 0;
     int P = 0, Vv = 0, S = 0, R0 = 0, D = 0, ID = 0;
     DBuf<double4> dpos, dvel, dst, dnorm;
@@ -505,6 +655,8 @@ struct SphScene {
         d.pos = pos[P].p; d.vel = vel[Vv].p; d.st = st[S].p; d.rho0 = rho0[R0].p; d.drho = drho[D].p;
         d.acc = acc.p;
         d.dpos = dpos.p; d.dvel = dvel.p; d.dst = dst.p; d.dnorm = dnorm.p;
+        d.velf = velf[Vv].p; d.stf = stf[S].p;
+        d.dvelf = dvelf.p; d.dstf = dstf.p; d.dnormf = dnormf.p;
         d.nbF = nbF.p; d.cntF = cntF.p; d.nbD = nbD.p; d.cntD = cntD.p;
         d.posf = posf.p; d.dposf = dposf.p; d.eps = eps;
         d.gravity = gravity;
@@ -522,16 +674,48 @@ struct SphScene {
 
     // WCSPHSolver::neighborSearch (WCSPHSolver.h:150-285): fluid cell sort,
     // reorder, neighbour lists.
+    // all fluid and dummy particles share one h: the list build keeps the
+    // candidate index in the staged record
+    bool uniformH = false;
+    int listShape = 0;  // index into kListShapes (autotuned)
+    template <int S>
+    void launch_lists_shape(const SphDev& d) {
+        constexpr int W = kListShapes[S].warps;
+        const unsigned grid = grid_for(fCells.ncell, W);
+        if (uniformH) k_sph_lists_cell<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        else k_sph_lists_cell<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+    }
+    void launch_lists(const SphDev& d) {
+        switch (listShape) {
+            case 0: launch_lists_shape<0>(d); break;
+            case 1: launch_lists_shape<1>(d); break;
+            case 2: launch_lists_shape<2>(d); break;
+            default: launch_lists_shape<3>(d); break;
+        }
+    }
+    // Moves the fluid records (and their FP32 shadows) into this step's cell order.
+    void permute() {
+        const int n = N();
+        k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
+                                                       drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
+                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p,
+                                                       velf[Vv ^ 1].p, stf[S ^ 1].p, fCells.g.mn);
+        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+    }
+    // Rewrites the fluid shadows after a host-side change of the records.
+    void refresh_shadows() {
+        const int n = N();
+        k_sph_shadow<<<grid_for(n, 256), 256, 0, s>>>(n, vel[Vv].p, st[S].p, nullptr, velf[Vv].p, stf[S].p, nullptr);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+    }
     void neighbor_search() {
         const int n = N();
         fCells.build(pos[P].p, n, s, id[ID].p);
         g_launches += fCells.launches;
-        k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
-                                                       drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
-                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p, fCells.g.mn);
-        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        permute();
         SphDev d = dev();
-        k_sph_lists_cell<<<grid_for(fCells.ncell, kListWarps), 32 * kListWarps, 0, s>>>(d, fCells.ncell);
+        launch_lists(d);
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
@@ -541,6 +725,7 @@ struct SphScene {
         const int n = N();
         d.posOut = pos[P ^ 1].p;
         d.velOut = vel[Vv ^ 1].p;
+        d.velfOut = velf[Vv ^ 1].p;
         if (precision == DEMSPH_PRECISION_FP64)
             k_sph_accel<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
         else
@@ -554,6 +739,7 @@ struct SphScene {
         SphDev d = dev();
         const int n = N();
         d.stOut = st[S ^ 1].p;
+        d.stfOut = stf[S ^ 1].p;
         if (precision == DEMSPH_PRECISION_FP64) k_sph_density<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
         else k_sph_density<float><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
         g_launches += 1;
@@ -583,12 +769,9 @@ struct SphScene {
         fCells.build(pos[P].p, n, s, id[ID].p);
         g_launches += fCells.launches;
         DEMSPH_CUDA(cudaEventRecord(ev[1], s));
-        k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
-                                                       drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
-                                                       rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p, fCells.g.mn);
-        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        permute();
         SphDev d = dev();
-        k_sph_lists_cell<<<grid_for(fCells.ncell, kListWarps), 32 * kListWarps, 0, s>>>(d, fCells.ncell);
+        launch_lists(d);
         g_launches += 2;
         haveLists = true;
         DEMSPH_CUDA(cudaEventRecord(ev[2], s));
@@ -673,6 +856,13 @@ struct SphScene {
         double cell = 0;
         for (auto& p : hf.pos) cell = std::max(cell, p.w * 2.0);
         for (auto& p : hd.pos) cell = std::max(cell, p.w * 2.0);
+        {
+            // the same h everywhere, as the list build sees it (FP32)
+            const float h0 = (float)hf.pos[0].w;
+            uniformH = true;
+            for (auto& p : hf.pos) uniformH = uniformH && (float)p.w == h0;
+            for (auto& p : hd.pos) uniformH = uniformH && (float)p.w == h0;
+        }
         GridDesc gd{};
         if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
         status.alloc(1, s, true);
@@ -683,6 +873,7 @@ struct SphScene {
         for (int i = 0; i < n; i++) ids[i] = i;
         for (int b = 0; b < 2; b++) {
             pos[b].alloc(n, s, false); vel[b].alloc(n, s, false); st[b].alloc(n, s, false);
+            velf[b].alloc(n, s, false); stf[b].alloc(n, s, false);
             rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
         }
         P = Vv = S = R0 = D = ID = 0;
@@ -746,6 +937,10 @@ struct SphScene {
                 if (!st2.overflow) break;
                 KDD = st2.need_rev + st2.need_rev / 4 + 1;
             }
+            dvelf.alloc(nd, s, false); dstf.alloc(nd, s, false); dnormf.alloc(nd, s, false);
+            k_sph_shadow<<<grid_for(nd, 256), 256, 0, s>>>(nd, dvel.p, dst.p, dnorm.p, dvelf.p, dstf.p, dnormf.p);
+            g_launches += 1;
+            DEMSPH_LAUNCH_CHECK();
         } else {
             dCells.build(nullptr, 0, s);
             g_launches += dCells.launches;
@@ -849,7 +1044,7 @@ int demsph_sph_neighbor_search(demsph_sph_t h) {
         if (st2.overflow) {  // rebuild with room so that the lists are complete
             s.grow(st2);
             SphDev d = s.dev();
-            k_sph_lists_cell<<<grid_for(s.fCells.ncell, kListWarps), 32 * kListWarps, 0, s.s>>>(d, s.fCells.ncell);
+            s.launch_lists(d);
             g_launches += 1;
             DEMSPH_LAUNCH_CHECK();
         }
@@ -864,6 +1059,7 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         SphDev d = s.dev();
         d.posOut = s.pos[s.P ^ 1].p;
         d.velOut = s.vel[s.Vv ^ 1].p;
+        d.velfOut = s.velf[s.Vv ^ 1].p;
         if (s.precision == DEMSPH_PRECISION_FP64)
             k_sph_accel<double><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
         else
@@ -884,6 +1080,66 @@ int demsph_sph_profile_steps(demsph_sph_t h, long n, double* phaseMs) {
         DevStatus st2 = s.read_status();
         if (st2.overflow) throw Status(DEMSPH_ERR_OVERFLOW, "neighbour lists overflowed during profiling");
         for (int k = 0; k < 5; k++) phaseMs[k] /= (double)(n > 0 ? n : 1);
+    });
+}
+int demsph_sph_tune(demsph_sph_t h, int trials, int* chosen, double* msPerShape) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (trials < 1) throw Status(DEMSPH_ERR_INVALID, "trials must be positive");
+        // one full neighbour search sorts the fluid and sizes the lists for
+        // the current state; then each block shape rebuilds the same lists
+        s.clear_status();
+        s.neighbor_search();
+        DevStatus st0 = s.read_status();
+        if (st0.overflow) {
+            s.grow(st0);
+            s.clear_status();
+            s.neighbor_search();
+        }
+        cudaEvent_t e0, e1;
+        DEMSPH_CUDA(cudaEventCreate(&e0));
+        DEMSPH_CUDA(cudaEventCreate(&e1));
+        const int keep = s.listShape;
+        int best = keep;
+        double bestMs = 1e300;
+        for (int v = 0; v < kNumListShapes; v++) {
+            s.listShape = v;
+            SphDev d = s.dev();
+            s.launch_lists(d);  // warm-up
+            DEMSPH_CUDA(cudaEventRecord(e0, s.s));
+            for (int t = 0; t < trials; t++) s.launch_lists(d);
+            DEMSPH_CUDA(cudaEventRecord(e1, s.s));
+            DEMSPH_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            DEMSPH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double per = ms / trials;
+            if (msPerShape) msPerShape[v] = per;
+            if (per < bestMs) {
+                bestMs = per;
+                best = v;
+            }
+        }
+        g_launches += (long long)kNumListShapes * (trials + 1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        s.listShape = best;
+        // leave lists built by the chosen shape
+        s.launch_lists(s.dev());
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        if (chosen) *chosen = best;
+        (void)keep;
+    });
+}
+int demsph_sph_num_list_shapes(void) { return kNumListShapes; }
+int demsph_sph_set_list_shape(demsph_sph_t h, int shape) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (shape < 0 || shape >= kNumListShapes) throw Status(DEMSPH_ERR_INVALID, "unknown list block shape");
+        h->sc.listShape = shape;
     });
 }
 int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, const int* dstOf, const double* shift) {
@@ -917,6 +1173,7 @@ int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, const int* dst
                                                               d.pos[d.P].p, d.vel[d.Vv].p, d.st[d.S].p, d.drho[d.D].p);
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
+        d.refresh_shadows();
         DEMSPH_CUDA(cudaStreamSynchronize(d.s));
         d.haveLists = false;
     });
@@ -1016,6 +1273,7 @@ int demsph_sph_set(demsph_sph_t h, const double* pos, const double* vel, const d
         DEMSPH_CUDA(cudaMemcpyAsync(s.vel[s.Vv].p, V4.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s.s));
         DEMSPH_CUDA(cudaMemcpyAsync(s.st[s.S].p, S4.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s.s));
         DEMSPH_CUDA(cudaMemcpyAsync(s.drho[s.D].p, DR.data(), n * sizeof(double), cudaMemcpyHostToDevice, s.s));
+        s.refresh_shadows();
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         s.haveLists = false;
     });

@@ -363,6 +363,18 @@ class WCSPHSolver:
         call("demsph_sph_set", self._h, _dp(f(position, (n, 3))), _dp(f(velocity, (n, 3))), _dp(f(density, (n,))),
              _dp(f(pressure, (n,))), _dp(f(densityChange, (n,))))
 
+    def tune(self, trials=5):
+        """Autotunes the neighbour-list build's block shape on the current
+        state; returns (chosen shape, milliseconds per build of each shape)."""
+        ns = _lib.lib().demsph_sph_num_list_shapes()
+        ms = np.zeros(ns)
+        ch = C.c_int()
+        call("demsph_sph_tune", self._h, int(trials), C.byref(ch), _dp(ms))
+        return ch.value, ms
+
+    def setListShape(self, shape):
+        call("demsph_sph_set_list_shape", self._h, int(shape))
+
     def copyMembers(self, source, dstOf, shift):
         """Device-side carry of fluid state from `source` (a WCSPHSolver):
         source particle i goes to particle dstOf[i] (-1: not carried),
