@@ -53,6 +53,17 @@ struct SphDev {
     const float4* dvelf;
     const float4* dstf;
     const float4* dnormf;
+    // Fixed-point fluid / dummy positions for the mixed-precision passes:
+    // (x - grid min) / q rounded to an integer, kept modulo 2^32, with h's
+    // FP32 bits in w.  q is a power of two small enough that neighbours
+    // (|r| < 2 h, plus a step's drift) differ by less than 2^30 quanta, so
+    // the wrapped 32-bit difference of two positions is exact; r_ij is that
+    // difference times q, rounded once to FP32.
+    const int4* posq;
+    int4* posqOut;
+    const int4* dposq;
+    float q;
+    double invq;
     const float4* posf;   // fluid (x, y, z) - grid min and h, FP32, this step's order
     const float4* dposf;  // dummies, same form
     float eps;            // bound on |float coordinate - exact coordinate|
@@ -120,6 +131,21 @@ __device__ __forceinline__ T quad_sum(T v, unsigned m) {
 
 __device__ __forceinline__ float4 f4(double4 a) { return make_float4((float)a.x, (float)a.y, (float)a.z, (float)a.w); }
 
+__device__ __forceinline__ int4 fixq(double4 p, double3 o, double invq) {
+    const unsigned long long x = (unsigned long long)__double2ll_rn((p.x - o.x) * invq);
+    const unsigned long long y = (unsigned long long)__double2ll_rn((p.y - o.y) * invq);
+    const unsigned long long z = (unsigned long long)__double2ll_rn((p.z - o.z) * invq);
+    return make_int4((int)(unsigned)x, (int)(unsigned)y, (int)(unsigned)z, __float_as_int((float)p.w));
+}
+// a - b for two fixed-point coordinates of nearby particles, exact.
+__device__ __forceinline__ float fixdiff(int a, int b, float q) {
+    return (float)(int)((unsigned)a - (unsigned)b) * q;
+}
+__global__ void k_sph_fix(int n, const double4* __restrict__ pos, double3 o, double invq, int4* __restrict__ posq) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) posq[t] = fixq(pos[t], o, invq);
+}
+
 // Rewrites the FP32 shadows from the FP64 records (after a host-side change).
 __global__ void k_sph_shadow(int n, const double4* __restrict__ a, const double4* __restrict__ b,
                              const double4* __restrict__ c, float4* __restrict__ af, float4* __restrict__ bf,
@@ -138,12 +164,13 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
                               const int* __restrict__ id, double4* __restrict__ pos2, double4* __restrict__ vel2,
                               double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
                               int* __restrict__ id2, float4* __restrict__ posf, float4* __restrict__ velf2,
-                              float4* __restrict__ stf2, double3 origin) {
+                              float4* __restrict__ stf2, int4* __restrict__ posq2, double3 origin, double invq) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     int o = sorted[t];
     double4 p = pos[o];
     pos2[t] = p;
+    posq2[t] = fixq(p, origin, invq);
     posf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
     const double4 v = vel[o], q = st[o];
     vel2[t] = v;
@@ -369,6 +396,31 @@ __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ 
 // half, the drift (SPHPositionIntegrationKernel, :161-170).  Reads the state
 // arrays and writes the integrated particle into separate output arrays, so
 // no thread sees a neighbour's updated state.
+// r_ij = r_i - r_j and h_j: from the FP64 positions in the FP64 passes, from
+// the fixed-point positions in the mixed-precision ones.
+template <class R>
+struct OwnPos {
+    double3 r;
+    int4 q;
+};
+template <class R>
+__device__ __forceinline__ void pair_r(const OwnPos<R>& o, const double4* __restrict__ pos,
+                                       const int4* __restrict__ posq, float q, int j, V<R>& rij, R& hj) {
+    if constexpr (std::is_same<R, float>::value) {
+        const int4 b = posq[j];
+        rij = make_float3(fixdiff(o.q.x, b.x, q), fixdiff(o.q.y, b.y, q), fixdiff(o.q.z, b.z, q));
+        hj = __int_as_float(b.w);
+    } else {
+        const double4 b = pos[j];
+        rij = o.r - xyz(b);
+        hj = b.w;
+    }
+}
+// a / b: IEEE division in the FP64 passes, the fast reciprocal-based divide
+// (a couple of ulp) in the mixed-precision ones.
+__device__ __forceinline__ double div_r(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_r(float a, float b) { return __fdividef(a, b); }
+
 // Neighbour records in the precision of the pass: the FP64 records for the
 // FP64 passes, their FP32 shadows for the mixed-precision ones (the same
 // values those passes would compute by rounding the FP64 records).
@@ -412,6 +464,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
     const double3 ri = xyz(pi4);
+    OwnPos<R> op{ri, std::is_same<R, float>::value ? d.posq[i] : make_int4(0, 0, 0, 0)};
     const double4 vi4 = d.vel[i];
     const VR vi = cvt<R>(xyz(vi4));
     const double4 s4 = d.st[i];
@@ -419,11 +472,10 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     const HConst<R> hk = hconst<R>((R)pi4.w);
     VR acc = v3r<R>(0, 0, 0);
     quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-        double4 pj4 = d.pos[j];
-        VR vj;
-        R rhoj, PR, cj, nuj, mj;
+        VR rij, vj;
+        R hj, rhoj, PR, cj, nuj, mj;
+        pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
         load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
-        VR rij = cvt<R>(ri - xyz(pj4));
         R r2 = dot(rij, rij);
         // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
         // reference's normalize does (myVec.h:112-128)
@@ -431,11 +483,11 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
         R r = r2 * inv_r;
         VR e = rij * (-inv_r);
         R UL = dot(vi, e), UR = dot(vj, e);
-        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
         R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        R inv_rr = (R)1.0 / (rhoi * rhoj);
+        R inv_rr = div_r((R)1.0, rhoi * rhoj);
         acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
         R nuij = (R)0.5 * (nui + nuj);
         // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
@@ -443,25 +495,24 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     });
     const VR g = cvt<R>(d.gravity);
     if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
-        double4 pj4 = d.dpos[j];
-        VR nw, vj;
-        R cj, nuj, rho0j, mj;
+        VR rij, nw, vj;
+        R hj, cj, nuj, rho0j, mj;
+        pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
         load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
         R UL = dot(-nw, vi);
         R UR = -UL + (R)2.0 * dot(-nw, vj);
-        VR rij = cvt<R>(ri - xyz(pj4));
         R grj = -dot(g, rij);
         if (grj < (R)0.) grj = (R)0.;
         R PR = PL + rhoi * grj;
-        R rhoj = PR / (cj * cj) + rho0j;
+        R rhoj = div_r(PR, cj * cj) + rho0j;
         R r2 = dot(rij, rij);
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
         R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        R inv_rr = (R)1.0 / (rhoi * rhoj);
+        R inv_rr = div_r((R)1.0, rhoi * rhoj);
         acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
         R nuij = (R)0.5 * (nui + nuj);
         acc += (R)2.0 * nuij * dot(rij * inv_r, dW) * (vi - vj) * mj * inv_rr;
@@ -477,7 +528,11 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     const double4 v4 = d4(v, vi4.w);
     d.velOut[i] = v4;
     d.velfOut[i] = f4(v4);
-    if (first) d.posOut[i] = d4(ri + dt * v, pi4.w);
+    if (first) {
+        const double4 pn = d4(ri + dt * v, pi4.w);
+        d.posOut[i] = pn;
+        d.posqOut[i] = fixq(pn, d.g.mn, d.invq);
+    }
 }
 
 // updateWCSPHDensityChangeKernel + SPHDensityPressureIntegrationKernel
@@ -492,47 +547,46 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
     const double3 ri = xyz(pi4);
+    OwnPos<R> op{ri, std::is_same<R, float>::value ? d.posq[i] : make_int4(0, 0, 0, 0)};
     const VR vi = cvt<R>(xyz(d.vel[i]));
     const double4 s4 = d.st[i];
     const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z;
     const HConst<R> hk = hconst<R>((R)pi4.w);
     R dRho = (R)0;
     quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-        double4 pj4 = d.pos[j];
-        VR vj;
-        R rhoj, PR, cj, nuj, mj;
+        VR rij, vj;
+        R hj, rhoj, PR, cj, nuj, mj;
+        pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
         load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
-        VR rij = cvt<R>(ri - xyz(pj4));
         R r2 = dot(rij, rij);
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
         VR e = rij * (-inv_r);
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         VR vs = (R)0.5 * (vi + vj);
-        vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
-        dRho += mj / rhoj * dot(vi - vs, dW);
+        vs += (R)0.5 * div_r(PL - PR, rbar * cbar) * e;
+        dRho += div_r(mj, rhoj) * dot(vi - vs, dW);
     });
     const VR g = cvt<R>(d.gravity);
     if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
-        double4 pj4 = d.dpos[j];
-        VR nw, vj;
-        R cj, nuj, rho0j, mj;
+        VR rij, nw, vj;
+        R hj, cj, nuj, rho0j, mj;
+        pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
         load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
-        VR rij = cvt<R>(ri - xyz(pj4));
         R grj = -dot(g, rij);
         if (grj < (R)0.) grj = (R)0.;
         R PR = PL + rhoi * grj;
-        R rhoj = PR / (cj * cj) + rho0j;
+        R rhoj = div_r(PR, cj * cj) + rho0j;
         R r2 = dot(rij, rij);
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, (R)pj4.w) * rij;
+        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
         VR e = rij * (-inv_r);
         R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
         VR vs = (R)0.5 * (vi + vj);
-        vs += (R)0.5 * ((PL - PR) / (rbar * cbar)) * e;
-        dRho += mj / rhoj * dot(vi - vs, dW);
+        vs += (R)0.5 * div_r(PL - PR, rbar * cbar) * e;
+        dRho += div_r(mj, rhoj) * dot(vi - vs, dW);
     });
     double dsum = quad_sum((double)dRho, gm);
     if (sub != 0) return;
@@ -634,6 +688,9 @@ struct SphScene {
     DBuf<double4> acc;
     DBuf<float4> posf, dposf;
     DBuf<float4> velf[2], stf[2], dvelf, dstf, dnormf;  // FP32 shadows
+    DBuf<int4> posq[2], dposq;                           // fixed-point positions
+    float q = 0;
+    double invq = 0;
     float eps = 0;
     int P = 0, Vv = 0, S = 0, R0 = 0, D = 0, ID = 0;
     DBuf<double4> dpos, dvel, dst, dnorm;
@@ -656,6 +713,7 @@ struct SphScene {
         d.acc = acc.p;
         d.dpos = dpos.p; d.dvel = dvel.p; d.dst = dst.p; d.dnorm = dnorm.p;
         d.velf = velf[Vv].p; d.stf = stf[S].p;
+        d.posq = posq[P].p; d.dposq = dposq.p; d.q = q; d.invq = invq;
         d.dvelf = dvelf.p; d.dstf = dstf.p; d.dnormf = dnormf.p;
         d.nbF = nbF.p; d.cntF = cntF.p; d.nbD = nbD.p; d.cntD = cntD.p;
         d.posf = posf.p; d.dposf = dposf.p; d.eps = eps;
@@ -699,14 +757,16 @@ struct SphScene {
         k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
                                                        drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
                                                        rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p,
-                                                       velf[Vv ^ 1].p, stf[S ^ 1].p, fCells.g.mn);
+                                                       velf[Vv ^ 1].p, stf[S ^ 1].p, posq[P ^ 1].p, fCells.g.mn,
+                                                       invq);
         P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
     }
     // Rewrites the fluid shadows after a host-side change of the records.
     void refresh_shadows() {
         const int n = N();
         k_sph_shadow<<<grid_for(n, 256), 256, 0, s>>>(n, vel[Vv].p, st[S].p, nullptr, velf[Vv].p, stf[S].p, nullptr);
-        g_launches += 1;
+        k_sph_fix<<<grid_for(n, 256), 256, 0, s>>>(n, pos[P].p, fCells.g.mn, invq, posq[P].p);
+        g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
     }
     void neighbor_search() {
@@ -726,6 +786,7 @@ struct SphScene {
         d.posOut = pos[P ^ 1].p;
         d.velOut = vel[Vv ^ 1].p;
         d.velfOut = velf[Vv ^ 1].p;
+        d.posqOut = posq[P ^ 1].p;
         if (precision == DEMSPH_PRECISION_FP64)
             k_sph_accel<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
         else
@@ -873,7 +934,7 @@ struct SphScene {
         for (int i = 0; i < n; i++) ids[i] = i;
         for (int b = 0; b < 2; b++) {
             pos[b].alloc(n, s, false); vel[b].alloc(n, s, false); st[b].alloc(n, s, false);
-            velf[b].alloc(n, s, false); stf[b].alloc(n, s, false);
+            velf[b].alloc(n, s, false); stf[b].alloc(n, s, false); posq[b].alloc(n, s, false);
             rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
         }
         P = Vv = S = R0 = D = ID = 0;
@@ -892,6 +953,15 @@ struct SphScene {
         {
             double L = std::max(gd.mx.x - gd.mn.x, std::max(gd.mx.y - gd.mn.y, gd.mx.z - gd.mn.z));
             eps = (float)(2.0 * L * std::ldexp(1.0, -24));
+        }
+        // fixed-point quantum: the largest power of two with 8 h_max below 2^30 quanta
+        {
+            double hmax = 0;
+            for (auto& p : hf.pos) hmax = std::max(hmax, p.w);
+            for (auto& p : hd.pos) hmax = std::max(hmax, p.w);
+            const int k = (int)std::floor(std::log2(std::ldexp(1.0, 30) / (8.0 * hmax)));
+            q = (float)std::ldexp(1.0, -k);
+            invq = std::ldexp(1.0, k);
         }
         // dummies: sort once into cell order (initializeBoundaryCondition, WCSPHSolver.h:29-110)
         if (nd > 0) {
@@ -939,7 +1009,9 @@ struct SphScene {
             }
             dvelf.alloc(nd, s, false); dstf.alloc(nd, s, false); dnormf.alloc(nd, s, false);
             k_sph_shadow<<<grid_for(nd, 256), 256, 0, s>>>(nd, dvel.p, dst.p, dnorm.p, dvelf.p, dstf.p, dnormf.p);
-            g_launches += 1;
+            dposq.alloc(nd, s, false);
+            k_sph_fix<<<grid_for(nd, 256), 256, 0, s>>>(nd, dpos.p, gd.mn, invq, dposq.p);
+            g_launches += 2;
             DEMSPH_LAUNCH_CHECK();
         } else {
             dCells.build(nullptr, 0, s);
@@ -1060,6 +1132,7 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         d.posOut = s.pos[s.P ^ 1].p;
         d.velOut = s.vel[s.Vv ^ 1].p;
         d.velfOut = s.velf[s.Vv ^ 1].p;
+        d.posqOut = s.posq[s.P ^ 1].p;
         if (s.precision == DEMSPH_PRECISION_FP64)
             k_sph_accel<double><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
         else
