@@ -51,7 +51,9 @@ extern "C" {
 #define DEMSPH_PRECISION_MIXED 1 /* FP32 force laws, FP64 state            */
 
 typedef struct demsph_dem_scene* demsph_dem_t;
+typedef struct demsph_dem_member* demsph_dem_member_t;
 typedef struct demsph_sph_scene* demsph_sph_t;
+typedef struct demsph_sph_member* demsph_sph_member_t;
 
 const char* demsph_last_error(void);
 const char* demsph_version(void);
@@ -162,16 +164,33 @@ int demsph_dem_import_springs(demsph_dem_t s, long n, const int* objectPointed, 
  * scene's state moves between device scenes (batching). */
 int demsph_dem_import_wall_springs(demsph_dem_t s, long n, const int* ball, const int* triangle,
                                    const double* sliding, const double* rolling, const double* torsion);
-/* No counterpart in the reference (batching).  Copies the state of balls
- * carried over from scene src into scene dst on the device: for destination
- * ball a with srcOf[a] >= 0, its position (plus shift[3a..3a+2]), velocity,
- * angular velocity, its pair row with partner indices plus ballDelta[a], and
- * its ball-triangle row with triangle indices plus triDelta[a].  Arrays have
- * one entry per destination ball.  Partners must move with the ball (one
- * batch member's balls keep their relative order), and dst must have been
- * initialised with the same material / spring configuration. */
-int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf, const int* ballDelta,
-                            const int* triDelta, const double* shift);
+/* No counterpart in the reference (batching).  Copies the state of the
+ * continuing members of a batch from scene src into scene dst on the device.
+ * Member k's balls [srcStart[k], srcStart[k] + num[k]) in src become
+ * [dstStart[k], ...) in dst: positions (plus shift[3k..3k+2]), velocities,
+ * angular velocities, pair rows (partners moved by dstStart[k] - srcStart[k];
+ * partners must lie in the member's own range) and ball-triangle rows
+ * (triangle indices plus triDelta[k]).  dst must have been initialised with
+ * the same material / spring configuration. */
+int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, int count, const int* srcStart, const int* dstStart,
+                            const int* num, const int* triDelta, const double* shift);
+/* Batch members (no counterpart in the reference).  A member is one scene's
+ * balls uploaded once to the device: create, add balls exactly as
+ * demsph_dem_add_balls (no clumps), seal (validates, uploads, drops the host
+ * copy).  demsph_dem_assemble_balls places `count` sealed members' balls into
+ * a scene that has none yet -- member k translated by offsets[3k..3k+2], its
+ * material ids shifted by matOffset[k], member order kept -- as
+ * demsph_dem_add_balls would from the same balls; walls, materials and the
+ * rest are added as usual, then demsph_dem_initialize. */
+int demsph_dem_member_create(demsph_dem_member_t* out, void* stream);
+int demsph_dem_member_destroy(demsph_dem_member_t m);
+int demsph_dem_member_add_balls(demsph_dem_member_t m, long n, const double* position, const double* velocity,
+                                const double* angularVelocity, const double* radius, const double* density,
+                                const int* materialID, int fixed);
+int demsph_dem_member_seal(demsph_dem_member_t m);
+int demsph_dem_member_count(demsph_dem_member_t m, long* n);
+int demsph_dem_assemble_balls(demsph_dem_t s, int count, const demsph_dem_member_t* members, const double* offsets,
+                              const int* matOffset);
 /* getBondedInteraction (DEMSolver.h:1547) fields */
 int demsph_dem_get_bonds(demsph_dem_t s, int* objectPointed, int* objectPointing, int* isBonded, double* normalForce,
                          double* torsionTorque, double* shearForce, double* bendingTorque, double* normal,
@@ -222,12 +241,34 @@ int demsph_sph_num_list_shapes(void);
 int demsph_sph_set_list_shape(demsph_sph_t s, int shape);
 
 /* No counterpart in the reference (batching).  Copies the fluid state of
- * particles carried over from scene src into scene dst on the device: source
- * particle i (caller index) goes to destination particle dstOf[i] (-1: not
- * carried) with its position shifted by shift[3*dstOf[i]..]; velocity,
- * density, pressure and density change are copied.  shift has one entry per
- * destination particle; dst's neighbour lists are rebuilt at its next step. */
-int demsph_sph_copy_members(demsph_sph_t dst, demsph_sph_t src, const int* dstOf, const double* shift);
+ * the continuing members of a batch from scene src into scene dst on the
+ * device: member k's particles with caller ids [srcStart[k], srcStart[k] +
+ * num[k]) in src are ids [dstStart[k], ...) in dst; positions (plus
+ * shift[3k..3k+2]), velocities, density, pressure and density change are
+ * copied.  Source ranges must not overlap.  dst's neighbour lists are rebuilt
+ * at its next step. */
+int demsph_sph_copy_members(demsph_sph_t dst, demsph_sph_t src, int count, const int* srcStart, const int* dstStart,
+                            const int* num, const double* shift);
+
+/* Batch members (no counterpart in the reference).  A member is one scene's
+ * particles uploaded once to the device in the library's record layout:
+ * create, add fluid / dummy particles exactly as demsph_sph_add, seal
+ * (validates, uploads, drops the host copy).  demsph_sph_assemble then
+ * initialises an empty scene from `count` sealed members on the device --
+ * member k's fluid and dummies translated by offsets[3k..3k+2], fluid in
+ * member order (member 0's particles first) -- as demsph_sph_initialize
+ * would from the same particles added in that order.  Members stay valid and
+ * can be assembled again. */
+int demsph_sph_member_create(demsph_sph_member_t* out, void* stream);
+int demsph_sph_member_destroy(demsph_sph_member_t m);
+int demsph_sph_member_add(demsph_sph_member_t m, int dummy, long n, const double* position, const double* velocity,
+                          const double* soundSpeed, const double* spacing, const double* density,
+                          const double* viscosity);
+int demsph_sph_member_seal(demsph_sph_member_t m);
+int demsph_sph_member_count(demsph_sph_member_t m, int dummy, long* n);
+int demsph_sph_assemble(demsph_sph_t s, int count, const demsph_sph_member_t* members, const double* offsets,
+                        const double* minBoundary, const double* maxBoundary, const double* gravity, double timeStep,
+                        int precision);
 
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);

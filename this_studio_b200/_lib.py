@@ -64,7 +64,13 @@ SIGNATURES = {
     "demsph_dem_get_pairs": [_vp, _int, _i, _i, _d, _d, _d, _d, _d],
     "demsph_dem_import_springs": [_vp, _long, _i, _i, _d, _d, _d],
     "demsph_dem_import_wall_springs": [_vp, _long, _i, _i, _d, _d, _d],
-    "demsph_dem_copy_members": [_vp, _vp, _i, _i, _i, _d],
+    "demsph_dem_member_create": [_pvp, _vp],
+    "demsph_dem_member_destroy": [_vp],
+    "demsph_dem_member_add_balls": [_vp, _long, _d, _d, _d, _d, _d, _i, _int],
+    "demsph_dem_member_seal": [_vp],
+    "demsph_dem_member_count": [_vp, _l],
+    "demsph_dem_assemble_balls": [_vp, _int, _pvp, _d, _i],
+    "demsph_dem_copy_members": [_vp, _vp, _int, _i, _i, _i, _i, _d],
     "demsph_dem_get_bonds": [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d],
     "demsph_dem_get_clumps": [_vp, _d, _d, _d, _d],
     "demsph_dem_get_walls": [_vp, _d, _d, _d],
@@ -79,8 +85,14 @@ SIGNATURES = {
     "demsph_sph_tune": [_vp, _int, _i, _d],
     "demsph_sph_num_list_shapes": [],
     "demsph_sph_set_list_shape": [_vp, _int],
-    "demsph_sph_copy_members": [_vp, _vp, _i, _d],
+    "demsph_sph_copy_members": [_vp, _vp, _int, _i, _i, _i, _d],
     "demsph_sph_num": [_vp, _int, _l],
+    "demsph_sph_member_create": [_pvp, _vp],
+    "demsph_sph_member_destroy": [_vp],
+    "demsph_sph_member_add": [_vp, _int, _long, _d, _d, _d, _d, _d, _d],
+    "demsph_sph_member_seal": [_vp],
+    "demsph_sph_member_count": [_vp, _int, _l],
+    "demsph_sph_assemble": [_vp, _int, _pvp, _d, _d, _d, _d, _dbl, _int],
     "demsph_sph_num_pairs": [_vp, _int, _l],
     "demsph_sph_step_index": [_vp, _l, _d],
     "demsph_sph_get": [_vp, _int, _d, _d, _d, _d, _d, _d, _d],

@@ -46,6 +46,7 @@ class Member:
     # capture(); a member with a host state and no device home starts from it
     state: dict = field(default_factory=dict)
     home: object = None        # the device scene holding the member's live state
+    record: object = None      # the scene's device-resident member record (assembly source)
     range: tuple = None        # its particle index range there
     tri_range: tuple = None    # its triangle index range there (DEM)
 
@@ -128,35 +129,37 @@ class DEMBatch(_Batch):
 
     @staticmethod
     def _materials(members):
-        """One material id per distinct material row set; members that share
-        parameters share ids."""
+        """Material ids of the batch: members with the same parameter rows
+        share a block of ids, member ids shifted by the block's offset.
+        Returns per-member offsets and the shifted rows."""
         sig = {}
-        ids = []
+        offs = []
         rows_h, rows_l, rows_b = [], [], []
+        base = 0
         for m in members:
-            key = (tuple(map(tuple, m.scene.hertz)), tuple(map(tuple, m.scene.linear)),
-                   tuple(map(tuple, m.scene.bonded)))
+            sc = m.scene
+            key = (tuple(map(tuple, sc.hertz)), tuple(map(tuple, sc.linear)), tuple(map(tuple, sc.bonded)))
             if key not in sig:
-                mats = sorted({int(v) for v in np.unique(m.scene.material)} |
-                              {int(w["material"]) for w in m.scene.walls} |
-                              {int(r[i]) for r in m.scene.hertz + m.scene.linear + m.scene.bonded for i in (0, 1)})
-                base = sum(len(v[1]) for v in sig.values())
-                remap = {mid: base + k for k, mid in enumerate(mats)}
-                sig[key] = (remap, mats)
-                for r in m.scene.hertz:
-                    rows_h.append((remap[int(r[0])], remap[int(r[1])]) + tuple(r[2:]))
-                for r in m.scene.linear:
-                    rows_l.append((remap[int(r[0])], remap[int(r[1])]) + tuple(r[2:]))
-                for r in m.scene.bonded:
-                    rows_b.append((remap[int(r[0])], remap[int(r[1])]) + tuple(r[2:]))
-            ids.append(sig[key][0])
-        return ids, rows_h, rows_l, rows_b
+                top = max([int(np.max(sc.material))] + [int(w["material"]) for w in sc.walls] +
+                          [int(r[i]) for r in sc.hertz + sc.linear + sc.bonded for i in (0, 1)])
+                sig[key] = base
+                for r in sc.hertz:
+                    rows_h.append((base + int(r[0]), base + int(r[1])) + tuple(r[2:]))
+                for r in sc.linear:
+                    rows_l.append((base + int(r[0]), base + int(r[1])) + tuple(r[2:]))
+                for r in sc.bonded:
+                    rows_b.append((base + int(r[0]), base + int(r[1])) + tuple(r[2:]))
+                base += top + 1
+            offs.append(sig[key])
+        return offs, rows_h, rows_l, rows_b
 
     def prepare(self, members):
-        """Builds and initialises the device scene for `members`: each from
-        its host state if it has one and lives in no device scene, else from
-        its initial scene."""
+        """Builds and initialises the device scene for `members`.  Members
+        without a host state are assembled on the device from their member
+        records (uploaded once, on first use); a member with a host state
+        (and no device home) starts from it."""
         from .scenes import DEMScene
+        from .solvers import DEMMember, DEMSolver
 
         tic = time.perf_counter()
         for m in members:
@@ -166,34 +169,20 @@ class DEMBatch(_Batch):
         cell = max(self.cell_of(m.scene) for m in members)
         boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in members]
         offs = tile_offsets(boxes, gap=2.0 * cell)
-        remaps, rows_h, rows_l, rows_b = self._materials(members)
-        pos, vel, w, rad, den, mat, fixed = [], [], [], [], [], [], []
-        walls = []
+        moffs, rows_h, rows_l, rows_b = self._materials(members)
         lo = np.full(3, np.inf)
         hi = np.full(3, -np.inf)
         ranges, tri_ranges = [], []
         start = 0
         tstart = 0
-        for m, off, remap in zip(members, offs, remaps):
+        walls = []
+        for m, off, mo in zip(members, offs, moffs):
             sc = m.scene
-            st = m.state if m.home is None else {}
             n = sc.position.shape[0]
-            pos.append((st["position"] if "position" in st else sc.position) + off)
-            v0 = sc.velocity if sc.velocity is not None else np.zeros((n, 3))
-            w0 = getattr(sc, "angvel", None)
-            w0 = w0 if w0 is not None else np.zeros((n, 3))
-            vel.append(st.get("velocity", v0))
-            w.append(st.get("angularVelocity", w0))
-            rad.append(sc.radius)
-            den.append(sc.density)
-            lut = np.zeros(max(remap) + 1, np.int32)
-            lut[list(remap)] = list(remap.values())
-            mat.append(lut[np.asarray(sc.material, np.int64)])
-            fixed.append(np.zeros(n, bool) if sc.fixed is None else sc.fixed)
             for wl in sc.walls:
                 d = dict(wl)
                 d["position"] = np.asarray(wl["position"], float) + off
-                d["material"] = remap[int(wl["material"])]
+                d["material"] = mo + int(wl["material"])
                 walls.append(d)
             nt = sum(len(wl["tri0"]) for wl in sc.walls)
             ranges.append((start, start + n))
@@ -203,35 +192,84 @@ class DEMBatch(_Batch):
             lo = np.minimum(lo, np.asarray(sc.minb) + off)
             hi = np.maximum(hi, np.asarray(sc.maxb) + off)
         first = members[0].scene
-        big = DEMScene(name="batch", position=np.concatenate(pos), radius=np.concatenate(rad),
-                       density=np.concatenate(den), material=np.concatenate(mat),
-                       velocity=np.concatenate(vel), fixed=np.concatenate(fixed), hertz=rows_h, linear=rows_l,
-                       bonded=rows_b, walls=walls, minb=tuple(lo), maxb=tuple(hi), gravity=first.gravity,
-                       dt=first.dt)
-        big.angvel = np.concatenate(w)
         si = 1 - self.cur_stream
-        new = S.build_dem(big, self.precision, self.streams[si])
-        # members entering from a host state: their springs, renumbered
-        A, B, SL, RO, TO = [], [], [], [], []
-        WA, WT, WS, WR, WTo = [], [], [], [], []
-        for m, (b0, _), (t0, _) in zip(members, ranges, tri_ranges):
-            if m.home is not None:
-                continue
-            st = m.state
-            if "pairs" in st:
-                p = st["pairs"]
-                A.append(p["a"] + b0); B.append(p["b"] + b0)
-                SL.append(p["sliding"]); RO.append(p["rolling"]); TO.append(p["torsion"])
-            if "wall_pairs" in st:
-                p = st["wall_pairs"]
-                WA.append(p["a"] + b0); WT.append(p["b"] + t0)
-                WS.append(p["sliding"]); WR.append(p["rolling"]); WTo.append(p["torsion"])
-        if A:
-            new.importSprings(np.concatenate(A), np.concatenate(B), np.concatenate(SL), np.concatenate(RO),
-                              np.concatenate(TO))
-        if WA:
-            new.importWallSprings(np.concatenate(WA), np.concatenate(WT), np.concatenate(WS),
-                                  np.concatenate(WR), np.concatenate(WTo))
+        hosted = [m.home is None and "position" in m.state for m in members]
+        if not any(hosted):
+            new = DEMSolver(self.streams[si])
+            for r in rows_h:
+                new.setHertzianPair(*r)
+            for r in rows_l:
+                new.setLinearPair(*r)
+            for r in rows_b:
+                new.setBondedPair(*r)
+            recs = []
+            for m in members:
+                if m.record is None:
+                    sc = m.scene
+                    rec = DEMMember(self.streams[si])
+                    fixed = np.zeros(sc.position.shape[0], bool) if sc.fixed is None else sc.fixed
+                    w0 = getattr(sc, "angvel", None)
+                    # balls in scene order: runs of moving / fixed balls
+                    idx = np.flatnonzero(np.diff(np.r_[-1, fixed.astype(int)]) != 0)
+                    bounds = list(idx) + [len(fixed)]
+                    for a, b in zip(bounds[:-1], bounds[1:]):
+                        sl = slice(a, b)
+                        rec.addBalls(sc.position[sl], None if sc.velocity is None else sc.velocity[sl],
+                                     None if w0 is None else w0[sl], sc.radius[sl], sc.density[sl],
+                                     sc.material[sl], fixed=bool(fixed[a]))
+                    m.record = rec.seal()
+                recs.append(m.record)
+            new.assembleBalls(recs, offs, moffs)
+            for k, wl in enumerate(walls):
+                new.addMeshWall(wl["vertices"], wl["tri0"], wl["tri1"], wl["tri2"], wl["position"],
+                                materialID=wl["material"])
+                if "velocity" in wl:
+                    new.setMeshWallMotion(k, wl["velocity"], wl.get("angularVelocity", (0, 0, 0)))
+            new.initialize(tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
+        else:
+            pos, vel, w, rad, den, mat, fixed = [], [], [], [], [], [], []
+            for m, off, mo, h in zip(members, offs, moffs, hosted):
+                sc = m.scene
+                st = m.state if h else {}
+                n = sc.position.shape[0]
+                pos.append((st["position"] if "position" in st else sc.position) + off)
+                v0 = sc.velocity if sc.velocity is not None else np.zeros((n, 3))
+                w0 = getattr(sc, "angvel", None)
+                w0 = w0 if w0 is not None else np.zeros((n, 3))
+                vel.append(st.get("velocity", v0))
+                w.append(st.get("angularVelocity", w0))
+                rad.append(sc.radius)
+                den.append(sc.density)
+                mat.append(np.asarray(sc.material, np.int32) + mo)
+                fixed.append(np.zeros(n, bool) if sc.fixed is None else sc.fixed)
+            big = DEMScene(name="batch", position=np.concatenate(pos), radius=np.concatenate(rad),
+                           density=np.concatenate(den), material=np.concatenate(mat),
+                           velocity=np.concatenate(vel), fixed=np.concatenate(fixed), hertz=rows_h, linear=rows_l,
+                           bonded=rows_b, walls=walls, minb=tuple(lo), maxb=tuple(hi), gravity=first.gravity,
+                           dt=first.dt)
+            big.angvel = np.concatenate(w)
+            new = S.build_dem(big, self.precision, self.streams[si])
+            # springs of members entering from a host state, renumbered
+            A, B, SL, RO, TO = [], [], [], [], []
+            WA, WT, WS, WR, WTo = [], [], [], [], []
+            for m, h, (b0, _), (t0, _) in zip(members, hosted, ranges, tri_ranges):
+                if not h:
+                    continue
+                st = m.state
+                if "pairs" in st:
+                    p = st["pairs"]
+                    A.append(p["a"] + b0); B.append(p["b"] + b0)
+                    SL.append(p["sliding"]); RO.append(p["rolling"]); TO.append(p["torsion"])
+                if "wall_pairs" in st:
+                    p = st["wall_pairs"]
+                    WA.append(p["a"] + b0); WT.append(p["b"] + t0)
+                    WS.append(p["sliding"]); WR.append(p["rolling"]); WTo.append(p["torsion"])
+            if A:
+                new.importSprings(np.concatenate(A), np.concatenate(B), np.concatenate(SL), np.concatenate(RO),
+                                  np.concatenate(TO))
+            if WA:
+                new.importWallSprings(np.concatenate(WA), np.concatenate(WT), np.concatenate(WS),
+                                      np.concatenate(WR), np.concatenate(WTo))
         self.timing["initialize_s"] += time.perf_counter() - tic
         return Prepared(new, list(members), ranges, tri_ranges, offs, si)
 
@@ -242,19 +280,12 @@ class DEMBatch(_Batch):
         old = self.solver
         carried = self._carried(prep)
         if carried:
-            n = prep.ranges[-1][1]
-            srcOf = np.full(n, -1, np.int32)
-            bdel = np.zeros(n, np.int32)
-            tdel = np.zeros(n, np.int32)
-            shift = np.zeros((n, 3))
-            for m, k in carried:
-                b0, b1 = prep.ranges[k]
-                s0 = m.range[0]
-                srcOf[b0:b1] = np.arange(s0, s0 + (b1 - b0), dtype=np.int32)
-                bdel[b0:b1] = b0 - s0
-                tdel[b0:b1] = prep.tri_ranges[k][0] - m.tri_range[0]
-                shift[b0:b1] = prep.offsets[k] - m.offset
-            prep.solver.copyMembers(old, srcOf, bdel, tdel, shift)
+            ss = [m.range[0] for m, k in carried]
+            ds = [prep.ranges[k][0] for m, k in carried]
+            nn = [m.range[1] - m.range[0] for m, k in carried]
+            td = [prep.tri_ranges[k][0] - m.tri_range[0] for m, k in carried]
+            sh = [prep.offsets[k] - m.offset for m, k in carried]
+            prep.solver.copyMembers(old, ss, ds, nn, td, sh)
         for m, r, t, off in zip(prep.members, prep.ranges, prep.tri_ranges, prep.offsets):
             m.home, m.range, m.tri_range, m.offset = prep.solver, r, t, off
         self.members = prep.members
@@ -297,8 +328,9 @@ class SPHBatch(_Batch):
 
     def prepare(self, members):
         """Builds and initialises the device scene for `members` (see
-        DEMBatch.prepare)."""
-        from .solvers import WCSPHSolver
+        DEMBatch.prepare).  Members without a host state are assembled on the
+        device from their member records (uploaded once, on first use)."""
+        from .solvers import SPHMember, WCSPHSolver
 
         tic = time.perf_counter()
         cell = max(2.0 * 1.3 * m.scene.spacing for m in members)
@@ -313,29 +345,43 @@ class SPHBatch(_Batch):
         for m, off in zip(members, offs):
             sc = m.scene
             n = sc.fluid.shape[0]
-            st = m.state if m.home is None else {}
-            s.addSPHs(st.get("position", sc.fluid) + off, st.get("velocity"), sc.sound_speed, sc.spacing,
-                      sc.density, sc.viscosity)
             ranges.append((start, start + n))
             start += n
             lo = np.minimum(lo, np.asarray(sc.minb) + off)
             hi = np.maximum(hi, np.asarray(sc.maxb) + off)
-        for m, off in zip(members, offs):
-            sc = m.scene
-            s.addDummies(sc.dummy + off, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
         first = members[0].scene
-        s.initialize(tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
-        hosted = [m.home is None and "density" in m.state for m in members]
-        if any(hosted):
-            rho = np.empty(start)
-            p = np.empty(start)
-            dr = np.empty(start)
-            for m, h, (a, b) in zip(members, hosted, ranges):
+        hosted = [m.home is None and "position" in m.state for m in members]
+        if not any(hosted):
+            recs = []
+            for m in members:
+                if m.record is None:
+                    sc = m.scene
+                    r = SPHMember(self.streams[si])
+                    r.addSPHs(sc.fluid, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+                    r.addDummies(sc.dummy, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+                    m.record = r.seal()
+                recs.append(m.record)
+            s.assemble(recs, offs, tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
+        else:
+            for m, h, off in zip(members, hosted, offs):
+                sc = m.scene
                 st = m.state if h else {}
-                rho[a:b] = st.get("density", np.full(b - a, m.scene.density))
-                p[a:b] = st.get("pressure", np.zeros(b - a))
-                dr[a:b] = st.get("densityChange", np.zeros(b - a))
-            s.setSPH(density=rho, pressure=p, densityChange=dr)
+                s.addSPHs(st.get("position", sc.fluid) + off, st.get("velocity"), sc.sound_speed, sc.spacing,
+                          sc.density, sc.viscosity)
+            for m, off in zip(members, offs):
+                sc = m.scene
+                s.addDummies(sc.dummy + off, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+            s.initialize(tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
+            if any(h and "density" in m.state for m, h in zip(members, hosted)):
+                rho = np.empty(start)
+                p = np.empty(start)
+                dr = np.empty(start)
+                for m, h, (a, b) in zip(members, hosted, ranges):
+                    st = m.state if h else {}
+                    rho[a:b] = st.get("density", np.full(b - a, m.scene.density))
+                    p[a:b] = st.get("pressure", np.zeros(b - a))
+                    dr[a:b] = st.get("densityChange", np.zeros(b - a))
+                s.setSPH(density=rho, pressure=p, densityChange=dr)
         self.timing["initialize_s"] += time.perf_counter() - tic
         return Prepared(s, list(members), ranges, [None] * len(members), offs, si)
 
@@ -346,14 +392,11 @@ class SPHBatch(_Batch):
         old = self.solver
         carried = self._carried(prep)
         if carried:
-            dstOf = np.full(old.num(), -1, np.int32)
-            shift = np.zeros((prep.ranges[-1][1], 3))
-            for m, k in carried:
-                a, b = prep.ranges[k]
-                s0 = m.range[0]
-                dstOf[s0:s0 + (b - a)] = np.arange(a, b, dtype=np.int32)
-                shift[a:b] = prep.offsets[k] - m.offset
-            prep.solver.copyMembers(old, dstOf, shift)
+            ss = [m.range[0] for m, k in carried]
+            ds = [prep.ranges[k][0] for m, k in carried]
+            nn = [m.range[1] - m.range[0] for m, k in carried]
+            sh = [prep.offsets[k] - m.offset for m, k in carried]
+            prep.solver.copyMembers(old, ss, ds, nn, sh)
         for m, r, off in zip(prep.members, prep.ranges, prep.offsets):
             m.home, m.range, m.offset = prep.solver, r, off
         self.members = prep.members

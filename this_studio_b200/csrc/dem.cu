@@ -13,6 +13,7 @@
 // Kernels walk balls in cell order (the order array of the last rebuild) so
 // that neighbouring threads touch neighbouring memory.
 #include <algorithm>
+#include <climits>
 #include <array>
 #include <atomic>
 #include <cmath>
@@ -622,36 +623,46 @@ __global__ void k_dem_circumcenters(DemDev d) {
 }
 
 // ------------------------------------------------------------ batching ----
-// Copies the state of continuing batch members from another scene: ball
-// kinematics (translated), pair rows with partner indices shifted by the
-// member's index offset, and ball-triangle rows with triangle indices
-// shifted.  srcOf[a] is the source ball of destination ball a (-1: new ball,
-// keeps its freshly initialised state).
-struct CopyMap {
-    const int* srcOf;
-    const int* ballDelta;  // destination index - source index, per destination ball
-    const int* triDelta;
-    const double4* shift;  // per destination ball
-};
-__global__ void k_dem_copy_members(DemDev dst, DemDev src, CopyMap cm) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= dst.N) return;
-    int s = cm.srcOf[a];
-    if (s < 0) return;
+// Places one batch member's balls at [start, start + n) of the batch arrays,
+// translated by off, with material ids shifted by matOff.
+__global__ void k_dem_place(int n, int start, double3 off, int matOff, const double4* __restrict__ pos,
+                            const double4* __restrict__ vel, const double4* __restrict__ angv,
+                            const int* __restrict__ mat, double4* __restrict__ pos2, double4* __restrict__ vel2,
+                            double4* __restrict__ angv2, int* __restrict__ mat2, int* __restrict__ clump2) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double4 p = pos[t];
+    pos2[start + t] = make_double4(p.x + off.x, p.y + off.y, p.z + off.z, p.w);
+    vel2[start + t] = vel[t];
+    angv2[start + t] = angv[t];
+    mat2[start + t] = mat[t] + matOff;
+    clump2[start + t] = -1;
+}
+
+// Copies the state of one continuing batch member from another scene: its n
+// balls at [srcStart, srcStart + n) there go to [dstStart, dstStart + n) here
+// -- kinematics translated by shift, pair rows with partner indices moved by
+// dstStart - srcStart, ball-triangle rows with triangle indices moved by
+// triDelta.  A partner outside the member's range means inconsistent maps:
+// the entry is dropped and bad_index set.
+__global__ void k_dem_copy_member(DemDev dst, DemDev src, int n, int srcStart, int dstStart, int triDelta,
+                                  double3 shift) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int s = srcStart + t, a = dstStart + t;
+    const int bd = dstStart - srcStart;
     double4 p = src.pos[s];
-    double4 sh = cm.shift[a];
-    dst.pos[a] = make_double4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
+    dst.pos[a] = make_double4(p.x + shift.x, p.y + shift.y, p.z + shift.z, p.w);
     dst.vel[a] = src.vel[s];
     dst.angv[a] = src.angv[s];
     dst.force[a] = src.force[s];
     dst.torque[a] = src.torque[s];
-    int bd = cm.ballDelta[a];
     int c = src.pcnt[s];
     int kept = 0;
     for (int k = 0; k < c; k++) {
         size_t so = (size_t)k * src.N + s, dO = (size_t)kept * dst.N + a;
         int j = src.pj[so] + bd;
-        if (j < 0 || j >= dst.N) {  // a partner outside the batch: the maps were inconsistent
+        if (j < dstStart || j >= dstStart + n) {
             atomicExch(&dst.status->bad_index, 1);
             continue;
         }
@@ -663,17 +674,16 @@ __global__ void k_dem_copy_members(DemDev dst, DemDev src, CopyMap cm) {
     }
     dst.pcnt[a] = kept;
     if (dst.nTri && src.nTri && src.wcnt) {
-        int td = cm.triDelta[a];
         int cw = src.wcnt[s];
         kept = 0;
         for (int k = 0; k < cw; k++) {
             size_t so = (size_t)k * src.N + s, dO = (size_t)kept * dst.N + a;
-            int t = src.wtj[so] + td;
-            if (t < 0 || t >= dst.nTri) {
+            int tr = src.wtj[so] + triDelta;
+            if (tr < 0 || tr >= dst.nTri) {
                 atomicExch(&dst.status->bad_index, 1);
                 continue;
             }
-            dst.wtj[dO] = t;
+            dst.wtj[dO] = tr;
             dst.wS[dO] = src.wS[so];
             if (dst.roll) dst.wR[dO] = src.wR[so];
             if (dst.tors) dst.wT[dO] = src.wT[so];
@@ -749,7 +759,10 @@ struct DemScene {
     DBuf<double4> fconst;
     DBuf<DevStatus> status;
 
-    int N() const { return (int)hPos.size(); }
+    int nB = 0;                // balls (the host arrays' size until a batch assembly)
+    bool assembled = false;    // balls placed on the device from member records
+    double assembledRmax = 0;  // their largest radius
+    int N() const { return nB; }
 
     DemDev dev(bool withOld) {
         DemDev d{};
@@ -1082,24 +1095,27 @@ struct DemScene {
     }
 
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
-        if (hPos.empty()) throw Status(DEMSPH_ERR_SCENE, "the number of particles is equal to 0");
+        if (N() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of particles is equal to 0");
         if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
-        for (auto& p : hPos) {
-            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
-                throw Status(DEMSPH_ERR_SCENE, "ball with non-finite position or non-positive radius");
+        double cell = 0;
+        if (!assembled) {
+            for (auto& p : hPos) {
+                if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
+                    throw Status(DEMSPH_ERR_SCENE, "ball with non-finite position or non-positive radius");
+            }
+            pos.upload(hPos, s); vel.upload(hVel, s); angv.upload(hAngv, s);
+            mat.upload(hMat, s); clump.upload(hClump, s);
+            for (auto& p : hPos) cell = std::max(cell, p.w * 2.0);
+        } else {
+            cell = 2.0 * assembledRmax;
         }
         precision = prec;
         gmin = mn; gmax = mx; gravity = g; dt = timeStep;
         build_materials();
         int n = N();
-        pos.upload(hPos, s); vel.upload(hVel, s); angv.upload(hAngv, s);
-        std::vector<double4> z(n, make_double4(0, 0, 0, 0));
-        force.upload(z, s); torque.upload(z, s); forceA.upload(z, s); torqueA.upload(z, s);
-        mat.upload(hMat, s); clump.upload(hClump, s);
+        force.alloc(n, s, true); torque.alloc(n, s, true); forceA.alloc(n, s, true); torqueA.alloc(n, s, true);
         status.alloc(1, s, true);
         // grids (DEMSolver.h:245-263)
-        double cell = 0;
-        for (auto& p : hPos) cell = std::max(cell, p.w * 2.0);
         GridDesc bg{};
         if (!grid_set(bg, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
         ballCells.setup(bg, n, s);
@@ -1224,7 +1240,7 @@ int demsph_dem_add_balls(demsph_dem_t h, long n, const double* pos, const double
     return guarded([&] {
         SCENE_CHECK(h);
         DemScene& s = h->sc;
-        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "balls must be added before initialisation");
+        if (s.ready || s.assembled) throw Status(DEMSPH_ERR_INVALID, "balls must be added before initialisation");
         if (n < 0 || (n > 0 && (!pos || !rad || !mat))) throw Status(DEMSPH_ERR_INVALID, "missing ball arrays");
         for (long i = 0; i < n; i++) {
             double r = rad[i];
@@ -1239,6 +1255,119 @@ int demsph_dem_add_balls(demsph_dem_t h, long n, const double* pos, const double
             s.hMat.push_back(mat[i]);
             s.hClump.push_back(clump ? clump[i] : -1);
         }
+        s.nB = (int)s.hPos.size();
+    });
+}
+// ------------------------------------------------------ batch members ----
+// One scene's balls uploaded once to the device in the library's record
+// layout, from which batch scenes are assembled on the device.
+struct demsph_dem_member {
+    cudaStream_t s = 0;
+    std::vector<double4> hPos, hVel, hAngv;  // staging until sealed
+    std::vector<int> hMat;
+    bool sealed = false;
+    int n = 0, matMax = -1;
+    double rmax = 0;
+    DBuf<double4> pos, vel, angv;
+    DBuf<int> mat;
+};
+int demsph_dem_member_create(demsph_dem_member_t* out, void* stream) {
+    return guarded([&] {
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        auto* m = new demsph_dem_member();
+        m->s = (cudaStream_t)stream;
+        *out = m;
+    });
+}
+int demsph_dem_member_destroy(demsph_dem_member_t m) {
+    return guarded([&] {
+        if (!m) return;
+        cudaStream_t s = m->s;
+        delete m;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int demsph_dem_member_add_balls(demsph_dem_member_t m, long n, const double* pos, const double* vel, const double* w,
+                                const double* rad, const double* dens, const int* mat, int fixed) {
+    return guarded([&] {
+        if (!m) throw Status(DEMSPH_ERR_INVALID, "null member handle");
+        if (m->sealed) throw Status(DEMSPH_ERR_INVALID, "member already sealed");
+        if (n < 0 || (n > 0 && (!pos || !rad || !mat))) throw Status(DEMSPH_ERR_INVALID, "missing ball arrays");
+        for (long i = 0; i < n; i++) {
+            double r = rad[i];
+            double im = 0.0;
+            if (!fixed) {
+                double mass = 4. / 3. * r * r * r * kPi * (dens ? dens[i] : 0.0);
+                if (mass > 0.0) im = 1.0 / mass;
+            }
+            m->hPos.push_back(d4(ld3(pos, i), r));
+            m->hVel.push_back(d4(fixed || !vel ? mk3(0, 0, 0) : ld3(vel, i), im));
+            m->hAngv.push_back(d4(fixed || !w ? mk3(0, 0, 0) : ld3(w, i), 0));
+            m->hMat.push_back(mat[i]);
+        }
+    });
+}
+int demsph_dem_member_seal(demsph_dem_member_t m) {
+    return guarded([&] {
+        if (!m) throw Status(DEMSPH_ERR_INVALID, "null member handle");
+        if (m->sealed) return;
+        if (m->hPos.empty()) throw Status(DEMSPH_ERR_SCENE, "the number of particles is equal to 0");
+        for (auto& p : m->hPos) {
+            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
+                throw Status(DEMSPH_ERR_SCENE, "ball with non-finite position or non-positive radius");
+            m->rmax = std::max(m->rmax, p.w);
+        }
+        for (int v : m->hMat) {
+            if (v < 0) throw Status(DEMSPH_ERR_SCENE, "negative material index");
+            m->matMax = std::max(m->matMax, v);
+        }
+        m->n = (int)m->hPos.size();
+        m->pos.upload(m->hPos, m->s); m->vel.upload(m->hVel, m->s); m->angv.upload(m->hAngv, m->s);
+        m->mat.upload(m->hMat, m->s);
+        DEMSPH_CUDA(cudaStreamSynchronize(m->s));
+        m->hPos = {}; m->hVel = {}; m->hAngv = {}; m->hMat = {};
+        m->sealed = true;
+    });
+}
+int demsph_dem_member_count(demsph_dem_member_t m, long* n) {
+    return guarded([&] {
+        if (!m || !n) throw Status(DEMSPH_ERR_INVALID, "null argument");
+        *n = m->sealed ? m->n : (long)m->hPos.size();
+    });
+}
+int demsph_dem_assemble_balls(demsph_dem_t h, int count, const demsph_dem_member_t* members, const double* offsets,
+                              const int* matOffset) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready || s.assembled || !s.hPos.empty())
+            throw Status(DEMSPH_ERR_INVALID, "assemble needs a scene without balls");
+        if (count < 1 || !members || !offsets || !matOffset) throw Status(DEMSPH_ERR_INVALID, "no members");
+        long n = 0;
+        double rmax = 0;
+        for (int k = 0; k < count; k++) {
+            const demsph_dem_member* m = members[k];
+            if (!m || !m->sealed) throw Status(DEMSPH_ERR_NOT_READY, "member not sealed");
+            if (matOffset[k] < 0) throw Status(DEMSPH_ERR_INVALID, "negative material offset");
+            n += m->n;
+            rmax = std::max(rmax, m->rmax);
+        }
+        if (n > INT_MAX / 64) throw Status(DEMSPH_ERR_INVALID, "batch too large");
+        s.nB = (int)n;
+        s.pos.alloc(n, s.s, false); s.vel.alloc(n, s.s, false); s.angv.alloc(n, s.s, false);
+        s.mat.alloc(n, s.s, false); s.clump.alloc(n, s.s, false);
+        int b0 = 0;
+        for (int k = 0; k < count; k++) {
+            const demsph_dem_member* m = members[k];
+            k_dem_place<<<grid_for(m->n, 256), 256, 0, s.s>>>(m->n, b0, ld3(offsets, k), matOffset[k], m->pos.p,
+                                                             m->vel.p, m->angv.p, m->mat.p, s.pos.p, s.vel.p,
+                                                             s.angv.p, s.mat.p, s.clump.p);
+            b0 += m->n;
+        }
+        g_launches += count;
+        DEMSPH_LAUNCH_CHECK();
+        s.assembled = true;
+        s.assembledRmax = rmax;
     });
 }
 int demsph_dem_add_clump(demsph_dem_t h, long np, const double* pts, const double* rad, const double* centroid,
@@ -1246,7 +1375,7 @@ int demsph_dem_add_clump(demsph_dem_t h, long np, const double* pts, const doubl
     return guarded([&] {
         SCENE_CHECK(h);
         DemScene& s = h->sc;
-        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "clumps must be added before initialisation");
+        if (s.ready || s.assembled) throw Status(DEMSPH_ERR_INVALID, "clumps must be added before initialisation");
         int cid = (int)s.hCpos.size();
         int ps = s.N(), pe = ps + (int)np;
         double3 c = ld3(centroid, 0), v = ld3(vel, 0), ww = ld3(w, 0);
@@ -1283,6 +1412,7 @@ int demsph_dem_add_clump(demsph_dem_t h, long np, const double* pts, const doubl
         s.hCinvIb.push_back(make_double4(ixz, iyz, 0, 0));
         s.hCinvm.push_back(im);
         s.hCpeb.push_back(make_int2(ps, pe));
+        s.nB = (int)s.hPos.size();
     });
 }
 int demsph_dem_add_mesh_wall(demsph_dem_t h, long nv, const double* verts, long nt, const int* i0, const int* i1,
@@ -1426,7 +1556,7 @@ int demsph_dem_get_balls(demsph_dem_t h, double* pos, double* vel, double* w, do
     return guarded([&] {
         SCENE_CHECK(h);
         DemScene& s = h->sc;
-        if (!s.ready) {
+        if (!s.ready && !s.assembled) {
             for (int i = 0; i < s.N(); i++) {
                 if (pos) st3(pos, i, xyz(s.hPos[i]));
                 if (vel) st3(vel, i, xyz(s.hVel[i]));
@@ -1443,24 +1573,43 @@ int demsph_dem_get_balls(demsph_dem_t h, double* pos, double* vel, double* w, do
             DEMSPH_CUDA(cudaStreamSynchronize(s.s));
             for (int i = 0; i < s.N(); i++) st3(o, i, xyz(a[i]));
         };
-        get(s.pos, pos); get(s.vel, vel); get(s.angv, w); get(s.force, force); get(s.torque, torque);
+        get(s.pos, pos); get(s.vel, vel); get(s.angv, w);
+        if (s.ready) {
+            get(s.force, force); get(s.torque, torque);
+        } else {
+            for (int i = 0; i < s.N(); i++) {
+                if (force) st3(force, i, mk3(0, 0, 0));
+                if (torque) st3(torque, i, mk3(0, 0, 0));
+            }
+        }
     });
 }
 int demsph_dem_set_balls(demsph_dem_t h, const double* pos, const double* vel, const double* w) {
     return guarded([&] {
         SCENE_CHECK(h);
         DemScene& s = h->sc;
-        for (int i = 0; i < s.N(); i++) {
-            if (pos) { double3 p = ld3(pos, i); s.hPos[i].x = p.x; s.hPos[i].y = p.y; s.hPos[i].z = p.z; }
-            if (vel) { double3 p = ld3(vel, i); s.hVel[i].x = p.x; s.hVel[i].y = p.y; s.hVel[i].z = p.z; }
-            if (w) { double3 p = ld3(w, i); s.hAngv[i].x = p.x; s.hAngv[i].y = p.y; s.hAngv[i].z = p.z; }
+        if (!s.ready && !s.assembled) {
+            for (int i = 0; i < s.N(); i++) {
+                if (pos) { double3 p = ld3(pos, i); s.hPos[i].x = p.x; s.hPos[i].y = p.y; s.hPos[i].z = p.z; }
+                if (vel) { double3 p = ld3(vel, i); s.hVel[i].x = p.x; s.hVel[i].y = p.y; s.hVel[i].z = p.z; }
+                if (w) { double3 p = ld3(w, i); s.hAngv[i].x = p.x; s.hAngv[i].y = p.y; s.hAngv[i].z = p.z; }
+            }
+            return;
         }
-        if (s.ready) {
-            if (pos) s.pos.upload(s.hPos, s.s);
-            if (vel) s.vel.upload(s.hVel, s.s);
-            if (w) s.angv.upload(s.hAngv, s.s);
+        // on the device: replace xyz, keep w (radius / inverse mass)
+        std::vector<double4> a;
+        auto put = [&](DBuf<double4>& b, const double* in) {
+            if (!in) return;
+            b.download(a, s.s);
             DEMSPH_CUDA(cudaStreamSynchronize(s.s));
-        }
+            for (int i = 0; i < s.N(); i++) {
+                double3 p = ld3(in, i);
+                a[i].x = p.x; a[i].y = p.y; a[i].z = p.z;
+            }
+            DEMSPH_CUDA(cudaMemcpyAsync(b.p, a.data(), a.size() * sizeof(double4), cudaMemcpyHostToDevice, s.s));
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        };
+        put(s.pos, pos); put(s.vel, vel); put(s.angv, w);
     });
 }
 
@@ -1577,8 +1726,8 @@ int demsph_dem_import_wall_springs(demsph_dem_t h, long n, const int* ball, cons
         import_rows(h->sc, 1, n, ball, tri, sl, ro, to);
     });
 }
-int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf, const int* ballDelta,
-                            const int* triDelta, const double* shift) {
+int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, int count, const int* srcStart, const int* dstStart,
+                            const int* num, const int* triDelta, const double* shift) {
     return guarded([&] {
         SCENE_CHECK(dst);
         SCENE_CHECK(src);
@@ -1588,19 +1737,14 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf
         if (!s.havePairs || !d.havePairs) throw Status(DEMSPH_ERR_NOT_READY, "scene has no pair list");
         if (d.roll != s.roll || d.tors != s.tors)
             throw Status(DEMSPH_ERR_INVALID, "source and destination differ in rolling / torsion springs");
-        const int n = d.N();
-        for (int a = 0; a < n; a++)
-            if (srcOf[a] < -1 || srcOf[a] >= s.N()) throw Status(DEMSPH_ERR_INVALID, "source ball index out of range");
+        if (count < 0 || (count > 0 && (!srcStart || !dstStart || !num || !triDelta || !shift)))
+            throw Status(DEMSPH_ERR_INVALID, "missing member tables");
+        for (int k = 0; k < count; k++)
+            if (num[k] < 0 || srcStart[k] < 0 || dstStart[k] < 0 || srcStart[k] + num[k] > s.N() ||
+                dstStart[k] + num[k] > d.N())
+                throw Status(DEMSPH_ERR_INVALID, "member range out of bounds");
         // the rows keep their counts, so give the destination at least the source's capacities
         d.grow(s.K, 0, s.haveWallRows ? s.KT : 0);
-        std::vector<double4> sh(n);
-        for (int a = 0; a < n; a++) sh[a] = make_double4(shift[3 * a], shift[3 * a + 1], shift[3 * a + 2], 0);
-        DBuf<int> so, bd, td;
-        DBuf<double4> shd;
-        so.upload(std::vector<int>(srcOf, srcOf + n), d.s);
-        bd.upload(std::vector<int>(ballDelta, ballDelta + n), d.s);
-        td.upload(std::vector<int>(triDelta, triDelta + n), d.s);
-        shd.upload(sh, d.s);
         // the source's work must be finished before the destination reads it
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         d.clear_status();
@@ -1608,12 +1752,17 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, const int* srcOf
         if (!d.haveWallRows || d.hTris.empty()) dd.nTri = 0;
         DemDev sd = s.dev(false);
         if (!s.haveWallRows) sd.wcnt = nullptr;
-        k_dem_copy_members<<<grid_for(n, 128), 128, 0, d.s>>>(dd, sd, CopyMap{so.p, bd.p, td.p, shd.p});
-        d.launch_count(1);
+        for (int k = 0; k < count; k++) {
+            if (num[k] == 0) continue;
+            k_dem_copy_member<<<grid_for(num[k], 128), 128, 0, d.s>>>(dd, sd, num[k], srcStart[k], dstStart[k],
+                                                                     triDelta[k], ld3(shift, k));
+            d.launch_count(1);
+        }
         DEMSPH_LAUNCH_CHECK();
         DevStatus cs = d.read_status();
-        if (cs.bad_index) throw Status(DEMSPH_ERR_INVALID, "a carried pair partner or triangle left the batch");
+        if (cs.bad_index) throw Status(DEMSPH_ERR_INVALID, "a carried pair partner or triangle left its member");
         // reverse lists for the copied rows
+        const int n = d.N();
         DEMSPH_CUDA(cudaMemsetAsync(d.rcnt.p, 0, sizeof(int) * n, d.s));
         DemDev dr = d.dev(false);
         k_dem_reverse<<<grid_for(n, 256), 256, 0, d.s>>>(dr);

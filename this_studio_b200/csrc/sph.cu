@@ -12,6 +12,7 @@
 //   dummy  pos | vel | st (c,nu,rho0,-) | normal : double4, sorted once.
 //   lists  ELL, column-major: nb[k*N + i] = k-th neighbour of fluid i.
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cmath>
 #include <memory>
@@ -155,6 +156,44 @@ __global__ void k_sph_shadow(int n, const double4* __restrict__ a, const double4
     af[t] = f4(a[t]);
     bf[t] = f4(b[t]);
     if (c) cf[t] = f4(c[t]);
+}
+
+__global__ void k_iota(int n, int* __restrict__ a) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] = t;
+}
+// Copies one batch member's particles to [start, start + n) of the batch
+// arrays, translated by off: (pos, vel, st) records and, for fluid, rho0 and
+// a zero density change; for dummies `extra` is the dummy density.
+__global__ void k_sph_place(int n, int start, double3 off, const double4* __restrict__ pos,
+                            const double4* __restrict__ vel, const double4* __restrict__ st,
+                            const double* __restrict__ extra, double4* __restrict__ pos2, double4* __restrict__ vel2,
+                            double4* __restrict__ st2, double* __restrict__ extra2, double* __restrict__ zero2) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double4 p = pos[t];
+    pos2[start + t] = make_double4(p.x + off.x, p.y + off.y, p.z + off.z, p.w);
+    vel2[start + t] = vel[t];
+    st2[start + t] = st[t];
+    extra2[start + t] = extra[t];
+    if (zero2) zero2[start + t] = 0.0;
+}
+// Puts the dummies into cell order (sorted[t] = caller index of slot t).
+__global__ void k_sph_dummy_gather(int nd, const int* __restrict__ sorted, const double4* __restrict__ tp,
+                                   const double4* __restrict__ tv, const double4* __restrict__ ts,
+                                   const double* __restrict__ trh, double3 origin, double4* __restrict__ dpos,
+                                   double4* __restrict__ dvel, double4* __restrict__ dst, double* __restrict__ drh,
+                                   float4* __restrict__ dposf, int* __restrict__ did) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd) return;
+    const int o = sorted[t];
+    const double4 p = tp[o];
+    dpos[t] = p;
+    dvel[t] = tv[o];
+    dst[t] = ts[o];
+    drh[t] = trh[o];
+    dposf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
+    did[t] = o;
 }
 
 // Permutes the fluid into this step's cell order.
@@ -638,23 +677,36 @@ __global__ void k_sph_dummy_normals(int nd, GridDesc g, const int* __restrict__ 
     dnorm[i] = (len2(th) > 1.e-10) ? d4(th / len(th), 0) : make_double4(0, 0, 0, 0);
 }
 
-// Copies continuing batch members' fluid state from another scene.  For the
-// source particle at sorted slot t with caller id i, dstOf[i] is its caller id
-// in the destination (-1: retired); dstSlot maps destination ids to their
-// current sorted slot.  Positions are translated by the member's shift.
+// Copies continuing batch members' fluid state from another scene.  Member k
+// holds caller ids [srcStart[k], srcStart[k] + num[k]) there (the table is
+// sorted by srcStart) and [dstStart[k], ...) here; for the source particle at
+// sorted slot t, dstSlot maps its destination id to its current slot here.
+// Positions are translated by the member's shift.
 __global__ void k_sph_copy_members(int nsrc, const int* __restrict__ srcId, const double4* __restrict__ spos,
                                    const double4* __restrict__ svel, const double4* __restrict__ sst,
-                                   const double* __restrict__ sdrho, const int* __restrict__ dstOf,
-                                   const int* __restrict__ dstSlot, const double4* __restrict__ shift,
+                                   const double* __restrict__ sdrho, int count, const int* __restrict__ srcStart,
+                                   const int* __restrict__ dstStart, const int* __restrict__ num,
+                                   const double4* __restrict__ shift, const int* __restrict__ dstSlot,
                                    double4* __restrict__ dpos, double4* __restrict__ dvel, double4* __restrict__ dst,
                                    double* __restrict__ ddrho) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nsrc) return;
-    int nid = dstOf[srcId[t]];
-    if (nid < 0) return;
-    int u = dstSlot[nid];
-    double4 p = spos[t];
-    double4 sh = shift[nid];
+    const int id = srcId[t];
+    // last member starting at or before id
+    int lo = 0, hi = count - 1, k = -1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        if (srcStart[mid] <= id) {
+            k = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    if (k < 0 || id >= srcStart[k] + num[k]) return;  // not carried
+    const int u = dstSlot[dstStart[k] + (id - srcStart[k])];
+    const double4 p = spos[t];
+    const double4 sh = shift[k];
     dpos[u] = make_double4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
     dvel[u] = svel[t];
     dst[u] = sst[t];
@@ -700,8 +752,9 @@ struct SphScene {
     DBuf<DevStatus> status;
     bool haveLists = false;
 
-    int N() const { return (int)hf.size(); }
-    int ND() const { return (int)hd.size(); }
+    int nF = 0, nD = 0;  // fluid / dummy counts (the host sets before initialisation)
+    int N() const { return nF; }
+    int ND() const { return nD; }
 
     SphDev dev() {
         SphDev d{};
@@ -905,46 +958,72 @@ struct SphScene {
         if (st2.overflow) grow(st2);
     }
 
+    // Host particle sets -> device scene (WCSPHSolver::initialize, WCSPHSolver.h:578-612).
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
         if (hf.size() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
-        if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
         for (auto& p : hf.pos)
             if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
                 throw Status(DEMSPH_ERR_SCENE, "fluid particle with non-finite position or non-positive h");
-        precision = prec;
-        gravity = g;
-        dt = timeStep;
-        double cell = 0;
-        for (auto& p : hf.pos) cell = std::max(cell, p.w * 2.0);
-        for (auto& p : hd.pos) cell = std::max(cell, p.w * 2.0);
-        {
-            // the same h everywhere, as the list build sees it (FP32)
-            const float h0 = (float)hf.pos[0].w;
-            uniformH = true;
-            for (auto& p : hf.pos) uniformH = uniformH && (float)p.w == h0;
-            for (auto& p : hd.pos) uniformH = uniformH && (float)p.w == h0;
-        }
-        GridDesc gd{};
-        if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
-        status.alloc(1, s, true);
+        double hmax = 0;
+        for (auto& p : hf.pos) hmax = std::max(hmax, p.w);
+        for (auto& p : hd.pos) hmax = std::max(hmax, p.w);
+        // the same h everywhere, as the list build sees it (FP32)
+        const float h0 = (float)hf.pos[0].w;
+        bool uni = true;
+        for (auto& p : hf.pos) uni = uni && (float)p.w == h0;
+        for (auto& p : hd.pos) uni = uni && (float)p.w == h0;
+        nF = (int)hf.size();
+        nD = (int)hd.size();
+        init_grid(mn, mx, g, timeStep, prec, hmax, uni);
         const int n = N(), nd = ND();
-        fCells.setup(gd, n, s);
-        dCells.setup(gd, std::max(nd, 1), s);
-        std::vector<int> ids(n);
-        for (int i = 0; i < n; i++) ids[i] = i;
-        for (int b = 0; b < 2; b++) {
-            pos[b].alloc(n, s, false); vel[b].alloc(n, s, false); st[b].alloc(n, s, false);
-            velf[b].alloc(n, s, false); stf[b].alloc(n, s, false); posq[b].alloc(n, s, false);
-            rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
-        }
-        P = Vv = S = R0 = D = ID = 0;
         auto up4 = [&](DBuf<double4>& b, const std::vector<double4>& h) {
             DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
         };
         up4(pos[0], hf.pos); up4(vel[0], hf.vel); up4(st[0], hf.st);
         DEMSPH_CUDA(cudaMemcpyAsync(rho0[0].p, hf.rho0.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
         DEMSPH_CUDA(cudaMemcpyAsync(drho[0].p, hf.drho.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
-        DEMSPH_CUDA(cudaMemcpyAsync(id[0].p, ids.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        // dummies in caller order: (pos, vel), (c, nu, rho0, 0), rho
+        DBuf<double4> tp, tv, ts;
+        DBuf<double> trh;
+        if (nd > 0) {
+            tp.upload(hd.pos, s); tv.upload(hd.vel, s);
+            std::vector<double4> dst4(nd);
+            std::vector<double> rh(nd);
+            for (int i = 0; i < nd; i++) {
+                dst4[i] = make_double4(hd.st[i].z, hd.st[i].w, hd.rho0[i], 0);
+                rh[i] = hd.st[i].x;
+            }
+            ts.upload(dst4, s);
+            trh.upload(rh, s);
+        }
+        init_finish(tp, tv, ts, trh);
+    }
+
+    // Grid, buffers and the precision constants of a scene of nF fluid and
+    // nD dummy particles (no particle data yet).
+    void init_grid(double3 mn, double3 mx, double3 g, double timeStep, int prec, double hmax, bool uni) {
+        if (nF == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
+        if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
+        if (!(hmax > 0)) throw Status(DEMSPH_ERR_SCENE, "non-positive smoothing length");
+        precision = prec;
+        gravity = g;
+        dt = timeStep;
+        uniformH = uni;
+        const double cell = 2.0 * hmax;
+        GridDesc gd{};
+        if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
+        status.alloc(1, s, true);
+        const int n = N(), nd = ND();
+        fCells.setup(gd, n, s);
+        dCells.setup(gd, std::max(nd, 1), s);
+        for (int b = 0; b < 2; b++) {
+            pos[b].alloc(n, s, false); vel[b].alloc(n, s, false); st[b].alloc(n, s, false);
+            velf[b].alloc(n, s, false); stf[b].alloc(n, s, false); posq[b].alloc(n, s, false);
+            rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
+        }
+        P = Vv = S = R0 = D = ID = 0;
+        k_iota<<<grid_for(n, 256), 256, 0, s>>>(n, id[0].p);
+        g_launches += 1;
         acc.alloc(n, s, true);
         posf.alloc(n, s, true);
         // FP32 prefilter bound: coordinates are stored relative to the grid
@@ -956,44 +1035,26 @@ struct SphScene {
         }
         // fixed-point quantum: the largest power of two with 8 h_max below 2^30 quanta
         {
-            double hmax = 0;
-            for (auto& p : hf.pos) hmax = std::max(hmax, p.w);
-            for (auto& p : hd.pos) hmax = std::max(hmax, p.w);
             const int k = (int)std::floor(std::log2(std::ldexp(1.0, 30) / (8.0 * hmax)));
             q = (float)std::ldexp(1.0, -k);
             invq = std::ldexp(1.0, k);
         }
-        // dummies: sort once into cell order (initializeBoundaryCondition, WCSPHSolver.h:29-110)
+    }
+
+    // With the fluid in pos[0].. and the dummies in caller order in tp/tv/ts/trh:
+    // dummies into cell order (initializeBoundaryCondition, WCSPHSolver.h:29-110),
+    // wall normals, FP32 shadows, list capacities.
+    void init_finish(DBuf<double4>& tp, DBuf<double4>& tv, DBuf<double4>& ts, DBuf<double>& trh) {
+        const int nd = ND();
+        const GridDesc gd = fCells.g;
         if (nd > 0) {
-            DBuf<double4> tp, tv, ts;
-            tp.upload(hd.pos, s); tv.upload(hd.vel, s);
-            std::vector<double4> dst4(nd);
-            std::vector<double> rh(nd);
-            for (int i = 0; i < nd; i++) {
-                dst4[i] = make_double4(hd.st[i].z, hd.st[i].w, hd.rho0[i], 0);
-                rh[i] = hd.st[i].x;
-            }
-            ts.upload(dst4, s);
-            DBuf<double> trh;
-            trh.upload(rh, s);
             dCells.build(tp.p, nd, s);
             g_launches += dCells.launches;
-            std::vector<int> order(nd);
-            DEMSPH_CUDA(cudaMemcpyAsync(order.data(), dCells.sorted.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s));
-            DEMSPH_CUDA(cudaStreamSynchronize(s));
-            std::vector<double4> sp(nd), sv(nd), ss(nd);
-            std::vector<double> sr(nd);
-            for (int t = 0; t < nd; t++) {
-                int o = order[t];
-                sp[t] = hd.pos[o]; sv[t] = hd.vel[o]; ss[t] = dst4[o]; sr[t] = rh[o];
-            }
-            dpos.upload(sp, s); dvel.upload(sv, s); dst.upload(ss, s); drhoD.upload(sr, s);
-            std::vector<float4> spf(nd);
-            for (int t = 0; t < nd; t++)
-                spf[t] = make_float4((float)(sp[t].x - gd.mn.x), (float)(sp[t].y - gd.mn.y), (float)(sp[t].z - gd.mn.z),
-                                     (float)sp[t].w);
-            dposf.upload(spf, s);
-            did.upload(order, s);
+            dpos.alloc(nd, s, false); dvel.alloc(nd, s, false); dst.alloc(nd, s, false); drhoD.alloc(nd, s, false);
+            dposf.alloc(nd, s, false); did.alloc(nd, s, false);
+            k_sph_dummy_gather<<<grid_for(nd, 256), 256, 0, s>>>(nd, dCells.sorted.p, tp.p, tv.p, ts.p, trh.p, gd.mn,
+                                                                 dpos.p, dvel.p, dst.p, drhoD.p, dposf.p, did.p);
+            g_launches += 1;
             dnorm.alloc(nd, s, true);
             for (int attempt = 0; attempt < 8; attempt++) {
                 nbDD.alloc((size_t)nd * KDD, s, false);
@@ -1072,23 +1133,157 @@ int demsph_sph_destroy(demsph_sph_t h) {
         DEMSPH_CUDA(cudaStreamSynchronize(s));
     });
 }
+// addSPH / addDummy (WCSPHSolver.h:520-560): h = 1.3 spacing, m = spacing^3 rho.
+static void add_particles(SphScene::HostSet& t, long n, const double* pos, const double* vel, const double* c,
+                          const double* spacing, const double* dens, const double* visc) {
+    t.pos.reserve(t.pos.size() + n); t.vel.reserve(t.vel.size() + n); t.st.reserve(t.st.size() + n);
+    t.rho0.reserve(t.rho0.size() + n); t.drho.reserve(t.drho.size() + n);
+    for (long i = 0; i < n; i++) {
+        double rho = dens[i], cc = c[i], sp = spacing[i];
+        if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
+        double m = sp * sp * sp * rho;
+        t.pos.push_back(d4(sld3(pos, i), 1.3 * sp));
+        t.vel.push_back(d4(vel ? sld3(vel, i) : mk3(0, 0, 0), m));
+        t.st.push_back(make_double4(rho, 0.0, cc, visc[i]));
+        t.rho0.push_back(rho);
+        t.drho.push_back(0.0);
+    }
+}
 int demsph_sph_add(demsph_sph_t h, int dummy, long n, const double* pos, const double* vel, const double* c,
                    const double* spacing, const double* dens, const double* visc) {
     return guarded([&] {
         SPH_CHECK(h);
         SphScene& s = h->sc;
         if (s.ready) throw Status(DEMSPH_ERR_INVALID, "particles must be added before initialisation");
-        SphScene::HostSet& t = dummy ? s.hd : s.hf;
-        for (long i = 0; i < n; i++) {
-            double rho = dens[i], cc = c[i], sp = spacing[i];
-            if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
-            double m = sp * sp * sp * rho;
-            t.pos.push_back(d4(sld3(pos, i), 1.3 * sp));
-            t.vel.push_back(d4(vel ? sld3(vel, i) : mk3(0, 0, 0), m));
-            t.st.push_back(make_double4(rho, 0.0, cc, visc[i]));
-            t.rho0.push_back(rho);
-            t.drho.push_back(0.0);
+        add_particles(dummy ? s.hd : s.hf, n, pos, vel, c, spacing, dens, visc);
+        s.nF = (int)s.hf.size();
+        s.nD = (int)s.hd.size();
+    });
+}
+
+// ------------------------------------------------------ batch members ----
+// A scene uploaded once to the device in the library's record layout, from
+// which batch scenes are assembled on the device.
+struct demsph_sph_member {
+    cudaStream_t s = 0;
+    SphScene::HostSet hf, hd;  // staging until sealed
+    bool sealed = false;
+    int nf = 0, nd = 0;
+    double hmax = 0;
+    float h0 = 0;
+    bool uni = true;
+    DBuf<double4> fpos, fvel, fst, dpos, dvel, dst;
+    DBuf<double> frho0, drh;
+};
+int demsph_sph_member_create(demsph_sph_member_t* out, void* stream) {
+    return guarded([&] {
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        auto* m = new demsph_sph_member();
+        m->s = (cudaStream_t)stream;
+        *out = m;
+    });
+}
+int demsph_sph_member_destroy(demsph_sph_member_t m) {
+    return guarded([&] {
+        if (!m) return;
+        cudaStream_t s = m->s;
+        delete m;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int demsph_sph_member_add(demsph_sph_member_t m, int dummy, long n, const double* pos, const double* vel,
+                          const double* c, const double* spacing, const double* dens, const double* visc) {
+    return guarded([&] {
+        if (!m) throw Status(DEMSPH_ERR_INVALID, "null member handle");
+        if (m->sealed) throw Status(DEMSPH_ERR_INVALID, "member already sealed");
+        add_particles(dummy ? m->hd : m->hf, n, pos, vel, c, spacing, dens, visc);
+    });
+}
+int demsph_sph_member_seal(demsph_sph_member_t m) {
+    return guarded([&] {
+        if (!m) throw Status(DEMSPH_ERR_INVALID, "null member handle");
+        if (m->sealed) return;
+        if (m->hf.size() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
+        for (auto& p : m->hf.pos)
+            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
+                throw Status(DEMSPH_ERR_SCENE, "fluid particle with non-finite position or non-positive h");
+        m->h0 = (float)m->hf.pos[0].w;
+        for (auto* set : {&m->hf, &m->hd})
+            for (auto& p : set->pos) {
+                m->hmax = std::max(m->hmax, p.w);
+                m->uni = m->uni && (float)p.w == m->h0;
+            }
+        m->nf = (int)m->hf.size();
+        m->nd = (int)m->hd.size();
+        m->fpos.upload(m->hf.pos, m->s); m->fvel.upload(m->hf.vel, m->s); m->fst.upload(m->hf.st, m->s);
+        m->frho0.upload(m->hf.rho0, m->s);
+        if (m->nd > 0) {
+            std::vector<double4> dst4(m->nd);
+            std::vector<double> rh(m->nd);
+            for (int i = 0; i < m->nd; i++) {
+                dst4[i] = make_double4(m->hd.st[i].z, m->hd.st[i].w, m->hd.rho0[i], 0);
+                rh[i] = m->hd.st[i].x;
+            }
+            m->dpos.upload(m->hd.pos, m->s); m->dvel.upload(m->hd.vel, m->s);
+            m->dst.upload(dst4, m->s); m->drh.upload(rh, m->s);
         }
+        DEMSPH_CUDA(cudaStreamSynchronize(m->s));
+        m->hf = SphScene::HostSet{};
+        m->hd = SphScene::HostSet{};
+        m->sealed = true;
+    });
+}
+int demsph_sph_member_count(demsph_sph_member_t m, int dummy, long* n) {
+    return guarded([&] {
+        if (!m || !n) throw Status(DEMSPH_ERR_INVALID, "null argument");
+        *n = m->sealed ? (dummy ? m->nd : m->nf) : (long)(dummy ? m->hd.size() : m->hf.size());
+    });
+}
+int demsph_sph_assemble(demsph_sph_t h, int count, const demsph_sph_member_t* members, const double* offsets,
+                        const double* mn, const double* mx, const double* g, double dt, int prec) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (s.ready || s.hf.size() || s.hd.size()) throw Status(DEMSPH_ERR_INVALID, "assemble needs an empty scene");
+        if (prec != DEMSPH_PRECISION_FP64 && prec != DEMSPH_PRECISION_MIXED)
+            throw Status(DEMSPH_ERR_INVALID, "unknown precision mode");
+        if (count < 1 || !members || !offsets) throw Status(DEMSPH_ERR_INVALID, "no members");
+        long nf = 0, nd = 0;
+        double hmax = 0;
+        bool uni = true;
+        for (int k = 0; k < count; k++) {
+            const demsph_sph_member* m = members[k];
+            if (!m || !m->sealed) throw Status(DEMSPH_ERR_NOT_READY, "member not sealed");
+            nf += m->nf;
+            nd += m->nd;
+            hmax = std::max(hmax, m->hmax);
+            uni = uni && m->uni && m->h0 == members[0]->h0;
+        }
+        if (nf + nd > INT_MAX / 2) throw Status(DEMSPH_ERR_INVALID, "batch too large");
+        s.nF = (int)nf;
+        s.nD = (int)nd;
+        s.init_grid(sld3(mn, 0), sld3(mx, 0), sld3(g, 0), dt, prec, hmax, uni);
+        DBuf<double4> tp, tv, ts;
+        DBuf<double> trh;
+        if (nd > 0) {
+            tp.alloc(nd, s.s, false); tv.alloc(nd, s.s, false); ts.alloc(nd, s.s, false); trh.alloc(nd, s.s, false);
+        }
+        int f0 = 0, d0 = 0;
+        for (int k = 0; k < count; k++) {
+            const demsph_sph_member* m = members[k];
+            const double3 off = sld3(offsets, k);
+            k_sph_place<<<grid_for(m->nf, 256), 256, 0, s.s>>>(m->nf, f0, off, m->fpos.p, m->fvel.p, m->fst.p,
+                                                               m->frho0.p, s.pos[0].p, s.vel[0].p, s.st[0].p,
+                                                               s.rho0[0].p, s.drho[0].p);
+            if (m->nd > 0)
+                k_sph_place<<<grid_for(m->nd, 256), 256, 0, s.s>>>(m->nd, d0, off, m->dpos.p, m->dvel.p, m->dst.p,
+                                                                   m->drh.p, tp.p, tv.p, ts.p, trh.p, nullptr);
+            g_launches += m->nd > 0 ? 2 : 1;
+            f0 += m->nf;
+            d0 += m->nd;
+        }
+        DEMSPH_LAUNCH_CHECK();
+        s.init_finish(tp, tv, ts, trh);
     });
 }
 int demsph_sph_initialize(demsph_sph_t h, const double* mn, const double* mx, const double* g, double dt, int prec) {
@@ -1215,35 +1410,44 @@ int demsph_sph_set_list_shape(demsph_sph_t h, int shape) {
         h->sc.listShape = shape;
     });
 }
-int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, const int* dstOf, const double* shift) {
+int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, int count, const int* srcStart,
+                            const int* dstStart, const int* num, const double* shift) {
     return guarded([&] {
         SPH_CHECK(dsth);
         SPH_CHECK(srch);
         SphScene& d = dsth->sc;
         SphScene& s = srch->sc;
         if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
+        if (count < 0 || (count > 0 && (!srcStart || !dstStart || !num || !shift)))
+            throw Status(DEMSPH_ERR_INVALID, "missing member tables");
         const int ns = s.N(), nd = d.N();
-        std::vector<char> hit(nd, 0);
-        for (int i = 0; i < ns; i++) {
-            int t = dstOf[i];
-            if (t < -1 || t >= nd) throw Status(DEMSPH_ERR_INVALID, "destination particle index out of range");
-            if (t >= 0) {
-                if (hit[t]) throw Status(DEMSPH_ERR_INVALID, "two source particles map to one destination");
-                hit[t] = 1;
-            }
+        std::vector<int> ord(count);
+        for (int k = 0; k < count; k++) {
+            ord[k] = k;
+            if (num[k] < 0 || srcStart[k] < 0 || dstStart[k] < 0 || srcStart[k] + num[k] > ns ||
+                dstStart[k] + num[k] > nd)
+                throw Status(DEMSPH_ERR_INVALID, "member range out of bounds");
         }
-        std::vector<double4> sh(nd);
-        for (int a = 0; a < nd; a++) sh[a] = make_double4(shift[3 * a], shift[3 * a + 1], shift[3 * a + 2], 0);
-        DBuf<int> dOf, slot;
-        DBuf<double4> shd;
-        dOf.upload(std::vector<int>(dstOf, dstOf + ns), d.s);
+        std::sort(ord.begin(), ord.end(), [&](int a, int b) { return srcStart[a] < srcStart[b]; });
+        std::vector<int> ss(count), ds(count), nn(count);
+        std::vector<double4> sh(count);
+        for (int k = 0; k < count; k++) {
+            const int o = ord[k];
+            ss[k] = srcStart[o]; ds[k] = dstStart[o]; nn[k] = num[o];
+            sh[k] = make_double4(shift[3 * o], shift[3 * o + 1], shift[3 * o + 2], 0);
+            if (k > 0 && ss[k] < ss[k - 1] + nn[k - 1]) throw Status(DEMSPH_ERR_INVALID, "member ranges overlap");
+        }
+        if (count == 0) return;
+        DBuf<int> dss, dds, dnn, slot;
+        DBuf<double4> dsh;
+        dss.upload(ss, d.s); dds.upload(ds, d.s); dnn.upload(nn, d.s); dsh.upload(sh, d.s);
         slot.alloc(nd, d.s, false);
-        shd.upload(sh, d.s);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         k_sph_slot_of<<<grid_for(nd, 256), 256, 0, d.s>>>(nd, d.id[d.ID].p, slot.p);
         k_sph_copy_members<<<grid_for(ns, 256), 256, 0, d.s>>>(ns, s.id[s.ID].p, s.pos[s.P].p, s.vel[s.Vv].p,
-                                                              s.st[s.S].p, s.drho[s.D].p, dOf.p, slot.p, shd.p,
-                                                              d.pos[d.P].p, d.vel[d.Vv].p, d.st[d.S].p, d.drho[d.D].p);
+                                                              s.st[s.S].p, s.drho[s.D].p, count, dss.p, dds.p, dnn.p,
+                                                              dsh.p, slot.p, d.pos[d.P].p, d.vel[d.Vv].p, d.st[d.S].p,
+                                                              d.drho[d.D].p);
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
         d.refresh_shadows();

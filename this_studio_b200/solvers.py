@@ -57,6 +57,43 @@ def num_steps(timeStep, maximumTime):
     return int(maximumTime / timeStep) + 1 + 1
 
 
+class DEMMember:
+    """One scene's balls held on the device, from which batch scenes are
+    assembled (DEMSolver.assembleBalls)."""
+
+    def __init__(self, stream=None):
+        self._h = C.c_void_p()
+        call("demsph_dem_member_create", C.byref(self._h), _stream_ptr(stream))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().demsph_dem_member_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def addBalls(self, position, velocity, angularVelocity, radius, density, materialID, fixed=False):
+        p = _f64(position, (-1, 3))
+        n = p.shape[0]
+        v = None if velocity is None else _f64(velocity, (n, 3))
+        w = None if angularVelocity is None else _f64(angularVelocity, (n, 3))
+        r = _f64(np.broadcast_to(radius, (n,)))
+        d = None if density is None else _f64(np.broadcast_to(density, (n,)))
+        m = _i32(np.broadcast_to(materialID, (n,)))
+        call("demsph_dem_member_add_balls", self._h, n, _dp(p), _dp(v), _dp(w), _dp(r), _dp(d), _ip(m), int(fixed))
+
+    def seal(self):
+        call("demsph_dem_member_seal", self._h)
+        return self
+
+    def num(self):
+        n = C.c_long()
+        call("demsph_dem_member_count", self._h, C.byref(n))
+        return n.value
+
+
 class DEMSolver:
     """Spheres, clumps, triangle-mesh walls, linear / Hertz-Mindlin / bonded contact."""
 
@@ -240,13 +277,22 @@ class DEMSolver:
         call("demsph_dem_import_wall_springs", self._h, a.shape[0], _ip(a), _ip(b), _dp(_f64(sliding, (-1, 3))),
              _dp(_f64(rolling, (-1, 3))), _dp(_f64(torsion, (-1, 3))))
 
-    def copyMembers(self, source, srcOf, ballDelta, triDelta, shift):
+    def copyMembers(self, source, srcStart, dstStart, num, triDelta, shift):
         """Device-side carry of continuing batch members from `source` (a
-        DEMSolver): per destination ball, its source ball (-1: keep), the index
-        shifts of its pair partners and wall triangles, and its translation."""
-        n = self.numBalls
-        call("demsph_dem_copy_members", self._h, source._h, _ip(_i32(srcOf)), _ip(_i32(ballDelta)),
-             _ip(_i32(triDelta)), _dp(_f64(shift, (n, 3))))
+        DEMSolver): member k's balls [srcStart[k], +num[k]) there become
+        [dstStart[k], ...) here, triangle indices moved by triDelta[k],
+        positions by shift[k]."""
+        k = len(num)
+        call("demsph_dem_copy_members", self._h, source._h, k, _ip(_i32(srcStart)), _ip(_i32(dstStart)),
+             _ip(_i32(num)), _ip(_i32(triDelta)), _dp(_f64(shift, (k, 3))))
+
+    def assembleBalls(self, members, offsets, matOffsets):
+        """Places sealed DEMMember records' balls into this scene (which has
+        none yet), member k translated by offsets[k], material ids shifted by
+        matOffsets[k]."""
+        arr = (C.c_void_p * len(members))(*[m._h.value for m in members])
+        call("demsph_dem_assemble_balls", self._h, len(members), arr, _dp(_f64(offsets, (len(members), 3))),
+             _ip(_i32(matOffsets)))
 
     def getBondedInteraction(self):
         n = self._n("demsph_dem_num_bonds")
@@ -274,6 +320,47 @@ class DEMSolver:
         call("demsph_dem_get_walls", self._h, _dp(out["position"]), _dp(out["orientation"]),
              _dp(out["vertexGlobal"]))
         return out
+
+
+class SPHMember:
+    """One scene's fluid and dummy particles held on the device, from which
+    batch scenes are assembled (WCSPHSolver.assemble)."""
+
+    def __init__(self, stream=None):
+        self._h = C.c_void_p()
+        call("demsph_sph_member_create", C.byref(self._h), _stream_ptr(stream))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().demsph_sph_member_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _add(self, dummy, position, velocity, soundSpeed, spacing, density, viscosity):
+        p = _f64(position, (-1, 3))
+        n = p.shape[0]
+        v = None if velocity is None else _f64(velocity, (n, 3))
+        b = lambda x: _f64(np.broadcast_to(x, (n,)))
+        call("demsph_sph_member_add", self._h, int(dummy), n, _dp(p), _dp(v), _dp(b(soundSpeed)), _dp(b(spacing)),
+             _dp(b(density)), _dp(b(viscosity)))
+
+    def addSPHs(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(0, position, velocity, soundSpeed, spacing, density, viscosity)
+
+    def addDummies(self, position, velocity, soundSpeed, spacing, density, viscosity):
+        self._add(1, position, velocity, soundSpeed, spacing, density, viscosity)
+
+    def seal(self):
+        call("demsph_sph_member_seal", self._h)
+        return self
+
+    def num(self, dummy=False):
+        n = C.c_long()
+        call("demsph_sph_member_count", self._h, int(dummy), C.byref(n))
+        return n.value
 
 
 class WCSPHSolver:
@@ -363,6 +450,15 @@ class WCSPHSolver:
         call("demsph_sph_set", self._h, _dp(f(position, (n, 3))), _dp(f(velocity, (n, 3))), _dp(f(density, (n,))),
              _dp(f(pressure, (n,))), _dp(f(densityChange, (n,))))
 
+    def assemble(self, members, offsets, minBoundary, maxBoundary, gravity, timeStep, precision="mixed"):
+        """Initialises this (empty) scene on the device from sealed
+        SPHMember records, member k translated by offsets[k]."""
+        arr = (C.c_void_p * len(members))(*[m._h.value for m in members])
+        off = _f64(offsets, (len(members), 3))
+        prec = _lib.PRECISION_MIXED if precision in ("mixed", _lib.PRECISION_MIXED) else _lib.PRECISION_FP64
+        call("demsph_sph_assemble", self._h, len(members), arr, _dp(off), _dp(_v3(minBoundary)),
+             _dp(_v3(maxBoundary)), _dp(_v3(gravity)), float(timeStep), prec)
+
     def tune(self, trials=5):
         """Autotunes the neighbour-list build's block shape on the current
         state; returns (chosen shape, milliseconds per build of each shape)."""
@@ -375,11 +471,13 @@ class WCSPHSolver:
     def setListShape(self, shape):
         call("demsph_sph_set_list_shape", self._h, int(shape))
 
-    def copyMembers(self, source, dstOf, shift):
+    def copyMembers(self, source, srcStart, dstStart, num, shift):
         """Device-side carry of fluid state from `source` (a WCSPHSolver):
-        source particle i goes to particle dstOf[i] (-1: not carried),
-        translated by shift[dstOf[i]]."""
-        call("demsph_sph_copy_members", self._h, source._h, _ip(_i32(dstOf)), _dp(_f64(shift, (self.num(), 3))))
+        member k's caller ids [srcStart[k], +num[k]) there are
+        [dstStart[k], ...) here, positions moved by shift[k]."""
+        k = len(num)
+        call("demsph_sph_copy_members", self._h, source._h, k, _ip(_i32(srcStart)), _ip(_i32(dstStart)),
+             _ip(_i32(num)), _dp(_f64(shift, (k, 3))))
 
     def getPairs(self, which=0):
         """which = 0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy; original indices, CSR order."""
