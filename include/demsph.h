@@ -134,6 +134,12 @@ int demsph_dem_initialize(demsph_dem_t s, const double* minBoundary, const doubl
  * DEMSolver.h:1376-1485): neighbour search every 5th step, two force
  * evaluations and the kick-drift-kick integration per step. */
 int demsph_dem_step(demsph_dem_t s, long numSteps);
+/* No counterpart in the reference.  step() replays the scene's step loop as
+ * CUDA graphs (blocks of 10 steps aligned to the re-sort cadence, captured on
+ * first use and whenever buffers were reallocated); enable = 0 launches every
+ * kernel directly instead.  Both give identical results.  Scenes with a force
+ * ramp (setConstantForce with rampTime > 0) always launch directly. */
+int demsph_dem_set_graphs(demsph_dem_t s, int enable);
 /* Protected step pieces of DEMSolver, exposed for parity checks:
  * neighborSearch (DEMSolver.h:698-777) and calculateBallContactForceTorque
  * (:599-695) followed, when walls != 0, by addTriangleContactForceTorque(dtWall) (:428-597). */
@@ -218,6 +224,10 @@ int demsph_sph_initialize(demsph_sph_t s, const double* minBoundary, const doubl
                           double timeStep, int precision);
 /* numSteps passes of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621). */
 int demsph_sph_step(demsph_sph_t s, long numSteps);
+/* No counterpart in the reference.  step() replays the step loop as CUDA
+ * graphs of two steps; enable = 0 launches every kernel directly.  Both give
+ * identical results. */
+int demsph_sph_set_graphs(demsph_sph_t s, int enable);
 /* Protected step pieces (WCSPHSolver.h:150-358), for parity checks. */
 int demsph_sph_neighbor_search(demsph_sph_t s);
 int demsph_sph_eval_accel(demsph_sph_t s);

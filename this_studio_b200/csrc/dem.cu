@@ -22,6 +22,7 @@
 #include <unordered_map>
 
 #include "cells.cuh"
+#include "graph.cuh"
 #include "dem_physics.cuh"
 
 namespace demsph {
@@ -884,6 +885,7 @@ struct DemScene {
     }
 
     void alloc_pairs() {
+        graph.reset();  // captured kernels hold the old buffers
         size_t n = (size_t)N();
         for (int b = 0; b < 2; b++) {
             pj[b].alloc(n * K, s, true);
@@ -898,6 +900,7 @@ struct DemScene {
         rslot.alloc(n * KR, s, true);
     }
     void alloc_wall_rows() {
+        graph.reset();
         size_t n = (size_t)N();
         for (int b = 0; b < 2; b++) {
             wtj[b].alloc(n * KT, s, true);
@@ -909,6 +912,7 @@ struct DemScene {
     }
     // Capacity growth keeps the k*N + A layout, so the first planes stay valid.
     void grow(int needPairs, int needRev, int needTri) {
+        if (needPairs > K || needRev > KR || needTri > KT) graph.reset();
         size_t n = (size_t)N();
         if (needPairs > K) {
             int nk = needPairs + needPairs / 4 + 1;
@@ -1016,6 +1020,15 @@ struct DemScene {
         force_eval(hdt, walls, dt, true, time - hdt, 1, hdt);
         force_eval(hdt, walls, dt, true, time, 2, hdt);
     }
+    // Ten steps per graph, starting one step after a re-sort: two re-sorts
+    // per replay, so the pair and wall-row buffer indices are back to their
+    // parity.  Only scenes whose step does not depend on the time (no force
+    // ramp) are captured, since the hook time is a kernel argument.
+    GraphSet graph;
+    bool useGraphs = true;
+    static constexpr int kGraphSteps = 10;
+    int index_key() const { return cur | wcur << 1; }
+    bool graphable() const { return useGraphs && !(framp > 0) && ready; }
 
     DevStatus read_status() {
         DevStatus h{};
@@ -1029,7 +1042,6 @@ struct DemScene {
     // Dynamic state copied before a batch of steps so that a capacity
     // overflow can be undone, the lists regrown and the steps replayed.
     struct Snap {
-        std::vector<std::pair<void*, std::vector<char>>> dev;  // unused on the fast path
         std::vector<std::unique_ptr<DBuf<char>>> bufs;
         std::vector<std::pair<void*, size_t>> src;
         long iStep;
@@ -1038,16 +1050,20 @@ struct DemScene {
         bool havePairs, haveWallRows;
         int K, KT;
     };
+    // The snapshot's device copies are kept between calls and reused while
+    // they are large enough, so a step() call allocates nothing after the first.
     template <class T>
     void snap_add(Snap& sn, DBuf<T>& b) {
         if (!b.p || b.n == 0) return;
-        auto c = std::make_unique<DBuf<char>>();
-        c->alloc(b.bytes(), s, false);
-        DEMSPH_CUDA(cudaMemcpyAsync(c->p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
+        const size_t k = sn.src.size();
+        if (k == sn.bufs.size()) sn.bufs.push_back(std::make_unique<DBuf<char>>());
+        DBuf<char>& c = *sn.bufs[k];
+        if (c.n < b.bytes()) c.alloc(b.bytes(), s, false);
+        DEMSPH_CUDA(cudaMemcpyAsync(c.p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
         sn.src.push_back({(void*)&b, b.bytes()});
-        sn.bufs.push_back(std::move(c));
     }
     void take(Snap& sn) {
+        sn.src.clear();
         sn.iStep = iStep; sn.time = time; sn.cur = cur; sn.wcur = wcur; sn.havePairs = havePairs;
         sn.haveWallRows = haveWallRows; sn.K = K; sn.KT = KT;
         snap_add(sn, pos); snap_add(sn, vel); snap_add(sn, angv); snap_add(sn, force); snap_add(sn, torque);
@@ -1066,6 +1082,7 @@ struct DemScene {
         snap_add(sn, wpos); snap_add(sn, wq); snap_add(sn, vglobal); snap_add(sn, tcenter);
         snap_add(sn, cpos); snap_add(sn, cvel); snap_add(sn, cangv); snap_add(sn, cq);
     }
+    Snap snap;
     void restore(Snap& sn) {
         // pair / reverse rows were regrown in place (layout k*N + A), so the
         // saved prefix is copied back into the start of each buffer.
@@ -1077,14 +1094,39 @@ struct DemScene {
         haveWallRows = sn.haveWallRows;
     }
 
+    void steps_graph(long n) {
+        long k = 0;
+        if (graphable()) {
+            for (; k < n && iStep % 5 != 0; k++) step_once();
+            if (n - k >= kGraphSteps) {
+                StepGraph& gr = graph.at(index_key());
+                if (!gr.ready()) {
+                    const long i0 = iStep;
+                    const double t0 = time;
+                    gr.capture(kGraphSteps, s, [&] {
+                        for (int j = 0; j < kGraphSteps; j++) step_once();
+                    });
+                    iStep = i0;
+                    time = t0;
+                }
+                for (; k + kGraphSteps <= n; k += kGraphSteps) {
+                    gr.launch(s);
+                    iStep += kGraphSteps;
+                    time += kGraphSteps * dt;
+                }
+            }
+        }
+        for (; k < n; k++) step_once();
+    }
+
     void run(long n) {
         if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         if (n <= 0) return;
         for (int attempt = 0; attempt < 8; attempt++) {
-            Snap sn;
+            Snap& sn = snap;
             take(sn);
             clear_status();
-            for (long k = 0; k < n; k++) step_once();
+            steps_graph(n);
             DevStatus st = read_status();
             if (!st.overflow) return;
             grow(st.need_pairs, st.need_rev, st.need_aux);
@@ -1095,6 +1137,7 @@ struct DemScene {
     }
 
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
+        graph.reset();
         if (N() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of particles is equal to 0");
         if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
         double cell = 0;
@@ -1452,6 +1495,7 @@ int demsph_dem_set_wall_motion(demsph_dem_t h, int wall, const double* vel, cons
 int demsph_dem_add_bonds(demsph_dem_t h, long n, const int* a0, const int* b0, const double* posHost, long npos) {
     return guarded([&] {
         SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
         DemScene& s = h->sc;
         std::map<std::pair<int, int>, int> have;
         for (auto& e : s.hBab) have[{e.x, e.y}] = 1;
@@ -1476,6 +1520,7 @@ int demsph_dem_add_bonds(demsph_dem_t h, long n, const int* a0, const int* b0, c
 int demsph_dem_set_constant_force(demsph_dem_t h, long n, const double* f, double ramp) {
     return guarded([&] {
         SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
         DemScene& s = h->sc;
         s.hFconst.assign(std::max<long>(n, 0), make_double4(0, 0, 0, 0));
         for (long i = 0; i < n; i++) s.hFconst[i] = d4(ld3(f, i), 0);
@@ -1487,11 +1532,16 @@ int demsph_dem_set_constant_force(demsph_dem_t h, long n, const double* f, doubl
     });
 }
 int demsph_dem_set_global_damping(demsph_dem_t h, double c) {
-    return guarded([&] { SCENE_CHECK(h); h->sc.damp = c; });
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
+        h->sc.damp = c;
+    });
 }
 int demsph_dem_set_buoyancy_drag(demsph_dem_t h, double rho, double cd, const double* g, const double* u, double lvl) {
     return guarded([&] {
         SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
         DemScene& s = h->sc;
         s.buoy = 1; s.brho = rho; s.bcd = cd; s.bg3 = ld3(g, 0); s.bu = ld3(u, 0); s.blevel = lvl;
     });
@@ -1534,6 +1584,13 @@ int demsph_dem_eval_forces(demsph_dem_t h, double dt, int walls, double dtWall) 
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         s.force_eval(dt, walls != 0, dtWall, false, 0.0, 0, 0.0);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_dem_set_graphs(demsph_dem_t h, int enable) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        h->sc.useGraphs = enable != 0;
+        h->sc.graph.reset();
     });
 }
 int demsph_dem_num_balls(demsph_dem_t h, long* n) {
@@ -1716,6 +1773,7 @@ int demsph_dem_import_springs(demsph_dem_t h, long n, const int* a, const int* b
                               const double* to) {
     return guarded([&] {
         SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
         import_rows(h->sc, 0, n, a, b, sl, ro, to);
     });
 }
@@ -1723,6 +1781,7 @@ int demsph_dem_import_wall_springs(demsph_dem_t h, long n, const int* ball, cons
                                    const double* ro, const double* to) {
     return guarded([&] {
         SCENE_CHECK(h);
+        h->sc.graph.reset();  // kernel arguments or buffers change
         import_rows(h->sc, 1, n, ball, tri, sl, ro, to);
     });
 }

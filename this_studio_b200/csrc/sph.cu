@@ -19,6 +19,7 @@
 #include <type_traits>
 
 #include "cells.cuh"
+#include "graph.cuh"
 
 namespace demsph {
 
@@ -776,6 +777,7 @@ struct SphScene {
     }
 
     void alloc_lists() {
+        graph.reset();  // the captured kernels hold the old list buffers
         size_t n = (size_t)N();
         nbF.alloc(n * KF, s, false);
         cntF.alloc(n, s, true);
@@ -861,14 +863,21 @@ struct SphScene {
         S ^= 1;
     }
     // One pass of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621).
-    void step_once() {
-        iStep++;
-        time += dt;
+    void step_body() {
         neighbor_search();
         accel(1);
         density();
         accel(0);
     }
+    void step_once() {
+        iStep++;
+        time += dt;
+        step_body();
+    }
+    // Two steps per graph: every ping-pong index is back to its parity.
+    GraphSet graph;
+    bool useGraphs = true;
+    int index_key() const { return P | Vv << 1 | S << 2 | R0 << 3 | D << 4 | ID << 5; }
 
     // One step with a CUDA event after every phase, on the scene stream:
     // 0 cell sort, 1 permute + lists, 2 accel + kick + drift, 3 continuity + EOS,
@@ -953,7 +962,17 @@ struct SphScene {
         if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         if (n <= 0) return;
         clear_status();
-        for (long k = 0; k < n; k++) step_once();
+        long k = 0;
+        if (useGraphs && n >= 2) {
+            StepGraph& gr = graph.at(index_key());
+            if (!gr.ready()) gr.capture(2, s, [&] { step_body(); step_body(); });
+            for (; k + 2 <= n; k += 2) {
+                gr.launch(s);
+                iStep += 2;
+                time += 2 * dt;
+            }
+        }
+        for (; k < n; k++) step_once();
         DevStatus st2 = read_status();
         if (st2.overflow) grow(st2);
     }
@@ -1005,6 +1024,7 @@ struct SphScene {
         if (nF == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
         if (!(timeStep > 0)) throw Status(DEMSPH_ERR_INVALID, "time step must be positive");
         if (!(hmax > 0)) throw Status(DEMSPH_ERR_SCENE, "non-positive smoothing length");
+        graph.reset();
         precision = prec;
         gravity = g;
         dt = timeStep;
@@ -1393,6 +1413,7 @@ int demsph_sph_tune(demsph_sph_t h, int trials, int* chosen, double* msPerShape)
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         s.listShape = best;
+        s.graph.reset();
         // leave lists built by the chosen shape
         s.launch_lists(s.dev());
         g_launches += 1;
@@ -1403,11 +1424,19 @@ int demsph_sph_tune(demsph_sph_t h, int trials, int* chosen, double* msPerShape)
     });
 }
 int demsph_sph_num_list_shapes(void) { return kNumListShapes; }
+int demsph_sph_set_graphs(demsph_sph_t h, int enable) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        h->sc.useGraphs = enable != 0;
+        h->sc.graph.reset();
+    });
+}
 int demsph_sph_set_list_shape(demsph_sph_t h, int shape) {
     return guarded([&] {
         SPH_CHECK(h);
         if (shape < 0 || shape >= kNumListShapes) throw Status(DEMSPH_ERR_INVALID, "unknown list block shape");
         h->sc.listShape = shape;
+        h->sc.graph.reset();
     });
 }
 int demsph_sph_copy_members(demsph_sph_t dsth, demsph_sph_t srch, int count, const int* srcStart,

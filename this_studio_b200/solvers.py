@@ -286,6 +286,10 @@ class DEMSolver:
         call("demsph_dem_copy_members", self._h, source._h, k, _ip(_i32(srcStart)), _ip(_i32(dstStart)),
              _ip(_i32(num)), _ip(_i32(triDelta)), _dp(_f64(shift, (k, 3))))
 
+    def setGraphs(self, enable=True):
+        """Replay the step loop as CUDA graphs (default) or launch directly."""
+        call("demsph_dem_set_graphs", self._h, int(bool(enable)))
+
     def assembleBalls(self, members, offsets, matOffsets):
         """Places sealed DEMMember records' balls into this scene (which has
         none yet), member k translated by offsets[k], material ids shifted by
@@ -458,6 +462,10 @@ class WCSPHSolver:
         prec = _lib.PRECISION_MIXED if precision in ("mixed", _lib.PRECISION_MIXED) else _lib.PRECISION_FP64
         call("demsph_sph_assemble", self._h, len(members), arr, _dp(off), _dp(_v3(minBoundary)),
              _dp(_v3(maxBoundary)), _dp(_v3(gravity)), float(timeStep), prec)
+
+    def setGraphs(self, enable=True):
+        """Replay the step loop as CUDA graphs (default) or launch directly."""
+        call("demsph_sph_set_graphs", self._h, int(bool(enable)))
 
     def tune(self, trials=5):
         """Autotunes the neighbour-list build's block shape on the current
