@@ -226,7 +226,7 @@ __global__ void k_dem_reverse_order(DemDev d) {
 // (contactKernel.cu:657-681).  The pair force and the B-side torque
 // contribution -(T_c + (r_c - r_B) x F_c) are stored for the B side.
 template <class R>
-__global__ void __launch_bounds__(256) k_dem_pair_forces(DemDev d, double dt) {
+__global__ void __launch_bounds__(128, 4) k_dem_pair_forces(DemDev d, double dt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= d.N) return;
     const int A = d.order[t];
@@ -971,8 +971,8 @@ struct DemScene {
     void force_eval(double dt, bool walls, double dtWall, bool ext, double extTime, int integ, double hdt) {
         DemDev d = dev(false);
         const int n = N();
-        if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 256), 256, 0, s>>>(d, dt);
-        else k_dem_pair_forces<float><<<grid_for(n, 256), 256, 0, s>>>(d, dt);
+        if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
         launch_count(1);
         if (d.nBond) {
             k_dem_bonds<<<grid_for(d.nBond, 128), 128, 0, s>>>(d, dt);

@@ -10,7 +10,7 @@
 //          cell order (double-buffered), so a cell's particles are contiguous
 //          and neighbour gathers stay in L1/L2.
 //   dummy  pos | vel | st (c,nu,rho0,-) | normal : double4, sorted once.
-//   lists  ELL, column-major: nb[k*N + i] = k-th neighbour of fluid i.
+//   lists  ELL, row-major: nb[i*K + k] = k-th neighbour of fluid i.
 #include <algorithm>
 #include <climits>
 #include <atomic>
@@ -354,12 +354,12 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
                 const unsigned hB = __ballot_sync(0xffffffffu, inB);
                 if (hA) {
                     const int k = na + __popc(hA & lt);
-                    if (inA && k < K) nb[(size_t)k * N + i0] = j;
+                    if (inA && k < K) nb[(size_t)i0 * K + k] = j;
                     na += __popc(hA);
                 }
                 if (hB) {
                     const int k = nbc + __popc(hB & lt);
-                    if (inB && k < K) nb[(size_t)k * N + i1] = j;
+                    if (inB && k < K) nb[(size_t)i1 * K + k] = j;
                     nbc += __popc(hB);
                 }
             }
@@ -409,13 +409,25 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
 // row when it fitted (cnt >= 0), otherwise by walking the cell stencil with
 // the list's cutoff test (a row that overflowed its capacity).
 template <class F>
-__device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ nb, int N, int i, int self,
+__device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ nb, int K, int i, int self,
                                                double4 pi, const GridDesc& g, const int* __restrict__ cellStart,
                                                const double4* __restrict__ other, F&& f) {
     const int sub = threadIdx.x & 3;
     if (cnt >= 0) {
-#pragma unroll 2
-        for (int k = sub; k < cnt; k += kQuad) f(nb[(size_t)k * N + i]);
+        // two neighbours per iteration, their row entries loaded one
+        // iteration ahead so the index load is off the gather's critical path
+        const int* __restrict__ row = nb + (size_t)i * K;
+        int k = sub;
+        int j0 = k < cnt ? __ldg(row + k) : -1;
+        int j1 = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
+        for (; k < cnt; k += 2 * kQuad) {
+            const int a = j0, b = j1;
+            const int kn = k + 2 * kQuad;
+            j0 = kn < cnt ? __ldg(row + kn) : -1;
+            j1 = kn + kQuad < cnt ? __ldg(row + kn + kQuad) : -1;
+            f(a);
+            if (b >= 0) f(b);
+        }
         return;
     }
     const double3 ri = xyz(pi);
@@ -511,7 +523,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, nui = (R)s4.w;
     const HConst<R> hk = hconst<R>((R)pi4.w);
     VR acc = v3r<R>(0, 0, 0);
-    quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         VR rij, vj;
         R hj, rhoj, PR, cj, nuj, mj;
         pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
@@ -534,7 +546,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
         acc += (R)2.0 * nuij * dot(-e, dW) * (vi - vj) * mj * inv_rr;
     });
     const VR g = cvt<R>(d.gravity);
-    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
+    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         VR rij, nw, vj;
         R hj, cj, nuj, rho0j, mj;
         pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
@@ -593,7 +605,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z;
     const HConst<R> hk = hconst<R>((R)pi4.w);
     R dRho = (R)0;
-    quad_neighbors(d.cntF[i], d.nbF, d.N, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         VR rij, vj;
         R hj, rhoj, PR, cj, nuj, mj;
         pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
@@ -609,7 +621,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
         dRho += div_r(mj, rhoj) * dot(vi - vs, dW);
     });
     const VR g = cvt<R>(d.gravity);
-    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.N, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
+    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
         VR rij, nw, vj;
         R hj, cj, nuj, rho0j, mj;
         pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
@@ -924,6 +936,7 @@ struct SphScene {
         if (st2.need_pairs > KF) KF = st2.need_pairs + st2.need_pairs / 4 + 1;
         if (st2.need_aux > KD) KD = st2.need_aux + st2.need_aux / 4 + 1;
         alloc_lists();
+        haveLists = false;  // rebuilt by the next neighbour search
     }
 
     // Saved dynamic state for overflow replay.
@@ -1624,7 +1637,6 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
         std::vector<int> didv;
         s.did.download(didv, s.s);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
-        (void)K;
         const std::vector<int>& col = (which == 0) ? rowId : didv;
         // rows emitted in the caller's original order
         std::vector<int> rowOf(rows);
@@ -1636,7 +1648,7 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
             int t = rowOf[o];
             for (int k = 0; k < cnt[t]; k++) {
                 a[w] = o;
-                b[w] = col[nb[(size_t)k * rows + t]];
+                b[w] = col[nb[which == 2 ? (size_t)k * rows + t : (size_t)t * K + k]];
                 w++;
             }
         }
