@@ -123,6 +123,21 @@ def algorithmic_bytes_momentum(nf, nd, first):
     return nf * (96 + 4 + 64 + (32 if first else 0)) + nd * 128
 
 
+def max_over_ranks(torch, dist, ms, device):
+    """The timed region's length as the slowest rank saw it (replicas: every
+    rank times its own scene; the job is done when the last one is)."""
+    if dist is None:
+        return float(ms)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_step, steps, world, ms):
+    """Whole-job throughput: the units all ranks processed / the max-over-ranks time."""
+    return units_per_step * steps * world / (ms / 1e3)
+
+
 def timed_steps(torch, solver, steps, flush):
     """Per-step CUDA-event times (ms) with an L2 flush before each step, outside
     the events."""
@@ -227,11 +242,8 @@ def native(args, rank, world, dist):
     launches = tsb.kernel_launches() - launches0
     clk = clocks.stop()
     total_ms = float(sum(times))
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = nf * args.steps * world / (total_ms / 1e3)
+    total_ms = max_over_ranks(torch, dist, total_ms, dev)
+    value = replica_value(nf, args.steps, world, total_ms)
 
     # per-kernel live timing for the roofline (same stream, events per phase)
     import ctypes as C
