@@ -202,6 +202,21 @@ int demsph_dem_get_bonds(demsph_dem_t s, int* objectPointed, int* objectPointing
                          double* torsionTorque, double* shearForce, double* bendingTorque, double* normal,
                          double* point);
 /* getClump (DEMSolver.h:1543) */
+/* outputBallVTU / outputMeshWallVTU / outputBallInteractionVTU /
+ * outputBondedInteractionVTU / outputBallTriangleInteractionVTU
+ * (DEMSolver.h:908-1370): writes <dir>/ball_NNNN.vtu, triangleWall_NNNN.vtu,
+ * ballInteraction_NNNN.vtu, bondedInteraction_NNNN.vtu and
+ * ballTriangleInteraction_NNNN.vtu (NNNN = frame) for the parts selected in
+ * `what` (DEMSPH_VTU_* bits), in the reference's layout.  Interaction frames
+ * evaluate each listed contact on the current state (zero time increment). */
+#define DEMSPH_VTU_BALLS 1
+#define DEMSPH_VTU_MESH_WALLS 2
+#define DEMSPH_VTU_BALL_INTERACTIONS 4
+#define DEMSPH_VTU_BONDED_INTERACTIONS 8
+#define DEMSPH_VTU_BALL_TRIANGLE_INTERACTIONS 16
+#define DEMSPH_VTU_FLUID 1
+#define DEMSPH_VTU_DUMMIES 2
+int demsph_dem_write_vtu(demsph_dem_t s, const char* dir, long frame, int what);
 int demsph_dem_get_clumps(demsph_dem_t s, double* position, double* velocity, double* angularVelocity,
                           double* orientation);
 /* getMeshWallBody (DEMSolver.h:1545) and vertex global positions */
@@ -279,6 +294,11 @@ int demsph_sph_member_count(demsph_sph_member_t m, int dummy, long* n);
 int demsph_sph_assemble(demsph_sph_t s, int count, const demsph_sph_member_t* members, const double* offsets,
                         const double* minBoundary, const double* maxBoundary, const double* gravity, double timeStep,
                         int precision);
+
+/* outputWCSPHVTU / outputDummyVTU (WCSPHSolver.h:360-520): writes
+ * <dir>/SPH_NNNN.vtu and/or <dir>/dummy_NNNN.vtu (what: DEMSPH_VTU_FLUID,
+ * DEMSPH_VTU_DUMMIES) in the reference's layout. */
+int demsph_sph_write_vtu(demsph_sph_t s, const char* dir, long frame, int what);
 
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);

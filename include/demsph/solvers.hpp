@@ -2,8 +2,8 @@
 // and method names (DEMSolver, DEMSPH/kernel/DEMSolver.h:144-2078;
 // WCSPHSolver, DEMSPH/kernel/WCSPHSolver.h:18-635), header-only.
 //
-// Differences from the reference: solve() writes no VTU files; failures throw
-// demsph::Error instead of exiting; the virtual hooks are configuration
+// Differences from the reference: failures throw demsph::Error instead of
+// exiting; the virtual hooks are configuration
 // (setConstantForce / setGlobalDamping / setBuoyancyDrag, and
 // addBondedInteraction after initialize() for bonded initial contacts).
 #pragma once
@@ -38,6 +38,26 @@ struct SymMatrix {
 // (DEMSolver.h:1988,1380) run numStep + 1 steps.
 inline long solveSteps(double timeStep, double maximumTime) {
     return (long)(size_t)(maximumTime / timeStep) + 2;
+}
+
+// The reference's frame cadence (DEMSolver.h:1984-2046, WCSPHSolver.h:587-621):
+// frame 0 after initialisation; numStep = total - 1, frameInterval = numStep /
+// numFrame (numStep when numFrame is 0, at least 1); after step iStep
+// (1-based) a frame whenever iStep % frameInterval == 0.
+template <class Step, class Write>
+inline void runFrames(long total, size_t numFrame, Step step, Write write) {
+    long numStep = total - 1;
+    long interval = numFrame > 0 ? numStep / (long)numFrame : numStep;
+    if (interval < 1) interval = 1;
+    write(0);
+    long done = 0, frame = 0;
+    while (done < total) {
+        long next = (done / interval + 1) * interval;
+        if (next > total) next = total;
+        step(next - done);
+        done = next;
+        if (done % interval == 0) write(++frame);
+    }
 }
 
 class DEMSolver {
@@ -82,6 +102,7 @@ public:
         check(demsph_dem_add_mesh_wall(h_, (long)vertices.size(), &vertices[0].x, (long)tri0.size(), tri0.data(),
                                        tri1.data(), tri2.data(), &position.x, mat),
               "addMeshWall");
+        walls_ += tri0.empty() ? 0 : 1;
     }
     void setMeshWallMotion(int wall, double3 v, double3 w) {
         check(demsph_dem_set_wall_motion(h_, wall, &v.x, &w.x), "setMeshWallMotion");
@@ -103,11 +124,20 @@ public:
         check(demsph_dem_initialize(h_, &mn.x, &mx.x, &g.x, dt, precision), "initialize");
     }
     void step(long n) { check(demsph_dem_step(h_, n), "step"); }
+    // DEMSolver::solve (DEMSolver.h:1961-2049); VTU frames in `dir` (none when empty).
     void solve(double3 mn, double3 mx, double3 g, double dt, double maximumTime, size_t numFrame,
                const std::string& dir, size_t deviceID = 0, size_t maximumThread = 256) {
-        (void)numFrame; (void)dir; (void)deviceID; (void)maximumThread;
+        (void)deviceID; (void)maximumThread;
         initialize(mn, mx, g, dt);
-        step(solveSteps(dt, maximumTime));
+        const long total = solveSteps(dt, maximumTime);
+        if (dir.empty()) {
+            step(total);
+            return;
+        }
+        const int what = DEMSPH_VTU_BALLS | DEMSPH_VTU_BONDED_INTERACTIONS | DEMSPH_VTU_BALL_INTERACTIONS |
+                         (walls_ ? DEMSPH_VTU_MESH_WALLS | DEMSPH_VTU_BALL_TRIANGLE_INTERACTIONS : 0);
+        runFrames(total, numFrame, [&](long n) { step(n); },
+                  [&](long f) { check(demsph_dem_write_vtu(h_, dir.c_str(), f, what), "writeVTU"); });
     }
     std::vector<double3> getBallPosition() {
         std::vector<double3> p(numBalls_);
@@ -129,6 +159,7 @@ private:
     }
     demsph_dem_t h_ = nullptr;
     long numBalls_ = 0;
+    int walls_ = 0;
 };
 
 class WCSPHSolver {
@@ -148,11 +179,19 @@ public:
         check(demsph_sph_initialize(h_, &mn.x, &mx.x, &g.x, dt, precision), "initialize");
     }
     void step(long n) { check(demsph_sph_step(h_, n), "step"); }
+    // WCSPHSolver::solve (WCSPHSolver.h:567-624); VTU frames in `dir` (none when empty).
     void solve(double3 mn, double3 mx, double3 g, double dt, double maximumTime, size_t numFrame,
                const std::string& dir, size_t deviceID = 0, size_t maximumThread = 256) {
-        (void)numFrame; (void)dir; (void)deviceID; (void)maximumThread;
+        (void)deviceID; (void)maximumThread;
         initialize(mn, mx, g, dt);
-        step(solveSteps(dt, maximumTime));
+        const long total = solveSteps(dt, maximumTime);
+        if (dir.empty()) {
+            step(total);
+            return;
+        }
+        runFrames(total, numFrame, [&](long n) { step(n); }, [&](long f) {
+            check(demsph_sph_write_vtu(h_, dir.c_str(), f, DEMSPH_VTU_FLUID | DEMSPH_VTU_DUMMIES), "writeVTU");
+        });
     }
     std::vector<double3> getSPHPosition() {
         long n = 0;

@@ -10,6 +10,10 @@ reference and writes small fixtures next to it:
 * ``dam_break_f1.npz`` -- frame 1 (step 670) of DEMSPH/damBreak/SPH_*.vtu for
   every 16th fluid particle (scene in DEMSPH/damBreak.cpp): index, position,
   velocity, density, pressure; plus frame-0 positions of the same subset.
+* ``vtu_frame0.json`` -- size and SHA-256 of the reference's frame-0 VTU files
+  of the elasticBounce, damBreak and iceCylinderInteraction scenes (the
+  initial state as the reference writes it), to check the VTU writer and the
+  scene generators byte for byte.
 
 Usage:  python tests/golden/make_golden.py /path/to/reference
 """
@@ -61,6 +65,17 @@ def main(ref):
         density=f1["density"][idx],
         pressure=f1["pressure"][idx],
     )
+    import hashlib
+    import json
+
+    frame0 = {}
+    for rel in ("elasticBounce/ball_0000.vtu", "damBreak/SPH_0000.vtu", "iceCylinderInteraction/ball_0000.vtu",
+                "iceCylinderInteraction/triangleWall_0000.vtu",
+                "iceCylinderInteraction/ballTriangleInteraction_0000.vtu"):
+        data = open(os.path.join(ref, "DEMSPH", rel), "rb").read()
+        frame0[rel] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
+    with open(os.path.join(here, "vtu_frame0.json"), "w") as f:
+        json.dump(frame0, f, indent=1)
     print("wrote fixtures to", here)
 
 

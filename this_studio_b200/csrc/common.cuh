@@ -164,10 +164,10 @@ __host__ __device__ __forceinline__ double3 up(float3 a) { return mk3(a.x, a.y, 
 template <class R> __host__ __device__ __forceinline__ V<R> v3r(R x, R y, R z);
 template <> __host__ __device__ __forceinline__ double3 v3r<double>(double x, double y, double z) { return mk3(x, y, z); }
 template <> __host__ __device__ __forceinline__ float3 v3r<float>(float x, float y, float z) { return make_float3(x, y, z); }
-__device__ __forceinline__ double rsq(double x) { return sqrt(x); }
-__device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
-__device__ __forceinline__ double rlen(double3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
-__device__ __forceinline__ float rlen(float3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+__host__ __device__ __forceinline__ double rsq(double x) { return sqrt(x); }
+__host__ __device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
+__host__ __device__ __forceinline__ double rlen(double3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__host__ __device__ __forceinline__ float rlen(float3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
 
 static constexpr double kPi = 3.14159265358979323846;
 

@@ -23,6 +23,7 @@
 
 #include "cells.cuh"
 #include "graph.cuh"
+#include "vtu.hpp"
 #include "dem_physics.cuh"
 
 namespace demsph {
@@ -708,6 +709,7 @@ struct DemScene {
     std::vector<double4> hPos, hVel, hAngv;
     std::vector<int> hMat, hClump;
     HostMatRows rows;
+    std::vector<MatPair> hMatTab;  // the pair-parameter table (host copy of `mats`)
     std::vector<double4> hCpos, hCvel, hCangv, hCq, hCinvIa, hCinvIb;
     std::vector<double> hCinvm;
     std::vector<int2> hCpeb;
@@ -856,8 +858,8 @@ struct DemScene {
                 if (m.ktks > 0 && m.G > 0) tors = 1;
             }
         }
-        std::vector<MatPair> v(tab.begin(), tab.end());
-        mats.upload(v, s);
+        hMatTab.assign(tab.begin(), tab.end());
+        mats.upload(hMatTab, s);
     }
 
     void upload_bonds() {
@@ -1862,6 +1864,187 @@ int demsph_dem_get_bonds(demsph_dem_t h, int* a, int* b, int* ok, double* fn, do
             if (tb) st3(tb, k, xyz(TB[k]));
             if (normal) st3(normal, k, xyz(NO[k]));
             if (point) st3(point, k, xyz(PO[k]));
+        }
+    });
+}
+// ------------------------------------------------------------ VTU frames --
+// outputBallVTU, outputMeshWallVTU, outputBallInteractionVTU,
+// outputBondedInteractionVTU, outputBallTriangleInteractionVTU
+// (DEMSolver.h:908-1370), same files and arrays.  The interaction frames
+// evaluate each listed contact on the current state (geometry from the
+// current positions, the contact law with a zero time increment on copies of
+// the stored springs); the reference writes the values of its last force
+// evaluation, half a drift earlier.
+static void ball_arrays(DemScene& s, std::vector<double4>& P, std::vector<double4>& V, std::vector<double4>& W,
+                        std::vector<int>& M, std::vector<int>& Cl) {
+    if (!s.ready && !s.assembled) {
+        P = s.hPos; V = s.hVel; W = s.hAngv; M = s.hMat; Cl = s.hClump;
+        return;
+    }
+    s.pos.download(P, s.s); s.vel.download(V, s.s); s.angv.download(W, s.s);
+    s.mat.download(M, s.s); s.clump.download(Cl, s.s);
+    DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+}
+static std::vector<double3> xyz_of(const std::vector<double4>& a) {
+    std::vector<double3> o(a.size());
+    for (size_t i = 0; i < a.size(); i++) o[i] = xyz(a[i]);
+    return o;
+}
+int demsph_dem_write_vtu(demsph_dem_t h, const char* dir, long frame, int what) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (!dir) throw Status(DEMSPH_ERR_INVALID, "null directory");
+        DemScene& s = h->sc;
+        const std::string d(dir);
+        const int n = s.N();
+        std::vector<double4> P, V, W;
+        std::vector<int> M, Cl;
+        ball_arrays(s, P, V, W, M, Cl);
+        if (what & DEMSPH_VTU_BALLS) {
+            vtu::File f(d, "ball", frame);
+            f.head(s.time, s.iStep, n, n);
+            f.points(xyz_of(P));
+            f.vertex_cells(n);
+            f.begin_data("PointData", "radius");
+            std::vector<double> r(n);
+            for (int i = 0; i < n; i++) r[i] = P[i].w;
+            f.floats("radius", r);
+            f.ints("materialID", M);
+            f.ints("clumpID", Cl);
+            f.vectors("velocity", xyz_of(V));
+            f.vectors("angularVelocity", xyz_of(W));
+            f.end_data("PointData");
+        }
+        if ((what & DEMSPH_VTU_MESH_WALLS) && !s.hTris.empty()) {
+            std::vector<double4> VG;
+            if (s.ready) {
+                s.vglobal.download(VG, s.s);
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            } else {
+                VG.resize(s.hVlocal.size());
+                for (size_t v = 0; v < s.hVlocal.size(); v++)
+                    VG[v] = d4(xyz(s.hVlocal[v]) + xyz(s.hWpos[s.hVwall[v]]), 0);
+            }
+            vtu::File f(d, "triangleWall", frame);
+            f.head(s.time, s.iStep, VG.size(), s.hTris.size());
+            f.points(xyz_of(VG));
+            f.triangle_cells(s.hTris);
+            f.begin_data("CellData", "materialID");
+            std::vector<int> wid(s.hTris.size()), tm(s.hTris.size());
+            for (size_t t = 0; t < s.hTris.size(); t++) {
+                wid[t] = s.hTris[t].w;
+                tm[t] = s.hWmat[s.hTris[t].w];
+            }
+            f.ints("wallID", wid);
+            f.ints("materialID", tm);
+            f.end_data("CellData");
+        }
+        auto contact_frame = [&](int which, const char* stem) {
+            std::vector<int> A, B;
+            std::vector<size_t> sl;
+            if (s.ready) collect_rows(s, which, A, B, sl);
+            std::vector<double4> S, R, T, VG;
+            const int c = which == 0 ? s.cur : s.wcur;
+            if (!A.empty()) {
+                (which == 0 ? s.spS[c] : s.wS[c]).download(S, s.s);
+                if (s.roll) (which == 0 ? s.spR[c] : s.wR[c]).download(R, s.s);
+                if (s.tors) (which == 0 ? s.spT[c] : s.wT[c]).download(T, s.s);
+                if (which == 1) s.vglobal.download(VG, s.s);
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            }
+            const size_t m = A.size();
+            std::vector<double3> pt(m), nrm(m), fc(m), tc(m), es(m), er(m), et(m);
+            std::vector<double> ov(m);
+            for (size_t k = 0; k < m; k++) {
+                const int a = A[k];
+                const double3 ra = xyz(P[a]);
+                es[k] = xyz(S[sl[k]]);
+                er[k] = s.roll ? xyz(R[sl[k]]) : mk3(0, 0, 0);
+                et[k] = s.tors ? xyz(T[sl[k]]) : mk3(0, 0, 0);
+                double3 rc, n, vc, wij;
+                double delta, mass, Rad;
+                int mb;
+                if (which == 0) {
+                    const int b = B[k];
+                    const double3 rb = xyz(P[b]);
+                    n = normalize(ra - rb);
+                    delta = P[a].w + P[b].w - len(ra - rb);
+                    rc = rb + (P[b].w - 0.5 * delta) * n;
+                    vc = xyz(V[a]) + cross(xyz(W[a]), rc - ra) - (xyz(V[b]) + cross(xyz(W[b]), rc - rb));
+                    wij = xyz(W[a]) - xyz(W[b]);
+                    mass = 1. / (V[a].w + V[b].w);
+                    Rad = P[a].w * P[b].w / (P[a].w + P[b].w);
+                    mb = M[b];
+                } else {
+                    const int4 tv = s.hTris[B[k]];
+                    rc = mk3(0, 0, 0);
+                    classify_sphere_triangle(ra, P[a].w, xyz(VG[tv.x]), xyz(VG[tv.y]), xyz(VG[tv.z]), rc);
+                    n = normalize(ra - rc);
+                    delta = P[a].w - len(ra - rc);
+                    const int wj = tv.w;
+                    const double3 rw = xyz(s.hWpos[wj]);
+                    vc = xyz(V[a]) + cross(xyz(W[a]), rc - ra) - (xyz(s.hWvel[wj]) + cross(xyz(s.hWangv[wj]), rc - rw));
+                    wij = xyz(W[a]) - xyz(s.hWangv[wj]);
+                    mass = V[a].w > 0 ? 1. / V[a].w : 0.0;
+                    Rad = P[a].w;
+                    mb = s.hWmat[wj];
+                }
+                pt[k] = rc;
+                nrm[k] = n;
+                ov[k] = delta;
+                double3 F = mk3(0, 0, 0), Tq = mk3(0, 0, 0);
+                if (delta > 0 && s.cap > 0 && mass > 0) {
+                    double3 s0 = es[k], r0 = er[k], t0 = et[k];
+                    const MatPair& mp = s.hMatTab[pair_param_index(M[a], mb, s.nMat, s.cap)];
+                    contact_law<double>(mp, F, Tq, s0, r0, t0, vc, wij, n, delta, mass, Rad, 0.0, s.roll, s.tors);
+                }
+                fc[k] = F;
+                tc[k] = Tq;
+            }
+            vtu::File f(d, stem, frame);
+            f.head(s.time, s.iStep, m, m);
+            f.points(pt);
+            f.vertex_cells(m);
+            f.begin_data("PointData", "overlap");
+            f.floats("overlap", ov);
+            f.vectors("contact normal", nrm);
+            f.vectors("contact force", fc);
+            f.vectors("contact torque", tc);
+            f.vectors("sliding spring", es);
+            f.vectors("rolling spring", er);
+            f.vectors("torsion spring", et);
+            f.end_data("PointData");
+        };
+        if (what & DEMSPH_VTU_BALL_INTERACTIONS) contact_frame(0, "ballInteraction");
+        if ((what & DEMSPH_VTU_BALL_TRIANGLE_INTERACTIONS) && !s.hTris.empty())
+            contact_frame(1, "ballTriangleInteraction");
+        if (what & DEMSPH_VTU_BONDED_INTERACTIONS) {
+            const int nb = (int)s.hBab.size();
+            std::vector<int> OK(nb, 1);
+            std::vector<double> FN(nb, 0.0), TT(nb, 0.0), SM(nb, 0.0), TM(nb, 0.0);
+            std::vector<double4> FS(nb), TB(nb), NO(s.hBnormal), PO(s.hBpoint);
+            if (s.ready && nb > 0) {
+                s.bok.download(OK, s.s); s.bFn.download(FN, s.s); s.bTt.download(TT, s.s); s.bFs.download(FS, s.s);
+                s.bTb.download(TB, s.s); s.bnormal.download(NO, s.s); s.bpoint.download(PO, s.s);
+                s.bsmax.download(SM, s.s); s.btmax.download(TM, s.s);
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            } else {
+                for (int k = 0; k < nb; k++) FS[k] = TB[k] = make_double4(0, 0, 0, 0);
+            }
+            vtu::File f(d, "bondedInteraction", frame);
+            f.head(s.time, s.iStep, nb, nb);
+            f.points(xyz_of(PO));
+            f.vertex_cells(nb);
+            f.begin_data("PointData", "overlap");
+            f.ints("is bonded", OK);
+            f.floats("normal force", FN);
+            f.floats("torsion torque", TT);
+            f.floats("maximum normal stress", SM);
+            f.floats("maximum shear stress", TM);
+            f.vectors("contact normal", xyz_of(NO));
+            f.vectors("shearing force", xyz_of(FS));
+            f.vectors("bending torque", xyz_of(TB));
+            f.end_data("PointData");
         }
     });
 }

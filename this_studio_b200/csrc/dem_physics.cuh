@@ -40,7 +40,7 @@ __host__ __device__ __forceinline__ int pair_param_index(int a, int b, int nMat,
 // integrateSlidingOrRollingSpring (contactKernel.cuh:64-97).  The spring is
 // accumulated in FP64; the trial force for the Coulomb cap uses R.
 template <class R>
-__device__ __forceinline__ double3 spring_slide(double3 sp, V<R> sv, double3 n, V<R> Fn, R mu, R k, R c, double dt) {
+__host__ __device__ __forceinline__ double3 spring_slide(double3 sp, V<R> sv, double3 n, V<R> Fn, R mu, R k, R c, double dt) {
     double3 s = mk3(0, 0, 0);
     if (k > (R)0) {
         double3 s1 = sp - dot(sp, n) * n;
@@ -61,7 +61,7 @@ __device__ __forceinline__ double3 spring_slide(double3 sp, V<R> sv, double3 n, 
 }
 // integrateTorsionSpring (contactKernel.cuh:99-126)
 template <class R>
-__device__ __forceinline__ double3 spring_torsion(double3 sp, V<R> tv, double3 n, V<R> Fn, R mu, R k, R c, double dt) {
+__host__ __device__ __forceinline__ double3 spring_torsion(double3 sp, V<R> tv, double3 n, V<R> Fn, R mu, R k, R c, double dt) {
     double3 s = mk3(0, 0, 0);
     if (k > (R)0) {
         s = dot(sp + up(tv) * dt, n) * n;
@@ -82,7 +82,7 @@ __device__ __forceinline__ double3 spring_torsion(double3 sp, V<R> tv, double3 n
 // the model's stiffness and damping have been formed.  Geometry (n, delta)
 // and relative velocities arrive in FP64; R is the arithmetic of the law.
 template <class R>
-__device__ __forceinline__ void law_tail(V<R>& F, V<R>& T, double3& es, double3& er, double3& et, double3 vc,
+__host__ __device__ __forceinline__ void law_tail(V<R>& F, V<R>& T, double3& es, double3& er, double3& et, double3 vc,
                                          double3 wij, double3 n, R delta, R Rad, double dt, R kn, R ks, R kr, R kt,
                                          R cn, R cs, R cr, R ct, R mus, R mur, R mut, bool roll, bool tors) {
     V<R> nr = cvt<R>(n);
@@ -117,7 +117,7 @@ __device__ __forceinline__ void law_tail(V<R>& F, V<R>& T, double3& es, double3&
 // the scene has a rolling / torsion stiffness (their springs then stay zero,
 // which is what the reference computes for k = 0).
 template <class R>
-__device__ __forceinline__ void contact_law(const MatPair& mp, V<R>& F, V<R>& T, double3& es, double3& er, double3& et,
+__host__ __device__ __forceinline__ void contact_law(const MatPair& mp, V<R>& F, V<R>& T, double3& es, double3& er, double3& et,
                                             double3 vc, double3 wij, double3 n, double delta, double m, double Rad,
                                             double dt, bool roll, bool tors) {
     F = v3r<R>(0, 0, 0);
@@ -201,10 +201,10 @@ __device__ __forceinline__ int parallel_bond(double& Fn, double& Tt, double3& Fs
 
 // ------------------------------------------------------ sphere/triangle ---
 enum : int { kCtNone = 0, kCtFace = 1, kCtEdge = 2, kCtVertex = 3 };
-__device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
-__device__ __forceinline__ double dist2(double3 a, double3 b) { double3 d = a - b; return dot(d, d); }
+__host__ __device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+__host__ __device__ __forceinline__ double dist2(double3 a, double3 b) { double3 d = a - b; return dot(d, d); }
 // closestPointOnSegment (contactKernel.cuh:315-330)
-__device__ __forceinline__ double3 closest_on_segment(double3 a, double3 b, double3 p, double& t) {
+__host__ __device__ __forceinline__ double3 closest_on_segment(double3 a, double3 b, double3 p, double& t) {
     double3 ab = b - a;
     double ab2 = dot(ab, ab);
     if (ab2 <= 1e-30) { t = 0.0; return a; }
@@ -213,7 +213,7 @@ __device__ __forceinline__ double3 closest_on_segment(double3 a, double3 b, doub
 }
 // classifySphereTriangleContact (contactKernel.cuh:367-501): Ericson's
 // Voronoi-region closest point; degenerate triangles as three segments.
-__device__ __forceinline__ int classify_sphere_triangle(double3 c, double r, double3 v0, double3 v1, double3 v2,
+__host__ __device__ __forceinline__ int classify_sphere_triangle(double3 c, double r, double3 v0, double3 v1, double3 v2,
                                                         double3& cp) {
     double r2 = r * r;
     double eps2 = 1e-12 * fmax(1.0, r2);

@@ -20,6 +20,7 @@
 
 #include "cells.cuh"
 #include "graph.cuh"
+#include "vtu.hpp"
 
 namespace demsph {
 
@@ -1555,6 +1556,65 @@ int demsph_sph_get(demsph_sph_t h, int dummy, double* pos, double* vel, double* 
             if (p) p[o] = S4[t].y;
             if (drho) drho[o] = DR[t];
             if (normal) sst3(normal, o, mk3(0, 0, 0));
+        }
+    });
+}
+// outputWCSPHVTU / outputDummyVTU (WCSPHSolver.h:360-520): <dir>/SPH_NNNN.vtu
+// and <dir>/dummy_NNNN.vtu in the reference's layout, particles in caller order.
+int demsph_sph_write_vtu(demsph_sph_t h, const char* dir, long frame, int what) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!dir) throw Status(DEMSPH_ERR_INVALID, "null directory");
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        const std::string d(dir);
+        if (what & DEMSPH_VTU_FLUID) {
+            const int n = s.N();
+            std::vector<double4> P4, V4, S4;
+            std::vector<int> ID;
+            s.pos[s.P].download(P4, s.s); s.vel[s.Vv].download(V4, s.s); s.st[s.S].download(S4, s.s);
+            s.id[s.ID].download(ID, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            std::vector<double3> p(n), v(n);
+            std::vector<double> hh(n), rho(n), pr(n);
+            for (int t = 0; t < n; t++) {
+                const int o = ID[t];
+                p[o] = xyz(P4[t]); v[o] = xyz(V4[t]); hh[o] = P4[t].w; rho[o] = S4[t].x; pr[o] = S4[t].y;
+            }
+            vtu::File f(d, "SPH", frame);
+            f.head(s.time, s.iStep, n, n);
+            f.points(p);
+            f.vertex_cells(n);
+            f.begin_data("PointData", "smoothLength");
+            f.floats("smoothLength", hh);
+            f.floats("density", rho);
+            f.floats("pressure", pr);
+            f.vectors("velocity", v);
+            f.end_data("PointData");
+        }
+        if (what & DEMSPH_VTU_DUMMIES) {
+            const int nd = s.ND();
+            std::vector<double4> P4, V4, N4;
+            std::vector<int> ID;
+            if (nd > 0) {
+                s.dpos.download(P4, s.s); s.dvel.download(V4, s.s); s.dnorm.download(N4, s.s); s.did.download(ID, s.s);
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            }
+            std::vector<double3> p(nd), v(nd), nn(nd);
+            std::vector<double> hh(nd);
+            for (int t = 0; t < nd; t++) {
+                const int o = ID[t];
+                p[o] = xyz(P4[t]); v[o] = xyz(V4[t]); nn[o] = xyz(N4[t]); hh[o] = P4[t].w;
+            }
+            vtu::File f(d, "dummy", frame);
+            f.head(s.time, s.iStep, nd, nd);
+            f.points(p);
+            f.vertex_cells(nd);
+            f.begin_data("PointData", "smoothLength");
+            f.floats("smoothLength", hh);
+            f.vectors("velocity", v);
+            f.vectors("normal", nn);
+            f.end_data("PointData");
         }
     });
 }

@@ -29,6 +29,144 @@ def uniform_point_cloud(mn, mx, dx):
 
 
 @dataclass
+class HexPBC2D:
+    """Periodic cell of a hexagonal x-y packing (DEMSPH/pointCloudGeneration.h:60-80)."""
+    min: tuple = (0.0, 0.0, 0.0)
+    max: tuple = (0.0, 0.0, 0.0)
+    Lx: float = 0.0
+    Ly: float = 0.0
+    shearX: float = 0.0
+    nx: int = 0
+    ny: int = 0
+    periodicX: bool = False
+    periodicY: bool = False
+
+
+def make_hex_pbc_2d(mn, mx, spacing, periodic_x, periodic_y):
+    """makeHexPBC2D (pointCloudGeneration.h:88-140): rows dy = a sqrt(3)/2
+    apart; a periodic axis is snapped up to a whole number of steps
+    (ceil(L/step - 1e-12)), a bounded one holds floor(L/step + 1e-12) steps."""
+    pbc = HexPBC2D(periodicX=bool(periodic_x), periodicY=bool(periodic_y))
+    if spacing <= 0.0:
+        return pbc
+    dx = spacing
+    dy = spacing * math.sqrt(3.0) * 0.5
+    lx = max(0.0, mx[0] - mn[0])
+    ly = max(0.0, mx[1] - mn[1])
+    nx = max(1, int(math.ceil(lx / dx - 1e-12))) if periodic_x else max(1, int(math.floor(lx / dx + 1e-12)))
+    ny = max(1, int(math.ceil(ly / dy - 1e-12))) if periodic_y else max(1, int(math.floor(ly / dy + 1e-12)))
+    pbc.nx, pbc.ny = nx, ny
+    pbc.min = tuple(float(v) for v in mn)
+    pbc.Lx = nx * dx
+    pbc.Ly = ny * dy
+    pbc.max = (mn[0] + pbc.Lx if periodic_x else float(mx[0]), mn[1] + pbc.Ly if periodic_y else float(mx[1]),
+               float(mx[2]))
+    pbc.shearX = 0.5 * dx if (periodic_y and (ny & 1)) else 0.0
+    return pbc
+
+
+def hex_point_cloud(mn, mx, spacing, periodic_x, periodic_y):
+    """generateHexPointCloud (pointCloudGeneration.h:152-196): rows along x,
+    odd rows shifted by dx/2, z = min z; a bounded axis stops at its max.
+    Returns (points, pbc)."""
+    pbc = make_hex_pbc_2d(mn, mx, spacing, periodic_x, periodic_y)
+    pts = []
+    if pbc.nx <= 0 or pbc.ny <= 0 or spacing <= 0.0:
+        return np.zeros((0, 3)), pbc
+    dx = spacing
+    dy = spacing * math.sqrt(3.0) * 0.5
+    x0, y0, z0 = pbc.min
+    for j in range(pbc.ny):
+        y = y0 + j * dy
+        if not periodic_y and y >= mx[1]:
+            break
+        shift = 0.5 * dx if (j & 1) else 0.0
+        for i in range(pbc.nx):
+            x = x0 + i * dx + shift
+            if not periodic_x and x >= mx[0]:
+                break
+            pts.append((x, y, z0))
+    return np.array(pts, float).reshape(-1, 3), pbc
+
+
+def _normalize(v):
+    l2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2]
+    if l2 < 1.0e-20:
+        return (0.0, 0.0, 0.0)
+    inv = 1.0 / math.sqrt(l2)
+    return (v[0] * inv, v[1] * inv, v[2] * inv)
+
+
+def _cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+def cylinder_mesh(center, axis, radius, height, n_around, n_height, caps=True):
+    """makeCylinderMesh (pointCloudGeneration.h:225-327): nHeight + 1 rings of
+    nAround vertices from -h/2 to +h/2 along the axis, two triangles per side
+    quad, and (with caps) a centre vertex and a fan per end.  The arithmetic
+    follows the reference's order so the vertices come out bit for bit."""
+    assert n_around >= 3 and n_height >= 1 and radius > 0 and height > 0
+    w = _normalize(axis)
+    tmp = (0.0, 0.0, 1.0) if abs(w[2]) < 0.9 else (0.0, 1.0, 0.0)
+    u = _normalize(_cross(tmp, w))
+    v = _normalize(_cross(w, u))
+    verts = []
+    for iz in range(n_height + 1):
+        t = iz / n_height
+        z = (t - 0.5) * height
+        c = (center[0] + z * w[0], center[1] + z * w[1], center[2] + z * w[2])
+        for ia in range(n_around):
+            ang = (2.0 * math.pi) * (ia / n_around)
+            ca, sa = math.cos(ang), math.sin(ang)
+            verts.append(tuple(c[k] + radius * (ca * u[k] + sa * v[k]) for k in range(3)))
+
+    def vid(iz, ia):
+        return iz * n_around + ia % n_around
+
+    t0, t1, t2 = [], [], []
+    for iz in range(n_height):
+        for ia in range(n_around):
+            i00, i01, i10, i11 = vid(iz, ia), vid(iz, ia + 1), vid(iz + 1, ia), vid(iz + 1, ia + 1)
+            t0 += [i00, i00]
+            t1 += [i10, i11]
+            t2 += [i11, i01]
+    if caps:
+        bottom = len(verts)
+        verts.append(tuple(center[k] + (-0.5 * height) * w[k] for k in range(3)))
+        top = len(verts)
+        verts.append(tuple(center[k] + (0.5 * height) * w[k] for k in range(3)))
+        for ia in range(n_around):
+            t0.append(bottom); t1.append(vid(0, ia + 1)); t2.append(vid(0, ia))
+        for ia in range(n_around):
+            t0.append(top); t1.append(vid(n_height, ia)); t2.append(vid(n_height, ia + 1))
+    return {"vertices": np.array(verts, float), "tri0": np.array(t0, np.int32), "tri1": np.array(t1, np.int32),
+            "tri2": np.array(t2, np.int32)}
+
+
+def static_sphere_water_level(R, rho_ball, rho_water):
+    """waterSurfaceHeightForStaticSphere (DEMSPH/iceCylinderInteraction.cpp:5-35):
+    the plane height h in [-R, R] at which the submerged volume fraction
+    (R + h)^2 (2R - h) / (4 R^3) equals rho_ball / rho_water, by 80 bisections."""
+    if not (R > 0.0) or not (rho_water > 0.0) or not (rho_ball >= 0.0):
+        return R
+    f = rho_ball / rho_water
+    if f <= 0.0:
+        return -R
+    if f >= 1.0:
+        return R
+    lo, hi = -R, R
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        b = R + mid
+        if (b * b) * (2.0 * R - mid) / (4.0 * R * R * R) < f:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+@dataclass
 class DEMScene:
     name: str
     position: np.ndarray
@@ -113,6 +251,34 @@ def dam_break_reference():
 # ---------------------------------------------------------------------------
 # Benchmark-sized synthetic scenes
 # ---------------------------------------------------------------------------
+def ice_cylinder_reference():
+    """DEMSPH/iceCylinderInteraction.cpp: a hexagonally packed ice sheet of
+    r = 0.1 spheres (rho 900, 100 x 116 rows over 20 x 20 m, periodic rows in
+    y) moving at -0.4 m/s in x against a fixed cylinder mesh (radius 1,
+    height 6, 36 x 36 segments) at (-1.1, 10, 0); linear contact, parallel
+    bonds on the initial contacts, buoyancy + drag against a water plane at
+    the static flotation height, dt = t_c / 50."""
+    tc, r, den = 0.0002, 0.1, 900.0
+    m = r * r * r * math.pi * 4.0 / 3.0 * den
+    kn = 0.5 * m * math.pi * math.pi / tc / tc
+    E = kn * 2.0 * r / (r * r * math.pi)
+    pts, pbc = hex_point_cloud((0.0, 0.0, 0.0), (200 * r, 200 * r, 0.0), 2 * r, False, True)
+    mesh = cylinder_mesh((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 1.0, 6.0, 36, 36)
+    n = pts.shape[0]
+    lin = (kn, kn / 2.6, 0.0, 0.0, 0.1, 0.1, 0.0, 0.0, 0.1, 0.0, 0.0)
+    level = static_sphere_water_level(r, den, 1000.0)
+    sc = DEMScene(
+        name="ice_cylinder", position=pts, radius=np.full(n, r), density=np.full(n, den),
+        material=np.zeros(n, np.int32), velocity=np.tile([-0.4, 0.0, 0.0], (n, 1)),
+        linear=[(0, 0) + lin, (0, 1) + lin], bonded=[(0, 0, 1.0, E, 2.6, 0.5e6, 0.5e6, 0.1)],
+        walls=[dict(mesh, position=(-1.1, 100 * r, 0.0), material=1)],
+        minb=(-pbc.max[0], pbc.min[1], -3.0), maxb=(pbc.max[0], pbc.max[1], 3.0), gravity=(0.0, 0.0, -9.81),
+        dt=tc / 50.0, steps=int(50.0 / (tc / 50.0)) + 2)
+    sc.buoyancy = (1000.0, 0.1, (0.0, 0.0, -9.81), (-0.4, 0.0, 0.0), level)
+    sc.bond_initial_contacts = True
+    return sc
+
+
 def hertz_params(E, nu):
     """Effective moduli for like materials: E* = E / (2 (1 - nu^2)),
     G* = E / (4 (2 - nu)(1 + nu))."""

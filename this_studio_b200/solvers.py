@@ -57,6 +57,27 @@ def num_steps(timeStep, maximumTime):
     return int(maximumTime / timeStep) + 1 + 1
 
 
+def _run_frames(solver, total, numFrame, write):
+    """The reference's frame cadence (DEMSolver.h:1984-2046, WCSPHSolver.h:
+    587-621): frame 0 after initialisation; numStep = total - 1 and
+    frameInterval = numStep / numFrame (numStep when numFrame is 0, at least
+    1); after step iStep (1-based), frame += 1 whenever iStep % frameInterval
+    == 0."""
+    num_step = total - 1
+    interval = num_step // numFrame if numFrame > 0 else num_step
+    interval = max(1, interval)
+    write(0)
+    done = 0
+    frame = 0
+    while done < total:
+        nxt = min(total, (done // interval + 1) * interval)
+        solver.step(nxt - done)
+        done = nxt
+        if done % interval == 0:
+            frame += 1
+            write(frame)
+
+
 class DEMMember:
     """One scene's balls held on the device, from which batch scenes are
     assembled (DEMSolver.assembleBalls)."""
@@ -212,8 +233,25 @@ class DEMSolver:
 
     def solve(self, minBoundary, maxBoundary, gravity, timeStep, maximumTime, numFrame=0, dir=None,
               deviceID=0, maximumThread=256, precision="mixed"):
+        """DEMSolver::solve (DEMSolver.h:1961-2049): initialise, then step to
+        maximumTime; with `dir`, VTU frames as the reference writes them
+        (frame 0 after initialisation, then every numStep / numFrame steps)."""
         self.initialize(minBoundary, maxBoundary, gravity, timeStep, precision)
-        self.step(num_steps(timeStep, maximumTime))
+        total = num_steps(timeStep, maximumTime)
+        if dir is None:
+            self.step(total)
+            return
+        _run_frames(self, total, numFrame, lambda f: self.writeVTU(dir, f))
+
+    def writeVTU(self, dir, frame, what=None):
+        """ball / triangleWall / ballInteraction / bondedInteraction /
+        ballTriangleInteraction _NNNN.vtu in `dir` (the reference's files)."""
+        if what is None:
+            what = 1 | 4 | 8 | (2 | 16 if self._has_walls() else 0)
+        call("demsph_dem_write_vtu", self._h, str(dir).encode(), int(frame), int(what))
+
+    def _has_walls(self):
+        return getattr(self, "_nvert", 0) > 0
 
     def neighborSearch(self):
         call("demsph_dem_neighbor_search", self._h)
@@ -413,8 +451,18 @@ class WCSPHSolver:
 
     def solve(self, minBoundary, maxBoundary, gravity, timeStep, maximumTime, numFrame=0, dir=None, deviceID=0,
               maximumThread=256, precision="fp64"):
+        """WCSPHSolver::solve (WCSPHSolver.h:567-624), with VTU frames in
+        `dir` as the reference writes them."""
         self.initialize(minBoundary, maxBoundary, gravity, timeStep, precision)
-        self.step(num_steps(timeStep, maximumTime))
+        total = num_steps(timeStep, maximumTime)
+        if dir is None:
+            self.step(total)
+            return
+        _run_frames(self, total, numFrame, lambda f: self.writeVTU(dir, f))
+
+    def writeVTU(self, dir, frame, what=3):
+        """SPH_NNNN.vtu and dummy_NNNN.vtu in `dir` (the reference's files)."""
+        call("demsph_sph_write_vtu", self._h, str(dir).encode(), int(frame), int(what))
 
     def neighborSearch(self):
         call("demsph_sph_neighbor_search", self._h)
