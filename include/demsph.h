@@ -128,6 +128,12 @@ int demsph_dem_set_buoyancy_drag(demsph_dem_t s, double fluidDensity, double dra
  * upload, grids (cell = 2 r_max; triangle cell >= 2 circumradius),
  * neighbour search, one force evaluation with dt = 0.  precision is
  * DEMSPH_PRECISION_*. */
+/* setPeriodicBoundary (DEMSolver.h:1944-1959), before initialize: periodic
+ * ghost passes along the flagged axes and their combinations, as the
+ * reference runs them (DEMSolver.h:279-426,1407-1534).  demsph_dem_get_pairs
+ * with which = 2 + k returns the pairs of the k-th active ghost set (order X,
+ * Y, Z, XY, YZ, XZ, XYZ over the active ones). */
+int demsph_dem_set_periodic(demsph_dem_t s, int x, int y, int z);
 int demsph_dem_initialize(demsph_dem_t s, const double* minBoundary, const double* maxBoundary,
                           const double* gravity, double timeStep, int precision);
 /* numSteps passes of the step loop (loop_ball / loop_ball_wall,
@@ -142,7 +148,9 @@ int demsph_dem_step(demsph_dem_t s, long numSteps);
 int demsph_dem_set_graphs(demsph_dem_t s, int enable);
 /* Protected step pieces of DEMSolver, exposed for parity checks:
  * neighborSearch (DEMSolver.h:698-777) and calculateBallContactForceTorque
- * (:599-695) followed, when walls != 0, by addTriangleContactForceTorque(dtWall) (:428-597). */
+ * (:599-695) followed, when walls & 1, by addTriangleContactForceTorque(dtWall)
+ * (:428-597) and, when walls & 2, by the periodic ghost passes
+ * addDummyContactForceTorque(dt) (:279-426). */
 int demsph_dem_neighbor_search(demsph_dem_t s);
 int demsph_dem_eval_forces(demsph_dem_t s, double dt, int walls, double dtWall);
 

@@ -546,6 +546,16 @@ struct DEM {
     long iStep = 0;
     double time = 0;
     bool initialized = false;
+    // periodic ghost sets (DEMSolver.h:81-86,1944-1959)
+    struct Ghost {
+        int dx, dy, dz;
+        std::vector<V3> gpos;
+        Grid grid;
+        std::vector<int> hashIndex, hashValue;
+        Pairs p;
+    };
+    bool perX = false, perY = false, perZ = false;
+    std::vector<Ghost> ghosts;
     size_t nb() const { return pos.size(); }
 };
 
@@ -696,6 +706,132 @@ static void demBallForces(DEM& s, double dt) {
             s.force[i] += Fi;
             s.torque[i] += Ti;
         }
+    }
+}
+
+// addDummyContactForceTorque (DEMSolver.h:279-426): ghost positions
+// (buildDummyPosition, neighborSearchKernel.cu:57-77), a cell table of the
+// ghosts that left the domain (calculateDummyHash, neighborSearchKernel.cu:
+// 29-55, then the stable sort of buildHashStartEnd), the pair rule of
+// count/writeBallInteractionsKernel on the ghost positions with springs
+// carried from the previous ghost list, the contact law, and the pointed /
+// pointing sums with the ghost positions as torque arms.
+static void demGhostForces(DEM& s, DEM::Ghost& g, double dt) {
+    const size_t N = s.nb();
+    const Grid& bg = s.ballGrid;
+    const V3 L = bg.mx - bg.mn;
+    g.gpos.resize(N);
+    for (size_t i = 0; i < N; i++) {
+        V3 p = s.pos[i];
+        if (g.dx == 1 && p.x - bg.mn.x < bg.cs.x) p.x += L.x;
+        if (g.dy == 1 && p.y - bg.mn.y < bg.cs.y) p.y += L.y;
+        if (g.dz == 1 && p.z - bg.mn.z < bg.cs.z) p.z += L.z;
+        g.gpos[i] = p;
+    }
+    g.hashValue.assign(N, -1);
+    g.hashIndex.resize(N);
+    for (size_t i = 0; i < N; i++) {
+        V3 p = g.gpos[i];
+        bool out = p.x < bg.mn.x || p.x >= bg.mx.x || p.y < bg.mn.y || p.y >= bg.mx.y || p.z < bg.mn.z ||
+                   p.z >= bg.mx.z;
+        if (out) g.hashValue[i] = clampedHash(p, bg);
+    }
+    std::iota(g.hashIndex.begin(), g.hashIndex.end(), 0);
+    std::stable_sort(g.hashIndex.begin(), g.hashIndex.end(),
+                     [&](int a, int b) { return g.hashValue[a] < g.hashValue[b]; });
+    std::vector<int> sortedKey(N);
+    for (size_t i = 0; i < N; i++) sortedKey[i] = g.hashValue[g.hashIndex[i]];
+    g.grid = bg;
+    std::fill(g.grid.start.begin(), g.grid.start.end(), -1);
+    std::fill(g.grid.end.begin(), g.grid.end.end(), -1);
+    for (size_t i = 0; i < N; i++) {
+        int h = sortedKey[i];
+        if (h < 0) continue;
+        if (i == 0 || sortedKey[i - 1] != h) g.grid.start[h] = (int)i;
+        if (i == N - 1 || sortedKey[i + 1] != h) g.grid.end[h] = (int)(i + 1);
+    }
+    Pairs old = g.p;
+    auto accept = [&](int A, int B) -> bool {
+        if (A >= B) return false;
+        if (s.invMass[A] == 0 && s.invMass[B] == 0) return false;
+        if (s.clump[B] >= 0 && s.clump[A] == s.clump[B]) return false;
+        double cut = 1.1 * (s.rad[A] + s.rad[B]);
+        V3 r = g.gpos[A] - g.gpos[B];
+        return (cut * cut - dot(r, r)) >= 0.;
+    };
+    std::vector<int> cnt(N, 0);
+    for (size_t A = 0; A < N; A++) {
+        int c = 0;
+        forEachStencilCell(g.gpos[A], g.grid, [&](int st, int en) {
+            for (int k = st; k < en; k++) if (accept((int)A, g.hashIndex[k])) c++;
+        });
+        cnt[A] = c;
+    }
+    std::vector<int> prefix(N);
+    std::partial_sum(cnt.begin(), cnt.end(), prefix.begin());
+    size_t P = N ? (size_t)prefix[N - 1] : 0;
+    g.p.resize(P);
+    g.p.prefix = prefix;
+    for (size_t A = 0; A < N; A++) {
+        int w = A > 0 ? prefix[A - 1] : 0;
+        forEachStencilCell(g.gpos[A], g.grid, [&](int st, int en) {
+            for (int k = st; k < en; k++) {
+                int B = g.hashIndex[k];
+                if (!accept((int)A, B)) continue;
+                g.p.pointed[w] = (int)A;
+                g.p.pointing[w] = B;
+                if (B < (int)old.iStart.size() && old.iStart[B] != -1) {
+                    for (int j = old.iStart[B]; j < old.iEnd[B]; j++) {
+                        int j1 = old.hashIndex[j];
+                        if (old.pointed[j1] == (int)A) {
+                            g.p.sl[w] = old.sl[j1]; g.p.ro[w] = old.ro[j1]; g.p.to[w] = old.to[j1];
+                            break;
+                        }
+                    }
+                }
+                w++;
+            }
+        });
+    }
+    g.p.buildPointing(N);
+    Pairs& p = g.p;
+    for (size_t k = 0; k < p.n; k++) {
+        int i = p.pointed[k], j = p.pointing[k];
+        V3 rij = g.gpos[i] - g.gpos[j];
+        V3 n = normalize(rij);
+        double delta = s.rad[i] + s.rad[j] - length(rij);
+        V3 rc = g.gpos[j] + (s.rad[j] - 0.5 * delta) * n;
+        p.cpoint[k] = rc; p.cnormal[k] = n; p.overlap[k] = delta;
+        double R = s.rad[i] * s.rad[j] / (s.rad[i] + s.rad[j]);
+        double m = 1. / (s.invMass[i] + s.invMass[j]);
+        V3 vc = s.vel[i] + cross(s.w[i], rc - g.gpos[i]) - (s.vel[j] + cross(s.w[j], rc - g.gpos[j]));
+        V3 wij = s.w[i] - s.w[j];
+        int ip = s.M.index(s.mat[i], s.mat[j]);
+        V3 F, T;
+        pairLaw(s.M, ip, F, T, p.sl[k], p.ro[k], p.to[k], vc, wij, n, delta, m, R, dt);
+        p.cforce[k] = F; p.ctorque[k] = T;
+    }
+    for (size_t i = 0; i < N; i++) {
+        V3 Fi = v3(0, 0, 0), Ti = v3(0, 0, 0);
+        for (int k = p.rowStart((int)i); k < p.prefix[i]; k++) {
+            Fi += p.cforce[k];
+            Ti += p.ctorque[k] + cross(p.cpoint[k] - g.gpos[i], p.cforce[k]);
+        }
+        s.force[i] += Fi;
+        s.torque[i] += Ti;
+    }
+    for (size_t i = 0; i < N; i++) {
+        V3 Fi = v3(0, 0, 0), Ti = v3(0, 0, 0);
+        if (p.iStart[i] != -1) {
+            for (int k = p.iStart[i]; k < p.iEnd[i]; k++) {
+                int k1 = p.hashIndex[k];
+                Fi -= p.cforce[k1];
+                Ti -= p.ctorque[k1];
+                Ti -= cross(p.cpoint[k1] - g.gpos[i], p.cforce[k1]);
+            }
+        }
+        s.force[i] += Fi;
+        s.torque[i] += Ti;
     }
 }
 
@@ -958,10 +1094,12 @@ static void demStep(DEM& s) {
     if (s.iStep % 5 == 0) demNeighborSearch(s);
     demBallForces(s, hdt);
     demTriangleForces(s, dt);
+    for (auto& g : s.ghosts) demGhostForces(s, g, hdt);
     demExternal(s, s.time - hdt);
     demFirstHalf(s, hdt);
     demBallForces(s, hdt);
     demTriangleForces(s, dt);
+    for (auto& g : s.ghosts) demGhostForces(s, g, hdt);
     demExternal(s, s.time);
     demSecondHalf(s, hdt);
 }
@@ -1354,6 +1492,19 @@ int oracle_dem_initialize(void* h, const double* mn, const double* mx, const dou
     if (!s.ballGrid.valid || s.nb() == 0) return 2;
     s.bb = Pairs();
     s.bt = Pairs();
+    s.ghosts.clear();
+    auto addGhost = [&](int x, int y, int z) {
+        DEM::Ghost g;
+        g.dx = x; g.dy = y; g.dz = z;
+        s.ghosts.push_back(g);
+    };
+    if (s.perX) addGhost(1, 0, 0);
+    if (s.perY) addGhost(0, 1, 0);
+    if (s.perZ) addGhost(0, 0, 1);
+    if (s.perX && s.perY) addGhost(1, 1, 0);
+    if (s.perY && s.perZ) addGhost(0, 1, 1);
+    if (s.perX && s.perZ) addGhost(1, 0, 1);
+    if (s.perX && s.perY && s.perZ) addGhost(1, 1, 1);
     demNeighborSearch(s);
     demBallForces(s, 0.0);
     demTriangleForces(s, 0.0);
@@ -1376,6 +1527,27 @@ void oracle_dem_eval_forces(void* h, double dt, int walls, double dtWall) {
     if (walls) demTriangleForces(s, dtWall);
 }
 long oracle_dem_num_balls(void* h) { return (long)((DEM*)h)->nb(); }
+void oracle_dem_set_periodic(void* h, int x, int y, int z) {
+    DEM& s = *(DEM*)h;
+    if (x) s.perX = true;
+    if (y) s.perY = true;
+    if (z) s.perZ = true;
+}
+long oracle_dem_num_ghost_pairs(void* h, int set) {
+    DEM& s = *(DEM*)h;
+    return set >= 0 && set < (int)s.ghosts.size() ? (long)s.ghosts[set].p.n : 0;
+}
+void oracle_dem_get_ghost_pairs(void* h, int set, int* a, int* b, double* sl, double* force) {
+    DEM& s = *(DEM*)h;
+    if (set < 0 || set >= (int)s.ghosts.size()) return;
+    Pairs& p = s.ghosts[set].p;
+    for (size_t k = 0; k < p.n; k++) {
+        if (a) a[k] = p.pointed[k];
+        if (b) b[k] = p.pointing[k];
+        if (sl) st3(sl, k, p.sl[k]);
+        if (force) st3(force, k, p.cforce[k]);
+    }
+}
 long oracle_dem_num_pairs(void* h) { return (long)((DEM*)h)->bb.n; }
 long oracle_dem_num_wall_pairs(void* h) { return (long)((DEM*)h)->bt.n; }
 long oracle_dem_num_bonds(void* h) { return (long)((DEM*)h)->bA.size(); }

@@ -61,6 +61,9 @@ def lib():
             "oracle_dem_get_balls": (None, [_vp, _d, _d, _d, _d, _d]),
             "oracle_dem_set_balls": (None, [_vp, _d, _d, _d]),
             "oracle_dem_get_pairs": (None, [_vp, C.c_int, _i, _i, _d, _d, _d, _d, _d, _d, _d]),
+            "oracle_dem_set_periodic": (None, [_vp, C.c_int, C.c_int, C.c_int]),
+            "oracle_dem_num_ghost_pairs": (C.c_long, [_vp, C.c_int]),
+            "oracle_dem_get_ghost_pairs": (None, [_vp, C.c_int, _i, _i, _d, _d]),
             "oracle_dem_import_springs": (None, [_vp, C.c_long, _i, _i, _d, _d, _d]),
             "oracle_dem_get_bonds": (None, [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d]),
             "oracle_dem_num_clumps": (C.c_long, [_vp]),
@@ -227,6 +230,17 @@ class OracleDEM:
         self._L.oracle_dem_get_pairs(self.h, which, _ip(out["a"]), _ip(out["b"]), _dp(out["sliding"]),
                                      _dp(out["rolling"]), _dp(out["torsion"]), _dp(out["force"]),
                                      _dp(out["torque"]), _dp(out["point"]), _dp(out["overlap"]))
+        return out
+
+    def set_periodic(self, x, y, z):
+        self._L.oracle_dem_set_periodic(self.h, int(bool(x)), int(bool(y)), int(bool(z)))
+
+    def ghost_pairs(self, ghost_set):
+        n = self._L.oracle_dem_num_ghost_pairs(self.h, int(ghost_set))
+        out = {"a": np.zeros(n, np.int32), "b": np.zeros(n, np.int32), "sliding": np.zeros((n, 3)),
+               "force": np.zeros((n, 3))}
+        self._L.oracle_dem_get_ghost_pairs(self.h, int(ghost_set), _ip(out["a"]), _ip(out["b"]),
+                                           _dp(out["sliding"]), _dp(out["force"]))
         return out
 
     def import_springs(self, a, b, sliding, rolling, torsion):

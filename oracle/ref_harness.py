@@ -57,7 +57,10 @@ def lib():
         L.luanchSumBallContactForceTorque.argtypes = [p] * 10 + [sz, sz, sz, vp]
         L.buildHashStartEnd.argtypes = [p, p, p, p, sz, sz, sz, sz, vp]
         L.ref_set_contact_tables.argtypes = [C.c_int, p, C.c_int, p, C.c_int, p, vp]
-        for f in ("launchUpdateSpatialGridCellHashStartEnd", "launchCountSPHInteractions",
+        L.launchBuildDummyPosition.argtypes = [p, p, D3, D3, D3, I3, sz, sz, sz, vp]
+        L.launchUpdateDummySpatialGridCellHashStartEnd.argtypes = [p, p, p, p, p, D3, D3, D3, I3, sz, sz, sz, sz, vp]
+        for f in ("launchBuildDummyPosition", "launchUpdateDummySpatialGridCellHashStartEnd",
+                  "launchUpdateSpatialGridCellHashStartEnd", "launchCountSPHInteractions",
                   "launchWriteSPHInteractions", "launchCountSPHDummyInteractions", "launchWriteSPHDummyInteractions",
                   "launchCalDummyParticleNormal", "launchWCSPH1stHalfIntegration", "launchWCSPH2ndHalfIntegration",
                   "launchCountBallInteractions", "launchWriteBallInteractions",
@@ -341,3 +344,51 @@ class RefDEMPairs:
     def pairs(self):
         self.t.cuda.synchronize()
         return self.pointed[:self.P].cpu().numpy(), self.pointing[:self.P].cpu().numpy()
+
+    def ghost_pass(self, direction, dt):
+        """addDummyContactForceTorque(periodic, direction, dt) (DEMSolver.h:
+        279-426) from fresh lists, adding into force / torque; returns the
+        ghost pairs (pointed, pointing) and their contact forces."""
+        L, t, n = lib(), self.t, self.n
+        f64, i32 = t.float64, t.int32
+        dummy = t.zeros((n, 3), dtype=f64, device=self.dev)
+        L.launchBuildDummyPosition(P(dummy), P(self.pos), self.mn, self.mx, self.cs, I3(*direction), n,
+                                   self.grid[0], self.grid[1], self.stream)
+        L.launchUpdateDummySpatialGridCellHashStartEnd(P(dummy), P(self.hashIndex), P(self.hashValue),
+                                                       P(self.cellStart), P(self.cellEnd), self.mn, self.mx, self.cs,
+                                                       self.gs, self.ng, n, self.grid[0], self.grid[1], self.stream)
+        count = t.zeros(n, dtype=i32, device=self.dev)
+        prefix = t.zeros(n, dtype=i32, device=self.dev)
+        L.launchCountBallInteractions(P(dummy), P(self.rad), P(self.invm), P(self.clump), P(self.hashIndex),
+                                      P(count), P(prefix), P(self.cellStart), P(self.cellEnd), self.mn, self.cs,
+                                      self.gs, n, self.grid[0], self.grid[1], self.stream)
+        t.cuda.synchronize()
+        Pn = int(prefix[n - 1].item())
+        cap = max(Pn, 1)
+        z3 = lambda: t.zeros((cap, 3), dtype=f64, device=self.dev)
+        sl, ro, to, cF, cT, cP, cN = z3(), z3(), z3(), z3(), z3(), z3(), z3()
+        ov = t.zeros(cap, dtype=f64, device=self.dev)
+        pointed = t.zeros(cap, dtype=i32, device=self.dev)
+        pointing = t.zeros(cap, dtype=i32, device=self.dev)
+        iStart = t.full((n,), -1, dtype=i32, device=self.dev)
+        iEnd = t.full((n,), -1, dtype=i32, device=self.dev)
+        oldHash = t.full((cap,), -1, dtype=i32, device=self.dev)
+        oldPointed = t.zeros(cap, dtype=i32, device=self.dev)
+        L.launchWriteBallInteractions(P(dummy), P(self.rad), P(self.invm), P(self.clump), P(self.hashIndex),
+                                      P(prefix), P(iStart), P(iEnd), P(sl), P(ro), P(to), P(pointed), P(pointing),
+                                      P(sl), P(ro), P(to), P(oldPointed), P(oldHash), P(self.cellStart),
+                                      P(self.cellEnd), self.mn, self.cs, self.gs, n, self.grid[0], self.grid[1],
+                                      self.stream)
+        pHash = t.full((cap,), -1, dtype=i32, device=self.dev)
+        if Pn > 0:
+            pValue = pointing.clone()
+            pg = _launch_dims(Pn)
+            L.buildHashStartEnd(P(iStart), P(iEnd), P(pHash), P(pValue), n, Pn, pg[0], pg[1], self.stream)
+            g = _launch_dims(Pn)
+            L.luanchCalculateBallContactForceTorque(P(dummy), P(self.vel), P(self.w), P(self.rad), P(self.invm),
+                                                    P(self.mat), P(sl), P(ro), P(to), P(cF), P(cT), P(cP), P(cN),
+                                                    P(ov), P(pointed), P(pointing), dt, Pn, g[0], g[1], self.stream)
+        L.luanchSumBallContactForceTorque(P(dummy), P(self.force), P(self.torque), P(prefix), P(iStart), P(iEnd),
+                                          P(cF), P(cT), P(cP), P(pHash), n, self.grid[0], self.grid[1], self.stream)
+        t.cuda.synchronize()
+        return (pointed[:Pn].cpu().numpy(), pointing[:Pn].cpu().numpy(), cF[:Pn].cpu().numpy())

@@ -32,6 +32,8 @@ def oracle_dem(scene):
             o.set_wall_motion(k, wl["velocity"], wl.get("angularVelocity", (0, 0, 0)))
     if scene.buoyancy is not None:
         o.set_buoyancy_drag(*scene.buoyancy)
+    if getattr(scene, "periodic", None) is not None:
+        o.set_periodic(*scene.periodic)
     o.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt)
     if scene.bond_initial_contacts:
         p = o.pairs(0)

@@ -16,12 +16,19 @@ constexpr int kScanBlock = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanBlock * kScanItems;
 
-// Histogram: key[i] = clamped cell key of object i; cnt[key]++.
+// Histogram: key[i] = clamped cell key of object i; cnt[key]++.  With
+// outsideOnly, objects inside the domain get key -1 and stay out of the table
+// (calculateDummyHash, neighborSearchKernel.cu:29-55).
 static __global__ void k_cell_count(const double4* __restrict__ p, int n, GridDesc g, int* __restrict__ key,
-                             int* __restrict__ cnt) {
+                             int* __restrict__ cnt, int outsideOnly) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 q = p[i];
+    if (outsideOnly && q.x >= g.mn.x && q.x < g.mx.x && q.y >= g.mn.y && q.y < g.mx.y && q.z >= g.mn.z &&
+        q.z < g.mx.z) {
+        key[i] = -1;
+        return;
+    }
     int k = clamped_key(mk3(q.x, q.y, q.z), g);
     key[i] = k;
     atomicAdd(cnt + k, 1);
@@ -79,6 +86,7 @@ static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const 
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int k = key[i];
+    if (k < 0) return;
     int slot = start[k] + atomicSub(cnt + k, 1) - 1;
     sorted[slot] = i;
 }
@@ -89,9 +97,9 @@ static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const 
 // cell costs O(members) per thread instead of a serial insertion sort.
 static __global__ void k_cell_rank(int n, const int* __restrict__ key, const int* __restrict__ start,
                                    const int* __restrict__ unordered, int* __restrict__ sorted,
-                                   const int* __restrict__ orderKey) {
+                                   const int* __restrict__ orderKey, int ncell) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= n || s >= start[ncell]) return;  // start[ncell] = objects in the table
     int v = unordered[s];
     int c = key[v];
     int b = start[c], e = start[c + 1];
@@ -155,16 +163,17 @@ struct CellTable {
         launches++;
     }
     // Sorts objects p[0..n) (positions in .xyz) into cells.
-    void build(const double4* p, int n, cudaStream_t s, const int* orderKey = nullptr) {
+    // outsideOnly: only objects outside the domain enter the table.
+    void build(const double4* p, int n, cudaStream_t s, const int* orderKey = nullptr, bool outsideOnly = false) {
         launches = 0;
         if (n > 0) {
-            k_cell_count<<<grid_for(n, 256), 256, 0, s>>>(p, n, g, key.p, cnt.p);
+            k_cell_count<<<grid_for(n, 256), 256, 0, s>>>(p, n, g, key.p, cnt.p, outsideOnly ? 1 : 0);
             launches++;
         }
         scan(cnt.p, start.p, ncell, 0, s);
         if (n > 0) {
             k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, unordered.p);
-            k_cell_rank<<<grid_for(n, 256), 256, 0, s>>>(n, key.p, start.p, unordered.p, sorted.p, orderKey);
+            k_cell_rank<<<grid_for(n, 256), 256, 0, s>>>(n, key.p, start.p, unordered.p, sorted.p, orderKey, ncell);
             launches += 2;
         }
         DEMSPH_LAUNCH_CHECK();

@@ -47,8 +47,9 @@ struct DemDev {
     double4* torqueA;
     const int* mat;
     const int* clump;
-    const int* order;      // cell-sorted ball list
-    const int* cellStart;  // ball grid
+    const int* order;      // cell-sorted candidate list (balls, or periodic ghosts)
+    const int* qorder;     // the balls that query the lists, in cell order
+    const int* cellStart;  // candidate grid
     // current / previous pair lists
     int* pj;
     int* pcnt;
@@ -133,7 +134,7 @@ struct DemDev {
 __global__ void k_dem_build_pairs(DemDev d) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= d.N) return;
-    const int A = d.order[t];
+    const int A = d.qorder[t];
     const double4 pa = d.pos[A];
     const double3 ra = xyz(pa);
     const double imA = d.vel[A].w;
@@ -230,7 +231,7 @@ template <class R>
 __global__ void __launch_bounds__(128, 4) k_dem_pair_forces(DemDev d, double dt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= d.N) return;
-    const int A = d.order[t];
+    const int A = d.qorder[t];
     const double4 pa = d.pos[A];
     const double3 ra = xyz(pa);
     const double4 va4 = d.vel[A];
@@ -624,6 +625,43 @@ __global__ void k_dem_circumcenters(DemDev d) {
     d.tcenter[t] = d4(circumcenter(xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]), xyz(d.vglobal[tv.z])), 0);
 }
 
+// -------------------------------------------------------- periodic ghosts --
+// buildDummyPosition (neighborSearchKernel.cu:57-77): every ball, shifted by
+// the domain length along each flagged axis where it lies within one cell of
+// the lower face.
+__global__ void k_dem_ghost_pos(int n, const double4* __restrict__ pos, double4* __restrict__ gpos, GridDesc g,
+                                int3 dir) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = pos[i];
+    const double3 L = g.mx - g.mn;
+    if (dir.x == 1 && p.x - g.mn.x < g.cs.x) p.x += L.x;
+    if (dir.y == 1 && p.y - g.mn.y < g.cs.y) p.y += L.y;
+    if (dir.z == 1 && p.z - g.mn.z < g.cs.z) p.z += L.z;
+    gpos[i] = p;
+}
+// Adds one ghost pass's pair forces into the A-side accumulators: the
+// pointed-side sums (written by k_dem_pair_forces into FA / TA) and the
+// pointing-side sums over the ghost reverse lists
+// (sumObjectPointed / sumObjectPointingForceTorqueFromInteractionKernel,
+// contactKernel.cu:657-714, with the ghost positions as torque arms).
+__global__ void k_dem_ghost_sum(int n, const double4* __restrict__ FA, const double4* __restrict__ TA,
+                                const int* __restrict__ rcnt, const int* __restrict__ rslot, int KR,
+                                const double4* __restrict__ pF, const double4* __restrict__ pTB,
+                                double4* __restrict__ forceA, double4* __restrict__ torqueA) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 F = xyz(FA[i]), T = xyz(TA[i]);
+    const int c = min(rcnt[i], KR);
+    for (int r = 0; r < c; r++) {
+        const int slot = rslot[(size_t)r * n + i];
+        F -= xyz(pF[slot]);
+        T += xyz(pTB[slot]);
+    }
+    forceA[i] = d4(xyz(forceA[i]) + F, 0);
+    torqueA[i] = d4(xyz(torqueA[i]) + T, 0);
+}
+
 // ------------------------------------------------------------ batching ----
 // Places one batch member's balls at [start, start + n) of the batch arrays,
 // translated by off, with material ids shifted by matOff.
@@ -762,6 +800,29 @@ struct DemScene {
     DBuf<double4> fconst;
     DBuf<DevStatus> status;
 
+    // Periodic boundaries (setPeriodicBoundary, DEMSolver.h:1944-1959): one
+    // ghost set per active direction, passed in the reference's order X, Y,
+    // Z, XY, YZ, XZ, XYZ (DEMSolver.h:1416-1422).  Each force evaluation of a
+    // step rebuilds the set's ghost positions, its table of ghosts that left
+    // the domain, its ghost pair list (springs carried from the previous
+    // evaluation's list) and adds the ghost pair forces
+    // (addDummyContactForceTorque, DEMSolver.h:279-426).
+    struct GhostSet {
+        int3 dir;
+        DBuf<double4> gpos;
+        CellTable cells;
+        DBuf<int> pj[2], pcnt[2];
+        DBuf<double4> spS[2], spR[2], spT[2];
+        int cur = 0;
+        bool have = false;
+        DBuf<double4> pF, pTB, FA, TA;
+        DBuf<int> rcnt, rslot;
+        int K = 8, KR = 8;
+    };
+    bool perX = false, perY = false, perZ = false;
+    std::vector<std::unique_ptr<GhostSet>> ghosts;
+    DBuf<DevStatus> gstatus;
+
     int nB = 0;                // balls (the host arrays' size until a batch assembly)
     bool assembled = false;    // balls placed on the device from member records
     double assembledRmax = 0;  // their largest radius
@@ -777,7 +838,7 @@ struct DemScene {
         d.mats = mats.p;
         d.pos = pos.p; d.vel = vel.p; d.angv = angv.p; d.force = force.p; d.torque = torque.p;
         d.forceA = forceA.p; d.torqueA = torqueA.p; d.mat = mat.p; d.clump = clump.p;
-        d.order = ballCells.sorted.p; d.cellStart = ballCells.start.p;
+        d.order = ballCells.sorted.p; d.qorder = ballCells.sorted.p; d.cellStart = ballCells.start.p;
         int o = cur ^ 1;
         d.pj = pj[cur].p; d.pcnt = pcnt[cur].p; d.spS = spS[cur].p; d.spR = spR[cur].p; d.spT = spT[cur].p;
         if (withOld && havePairs) {
@@ -949,6 +1010,119 @@ struct DemScene {
 
     void launch_count(int k) { g_launches += k; }
 
+    // ------------------------------------------------- periodic ghosts -----
+    void ghost_alloc(GhostSet& g) {
+        const size_t n = (size_t)N();
+        for (int b = 0; b < 2; b++) {
+            g.pj[b].alloc(n * g.K, s, true);
+            g.pcnt[b].alloc(n, s, true);
+            g.spS[b].alloc(n * g.K, s, true);
+            g.spR[b].alloc(roll ? n * g.K : 1, s, true);
+            g.spT[b].alloc(tors ? n * g.K : 1, s, true);
+        }
+        g.pF.alloc(n * g.K, s, true);
+        g.pTB.alloc(n * g.K, s, true);
+        g.FA.alloc(n, s, true);
+        g.TA.alloc(n, s, true);
+        g.rcnt.alloc(n, s, true);
+        g.rslot.alloc(n * g.KR, s, true);
+    }
+    void ghost_setup() {
+        ghosts.clear();
+        auto add = [&](int x, int y, int z) {
+            auto g = std::make_unique<GhostSet>();
+            g->dir = make_int3(x, y, z);
+            ghosts.push_back(std::move(g));
+        };
+        if (perX) add(1, 0, 0);
+        if (perY) add(0, 1, 0);
+        if (perZ) add(0, 0, 1);
+        if (perX && perY) add(1, 1, 0);
+        if (perY && perZ) add(0, 1, 1);
+        if (perX && perZ) add(1, 0, 1);
+        if (perX && perY && perZ) add(1, 1, 1);
+        for (auto& g : ghosts) {
+            g->gpos.alloc(N(), s, false);
+            g->cells.setup(ballCells.g, N(), s);
+            ghost_alloc(*g);
+        }
+        gstatus.alloc(1, s, true);
+    }
+    // Capacity growth keeps the k*N + A layout, as for the main lists.
+    void ghost_grow(int needPairs, int needRev) {
+        const size_t n = (size_t)N();
+        for (auto& gp : ghosts) {
+            GhostSet& g = *gp;
+            if (needPairs > g.K) {
+                graph.reset();
+                const int nk = needPairs + needPairs / 4 + 1;
+                for (int b = 0; b < 2; b++) {
+                    g.pj[b].grow(n * nk, s);
+                    g.spS[b].grow(n * nk, s);
+                    if (roll) g.spR[b].grow(n * nk, s);
+                    if (tors) g.spT[b].grow(n * nk, s);
+                }
+                g.pF.alloc(n * nk, s, true);
+                g.pTB.alloc(n * nk, s, true);
+                g.K = nk;
+            }
+            if (needRev > g.KR) {
+                graph.reset();
+                const int nk = needRev + needRev / 4 + 1;
+                g.rslot.alloc(n * nk, s, true);
+                g.KR = nk;
+            }
+        }
+    }
+    DemDev ghost_view(GhostSet& g) {
+        DemDev d = dev(false);
+        d.pos = g.gpos.p;
+        d.order = g.cells.sorted.p;
+        d.cellStart = g.cells.start.p;
+        d.K = g.K;
+        d.KR = g.KR;
+        const int o = g.cur ^ 1;
+        d.pj = g.pj[g.cur].p; d.pcnt = g.pcnt[g.cur].p;
+        d.spS = g.spS[g.cur].p; d.spR = g.spR[g.cur].p; d.spT = g.spT[g.cur].p;
+        if (g.have) {
+            d.pjOld = g.pj[o].p; d.pcntOld = g.pcnt[o].p;
+            d.spSOld = g.spS[o].p; d.spROld = g.spR[o].p; d.spTOld = g.spT[o].p;
+        } else {
+            d.pjOld = nullptr; d.pcntOld = nullptr; d.spSOld = nullptr; d.spROld = nullptr; d.spTOld = nullptr;
+        }
+        d.pF = g.pF.p; d.pTB = g.pTB.p;
+        d.forceA = g.FA.p; d.torqueA = g.TA.p;
+        d.rcnt = g.rcnt.p; d.rslot = g.rslot.p;
+        d.status = gstatus.p;
+        d.nBond = 0;
+        d.nTri = 0;
+        return d;
+    }
+    // addDummyContactForceTorque (DEMSolver.h:279-426) of every active set,
+    // added into the pointed-side accumulators of this force evaluation.
+    void ghost_passes(double dt) {
+        const int n = N();
+        for (auto& gp : ghosts) {
+            GhostSet& g = *gp;
+            k_dem_ghost_pos<<<grid_for(n, 256), 256, 0, s>>>(n, pos.p, g.gpos.p, ballCells.g, g.dir);
+            g.cells.build(g.gpos.p, n, s, nullptr, true);
+            launch_count(1 + g.cells.launches);
+            g.cur ^= 1;
+            DemDev d = ghost_view(g);
+            k_dem_build_pairs<<<grid_for(n, 128), 128, 0, s>>>(d);
+            DEMSPH_CUDA(cudaMemsetAsync(g.rcnt.p, 0, sizeof(int) * n, s));
+            k_dem_reverse<<<grid_for(n, 256), 256, 0, s>>>(d);
+            k_dem_reverse_order<<<grid_for(n, 256), 256, 0, s>>>(d);
+            if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+            else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+            k_dem_ghost_sum<<<grid_for(n, 256), 256, 0, s>>>(n, g.FA.p, g.TA.p, g.rcnt.p, g.rslot.p, g.KR, g.pF.p,
+                                                             g.pTB.p, forceA.p, torqueA.p);
+            launch_count(5);
+            DEMSPH_LAUNCH_CHECK();
+            g.have = true;
+        }
+    }
+
     // ------------------------------------------------------- pieces ------
     void neighbor_search() {
         ballCells.build(pos.p, N(), s);
@@ -970,12 +1144,14 @@ struct DemScene {
     }
     // calculateBallContactForceTorque(dt) [+ addTriangleContactForceTorque(dtWall)]
     // [+ external hook at extTime] [+ half-step integration]
-    void force_eval(double dt, bool walls, double dtWall, bool ext, double extTime, int integ, double hdt) {
+    void force_eval(double dt, bool walls, double dtWall, bool ext, double extTime, int integ, double hdt,
+                    bool ghostPass = false) {
         DemDev d = dev(false);
         const int n = N();
         if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
         else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
         launch_count(1);
+        if (ghostPass && !ghosts.empty()) ghost_passes(dt);
         if (d.nBond) {
             k_dem_bonds<<<grid_for(d.nBond, 128), 128, 0, s>>>(d, dt);
             launch_count(1);
@@ -1019,8 +1195,8 @@ struct DemScene {
         time += dt;
         if (iStep % 5 == 0) neighbor_search();
         bool walls = !hTris.empty();
-        force_eval(hdt, walls, dt, true, time - hdt, 1, hdt);
-        force_eval(hdt, walls, dt, true, time, 2, hdt);
+        force_eval(hdt, walls, dt, true, time - hdt, 1, hdt, true);
+        force_eval(hdt, walls, dt, true, time, 2, hdt, true);
     }
     // Ten steps per graph, starting one step after a re-sort: two re-sorts
     // per replay, so the pair and wall-row buffer indices are back to their
@@ -1029,7 +1205,11 @@ struct DemScene {
     GraphSet graph;
     bool useGraphs = true;
     static constexpr int kGraphSteps = 10;
-    int index_key() const { return cur | wcur << 1; }
+    int index_key() const {
+        int k = cur | wcur << 1;
+        for (size_t g = 0; g < ghosts.size(); g++) k |= (ghosts[g]->cur | (ghosts[g]->have ? 2 : 0)) << (2 + 2 * g);
+        return k;
+    }
     bool graphable() const { return useGraphs && !(framp > 0) && ready; }
 
     DevStatus read_status() {
@@ -1051,6 +1231,7 @@ struct DemScene {
         int cur, wcur;
         bool havePairs, haveWallRows;
         int K, KT;
+        std::vector<std::pair<int, bool>> ghost;  // (cur, have) per ghost set
     };
     // The snapshot's device copies are kept between calls and reused while
     // they are large enough, so a step() call allocates nothing after the first.
@@ -1083,6 +1264,16 @@ struct DemScene {
         snap_add(sn, bFn); snap_add(sn, bTt); snap_add(sn, bsmax); snap_add(sn, btmax);
         snap_add(sn, wpos); snap_add(sn, wq); snap_add(sn, vglobal); snap_add(sn, tcenter);
         snap_add(sn, cpos); snap_add(sn, cvel); snap_add(sn, cangv); snap_add(sn, cq);
+        sn.ghost.clear();
+        for (auto& gp : ghosts) {
+            GhostSet& g = *gp;
+            sn.ghost.push_back({g.cur, g.have});
+            for (int b = 0; b < 2; b++) {
+                snap_add(sn, g.pj[b]); snap_add(sn, g.pcnt[b]); snap_add(sn, g.spS[b]);
+                if (roll) snap_add(sn, g.spR[b]);
+                if (tors) snap_add(sn, g.spT[b]);
+            }
+        }
     }
     Snap snap;
     void restore(Snap& sn) {
@@ -1094,13 +1285,19 @@ struct DemScene {
         }
         iStep = sn.iStep; time = sn.time; cur = sn.cur; wcur = sn.wcur; havePairs = sn.havePairs;
         haveWallRows = sn.haveWallRows;
+        for (size_t g = 0; g < ghosts.size() && g < sn.ghost.size(); g++) {
+            ghosts[g]->cur = sn.ghost[g].first;
+            ghosts[g]->have = sn.ghost[g].second;
+        }
     }
 
     void steps_graph(long n) {
         long k = 0;
         if (graphable()) {
             for (; k < n && iStep % 5 != 0; k++) step_once();
-            if (n - k >= kGraphSteps) {
+            // the buffer-state key is taken per block: the first block after
+            // initialisation also switches ghost lists to spring carry
+            for (; k + kGraphSteps <= n; k += kGraphSteps) {
                 StepGraph& gr = graph.at(index_key());
                 if (!gr.ready()) {
                     const long i0 = iStep;
@@ -1111,11 +1308,9 @@ struct DemScene {
                     iStep = i0;
                     time = t0;
                 }
-                for (; k + kGraphSteps <= n; k += kGraphSteps) {
-                    gr.launch(s);
-                    iStep += kGraphSteps;
-                    time += kGraphSteps * dt;
-                }
+                gr.launch(s);
+                iStep += kGraphSteps;
+                time += kGraphSteps * dt;
             }
         }
         for (; k < n; k++) step_once();
@@ -1128,10 +1323,17 @@ struct DemScene {
             Snap& sn = snap;
             take(sn);
             clear_status();
+            if (!ghosts.empty()) DEMSPH_CUDA(cudaMemsetAsync(gstatus.p, 0, sizeof(DevStatus), s));
             steps_graph(n);
             DevStatus st = read_status();
-            if (!st.overflow) return;
-            grow(st.need_pairs, st.need_rev, st.need_aux);
+            DevStatus gs{};
+            if (!ghosts.empty()) {
+                DEMSPH_CUDA(cudaMemcpyAsync(&gs, gstatus.p, sizeof gs, cudaMemcpyDeviceToHost, s));
+                DEMSPH_CUDA(cudaStreamSynchronize(s));
+            }
+            if (!st.overflow && !gs.overflow) return;
+            if (st.overflow) grow(st.need_pairs, st.need_rev, st.need_aux);
+            if (gs.overflow) ghost_grow(gs.need_pairs, gs.need_rev);
             restore(sn);
             // rows past the old capacity hold stale data; the rebuild rewrites them.
         }
@@ -1199,6 +1401,7 @@ struct DemScene {
         // lists
         alloc_pairs();
         alloc_wall_rows();
+        ghost_setup();
         cur = 0; wcur = 0; havePairs = false; haveWallRows = false;
         // neighbour search + one dt = 0 force evaluation (DEMSolver.h:1995-1997);
         // grow and redo when a first guess of a capacity was too small.
@@ -1548,6 +1751,17 @@ int demsph_dem_set_buoyancy_drag(demsph_dem_t h, double rho, double cd, const do
         s.buoy = 1; s.brho = rho; s.bcd = cd; s.bg3 = ld3(g, 0); s.bu = ld3(u, 0); s.blevel = lvl;
     });
 }
+int demsph_dem_set_periodic(demsph_dem_t h, int x, int y, int z) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "periodic boundaries must be set before initialisation");
+        // setPeriodicBoundary (DEMSolver.h:1944-1959): flags accumulate
+        if (x) s.perX = true;
+        if (y) s.perY = true;
+        if (z) s.perZ = true;
+    });
+}
 int demsph_dem_initialize(demsph_dem_t h, const double* mn, const double* mx, const double* g, double dt, int prec) {
     return guarded([&] {
         SCENE_CHECK(h);
@@ -1584,7 +1798,8 @@ int demsph_dem_eval_forces(demsph_dem_t h, double dt, int walls, double dtWall) 
         SCENE_CHECK(h);
         DemScene& s = h->sc;
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
-        s.force_eval(dt, walls != 0, dtWall, false, 0.0, 0, 0.0);
+        s.graph.reset();  // the ghost passes flip list buffers outside a graph
+        s.force_eval(dt, (walls & 1) != 0, dtWall, false, 0.0, 0, 0.0, (walls & 2) != 0);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
     });
 }
@@ -1676,7 +1891,14 @@ int demsph_dem_set_balls(demsph_dem_t h, const double* pos, const double* vel, c
 static void collect_rows(DemScene& s, int which, std::vector<int>& A, std::vector<int>& B, std::vector<size_t>& slot) {
     int n = s.N();
     std::vector<int> cnt, ids;
-    if (which == 0) {
+    if (which >= 2) {  // periodic ghost set which - 2
+        const size_t g = (size_t)(which - 2);
+        if (g >= s.ghosts.size()) throw Status(DEMSPH_ERR_INVALID, "no such periodic ghost set");
+        DemScene::GhostSet& gs = *s.ghosts[g];
+        if (!gs.have) return;
+        gs.pcnt[gs.cur].download(cnt, s.s);
+        gs.pj[gs.cur].download(ids, s.s);
+    } else if (which == 0) {
         if (!s.havePairs) return;
         s.pcnt[s.cur].download(cnt, s.s);
         s.pj[s.cur].download(ids, s.s);
@@ -1712,12 +1934,23 @@ int demsph_dem_get_pairs(demsph_dem_t h, int which, int* a, int* b, double* slid
         std::vector<size_t> sl;
         collect_rows(s, which, A, B, sl);
         std::vector<double4> S, Rr, T, F, TB;
-        int c = which == 0 ? s.cur : s.wcur;
-        if (sliding) (which == 0 ? s.spS[c] : s.wS[c]).download(S, s.s);
-        if (rolling && s.roll) (which == 0 ? s.spR[c] : s.wR[c]).download(Rr, s.s);
-        if (torsion && s.tors) (which == 0 ? s.spT[c] : s.wT[c]).download(T, s.s);
-        if (which == 0 && force) s.pF.download(F, s.s);
-        if (which == 0 && torque) s.pTB.download(TB, s.s);
+        if (which >= 2) {
+            DemScene::GhostSet& g = *s.ghosts[which - 2];
+            if (!A.empty()) {
+                if (sliding) g.spS[g.cur].download(S, s.s);
+                if (rolling && s.roll) g.spR[g.cur].download(Rr, s.s);
+                if (torsion && s.tors) g.spT[g.cur].download(T, s.s);
+                if (force) g.pF.download(F, s.s);
+                if (torque) g.pTB.download(TB, s.s);
+            }
+        } else {
+            int c = which == 0 ? s.cur : s.wcur;
+            if (sliding) (which == 0 ? s.spS[c] : s.wS[c]).download(S, s.s);
+            if (rolling && s.roll) (which == 0 ? s.spR[c] : s.wR[c]).download(Rr, s.s);
+            if (torsion && s.tors) (which == 0 ? s.spT[c] : s.wT[c]).download(T, s.s);
+            if (which == 0 && force) s.pF.download(F, s.s);
+            if (which == 0 && torque) s.pTB.download(TB, s.s);
+        }
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         std::vector<double4> P;
         if (which == 0 && torque) s.pos.download(P, s.s);
@@ -1728,8 +1961,8 @@ int demsph_dem_get_pairs(demsph_dem_t h, int which, int* a, int* b, double* slid
             if (sliding) st3(sliding, k, xyz(S[sl[k]]));
             if (rolling) st3(rolling, k, s.roll ? xyz(Rr[sl[k]]) : mk3(0, 0, 0));
             if (torsion) st3(torsion, k, s.tors ? xyz(T[sl[k]]) : mk3(0, 0, 0));
-            if (force) st3(force, k, which == 0 ? xyz(F[sl[k]]) : mk3(0, 0, 0));
-            if (torque) st3(torque, k, which == 0 ? xyz(TB[sl[k]]) : mk3(0, 0, 0));
+            if (force) st3(force, k, which != 1 ? xyz(F[sl[k]]) : mk3(0, 0, 0));
+            if (torque) st3(torque, k, which != 1 ? xyz(TB[sl[k]]) : mk3(0, 0, 0));
         }
     });
 }

@@ -182,6 +182,7 @@ class DEMScene:
     clumps: list = field(default_factory=list)   # dicts of addClump args
     bond_initial_contacts: bool = False          # the addInitialCondition hook of the bonded scenes
     buoyancy: tuple = None                       # (rho, Cd, g, u, level)
+    periodic: tuple = None                       # setPeriodicBoundary(X, Y, Z)
     minb: tuple = (0, 0, 0)
     maxb: tuple = (1, 1, 1)
     gravity: tuple = (0, 0, -9.81)
@@ -276,6 +277,29 @@ def ice_cylinder_reference():
         dt=tc / 50.0, steps=int(50.0 / (tc / 50.0)) + 2)
     sc.buoyancy = (1000.0, 0.1, (0.0, 0.0, -9.81), (-0.4, 0.0, 0.0), level)
     sc.bond_initial_contacts = True
+    return sc
+
+
+def dem_periodic_box(n_side=10, radius=0.005, density=2500.0, squeeze=0.985, seed=5, periodic=(True, True, False),
+                     E=1e8, nu=0.3, restitution=0.8, mu=0.3, speed=0.05, dt=1e-5):
+    """A box exactly tiled by an n_side^3 lattice of Hertz-Mindlin spheres
+    (pitch 2 r squeeze, so neighbours overlap by 1.5% of a diameter), with
+    seeded random velocities: the lattice is continuous across the box faces,
+    so the periodic ghost passes (setPeriodicBoundary) find contacts across
+    every periodic face."""
+    rng = np.random.default_rng(seed)
+    pitch = 2.0 * radius * squeeze
+    g = (np.arange(n_side) + 0.5) * pitch
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    n = p.shape[0]
+    L = n_side * pitch
+    Es, Gs = hertz_params(E, nu)
+    sc = DEMScene(name="dem_periodic_box", position=p, radius=np.full(n, radius), density=np.full(n, density),
+                  material=np.zeros(n, np.int32), velocity=rng.uniform(-speed, speed, (n, 3)),
+                  hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)], minb=(0.0, 0.0, 0.0),
+                  maxb=(L, L, L), gravity=(0.0, 0.0, 0.0), dt=dt, steps=100)
+    sc.periodic = tuple(bool(v) for v in periodic)
     return sc
 
 
@@ -452,6 +476,8 @@ def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
             s.setMeshWallMotion(k, w["velocity"], w.get("angularVelocity", (0, 0, 0)))
     if scene.buoyancy is not None:
         s.setBuoyancyDrag(*scene.buoyancy)
+    if scene.periodic is not None:
+        s.setPeriodicBoundary(*scene.periodic)
     if initialize:
         s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
         if scene.bond_initial_contacts:

@@ -207,8 +207,9 @@ class DEMSolver:
         call("demsph_dem_add_bonds", self._h, a.shape[0], _ip(a), _ip(b), _dp(p), p.shape[0])
 
     def setPeriodicBoundary(self, X, Y, Z):
-        if X or Y or Z:
-            raise NotImplementedError("periodic boundaries are not built in this library yet")
+        """setPeriodicBoundary (DEMSolver.h:1944-1959): periodic ghost passes
+        along the flagged axes (before initialize)."""
+        call("demsph_dem_set_periodic", self._h, int(bool(X)), int(bool(Y)), int(bool(Z)))
 
     # ------------------------------------------------ external force hook --
     def setConstantForce(self, force, rampTime=0.0):
@@ -259,8 +260,9 @@ class DEMSolver:
     def calculateBallContactForceTorque(self, timeStep):
         call("demsph_dem_eval_forces", self._h, float(timeStep), 0, 0.0)
 
-    def evalForces(self, timeStep, walls=False, wallTimeStep=0.0):
-        call("demsph_dem_eval_forces", self._h, float(timeStep), int(bool(walls)), float(wallTimeStep))
+    def evalForces(self, timeStep, walls=False, wallTimeStep=0.0, periodic=False):
+        flags = (1 if walls else 0) | (2 if periodic else 0)
+        call("demsph_dem_eval_forces", self._h, float(timeStep), flags, float(wallTimeStep))
 
     # ------------------------------------------------------------ getters --
     def _n(self, fn, *a):
