@@ -134,6 +134,12 @@ int demsph_dem_set_buoyancy_drag(demsph_dem_t s, double fluidDensity, double dra
  * with which = 2 + k returns the pairs of the k-th active ghost set (order X,
  * Y, Z, XY, YZ, XZ, XYZ over the active ones). */
 int demsph_dem_set_periodic(demsph_dem_t s, int x, int y, int z);
+/* No counterpart in the reference.  List capacities per ball (pair rows,
+ * reverse rows, candidate triangles): reserve raises the initial capacities
+ * before initialize (they still grow on demand), capacity reads the current
+ * ones. */
+int demsph_dem_reserve(demsph_dem_t s, int pairsPerBall, int reversePerBall, int trianglesPerBall);
+int demsph_dem_capacity(demsph_dem_t s, int* pairsPerBall, int* reversePerBall, int* trianglesPerBall);
 int demsph_dem_initialize(demsph_dem_t s, const double* minBoundary, const double* maxBoundary,
                           const double* gravity, double timeStep, int precision);
 /* numSteps passes of the step loop (loop_ball / loop_ball_wall,

@@ -72,6 +72,8 @@ SIGNATURES = {
     "demsph_dem_assemble_balls": [_vp, _int, _pvp, _d, _i],
     "demsph_dem_set_graphs": [_vp, _int],
     "demsph_dem_set_periodic": [_vp, _int, _int, _int],
+    "demsph_dem_reserve": [_vp, _int, _int, _int],
+    "demsph_dem_capacity": [_vp, _i, _i, _i],
     "demsph_dem_write_vtu": [_vp, C.c_char_p, _long, _int],
     "demsph_dem_copy_members": [_vp, _vp, _int, _i, _i, _i, _i, _d],
     "demsph_dem_get_bonds": [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d],

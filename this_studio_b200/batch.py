@@ -28,6 +28,8 @@ the edge cells of the batch domain rather than of its own.
 from __future__ import annotations
 
 import math
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -79,6 +81,36 @@ def tile_offsets(boxes, gap):
         x += sz[0] + gap
         row_h = max(row_h, sz[1])
     return offs
+
+
+class _Reaper:
+    """Destroys replaced device scenes on a background thread: tearing a
+    scene down synchronises its stream and frees its buffers, which need not
+    hold up the next chunk."""
+
+    def __init__(self):
+        self.q = queue.Queue()
+        t = threading.Thread(target=self._run, daemon=True)
+        t.start()
+
+    def _run(self):
+        while True:
+            obj = self.q.get()
+            del obj
+
+    def drop(self, obj):
+        if obj is not None:
+            self.q.put(obj)
+
+
+_reaper = None
+
+
+def _drop(obj):
+    global _reaper
+    if _reaper is None:
+        _reaper = _Reaper()
+    _reaper.drop(obj)
 
 
 class _Batch:
@@ -292,6 +324,8 @@ class DEMBatch(_Batch):
         self.ranges, self.tri_ranges = prep.ranges, prep.tri_ranges
         self.solver = prep.solver
         self.cur_stream = prep.stream
+        _drop(old)
+        del old
         self.timing["carry_s"] += time.perf_counter() - tic
         self.timing["rebuilds"] += 1
 
@@ -403,6 +437,8 @@ class SPHBatch(_Batch):
         self.ranges = prep.ranges
         self.solver = prep.solver
         self.cur_stream = prep.stream
+        _drop(old)
+        del old
         self.timing["carry_s"] += time.perf_counter() - tic
         self.timing["rebuilds"] += 1
 

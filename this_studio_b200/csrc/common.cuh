@@ -109,6 +109,14 @@ struct DBuf {
 
 static inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
+// Zero-fill as a kernel: inside captured step loops every node is a kernel,
+// so a pooled graph of the same shape can be updated to another scene's
+// sizes (memset nodes cannot change their size in an update).
+static __global__ void k_zero_ints(int* __restrict__ a, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0;
+}
+
 // ------------------------------------------------------------ vector math --
 // double3 algebra in the form the reference uses (myVec.h:25-176).
 __host__ __device__ __forceinline__ double3 mk3(double x, double y, double z) { return make_double3(x, y, z); }

@@ -1110,14 +1110,14 @@ struct DemScene {
             g.cur ^= 1;
             DemDev d = ghost_view(g);
             k_dem_build_pairs<<<grid_for(n, 128), 128, 0, s>>>(d);
-            DEMSPH_CUDA(cudaMemsetAsync(g.rcnt.p, 0, sizeof(int) * n, s));
+            k_zero_ints<<<grid_for(n, 256), 256, 0, s>>>(g.rcnt.p, n);
             k_dem_reverse<<<grid_for(n, 256), 256, 0, s>>>(d);
             k_dem_reverse_order<<<grid_for(n, 256), 256, 0, s>>>(d);
             if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
             else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
             k_dem_ghost_sum<<<grid_for(n, 256), 256, 0, s>>>(n, g.FA.p, g.TA.p, g.rcnt.p, g.rslot.p, g.KR, g.pF.p,
                                                              g.pTB.p, forceA.p, torqueA.p);
-            launch_count(5);
+            launch_count(6);
             DEMSPH_LAUNCH_CHECK();
             g.have = true;
         }
@@ -1130,10 +1130,10 @@ struct DemScene {
         cur ^= 1;
         DemDev d = dev(true);
         k_dem_build_pairs<<<grid_for(N(), 128), 128, 0, s>>>(d);
-        DEMSPH_CUDA(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * N(), s));
+        k_zero_ints<<<grid_for(N(), 256), 256, 0, s>>>(rcnt.p, N());
         k_dem_reverse<<<grid_for(N(), 256), 256, 0, s>>>(d);
         k_dem_reverse_order<<<grid_for(N(), 256), 256, 0, s>>>(d);
-        launch_count(3);
+        launch_count(4);
         DEMSPH_LAUNCH_CHECK();
         havePairs = true;
     }
@@ -1749,6 +1749,26 @@ int demsph_dem_set_buoyancy_drag(demsph_dem_t h, double rho, double cd, const do
         h->sc.graph.reset();  // kernel arguments or buffers change
         DemScene& s = h->sc;
         s.buoy = 1; s.brho = rho; s.bcd = cd; s.bg3 = ld3(g, 0); s.bu = ld3(u, 0); s.blevel = lvl;
+    });
+}
+int demsph_dem_reserve(demsph_dem_t h, int pairsPerBall, int reversePerBall, int trianglesPerBall) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "capacities must be reserved before initialisation");
+        if (pairsPerBall < 0 || reversePerBall < 0 || trianglesPerBall < 0)
+            throw Status(DEMSPH_ERR_INVALID, "negative capacity");
+        s.K = std::max(s.K, pairsPerBall);
+        s.KR = std::max(s.KR, reversePerBall);
+        s.KT = std::max(s.KT, std::min(trianglesPerBall, kMaxTriPerBall));
+    });
+}
+int demsph_dem_capacity(demsph_dem_t h, int* pairsPerBall, int* reversePerBall, int* trianglesPerBall) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (pairsPerBall) *pairsPerBall = h->sc.K;
+        if (reversePerBall) *reversePerBall = h->sc.KR;
+        if (trianglesPerBall) *trianglesPerBall = h->sc.KT;
     });
 }
 int demsph_dem_set_periodic(demsph_dem_t h, int x, int y, int z) {

@@ -110,8 +110,13 @@ class SceneServer:
         # batches are re-created at membership changes: keep their memory pooled
         _lib.retain_device_memory(int(2 * hbm_budget))
         # two streams per kind: the next batch scene is prepared on one while
-        # the current scene steps on the other
-        self.streams = {k: [torch.cuda.Stream(), torch.cuda.Stream()] for k in ("dem", "sph")}
+        # the current scene steps on the other.  The DEM step is many short
+        # kernels and the SPH step a few long ones; the DEM streams get the
+        # higher priority so their blocks are scheduled as SMs free up instead
+        # of queueing behind whole SPH kernels.
+        lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+        self.streams = {"dem": [torch.cuda.Stream(priority=hi), torch.cuda.Stream(priority=hi)],
+                        "sph": [torch.cuda.Stream(priority=lo), torch.cuda.Stream(priority=lo)]}
         self.batches = {"dem": DEMBatch(precision, streams=self.streams["dem"]),
                         "sph": SPHBatch(precision, streams=self.streams["sph"])}
 

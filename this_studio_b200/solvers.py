@@ -330,6 +330,15 @@ class DEMSolver:
         """Replay the step loop as CUDA graphs (default) or launch directly."""
         call("demsph_dem_set_graphs", self._h, int(bool(enable)))
 
+    def reserve(self, pairs=0, reverse=0, triangles=0):
+        """Raise the initial list capacities per ball (before initialize)."""
+        call("demsph_dem_reserve", self._h, int(pairs), int(reverse), int(triangles))
+
+    def capacity(self):
+        k = [C.c_int(), C.c_int(), C.c_int()]
+        call("demsph_dem_capacity", self._h, *[C.byref(x) for x in k])
+        return tuple(x.value for x in k)
+
     def assembleBalls(self, members, offsets, matOffsets):
         """Places sealed DEMMember records' balls into this scene (which has
         none yet), member k translated by offsets[k], material ids shifted by
