@@ -327,6 +327,49 @@ int demsph_sph_set(demsph_sph_t s, const double* position, const double* velocit
 int demsph_sph_get_pairs(demsph_sph_t s, int which, int* objectPointed, int* objectPointing);
 
 /* ======================================================================= */
+/* Particle-level DEM-SPH coupling                                          */
+/* ======================================================================= */
+/* The reference couples DEM balls to a fluid only through a buoyancy-drag
+ * plane (addBuoyancyDragKernel, externalForceTorque.cu:66-133, kept as
+ * demsph_dem_set_buoyancy_drag).  These calls couple balls of an initialised
+ * DEM scene to the fluid of an initialised SPH scene particle by particle.
+ *
+ * Each coupled ball is sampled by markers: moving boundary particles on
+ * shells r_l = R - (l + 1/2) spacing inside its surface (l spacing < 2 h,
+ * r_l > spacing / 4), max(1, round(4 pi r_l^2 / spacing^2)) per shell on a
+ * golden-angle spiral (one marker at the centre of a ball too small for a
+ * shell).  A marker carries its ball's rigid velocity v + omega x offset,
+ * the outward normal, mass density * spacing^3, and acts on the fluid
+ * exactly as a dummy particle does (the fluid-dummy terms of
+ * updateWCSPHAccelerationKernel and updateWCSPHDensityChangeKernel,
+ * WCSPHIntegrationKernel.cu:110-143,240-270).  The ball receives minus the
+ * sum of m_a times its markers' terms in the fluid accelerations (force, and
+ * offset x force as torque), so momentum is exchanged exactly.
+ *
+ * couple_balls: couples balls[0..n) (DEM indices) with markers of the given
+ * spacing, h (at most the fluid's largest h), sound speed, viscosity and
+ * rest density, placed at the balls' current state.  One SPH scene couples
+ * to one DEM scene; calls add balls.
+ * couple_step: n coupled steps.  Per step the markers follow the balls, the
+ * fluid takes one step with them, each ball's coupling force and torque
+ * are set to the mean of the reactions of the step's two acceleration
+ * passes, and the DEM takes demSubsteps steps (its time step times
+ * demSubsteps must equal the fluid's) with them held.  Both scenes run on
+ * the SPH scene's stream during the call; a DEM list overflow replays the
+ * call.  Stepping either scene alone keeps the markers and the coupling
+ * force where the last coupled step left them.
+ * get_markers: per marker in body order (balls in the order coupled):
+ * position, velocity, outward normal, last reaction on it (3 doubles each),
+ * and its ball.  get_coupling: per coupled ball its index, force, torque. */
+int demsph_sph_couple_balls(demsph_sph_t s, demsph_dem_t dem, long n, const int* balls, double spacing,
+                            double smoothingLength, double soundSpeed, double viscosity, double density);
+int demsph_sph_couple_step(demsph_sph_t s, demsph_dem_t dem, long n, int demSubsteps);
+int demsph_sph_num_markers(demsph_sph_t s, long* markers, long* balls);
+int demsph_sph_get_markers(demsph_sph_t s, double* position, double* velocity, double* normal, double* force,
+                           int* ball);
+int demsph_sph_get_coupling(demsph_sph_t s, int* ball, double* force, double* torque);
+
+/* ======================================================================= */
 /* Reference launcher compatibility                                          */
 /* ======================================================================= */
 /* The reference's sort / scan launchers with their exact signatures

@@ -541,6 +541,8 @@ struct DEM {
     double dampCoeff = 0;
     std::vector<V3> constForce;
     double constRamp = 0;
+    // force / torque of a coupled fluid per ball (particle-level coupling)
+    std::vector<V3> cplF, cplT;
     V3 gravity{0, 0, 0};
     double dt = 0;
     long iStep = 0;
@@ -985,6 +987,10 @@ static void demExternal(DEM& s, double time) {
         if (s.constRamp > 0) { c = time / s.constRamp; if (c > 1.0) c = 1.0; }
         for (size_t i = 0; i < N && i < s.constForce.size(); i++) s.force[i] += s.constForce[i] * c;
     }
+    for (size_t i = 0; i < N && i < s.cplF.size(); i++) {
+        s.force[i] += s.cplF[i];
+        s.torque[i] += s.cplT[i];
+    }
     if (s.dampCoeff != 0) {
         for (size_t i = 0; i < N; i++) {
             V3 f = s.force[i], t = s.torque[i];
@@ -1135,6 +1141,15 @@ struct SPH {
     Grid grid;
     std::vector<int> fHashIndex, fHashValue, dHashIndex, dHashValue;
     CSR ff, fd, dd;
+    // Particle-level coupling to DEM balls (no reference counterpart): the
+    // markers sampling each coupled ball, in body order, act on the fluid as
+    // dummies; mkF collects the fluid's reaction on each marker.
+    SPHSet mk;
+    std::vector<int> mkBall, body, bodyStart{0};
+    std::vector<V3> mkOff, mkF;
+    std::vector<int> mHashIndex, mHashValue;
+    CSR fm;
+    bool coupling = false;
     V3 gravity{0, 0, 0};
     double dt = 0;
     long iStep = 0;
@@ -1205,17 +1220,75 @@ static void sphInitBoundary(SPH& s) {
 static void sphNeighborSearch(SPH& s) {
     buildCellTable(s.grid, s.f.pos, s.fHashIndex, s.fHashValue);
     sphPairs(s.f, s.f, s.grid, s.fHashIndex, true, s.ff);
-    if (s.d.size() == 0) { s.fd.prefix.assign(s.f.size(), 0); s.fd.pointed.clear(); s.fd.pointing.clear(); return; }
-    buildCellTable(s.grid, s.d.pos, s.dHashIndex, s.dHashValue);
-    sphPairs(s.f, s.d, s.grid, s.dHashIndex, false, s.fd);
+    if (s.d.size() == 0) {
+        s.fd.prefix.assign(s.f.size(), 0); s.fd.pointed.clear(); s.fd.pointing.clear();
+    } else {
+        buildCellTable(s.grid, s.d.pos, s.dHashIndex, s.dHashValue);
+        sphPairs(s.f, s.d, s.grid, s.dHashIndex, false, s.fd);
+    }
+    if (s.mk.size() == 0) {
+        s.fm.prefix.assign(s.f.size(), 0); s.fm.pointed.clear(); s.fm.pointing.clear();
+    } else {
+        buildCellTable(s.grid, s.mk.pos, s.mHashIndex, s.mHashValue);
+        sphPairs(s.f, s.mk, s.grid, s.mHashIndex, false, s.fm);
+    }
+}
+
+// The fluid-dummy term of updateWCSPHAccelerationKernel
+// (WCSPHIntegrationKernel.cu:110-143) for fluid i and boundary particle j of
+// set d, accumulated into acc in the reference's order.
+static inline void sphBoundaryAcc(const SPH& s, const SPHSet& d, long i, int j, V3& acc) {
+    const SPHSet& f = s.f;
+    V3 g = s.gravity;
+    V3 ri = f.pos[i], vi = f.vel[i];
+    double ci = f.c[i], hi = f.h[i], nui = f.nu[i], rhoi = f.rho[i], PL = f.p[i];
+    V3 rj = d.pos[j], vj = d.vel[j];
+    double cj = d.c[j], hj = d.h[j], nuj = d.nu[j], mj = d.m[j];
+    V3 nw = d.normal[j];
+    double UL = dot(-nw, vi);
+    double UR = -UL + 2.0 * dot(-nw, vj);
+    double grj = dot(g, rj - ri);
+    if (grj < 0.) grj = 0.;
+    double PR = PL + rhoi * grj;
+    double rhoj = PR / (cj * cj) + d.rho0[j];
+    V3 rij = ri - rj;
+    V3 dW = gradW(rij, 0.5 * (hi + hj));
+    double cbar = 0.5 * (ci + cj), rbar = 0.5 * (rhoi + rhoj);
+    double beta = std::fmin(3.0 * std::fmax(UL - UR, 0.0), cbar);
+    double Ps = 0.5 * (PL + PR) + 0.5 * beta * rbar * (UL - UR);
+    acc -= 2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
+    double nuij = 0.5 * (nui + nuj);
+    acc += 2.0 * nuij * dot(normalize(rij), dW) * (vi - vj) * mj / (rhoi * rhoj);
+}
+// The fluid-dummy term of updateWCSPHDensityChangeKernel
+// (WCSPHIntegrationKernel.cu:240-270), before the factor 2 rho_i.
+static inline double sphBoundaryDrho(const SPH& s, const SPHSet& d, long i, int j) {
+    const SPHSet& f = s.f;
+    V3 g = s.gravity;
+    V3 ri = f.pos[i], vi = f.vel[i];
+    double ci = f.c[i], hi = f.h[i], rhoi = f.rho[i], PL = f.p[i];
+    V3 rj = d.pos[j], vj = d.vel[j];
+    double cj = d.c[j], hj = d.h[j], mj = d.m[j];
+    double grj = dot(g, rj - ri);
+    if (grj < 0.) grj = 0.;
+    double PR = PL + rhoi * grj;
+    double rhoj = PR / (cj * cj) + d.rho0[j];
+    V3 rij = ri - rj;
+    V3 dW = gradW(rij, 0.5 * (hi + hj));
+    V3 e = -normalize(rij);
+    double cbar = 0.5 * (ci + cj), rbar = 0.5 * (rhoi + rhoj);
+    V3 vs = 0.5 * (vi + vj);
+    vs += 0.5 * ((PL - PR) / (rbar * cbar)) * e;
+    return mj / rhoj * dot(vi - vs, dW);
 }
 
 // updateWCSPHAccelerationKernel (WCSPHIntegrationKernel.cu:42-148)
-static void sphAccel(SPH& s) {
+static void sphAccel(SPH& s, double reactionWeight = 0.0, bool resetReaction = false) {
     const SPHSet& f = s.f;
-    const SPHSet& d = s.d;
     V3 g = s.gravity;
     size_t N = f.size();
+    // per fluid-marker pair: the marker's term in the fluid acceleration
+    std::vector<V3> pairAcc(s.coupling ? s.fm.pointing.size() : 0);
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)N; i++) {
         V3 ri = f.pos[i], vi = f.vel[i];
@@ -1236,38 +1309,32 @@ static void sphAccel(SPH& s) {
             double nuij = 0.5 * (nui + nuj);
             acc += 2.0 * nuij * dot(normalize(rij), dW) * (vi - vj) * mj / (rhoi * rhoj);
         }
-        if (!s.fd.prefix.empty()) {
-            for (int k = i > 0 ? s.fd.prefix[i - 1] : 0; k < s.fd.prefix[i]; k++) {
-                int j = s.fd.pointing[k];
-                V3 rj = d.pos[j], vj = d.vel[j];
-                double cj = d.c[j], hj = d.h[j], nuj = d.nu[j], mj = d.m[j];
-                V3 nw = d.normal[j];
-                double UL = dot(-nw, vi);
-                double UR = -UL + 2.0 * dot(-nw, vj);
-                double grj = dot(g, rj - ri);
-                if (grj < 0.) grj = 0.;
-                double PR = PL + rhoi * grj;
-                double rhoj = PR / (cj * cj) + d.rho0[j];
-                V3 rij = ri - rj;
-                V3 dW = gradW(rij, 0.5 * (hi + hj));
-                double cbar = 0.5 * (ci + cj), rbar = 0.5 * (rhoi + rhoj);
-                double beta = std::fmin(3.0 * std::fmax(UL - UR, 0.0), cbar);
-                double Ps = 0.5 * (PL + PR) + 0.5 * beta * rbar * (UL - UR);
-                acc -= 2.0 * mj * (Ps / (rhoi * rhoj)) * dW;
-                double nuij = 0.5 * (nui + nuj);
-                acc += 2.0 * nuij * dot(normalize(rij), dW) * (vi - vj) * mj / (rhoi * rhoj);
+        if (!s.fd.prefix.empty())
+            for (int k = i > 0 ? s.fd.prefix[i - 1] : 0; k < s.fd.prefix[i]; k++)
+                sphBoundaryAcc(s, s.d, i, s.fd.pointing[k], acc);
+        if (!s.fm.prefix.empty())
+            for (int k = i > 0 ? s.fm.prefix[i - 1] : 0; k < s.fm.prefix[i]; k++) {
+                if (s.coupling) {
+                    V3 a = v3(0, 0, 0);
+                    sphBoundaryAcc(s, s.mk, i, s.fm.pointing[k], a);
+                    pairAcc[k] = a;
+                }
+                sphBoundaryAcc(s, s.mk, i, s.fm.pointing[k], acc);
             }
-        }
         s.f.acc[i] = acc + g;
     }
+    if (!s.coupling) return;
+    // reaction on each marker: minus m_a times its term in a_a
+    if (resetReaction) s.mkF.assign(s.mk.size(), v3(0, 0, 0));
+    std::vector<V3> r(s.mk.size(), v3(0, 0, 0));
+    for (size_t k = 0; k < pairAcc.size(); k++) r[s.fm.pointing[k]] -= f.m[s.fm.pointed[k]] * pairAcc[k];
+    for (size_t j = 0; j < r.size(); j++) s.mkF[j] += reactionWeight * r[j];
 }
 
 // updateWCSPHDensityChangeKernel + SPHDensityPressureIntegrationKernel
 // (WCSPHIntegrationKernel.cu:172-282)
 static void sphDensity(SPH& s, double dt) {
     const SPHSet& f = s.f;
-    const SPHSet& d = s.d;
-    V3 g = s.gravity;
     size_t N = f.size();
     std::vector<double> dr(N);
 #pragma omp parallel for schedule(static)
@@ -1287,24 +1354,12 @@ static void sphDensity(SPH& s, double dt) {
             vs += 0.5 * ((PL - PR) / (rbar * cbar)) * e;
             dRho += mj / rhoj * dot(vi - vs, dW);
         }
-        if (!s.fd.prefix.empty()) {
-            for (int k = i > 0 ? s.fd.prefix[i - 1] : 0; k < s.fd.prefix[i]; k++) {
-                int j = s.fd.pointing[k];
-                V3 rj = d.pos[j], vj = d.vel[j];
-                double cj = d.c[j], hj = d.h[j], mj = d.m[j];
-                double grj = dot(g, rj - ri);
-                if (grj < 0.) grj = 0.;
-                double PR = PL + rhoi * grj;
-                double rhoj = PR / (cj * cj) + d.rho0[j];
-                V3 rij = ri - rj;
-                V3 dW = gradW(rij, 0.5 * (hi + hj));
-                V3 e = -normalize(rij);
-                double cbar = 0.5 * (ci + cj), rbar = 0.5 * (rhoi + rhoj);
-                V3 vs = 0.5 * (vi + vj);
-                vs += 0.5 * ((PL - PR) / (rbar * cbar)) * e;
-                dRho += mj / rhoj * dot(vi - vs, dW);
-            }
-        }
+        if (!s.fd.prefix.empty())
+            for (int k = i > 0 ? s.fd.prefix[i - 1] : 0; k < s.fd.prefix[i]; k++)
+                dRho += sphBoundaryDrho(s, s.d, i, s.fd.pointing[k]);
+        if (!s.fm.prefix.empty())
+            for (int k = i > 0 ? s.fm.prefix[i - 1] : 0; k < s.fm.prefix[i]; k++)
+                dRho += sphBoundaryDrho(s, s.mk, i, s.fm.pointing[k]);
         dRho *= 2.0 * rhoi;
         dr[i] = dRho;
     }
@@ -1325,12 +1380,71 @@ static void sphStep(SPH& s) {
     s.time += dt;
     sphNeighborSearch(s);
     size_t N = s.f.size();
-    sphAccel(s);
+    sphAccel(s, 0.5, true);
     for (size_t i = 0; i < N; i++) s.f.vel[i] += (0.5 * dt) * s.f.acc[i];
     for (size_t i = 0; i < N; i++) s.f.pos[i] += dt * s.f.vel[i];
     sphDensity(s, dt);
-    sphAccel(s);
+    sphAccel(s, 0.5, false);
     for (size_t i = 0; i < N; i++) s.f.vel[i] += (0.5 * dt) * s.f.acc[i];
+}
+
+// ------------------------------------------- particle-level coupling ----
+// Marker offsets of a ball of radius R: shells l = 0, 1, ... at radius
+// r_l = R - (l + 1/2) dx while l dx < 2 h and r_l > dx / 4, shell l carrying
+// n_l = max(1, round(4 pi r_l^2 / dx^2)) points on the golden-angle spiral
+// z_k = 1 - (2k + 1) / n_l, phi_k = k pi (3 - sqrt 5); a ball too small for
+// any shell gets one marker at its centre.
+static std::vector<V3> markerOffsets(double R, double dx, double h) {
+    std::vector<V3> out;
+    const double ga = PI * (3.0 - std::sqrt(5.0));
+    for (int l = 0; l * dx < 2.0 * h; l++) {
+        const double r = R - (l + 0.5) * dx;
+        if (!(r > 0.25 * dx)) break;
+        const long nl = std::max(1L, std::lround(4.0 * PI * r * r / (dx * dx)));
+        for (long k = 0; k < nl; k++) {
+            const double z = 1.0 - (2.0 * k + 1.0) / (double)nl;
+            const double rho = std::sqrt(std::max(0.0, 1.0 - z * z));
+            const double phi = ga * (double)k;
+            out.push_back(v3(r * rho * std::cos(phi), r * rho * std::sin(phi), r * z));
+        }
+    }
+    if (out.empty()) out.push_back(v3(0, 0, 0));
+    return out;
+}
+
+// Markers at their balls' state: centre + offset, rigid velocity
+// v + omega x offset, outward normal offset / |offset|.
+static void placeMarkers(SPH& s, const DEM& d) {
+    for (size_t k = 0; k < s.mk.size(); k++) {
+        const int b = s.mkBall[k];
+        const V3 o = s.mkOff[k];
+        s.mk.pos[k] = d.pos[b] + o;
+        s.mk.vel[k] = d.vel[b] + cross(d.w[b], o);
+        const double l2 = dot(o, o);
+        s.mk.normal[k] = l2 > 0.0 ? o * (1.0 / std::sqrt(l2)) : v3(0, 0, 0);
+    }
+}
+
+// One coupled step: markers follow the balls, one fluid step with them,
+// each ball's coupling force / torque = the sum of its markers' reactions
+// (mean of the step's two acceleration passes), then `sub` DEM steps.
+static void coupledStep(SPH& s, DEM& d, int sub) {
+    placeMarkers(s, d);
+    s.coupling = true;
+    sphStep(s);
+    s.coupling = false;
+    d.cplF.assign(d.nb(), v3(0, 0, 0));
+    d.cplT.assign(d.nb(), v3(0, 0, 0));
+    for (size_t b = 0; b < s.body.size(); b++) {
+        V3 F = v3(0, 0, 0), T = v3(0, 0, 0);
+        for (int k = s.bodyStart[b]; k < s.bodyStart[b + 1]; k++) {
+            F += s.mkF[k];
+            T += cross(s.mkOff[k], s.mkF[k]);
+        }
+        d.cplF[s.body[b]] = F;
+        d.cplT[s.body[b]] = T;
+    }
+    for (int k = 0; k < sub; k++) demStep(d);
 }
 
 static inline V3 ld3(const double* a, size_t i) { return v3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
@@ -1693,6 +1807,58 @@ void oracle_sph_get(void* h, int dummy, double* pos, double* vel, double* acc, d
         if (p) p[i] = t.p[i];
         if (drho) drho[i] = t.drho[i];
         if (normal) st3(normal, i, t.normal[i]);
+    }
+}
+// Particle-level coupling (no reference counterpart): markers for balls[0..n)
+// of the DEM scene, placed at the balls' current state.
+int oracle_sph_couple_balls(void* h, void* dem, long n, const int* balls, double dx, double hm, double c, double nu,
+                            double rho0) {
+    SPH& s = *(SPH*)h;
+    DEM& d = *(DEM*)dem;
+    for (long k = 0; k < n; k++) {
+        const int b = balls[k];
+        if (b < 0 || (size_t)b >= d.nb()) return 1;
+        for (const V3& o : markerOffsets(d.rad[b], dx, hm)) {
+            s.mk.pos.push_back(v3(0, 0, 0)); s.mk.vel.push_back(v3(0, 0, 0));
+            s.mk.acc.push_back(v3(0, 0, 0)); s.mk.normal.push_back(v3(0, 0, 0));
+            s.mk.drho.push_back(0.0); s.mk.rho.push_back(rho0); s.mk.p.push_back(0.0); s.mk.rho0.push_back(rho0);
+            s.mk.h.push_back(hm); s.mk.m.push_back(rho0 * dx * dx * dx); s.mk.c.push_back(c); s.mk.nu.push_back(nu);
+            s.mkBall.push_back(b);
+            s.mkOff.push_back(o);
+        }
+        s.body.push_back(b);
+        s.bodyStart.push_back((int)s.mkBall.size());
+    }
+    s.mkF.assign(s.mk.size(), v3(0, 0, 0));
+    placeMarkers(s, d);
+    return 0;
+}
+int oracle_couple_step(void* h, void* dem, long n, int sub) {
+    SPH& s = *(SPH*)h;
+    DEM& d = *(DEM*)dem;
+    if (!s.initialized || !d.initialized) return 5;
+    for (long k = 0; k < n; k++) coupledStep(s, d, sub);
+    return 0;
+}
+long oracle_sph_num_markers(void* h) { return (long)((SPH*)h)->mk.size(); }
+void oracle_sph_get_markers(void* h, double* pos, double* vel, double* normal, double* force, int* ball) {
+    SPH& s = *(SPH*)h;
+    for (size_t k = 0; k < s.mk.size(); k++) {
+        if (pos) st3(pos, k, s.mk.pos[k]);
+        if (vel) st3(vel, k, s.mk.vel[k]);
+        if (normal) st3(normal, k, s.mk.normal[k]);
+        if (force) st3(force, k, s.mkF[k]);
+        if (ball) ball[k] = s.mkBall[k];
+    }
+}
+void oracle_sph_get_coupling(void* h, void* dem, int* ball, double* force, double* torque) {
+    SPH& s = *(SPH*)h;
+    DEM& d = *(DEM*)dem;
+    for (size_t b = 0; b < s.body.size(); b++) {
+        const int i = s.body[b];
+        if (ball) ball[b] = i;
+        if (force) st3(force, b, i < (int)d.cplF.size() ? d.cplF[i] : v3(0, 0, 0));
+        if (torque) st3(torque, b, i < (int)d.cplT.size() ? d.cplT[i] : v3(0, 0, 0));
     }
 }
 void oracle_sph_set(void* h, const double* pos, const double* vel, const double* rho, const double* p,

@@ -83,6 +83,12 @@ def lib():
             "oracle_sph_get_pairs": (None, [_vp, C.c_int, _i, _i]),
             "oracle_sph_get": (None, [_vp, C.c_int, _d, _d, _d, _d, _d, _d, _d]),
             "oracle_sph_set": (None, [_vp, _d, _d, _d, _d, _d]),
+            "oracle_sph_couple_balls": (C.c_int, [_vp, _vp, C.c_long, _i, C.c_double, C.c_double, C.c_double,
+                                                  C.c_double, C.c_double]),
+            "oracle_couple_step": (C.c_int, [_vp, _vp, C.c_long, C.c_int]),
+            "oracle_sph_num_markers": (C.c_long, [_vp]),
+            "oracle_sph_get_markers": (None, [_vp, _d, _d, _d, _d, _i]),
+            "oracle_sph_get_coupling": (None, [_vp, _vp, _i, _d, _d]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -340,3 +346,31 @@ class OracleSPH:
         f = lambda x, s: None if x is None else _f64(x, s)
         self._L.oracle_sph_set(self.h, _dp(f(pos, (n, 3))), _dp(f(vel, (n, 3))), _dp(f(rho, (n,))),
                                _dp(f(p, (n,))), _dp(f(drho, (n,))))
+
+    # particle-level coupling to DEM balls (no reference counterpart)
+    def couple_balls(self, dem, balls, spacing, h, c, nu, rho0):
+        balls = np.ascontiguousarray(balls, np.int32)
+        rc = self._L.oracle_sph_couple_balls(self.h, dem.h, len(balls), _ip(balls), float(spacing), float(h),
+                                             float(c), float(nu), float(rho0))
+        if rc != 0:
+            raise RuntimeError(f"oracle_sph_couple_balls failed with status {rc}")
+        self._dem = dem
+
+    def couple_step(self, dem, n=1, dem_substeps=1):
+        rc = self._L.oracle_couple_step(self.h, dem.h, int(n), int(dem_substeps))
+        if rc != 0:
+            raise RuntimeError(f"oracle_couple_step failed with status {rc}")
+
+    def markers(self):
+        n = self._L.oracle_sph_num_markers(self.h)
+        out = {"pos": np.zeros((n, 3)), "vel": np.zeros((n, 3)), "normal": np.zeros((n, 3)),
+               "force": np.zeros((n, 3)), "ball": np.zeros(n, np.int32)}
+        self._L.oracle_sph_get_markers(self.h, _dp(out["pos"]), _dp(out["vel"]), _dp(out["normal"]),
+                                       _dp(out["force"]), _ip(out["ball"]))
+        return out
+
+    def coupling(self, dem, nbodies):
+        ball = np.zeros(nbodies, np.int32)
+        F, T = np.zeros((nbodies, 3)), np.zeros((nbodies, 3))
+        self._L.oracle_sph_get_coupling(self.h, dem.h, _ip(ball), _dp(F), _dp(T))
+        return ball, F, T

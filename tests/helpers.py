@@ -58,3 +58,20 @@ def rel_err(x, ref):
     d = np.linalg.norm(np.asarray(x) - np.asarray(ref))
     n = np.linalg.norm(ref)
     return d / n if n > 0 else d
+
+
+def oracle_coupled(scene):
+    """(OracleSPH, OracleDEM) of a CoupledScene with its balls coupled."""
+    f = oracle_sph(scene.sph)
+    d = oracle_dem(scene.dem)
+    sp = scene.sph
+    f.couple_balls(d, scene.balls, scene.marker_spacing, scene.marker_h, sp.sound_speed, sp.viscosity, sp.density)
+    return f, d
+
+
+def coupled_momentum(scene, fluid_vel, ball_vel):
+    """Total linear momentum of the fluid (mass rho0 dx^3 each) and the balls."""
+    sp, dm = scene.sph, scene.dem
+    mf = sp.density * sp.spacing ** 3
+    mb = dm.density * (4.0 / 3.0) * np.pi * dm.radius ** 3
+    return mf * np.asarray(fluid_vel).sum(axis=0) + (mb[:, None] * np.asarray(ball_vel)).sum(axis=0)

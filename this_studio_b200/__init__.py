@@ -5,6 +5,6 @@ sm_100a CUDA kernels behind the C ABI in include/demsph.h).  This package
 mirrors the reference's DEMSolver / WCSPHSolver classes over that ABI.
 """
 from ._lib import DemsphError, kernel_launches, lib
-from .solvers import DEMSolver, WCSPHSolver, num_steps
+from .solvers import DEMSolver, DEMSPHCoupling, WCSPHSolver, num_steps
 
-__all__ = ["DEMSolver", "WCSPHSolver", "DemsphError", "kernel_launches", "lib", "num_steps"]
+__all__ = ["DEMSolver", "DEMSPHCoupling", "WCSPHSolver", "DemsphError", "kernel_launches", "lib", "num_steps"]

@@ -105,6 +105,11 @@ SIGNATURES = {
     "demsph_sph_get": [_vp, _int, _d, _d, _d, _d, _d, _d, _d],
     "demsph_sph_set": [_vp, _d, _d, _d, _d, _d],
     "demsph_sph_get_pairs": [_vp, _int, _i, _i],
+    "demsph_sph_couple_balls": [_vp, _vp, _long, _i, _dbl, _dbl, _dbl, _dbl, _dbl],
+    "demsph_sph_couple_step": [_vp, _vp, _long, _int],
+    "demsph_sph_num_markers": [_vp, _l, _l],
+    "demsph_sph_get_markers": [_vp, _d, _d, _d, _d, _i],
+    "demsph_sph_get_coupling": [_vp, _i, _d, _d],
     "buildHashStartEnd": [_vp, _vp, _vp, _vp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, _vp],
     "buildPrefixSum": [_vp, _vp, C.c_size_t, _vp],
     "demsph_build_hash_start_end_noalloc": [_vp, _vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp],

@@ -28,7 +28,8 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompil
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) +
+            glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def _stale(obj, src, headers):

@@ -258,6 +258,7 @@ struct DevStatus {
     int need_rev;      // largest reverse-list count
     int need_aux;      // largest per-row count for the secondary list
     int bad_index;     // nonzero: a remapped index fell outside its array
+    int need_mark;     // largest per-row count for the fluid-marker list
 };
 
 }  // namespace demsph

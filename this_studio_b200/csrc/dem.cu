@@ -25,6 +25,7 @@
 #include "graph.cuh"
 #include "vtu.hpp"
 #include "dem_physics.cuh"
+#include "coupling.hpp"
 
 namespace demsph {
 
@@ -117,6 +118,9 @@ struct DemDev {
     const int2* cpeb;
     // external force hook
     const double4* fconst;
+    // force and torque of a coupled fluid on each ball (or null)
+    const double4* cplF;
+    const double4* cplT;
     double framp;
     double damp;
     int buoy;
@@ -486,6 +490,10 @@ __global__ void __launch_bounds__(128) k_dem_finalize(DemDev d, double dtWall, d
             if (d.framp > 0) { c = extTime / d.framp; if (c > 1.0) c = 1.0; }
             F += xyz(d.fconst[i]) * c;
         }
+        if (d.cplF) {
+            F += xyz(d.cplF[i]);
+            T += xyz(d.cplT[i]);
+        }
         // launchAddGlobalDampingForceTorque (externalForceTorque.cu:26-57)
         if (d.damp != 0) {
             double3 f0 = F, t0 = T;
@@ -798,6 +806,10 @@ struct DemScene {
     DBuf<double> cinvm;
     DBuf<int2> cpeb;
     DBuf<double4> fconst;
+    DBuf<double4> cplF, cplT;  // fluid coupling force / torque per ball (allocated by a coupling)
+    // inside a coupled block: the DEM launches on the block's stream; its own is kept here
+    cudaStream_t blockOwn = 0;
+    bool inBlock = false;
     DBuf<DevStatus> status;
 
     // Periodic boundaries (setPeriodicBoundary, DEMSolver.h:1944-1959): one
@@ -859,6 +871,8 @@ struct DemScene {
         d.cpos = cpos.p; d.cvel = cvel.p; d.cangv = cangv.p; d.cforce = cforce.p; d.ctorque = ctorque.p; d.cq = cq.p;
         d.cinvIa = cinvIa.p; d.cinvIb = cinvIb.p; d.cinvm = cinvm.p; d.cpeb = cpeb.p;
         d.fconst = hFconst.empty() ? nullptr : fconst.p;
+        d.cplF = cplF.p;
+        d.cplT = cplT.p;
         d.framp = framp; d.damp = damp; d.buoy = buoy; d.brho = brho; d.bcd = bcd; d.blevel = blevel;
         d.bg3 = bg3; d.bu = bu; d.gravity = gravity;
         d.status = status.p;
@@ -1443,6 +1457,74 @@ static inline void st3(double* a, long i, double3 v) { a[3 * i] = v.x; a[3 * i +
 
 #define SCENE_CHECK(h) \
     if (!(h)) throw Status(DEMSPH_ERR_INVALID, "null scene handle")
+
+// ------------------------------------------- coupled DEM-SPH stepping ----
+namespace demsph {
+
+DemBodies dem_bodies(demsph_dem_t h) {
+    DemScene& sc = h->sc;
+    if (!sc.ready) throw Status(DEMSPH_ERR_NOT_READY, "DEM scene not initialised");
+    const int n = sc.N();
+    DEMSPH_CUDA(cudaStreamSynchronize(sc.s));  // the ball state is read on another stream
+    if (sc.cplF.n < (size_t)n) {
+        sc.cplF.alloc(n, sc.s, true);
+        sc.cplT.alloc(n, sc.s, true);
+        sc.graph.reset();  // captured finalize launches lack the hook
+    }
+    return DemBodies{n, sc.pos.p, sc.vel.p, sc.angv.p, sc.cplF.p, sc.cplT.p, sc.dt};
+}
+
+static void stream_after(cudaStream_t waiter, cudaStream_t done) {
+    if (waiter == done) return;
+    cudaEvent_t ev;
+    DEMSPH_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    DEMSPH_CUDA(cudaEventRecord(ev, done));
+    DEMSPH_CUDA(cudaStreamWaitEvent(waiter, ev, 0));
+    DEMSPH_CUDA(cudaEventDestroy(ev));
+}
+
+void dem_block_begin(demsph_dem_t h, cudaStream_t s) {
+    DemScene& sc = h->sc;
+    if (!sc.ready) throw Status(DEMSPH_ERR_NOT_READY, "DEM scene not initialised");
+    if (sc.inBlock) throw Status(DEMSPH_ERR_INVALID, "DEM scene already in a coupled block");
+    stream_after(s, sc.s);
+    sc.blockOwn = sc.s;
+    sc.inBlock = true;
+    sc.s = s;
+    sc.take(sc.snap);
+    sc.clear_status();
+    if (!sc.ghosts.empty()) DEMSPH_CUDA(cudaMemsetAsync(sc.gstatus.p, 0, sizeof(DevStatus), s));
+}
+
+void dem_block_steps(demsph_dem_t h, int n) {
+    DemScene& sc = h->sc;
+    for (int k = 0; k < n; k++) sc.step_once();
+}
+
+bool dem_block_end(demsph_dem_t h) {
+    DemScene& sc = h->sc;
+    if (!sc.inBlock) throw Status(DEMSPH_ERR_INVALID, "no coupled block in progress");
+    DevStatus st = sc.read_status();
+    DevStatus gs{};
+    if (!sc.ghosts.empty()) {
+        DEMSPH_CUDA(cudaMemcpyAsync(&gs, sc.gstatus.p, sizeof gs, cudaMemcpyDeviceToHost, sc.s));
+        DEMSPH_CUDA(cudaStreamSynchronize(sc.s));
+    }
+    bool ok = !st.overflow && !gs.overflow;
+    if (!ok) {
+        if (st.overflow) sc.grow(st.need_pairs, st.need_rev, st.need_aux);
+        if (gs.overflow) sc.ghost_grow(gs.need_pairs, gs.need_rev);
+        sc.restore(sc.snap);
+        DEMSPH_CUDA(cudaStreamSynchronize(sc.s));
+    }
+    sc.s = sc.blockOwn;
+    sc.inBlock = false;
+    return ok;
+}
+
+void dem_reset_graphs(demsph_dem_t h) { h->sc.graph.reset(); }
+
+}  // namespace demsph
 
 extern "C" {
 

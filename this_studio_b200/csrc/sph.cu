@@ -19,6 +19,7 @@
 #include <type_traits>
 
 #include "cells.cuh"
+#include "coupling.hpp"
 #include "graph.cuh"
 #include "vtu.hpp"
 
@@ -32,6 +33,7 @@ struct SphDev {
     const int* fStart;   // fluid cell start (new order)
     const int* dStart;   // dummy cell start (dummies stored in cell order)
     const double4* pos;  // current fluid pos
+    const double4* lpos; // fluid pos when this step's lists were built (same slot order)
     const double4* vel;
     const double4* st;
     const double* rho0;
@@ -74,9 +76,48 @@ struct SphDev {
     int* cntF;
     int* nbD;
     int* cntD;
+    // Moving boundary particles ("markers") that sample the DEM balls coupled
+    // to the fluid, in this step's cell order, with the dummies' record
+    // layout; mid maps a slot to the marker's index in body order, where
+    // mforce collects the reaction of the fluid on each marker.
+    int NM, KM;
+    const int* mStart;
+    const double4* mpos;
+    const double4* mvel;
+    const double4* mst;
+    const double4* mnorm;
+    const float4* mposf;
+    const float4* mvelf;
+    const float4* mstf;
+    const float4* mnormf;
+    const int4* mposq;
+    const int* mid;
+    int* nbM;
+    int* cntM;
+    double4* mforce;
+    double4* macc;   // per fluid particle: the markers' terms in its acceleration
+    double* mdrho;   // and in its density change (before 2 rho_i)
     double3 gravity;
     DevStatus* status;
 };
+
+// A boundary set (dummies or markers) as the fluid passes read it.
+struct BView {
+    const double4* pos;
+    const double4* vel;
+    const double4* st;
+    const double4* norm;
+    const float4* velf;
+    const float4* stf;
+    const float4* normf;
+    const int4* posq;
+};
+__device__ __forceinline__ BView dummy_view(const SphDev& d) {
+    return BView{d.dpos, d.dvel, d.dst, d.dnorm, d.dvelf, d.dstf, d.dnormf, d.dposq};
+}
+__device__ __forceinline__ BView marker_view(const SphDev& d) {
+    return BView{d.mpos, d.mvel, d.mst, d.mnorm, d.mvelf, d.mstf, d.mnormf, d.mposq};
+}
 
 // Wendland C2 kernel gradient (WCSPHIntegrationKernel.cuh:15-32), with the
 // powers written as products.  Returns the factor f with gradW = f * r_ij.
@@ -179,6 +220,69 @@ __global__ void k_sph_place(int n, int start, double3 off, const double4* __rest
     st2[start + t] = st[t];
     extra2[start + t] = extra[t];
     if (zero2) zero2[start + t] = 0.0;
+}
+// World position of marker k (body order): its ball's centre plus the
+// marker's offset, with h in w.
+__global__ void k_sph_marker_place(int nm, const int* __restrict__ mb, const double4* __restrict__ moff,
+                                   const double4* __restrict__ bpos, double4* __restrict__ tmp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nm) return;
+    const double4 o = moff[k];
+    tmp[k] = d4(xyz(bpos[mb[k]]) + xyz(o), o.w);
+}
+// Puts the markers into cell order (sorted[t] = body-order index of slot t)
+// with their ball's rigid-body velocity v + omega x offset, the outward
+// normal offset / |offset|, the record (c, nu, rho0, 0) and the mass in
+// vel.w from mrec = (c, nu, rho0, m),
+// and the FP32 and fixed-point copies the mixed-precision passes read.
+__global__ void k_sph_marker_gather(int nm, const int* __restrict__ sorted, const double4* __restrict__ tmp,
+                                    const int* __restrict__ mb, const double4* __restrict__ moff,
+                                    const double4* __restrict__ mrec, const double4* __restrict__ bvel,
+                                    const double4* __restrict__ bangv, double3 origin, double invq,
+                                    double4* __restrict__ mpos,
+                                    double4* __restrict__ mvel, double4* __restrict__ mst,
+                                    double4* __restrict__ mnorm, float4* __restrict__ mposf,
+                                    float4* __restrict__ mvelf, float4* __restrict__ mstf,
+                                    float4* __restrict__ mnormf, int4* __restrict__ mposq, int* __restrict__ mid) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nm) return;
+    const int k = sorted[t];
+    const double4 p = tmp[k];
+    const int b = mb[k];
+    const double3 off = xyz(moff[k]);
+    const double3 v = xyz(bvel[b]) + cross(xyz(bangv[b]), off);
+    const double l2 = dot(off, off);
+    const double3 n = l2 > 0.0 ? off * (1.0 / sqrt(l2)) : mk3(0, 0, 0);
+    const double4 r4 = mrec[k];
+    const double4 rec = make_double4(r4.x, r4.y, r4.z, 0);
+    const double4 v4 = d4(v, r4.w), n4 = d4(n, 0);
+    mpos[t] = p;
+    mvel[t] = v4;
+    mst[t] = rec;
+    mnorm[t] = n4;
+    mposf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
+    mvelf[t] = f4(v4);
+    mstf[t] = f4(rec);
+    mnormf[t] = f4(n4);
+    mposq[t] = fixq(p, origin, invq);
+    mid[t] = k;
+}
+// Coupling force and torque of each coupled ball: the sum of its markers'
+// reactions (body order, markers [start[b], start[b+1])), and of offset x
+// reaction, written at the ball's index.
+__global__ void k_sph_body_force(int nb, const int* __restrict__ start, const int* __restrict__ ball,
+                                 const double4* __restrict__ mforce, const double4* __restrict__ moff,
+                                 double4* __restrict__ force, double4* __restrict__ torque) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
+    for (int k = start[b]; k < start[b + 1]; k++) {
+        const double3 f = xyz(mforce[k]);
+        F += f;
+        T += cross(xyz(moff[k]), f);
+    }
+    force[ball[b]] = d4(F, 0);
+    torque[ball[b]] = d4(T, 0);
 }
 // Puts the dummies into cell order (sorted[t] = caller index of slot t).
 __global__ void k_sph_dummy_gather(int nd, const int* __restrict__ sorted, const double4* __restrict__ tp,
@@ -382,7 +486,7 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
     }
 }
 
-template <bool kUniformH, int kShape>
+template <bool kUniformH, int kShape, bool kMarkers>
 __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
     k_sph_lists_cell(SphDev d, int ncell) {
     constexpr int kListWarps = kListShapes[kShape].warps, kStage = kListShapes[kShape].stage;
@@ -404,14 +508,21 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
                               d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg);
     else
         for (int i = ps + (threadIdx.x & 31); i < pe; i += 32) d.cntD[i] = 0;
+    if (kMarkers)
+        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM, d.N,
+                                      d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
 }
 
 // Calls f(j) for this lane's share of particle i's neighbours: from the ELL
-// row when it fitted (cnt >= 0), otherwise by walking the cell stencil with
-// the list's cutoff test (a row that overflowed its capacity).
+// row when it fitted (cnt >= 0), otherwise (a row that overflowed its
+// capacity) by walking the cell stencil of pi with the list's cutoff test
+// against `other`.  With pi and `other` the positions the lists were built
+// from this yields the list's pair set; the fluid passes after the step's
+// drift pass the drifted positions (see k_sph_accel).
 template <class F>
 __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ nb, int K, int i, int self,
-                                               double4 pi, const GridDesc& g, const int* __restrict__ cellStart,
+                                               const double4 pi, const GridDesc& g,
+                                               const int* __restrict__ cellStart,
                                                const double4* __restrict__ other, F&& f) {
     const int sub = threadIdx.x & 3;
     if (cnt >= 0) {
@@ -492,15 +603,15 @@ __device__ __forceinline__ void load_fluid(const SphDev& d, int j, V<R>& vj, R& 
     }
 }
 template <class R>
-__device__ __forceinline__ void load_dummy(const SphDev& d, int j, V<R>& nw, V<R>& vj, R& mj, R& cj, R& nuj, R& rho0j) {
+__device__ __forceinline__ void load_dummy(const BView& b, int j, V<R>& nw, V<R>& vj, R& mj, R& cj, R& nuj, R& rho0j) {
     if constexpr (std::is_same<R, float>::value) {
-        const float4 n = d.dnormf[j], v = d.dvelf[j], q = d.dstf[j];
+        const float4 n = b.normf[j], v = b.velf[j], q = b.stf[j];
         nw = make_float3(n.x, n.y, n.z);
         vj = make_float3(v.x, v.y, v.z);
         mj = v.w;
         cj = q.x; nuj = q.y; rho0j = q.z;
     } else {
-        const double4 n = d.dnorm[j], v = d.dvel[j], q = d.dst[j];
+        const double4 n = b.norm[j], v = b.vel[j], q = b.st[j];
         nw = xyz(n);
         vj = xyz(v);
         mj = v.w;
@@ -508,8 +619,91 @@ __device__ __forceinline__ void load_dummy(const SphDev& d, int j, V<R>& nw, V<R
     }
 }
 
+// A fluid particle's own values as the passes use them.
 template <class R>
-__global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, double dt, int first) {
+struct FluidOwn {
+    OwnPos<R> op;
+    V<R> vi;
+    R rhoi, PL, ci, nui;
+    HConst<R> hk;
+};
+template <class R>
+__device__ __forceinline__ FluidOwn<R> fluid_own(const SphDev& d, int i, const double4& pi4, const double4& vi4,
+                                                 const double4& s4) {
+    return FluidOwn<R>{OwnPos<R>{xyz(pi4), std::is_same<R, float>::value ? d.posq[i] : make_int4(0, 0, 0, 0)},
+                       cvt<R>(xyz(vi4)),
+                       (R)s4.x,
+                       (R)s4.y,
+                       (R)s4.z,
+                       (R)s4.w,
+                       hconst<R>((R)pi4.w)};
+}
+
+// Fluid-boundary term of updateWCSPHAccelerationKernel
+// (WCSPHIntegrationKernel.cu:110-143): the boundary particle j takes the
+// mirrored normal velocity and the hydrostatically extrapolated pressure
+// PR = PL + rho_i max(0, -g . r_ij), rho_j = PR / c_j^2 + rho0_j.
+template <class R>
+__device__ __forceinline__ void boundary_acc(const SphDev& d, const FluidOwn<R>& o, const BView& bv, int j,
+                                             const V<R>& g, V<R>& acc) {
+    using VR = V<R>;
+    VR rij, nw, vj;
+    R hj, cj, nuj, rho0j, mj;
+    pair_r<R>(o.op, bv.pos, bv.posq, d.q, j, rij, hj);
+    load_dummy<R>(bv, j, nw, vj, mj, cj, nuj, rho0j);
+    R UL = dot(-nw, o.vi);
+    R UR = -UL + (R)2.0 * dot(-nw, vj);
+    R grj = -dot(g, rij);
+    if (grj < (R)0.) grj = (R)0.;
+    R PR = o.PL + o.rhoi * grj;
+    R rhoj = div_r(PR, cj * cj) + rho0j;
+    R r2 = dot(rij, rij);
+    R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+    R r = r2 * inv_r;
+    VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
+    R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
+    R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
+    R Ps = (R)0.5 * (o.PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
+    R inv_rr = div_r((R)1.0, o.rhoi * rhoj);
+    acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
+    R nuij = (R)0.5 * (o.nui + nuj);
+    acc += (R)2.0 * nuij * dot(rij * inv_r, dW) * (o.vi - vj) * mj * inv_rr;
+}
+
+// Fluid-boundary term of updateWCSPHDensityChangeKernel
+// (WCSPHIntegrationKernel.cu:240-270), before the factor 2 rho_i.
+template <class R>
+__device__ __forceinline__ void boundary_drho(const SphDev& d, const FluidOwn<R>& o, const BView& bv, int j,
+                                              const V<R>& g, R& dRho) {
+    using VR = V<R>;
+    VR rij, nw, vj;
+    R hj, cj, nuj, rho0j, mj;
+    pair_r<R>(o.op, bv.pos, bv.posq, d.q, j, rij, hj);
+    load_dummy<R>(bv, j, nw, vj, mj, cj, nuj, rho0j);
+    R grj = -dot(g, rij);
+    if (grj < (R)0.) grj = (R)0.;
+    R PR = o.PL + o.rhoi * grj;
+    R rhoj = div_r(PR, cj * cj) + rho0j;
+    R r2 = dot(rij, rij);
+    R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+    R r = r2 * inv_r;
+    VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
+    VR e = rij * (-inv_r);
+    R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
+    VR vs = (R)0.5 * (o.vi + vj);
+    vs += (R)0.5 * div_r(o.PL - PR, rbar * cbar) * e;
+    dRho += div_r(mj, rhoj) * dot(o.vi - vs, dW);
+}
+
+// Resident blocks per SM the passes' register budgets are fitted to (FP32 /
+// FP64 arithmetic): what the measured-fastest register allocations gave.
+template <class R>
+constexpr int kAccelBlocks = std::is_same<R, float>::value ? 6 : 4;
+template <class R>
+constexpr int kDensityBlocks = std::is_same<R, float>::value ? 8 : 5;
+
+template <class R, bool kMarkers>
+__global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
@@ -517,17 +711,13 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
     const double3 ri = xyz(pi4);
-    OwnPos<R> op{ri, std::is_same<R, float>::value ? d.posq[i] : make_int4(0, 0, 0, 0)};
     const double4 vi4 = d.vel[i];
-    const VR vi = cvt<R>(xyz(vi4));
-    const double4 s4 = d.st[i];
-    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z, nui = (R)s4.w;
-    const HConst<R> hk = hconst<R>((R)pi4.w);
+    const FluidOwn<R> o = fluid_own<R>(d, i, pi4, vi4, d.st[i]);
     VR acc = v3r<R>(0, 0, 0);
     quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         VR rij, vj;
         R hj, rhoj, PR, cj, nuj, mj;
-        pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
+        pair_r<R>(o.op, d.pos, d.posq, d.q, j, rij, hj);
         load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
         R r2 = dot(rij, rij);
         // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
@@ -535,46 +725,29 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
         VR e = rij * (-inv_r);
-        R UL = dot(vi, e), UR = dot(vj, e);
-        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
-        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
+        R UL = dot(o.vi, e), UR = dot(vj, e);
+        VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
+        R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
         R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
-        R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        R inv_rr = div_r((R)1.0, rhoi * rhoj);
+        R Ps = (R)0.5 * (o.PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
+        R inv_rr = div_r((R)1.0, o.rhoi * rhoj);
         acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
-        R nuij = (R)0.5 * (nui + nuj);
+        R nuij = (R)0.5 * (o.nui + nuj);
         // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
-        acc += (R)2.0 * nuij * dot(-e, dW) * (vi - vj) * mj * inv_rr;
+        acc += (R)2.0 * nuij * dot(-e, dW) * (o.vi - vj) * mj * inv_rr;
     });
     const VR g = cvt<R>(d.gravity);
-    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
-        VR rij, nw, vj;
-        R hj, cj, nuj, rho0j, mj;
-        pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
-        load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
-        R UL = dot(-nw, vi);
-        R UR = -UL + (R)2.0 * dot(-nw, vj);
-        R grj = -dot(g, rij);
-        if (grj < (R)0.) grj = (R)0.;
-        R PR = PL + rhoi * grj;
-        R rhoj = div_r(PR, cj * cj) + rho0j;
-        R r2 = dot(rij, rij);
-        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
-        R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
-        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
-        R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
-        R Ps = (R)0.5 * (PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        R inv_rr = div_r((R)1.0, rhoi * rhoj);
-        acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
-        R nuij = (R)0.5 * (nui + nuj);
-        acc += (R)2.0 * nuij * dot(rij * inv_r, dW) * (vi - vj) * mj * inv_rr;
-    });
+    if (d.ND > 0) {
+        const BView dv = dummy_view(d);
+        quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos,
+                       [&](int j) { boundary_acc<R>(d, o, dv, j, g, acc); });
+    }
     double3 a = up(acc);
     a.x = quad_sum(a.x, gm);
     a.y = quad_sum(a.y, gm);
     a.z = quad_sum(a.z, gm);
     if (sub != 0) return;
+    if (kMarkers) a += xyz(d.macc[i]);  // the markers' terms (k_sph_marker_pass)
     a += d.gravity;
     d.acc[i] = d4(a, 0);
     double3 v = xyz(vi4) + hdt * a;
@@ -591,59 +764,42 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_accel(SphDev d, double hdt, d
 // updateWCSPHDensityChangeKernel + SPHDensityPressureIntegrationKernel
 // (WCSPHIntegrationKernel.cu:172-282): drho += dt * 2 rho_i sum m_j/rho_j
 // (v_i - v*) . gradW; clamp drho >= -0.1 rho0; rho = rho0 + drho; p = c^2 drho.
-template <class R>
-__global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) {
+template <class R, bool kMarkers>
+__global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(SphDev d, double dt) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
     const unsigned gm = quad_mask();
     using VR = V<R>;
     const double4 pi4 = d.pos[i];
-    const double3 ri = xyz(pi4);
-    OwnPos<R> op{ri, std::is_same<R, float>::value ? d.posq[i] : make_int4(0, 0, 0, 0)};
-    const VR vi = cvt<R>(xyz(d.vel[i]));
     const double4 s4 = d.st[i];
-    const R rhoi = (R)s4.x, PL = (R)s4.y, ci = (R)s4.z;
-    const HConst<R> hk = hconst<R>((R)pi4.w);
+    const FluidOwn<R> o = fluid_own<R>(d, i, pi4, d.vel[i], s4);
     R dRho = (R)0;
     quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         VR rij, vj;
         R hj, rhoj, PR, cj, nuj, mj;
-        pair_r<R>(op, d.pos, d.posq, d.q, j, rij, hj);
+        pair_r<R>(o.op, d.pos, d.posq, d.q, j, rij, hj);
         load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
         R r2 = dot(rij, rij);
         R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
         R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
+        VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
         VR e = rij * (-inv_r);
-        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
-        VR vs = (R)0.5 * (vi + vj);
-        vs += (R)0.5 * div_r(PL - PR, rbar * cbar) * e;
-        dRho += div_r(mj, rhoj) * dot(vi - vs, dW);
+        R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
+        VR vs = (R)0.5 * (o.vi + vj);
+        vs += (R)0.5 * div_r(o.PL - PR, rbar * cbar) * e;
+        dRho += div_r(mj, rhoj) * dot(o.vi - vs, dW);
     });
     const VR g = cvt<R>(d.gravity);
-    if (d.ND > 0) quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
-        VR rij, nw, vj;
-        R hj, cj, nuj, rho0j, mj;
-        pair_r<R>(op, d.dpos, d.dposq, d.q, j, rij, hj);
-        load_dummy<R>(d, j, nw, vj, mj, cj, nuj, rho0j);
-        R grj = -dot(g, rij);
-        if (grj < (R)0.) grj = (R)0.;
-        R PR = PL + rhoi * grj;
-        R rhoj = div_r(PR, cj * cj) + rho0j;
-        R r2 = dot(rij, rij);
-        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
-        R r = r2 * inv_r;
-        VR dW = gradw_fast<R>(r, inv_r, hk, hj) * rij;
-        VR e = rij * (-inv_r);
-        R cbar = (R)0.5 * (ci + cj), rbar = (R)0.5 * (rhoi + rhoj);
-        VR vs = (R)0.5 * (vi + vj);
-        vs += (R)0.5 * div_r(PL - PR, rbar * cbar) * e;
-        dRho += div_r(mj, rhoj) * dot(vi - vs, dW);
-    });
+    if (d.ND > 0) {
+        const BView dv = dummy_view(d);
+        quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos,
+                       [&](int j) { boundary_drho<R>(d, o, dv, j, g, dRho); });
+    }
     double dsum = quad_sum((double)dRho, gm);
     if (sub != 0) return;
-    double dr = dsum * (2.0 * (double)rhoi);
+    if (kMarkers) dsum += d.mdrho[i];  // the markers' terms (k_sph_marker_pass)
+    double dr = dsum * (2.0 * (double)o.rhoi);
     double ch = d.drho[i] + dr * dt;
     d.drho[i] = ch;
     double r0 = d.rho0[i];
@@ -651,6 +807,92 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_density(SphDev d, double dt) 
     const double4 so = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
     d.stOut[i] = so;
     d.stfOut[i] = f4(so);
+}
+
+// The markers' terms in each fluid particle's acceleration (density = 0,
+// into macc) or density change (density = 1, into mdrho, before the factor
+// 2 rho_i), from the fluid-marker lists; the momentum and continuity passes
+// add them to their sums.  Kept out of those passes so their code stays as
+// small as without markers.
+template <class R>
+__global__ void __launch_bounds__(kSphBlock) k_sph_marker_pass(SphDev d, int density) {
+    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
+    if (i >= d.N) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
+    using VR = V<R>;
+    const int cnt = d.cntM[i];
+    if (cnt == 0) {
+        if (sub == 0) {
+            if (density) d.mdrho[i] = 0.0;
+            else d.macc[i] = make_double4(0, 0, 0, 0);
+        }
+        return;
+    }
+    const double4 pi4 = d.pos[i];
+    const double4 li4 = d.lpos[i];  // the list-build positions: the lists' pair set on an overflowed row
+    const FluidOwn<R> o = fluid_own<R>(d, i, pi4, d.vel[i], d.st[i]);
+    const VR g = cvt<R>(d.gravity);
+    const BView mv = marker_view(d);
+    if (density) {
+        R dRho = (R)0;
+        quad_neighbors(cnt, d.nbM, d.KM, i, -1, li4, d.g, d.mStart, d.mpos,
+                       [&](int j) { boundary_drho<R>(d, o, mv, j, g, dRho); });
+        const double s = quad_sum((double)dRho, gm);
+        if (sub == 0) d.mdrho[i] = s;
+    } else {
+        VR acc = v3r<R>(0, 0, 0);
+        quad_neighbors(cnt, d.nbM, d.KM, i, -1, li4, d.g, d.mStart, d.mpos,
+                       [&](int j) { boundary_acc<R>(d, o, mv, j, g, acc); });
+        double3 a = up(acc);
+        a.x = quad_sum(a.x, gm);
+        a.y = quad_sum(a.y, gm);
+        a.z = quad_sum(a.z, gm);
+        if (sub == 0) d.macc[i] = d4(a, 0);
+    }
+}
+
+// Reaction of the fluid on the markers: for marker t, minus the sum over
+// the fluid particles a in its list rows of m_a times marker t's term in a's
+// acceleration, evaluated by the same function from the same state as the
+// accel pass (so the pair set and the terms are the fluid's own).  Four
+// lanes walk the fluid cells of the marker's stencil; the result, times w,
+// is written (add = 0) or added (add = 1) at the marker's body-order index.
+template <class R>
+__global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double w, int add) {
+    const int t = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
+    if (t >= d.NM) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
+    using VR = V<R>;
+    const double4 pm = d.mpos[t];
+    const double3 rm = xyz(pm);
+    const BView mv = marker_view(d);
+    const VR g = cvt<R>(d.gravity);
+    double3 F = mk3(0, 0, 0);
+    Stencil st = stencil_of(rm, d.g);
+    for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
+        for (int a = b + sub; a < e; a += kQuad) {
+            // the pair set of the lists: the cutoff test on the build-time positions
+            const double4 la = d.lpos[a];
+            const double cut = 2.0 * fmax(la.w, pm.w);
+            const double3 r = xyz(la) - rm;
+            if ((cut * cut - dot(r, r)) < 0.) continue;
+            const double4 pa = d.pos[a];
+            const double4 va = d.vel[a];
+            const FluidOwn<R> o = fluid_own<R>(d, a, pa, va, d.st[a]);
+            VR acc = v3r<R>(0, 0, 0);
+            boundary_acc<R>(d, o, mv, t, g, acc);
+            F -= va.w * up(acc);
+        }
+    });
+    F.x = quad_sum(F.x, gm);
+    F.y = quad_sum(F.y, gm);
+    F.z = quad_sum(F.z, gm);
+    if (sub != 0) return;
+    const int k = d.mid[t];
+    const double3 prev = add ? xyz(d.mforce[k]) : mk3(0, 0, 0);
+    d.mforce[k] = d4(prev + w * F, 0);
 }
 
 // calDummyParticleNormalKernel (WCSPHIntegrationKernel.cu:4-40) over the
@@ -732,6 +974,28 @@ __global__ void k_sph_slot_of(int n, const int* __restrict__ id, int* __restrict
 }
 
 // ================================================================ host =====
+// Marker offsets of a ball of radius R: shells l = 0, 1, ... at radius
+// r_l = R - (l + 1/2) dx while l dx < 2 h and r_l > dx / 4 (the layers a
+// fluid particle outside the surface can reach), shell l carrying
+// n_l = max(1, round(4 pi r_l^2 / dx^2)) points on the golden-angle spiral
+// z_k = 1 - (2k + 1) / n_l, phi_k = k pi (3 - sqrt 5).  A ball too small
+// for any shell gets one marker at its centre.
+static void marker_offsets(double R, double dx, double h, std::vector<double3>& out) {
+    const double ga = kPi * (3.0 - std::sqrt(5.0));
+    for (int l = 0; l * dx < 2.0 * h; l++) {
+        const double r = R - (l + 0.5) * dx;
+        if (!(r > 0.25 * dx)) break;
+        const long nl = std::max(1L, std::lround(4.0 * kPi * r * r / (dx * dx)));
+        for (long k = 0; k < nl; k++) {
+            const double z = 1.0 - (2.0 * k + 1.0) / (double)nl;
+            const double rho = std::sqrt(std::max(0.0, 1.0 - z * z));
+            const double phi = ga * (double)k;
+            out.push_back(mk3(r * rho * std::cos(phi), r * rho * std::sin(phi), r * z));
+        }
+    }
+    if (out.empty()) out.push_back(mk3(0, 0, 0));
+}
+
 struct SphScene {
     cudaStream_t s = 0;
     int precision = DEMSPH_PRECISION_FP64;
@@ -759,6 +1023,7 @@ struct SphScene {
     double invq = 0;
     float eps = 0;
     int P = 0, Vv = 0, S = 0, R0 = 0, D = 0, ID = 0;
+    int L = 0;  // pos buffer the current lists were built from
     DBuf<double4> dpos, dvel, dst, dnorm;
     DBuf<double> drhoD;  // dummy densities (normals only)
     DBuf<int> did;
@@ -769,6 +1034,26 @@ struct SphScene {
     int nF = 0, nD = 0;  // fluid / dummy counts (the host sets before initialisation)
     int N() const { return nF; }
     int ND() const { return nD; }
+    float hUni = 0;      // the common h when uniformH
+
+    // Coupled DEM balls.  Each is sampled by markers (moving boundary
+    // particles) on shells inside its surface; body b owns the markers
+    // [hBStart[b], hBStart[b+1]) of the body-order arrays.  The markers are
+    // placed from the balls' state at the start of each coupled step and stay
+    // where they are when the fluid is stepped alone.
+    int nM = 0, KM = 48, nBody = 0;
+    std::vector<int> hBall, hBStart{0}, hMb;
+    std::vector<double4> hMoff, hMrec;  // offset (x, y, z, h); (c, nu, rho0, m)
+    demsph_dem_t coupledDem = nullptr;
+    DBuf<int> mb, mid, bBall, bStart;
+    DBuf<double4> moff, mrec, mtmp, mpos, mvel, mst, mnorm, mforce, macc;
+    DBuf<double> mdrho;
+    DBuf<float4> mposf, mvelf, mstf, mnormf;
+    DBuf<int4> mposq;
+    DBuf<int> nbM, cntM;
+    CellTable mCells;
+    DemBodies bodies{};
+    bool coupling = false;  // inside a coupled block: place markers, compute reactions
 
     SphDev dev() {
         SphDev d{};
@@ -776,7 +1061,7 @@ struct SphScene {
         d.g = fCells.g;
         d.fStart = fCells.start.p;
         d.dStart = dCells.start.p;
-        d.pos = pos[P].p; d.vel = vel[Vv].p; d.st = st[S].p; d.rho0 = rho0[R0].p; d.drho = drho[D].p;
+        d.pos = pos[P].p; d.lpos = pos[L].p; d.vel = vel[Vv].p; d.st = st[S].p; d.rho0 = rho0[R0].p; d.drho = drho[D].p;
         d.acc = acc.p;
         d.dpos = dpos.p; d.dvel = dvel.p; d.dst = dst.p; d.dnorm = dnorm.p;
         d.velf = velf[Vv].p; d.stf = stf[S].p;
@@ -786,6 +1071,12 @@ struct SphScene {
         d.posf = posf.p; d.dposf = dposf.p; d.eps = eps;
         d.gravity = gravity;
         d.status = status.p;
+        d.NM = nM; d.KM = KM;
+        d.mStart = mCells.start.p;
+        d.mpos = mpos.p; d.mvel = mvel.p; d.mst = mst.p; d.mnorm = mnorm.p;
+        d.mposf = mposf.p; d.mvelf = mvelf.p; d.mstf = mstf.p; d.mnormf = mnormf.p; d.mposq = mposq.p;
+        d.mid = mid.p; d.nbM = nbM.p; d.cntM = cntM.p; d.mforce = mforce.p;
+        d.macc = macc.p; d.mdrho = mdrho.p;
         return d;
     }
 
@@ -796,6 +1087,10 @@ struct SphScene {
         cntF.alloc(n, s, true);
         nbD.alloc(n * std::max(KD, 1), s, false);
         cntD.alloc(n, s, true);
+        if (nM > 0) {
+            nbM.alloc(n * KM, s, false);
+            cntM.alloc(n, s, true);
+        }
     }
 
     // WCSPHSolver::neighborSearch (WCSPHSolver.h:150-285): fluid cell sort,
@@ -808,8 +1103,13 @@ struct SphScene {
     void launch_lists_shape(const SphDev& d) {
         constexpr int W = kListShapes[S].warps;
         const unsigned grid = grid_for(fCells.ncell, W);
-        if (uniformH) k_sph_lists_cell<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
-        else k_sph_lists_cell<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        if (nM > 0) {
+            if (uniformH) k_sph_lists_cell<true, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+            else k_sph_lists_cell<false, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        } else {
+            if (uniformH) k_sph_lists_cell<true, S, false><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+            else k_sph_lists_cell<false, S, false><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        }
     }
     void launch_lists(const SphDev& d) {
         switch (listShape) {
@@ -828,6 +1128,7 @@ struct SphScene {
                                                        velf[Vv ^ 1].p, stf[S ^ 1].p, posq[P ^ 1].p, fCells.g.mn,
                                                        invq);
         P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        L = P;
     }
     // Rewrites the fluid shadows after a host-side change of the records.
     void refresh_shadows() {
@@ -837,8 +1138,19 @@ struct SphScene {
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
     }
+    // Markers from the coupled balls' current state, in cell order.
+    void place_markers() {
+        k_sph_marker_place<<<grid_for(nM, 256), 256, 0, s>>>(nM, mb.p, moff.p, bodies.pos, mtmp.p);
+        mCells.build(mtmp.p, nM, s);
+        k_sph_marker_gather<<<grid_for(nM, 256), 256, 0, s>>>(
+            nM, mCells.sorted.p, mtmp.p, mb.p, moff.p, mrec.p, bodies.vel, bodies.angv, fCells.g.mn, invq, mpos.p,
+            mvel.p, mst.p, mnorm.p, mposf.p, mvelf.p, mstf.p, mnormf.p, mposq.p, mid.p);
+        g_launches += 2 + mCells.launches;
+        DEMSPH_LAUNCH_CHECK();
+    }
     void neighbor_search() {
         const int n = N();
+        if (coupling && nM > 0) place_markers();
         fCells.build(pos[P].p, n, s, id[ID].p);
         g_launches += fCells.launches;
         permute();
@@ -848,19 +1160,40 @@ struct SphScene {
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
     }
+    // The momentum pass (k_sph_accel) on the state d reads, preceded, when
+    // there are markers, by their terms (k_sph_marker_pass) and, inside a
+    // coupled step, by the reaction on them (half of it from each of a
+    // step's two passes: first = 1 writes, first = 0 adds).
+    void launch_accel(const SphDev& d, double hdt, double tstep, int first, bool reaction) {
+        const int n = N();
+        const unsigned grid = grid_for(n, kSphPerBlock);
+        const bool fp64 = precision == DEMSPH_PRECISION_FP64;
+        if (nM > 0) {
+            if (reaction) {
+                const unsigned mg = grid_for(nM, kSphPerBlock);
+                if (fp64) k_sph_marker_force<double><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
+                else k_sph_marker_force<float><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
+                g_launches += 1;
+            }
+            if (fp64) k_sph_marker_pass<double><<<grid, kSphBlock, 0, s>>>(d, 0);
+            else k_sph_marker_pass<float><<<grid, kSphBlock, 0, s>>>(d, 0);
+            if (fp64) k_sph_accel<double, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            else k_sph_accel<float, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            g_launches += 2;
+        } else {
+            if (fp64) k_sph_accel<double, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            else k_sph_accel<float, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            g_launches += 1;
+        }
+        DEMSPH_LAUNCH_CHECK();
+    }
     void accel(int first) {
         SphDev d = dev();
-        const int n = N();
         d.posOut = pos[P ^ 1].p;
         d.velOut = vel[Vv ^ 1].p;
         d.velfOut = velf[Vv ^ 1].p;
         d.posqOut = posq[P ^ 1].p;
-        if (precision == DEMSPH_PRECISION_FP64)
-            k_sph_accel<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
-        else
-            k_sph_accel<float><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, 0.5 * dt, dt, first);
-        g_launches += 1;
-        DEMSPH_LAUNCH_CHECK();
+        launch_accel(d, 0.5 * dt, dt, first, coupling);
         if (first) P ^= 1;
         Vv ^= 1;
     }
@@ -869,9 +1202,19 @@ struct SphScene {
         const int n = N();
         d.stOut = st[S ^ 1].p;
         d.stfOut = stf[S ^ 1].p;
-        if (precision == DEMSPH_PRECISION_FP64) k_sph_density<double><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
-        else k_sph_density<float><<<grid_for(n, kSphPerBlock), kSphBlock, 0, s>>>(d, dt);
-        g_launches += 1;
+        const unsigned grid = grid_for(n, kSphPerBlock);
+        const bool fp64 = precision == DEMSPH_PRECISION_FP64;
+        if (nM > 0) {
+            if (fp64) k_sph_marker_pass<double><<<grid, kSphBlock, 0, s>>>(d, 1);
+            else k_sph_marker_pass<float><<<grid, kSphBlock, 0, s>>>(d, 1);
+            if (fp64) k_sph_density<double, true><<<grid, kSphBlock, 0, s>>>(d, dt);
+            else k_sph_density<float, true><<<grid, kSphBlock, 0, s>>>(d, dt);
+            g_launches += 2;
+        } else {
+            if (fp64) k_sph_density<double, false><<<grid, kSphBlock, 0, s>>>(d, dt);
+            else k_sph_density<float, false><<<grid, kSphBlock, 0, s>>>(d, dt);
+            g_launches += 1;
+        }
         DEMSPH_LAUNCH_CHECK();
         S ^= 1;
     }
@@ -936,6 +1279,7 @@ struct SphScene {
     void grow(const DevStatus& st2) {
         if (st2.need_pairs > KF) KF = st2.need_pairs + st2.need_pairs / 4 + 1;
         if (st2.need_aux > KD) KD = st2.need_aux + st2.need_aux / 4 + 1;
+        if (st2.need_mark > KM) KM = st2.need_mark + st2.need_mark / 4 + 1;
         alloc_lists();
         haveLists = false;  // rebuilt by the next neighbour search
     }
@@ -947,7 +1291,7 @@ struct SphScene {
         std::vector<size_t> bytes;
         long iStep;
         double time;
-        int P, Vv, S, R0, D, ID;
+        int P, Vv, S, R0, D, ID, L;
     };
     template <class T>
     void snap_add(Snap& sn, DBuf<T>& b) {
@@ -960,14 +1304,14 @@ struct SphScene {
         sn.bufs.push_back(std::move(c));
     }
     void take(Snap& sn) {
-        sn.iStep = iStep; sn.time = time; sn.P = P; sn.Vv = Vv; sn.S = S; sn.R0 = R0; sn.D = D; sn.ID = ID;
+        sn.iStep = iStep; sn.time = time; sn.P = P; sn.Vv = Vv; sn.S = S; sn.R0 = R0; sn.D = D; sn.ID = ID; sn.L = L;
         snap_add(sn, pos[P]); snap_add(sn, vel[Vv]); snap_add(sn, st[S]); snap_add(sn, rho0[R0]);
         snap_add(sn, drho[D]); snap_add(sn, id[ID]);
     }
     void restore(Snap& sn) {
         for (size_t k = 0; k < sn.bufs.size(); k++)
             DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
-        iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID;
+        iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID; L = sn.L;
     }
     // Steps without a state snapshot: a list row that overflows its capacity
     // is walked from the cell table by the passes (same neighbours), so an
@@ -991,6 +1335,110 @@ struct SphScene {
         if (st2.overflow) grow(st2);
     }
 
+    // ------------------------------------------------ coupled DEM balls ----
+    // Samples balls[0..n) of the DEM scene (radii read from its device
+    // state) with markers of spacing dx and smoothing length hm, sound speed
+    // c, viscosity nu and rest density rho0 (mass rho0 dx^3), and places them
+    // at the balls' current positions.
+    void add_bodies(demsph_dem_t dem, long n, const int* balls, double dx, double hm, double c, double nu,
+                    double rho0) {
+        if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (coupledDem && coupledDem != dem) throw Status(DEMSPH_ERR_INVALID, "scene is coupled to another DEM scene");
+        if (n <= 0 || !balls) throw Status(DEMSPH_ERR_INVALID, "no balls");
+        if (!(dx > 0) || !(hm > 0) || !(c > 0) || !(rho0 > 0) || !(nu >= 0))
+            throw Status(DEMSPH_ERR_INVALID, "marker spacing, h, sound speed and density must be positive");
+        const GridDesc& g = fCells.g;
+        if (2.0 * hm > std::min(g.cs.x, std::min(g.cs.y, g.cs.z)) * (1.0 + 1e-12))
+            throw Status(DEMSPH_ERR_INVALID, "marker h above the fluid's largest h");
+        const DemBodies B = dem_bodies(dem);
+        std::vector<double4> bp(B.n);
+        DEMSPH_CUDA(cudaMemcpyAsync(bp.data(), B.pos, B.n * sizeof(double4), cudaMemcpyDeviceToHost, s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+        std::vector<int> seen(B.n, 0);
+        for (int b : hBall) seen[b] = 1;
+        for (long k = 0; k < n; k++) {
+            const int b = balls[k];
+            if (b < 0 || b >= B.n) throw Status(DEMSPH_ERR_INVALID, "ball index out of range");
+            if (seen[b]) throw Status(DEMSPH_ERR_INVALID, "ball coupled twice");
+            seen[b] = 1;
+        }
+        const double mass = rho0 * dx * dx * dx;
+        for (long k = 0; k < n; k++) {
+            const int b = balls[k];
+            std::vector<double3> off;
+            marker_offsets(bp[b].w, dx, hm, off);
+            for (const double3& o : off) {
+                hMb.push_back(b);
+                hMoff.push_back(make_double4(o.x, o.y, o.z, hm));
+                hMrec.push_back(make_double4(c, nu, rho0, mass));
+            }
+            hBall.push_back(b);
+            hBStart.push_back((int)hMb.size());
+        }
+        if (hMb.size() > (size_t)INT_MAX / 2) throw Status(DEMSPH_ERR_INVALID, "too many markers");
+        coupledDem = dem;
+        nBody = (int)hBall.size();
+        nM = (int)hMb.size();
+        if (uniformH && (float)hm != hUni) uniformH = false;
+        mb.upload(hMb, s); moff.upload(hMoff, s); mrec.upload(hMrec, s);
+        bBall.upload(hBall, s); bStart.upload(hBStart, s);
+        mtmp.alloc(nM, s, false); mpos.alloc(nM, s, false); mvel.alloc(nM, s, false); mst.alloc(nM, s, false);
+        mnorm.alloc(nM, s, false); mposf.alloc(nM, s, false); mvelf.alloc(nM, s, false); mstf.alloc(nM, s, false);
+        mnormf.alloc(nM, s, false); mposq.alloc(nM, s, false); mid.alloc(nM, s, false);
+        mforce.alloc(nM, s, true);
+        macc.alloc(N(), s, true);
+        mdrho.alloc(N(), s, true);
+        mCells.setup(g, nM, s);
+        alloc_lists();  // resets the graphs
+        bodies = B;
+        coupling = true;
+        place_markers();
+        coupling = false;
+        haveLists = false;
+        DEMSPH_CUDA(cudaStreamSynchronize(s));
+    }
+
+    // n coupled steps: per step the markers follow the balls, the fluid takes
+    // one step (WCSPHSolver::solve's loop body) with the markers as moving
+    // boundary particles, the balls receive the mean of the reactions of the
+    // step's two acceleration passes, and the DEM takes demSub steps of
+    // dt / demSub with that force held.  A DEM list overflow replays the
+    // whole call after regrowth.
+    void coupled_run(demsph_dem_t dem, long n, int demSub) {
+        if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (!coupledDem || dem != coupledDem) throw Status(DEMSPH_ERR_INVALID, "scene is not coupled to this DEM scene");
+        if (demSub < 1) throw Status(DEMSPH_ERR_INVALID, "DEM substeps must be at least 1");
+        if (n <= 0) return;
+        const DemBodies B = dem_bodies(dem);
+        if (std::fabs(B.dt * demSub - dt) > 1e-9 * dt)
+            throw Status(DEMSPH_ERR_INVALID, "DEM time step times substeps differs from the fluid time step");
+        for (int attempt = 0; attempt < 8; attempt++) {
+            Snap sn;
+            take(sn);
+            clear_status();
+            dem_block_begin(dem, s);
+            bodies = B;
+            coupling = true;
+            for (long k = 0; k < n; k++) {
+                iStep++;
+                time += dt;
+                step_body();
+                k_sph_body_force<<<grid_for(nBody, 128), 128, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p, moff.p,
+                                                                      B.force, B.torque);
+                g_launches += 1;
+                DEMSPH_LAUNCH_CHECK();
+                dem_block_steps(dem, demSub);
+            }
+            coupling = false;
+            const bool ok = dem_block_end(dem);
+            DevStatus st2 = read_status();
+            if (st2.overflow) grow(st2);
+            if (ok) return;
+            restore(sn);
+        }
+        throw Status(DEMSPH_ERR_OVERFLOW, "DEM lists kept overflowing during coupled steps");
+    }
+
     // Host particle sets -> device scene (WCSPHSolver::initialize, WCSPHSolver.h:578-612).
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
         if (hf.size() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
@@ -1008,6 +1456,7 @@ struct SphScene {
         nF = (int)hf.size();
         nD = (int)hd.size();
         init_grid(mn, mx, g, timeStep, prec, hmax, uni);
+        hUni = h0;
         const int n = N(), nd = ND();
         auto up4 = [&](DBuf<double4>& b, const std::vector<double4>& h) {
             DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
@@ -1055,7 +1504,7 @@ struct SphScene {
             velf[b].alloc(n, s, false); stf[b].alloc(n, s, false); posq[b].alloc(n, s, false);
             rho0[b].alloc(n, s, false); drho[b].alloc(n, s, false); id[b].alloc(n, s, false);
         }
-        P = Vv = S = R0 = D = ID = 0;
+        P = Vv = S = R0 = D = ID = L = 0;
         k_iota<<<grid_for(n, 256), 256, 0, s>>>(n, id[0].p);
         g_launches += 1;
         acc.alloc(n, s, true);
@@ -1297,6 +1746,7 @@ int demsph_sph_assemble(demsph_sph_t h, int count, const demsph_sph_member_t* me
         s.nF = (int)nf;
         s.nD = (int)nd;
         s.init_grid(sld3(mn, 0), sld3(mx, 0), sld3(g, 0), dt, prec, hmax, uni);
+        s.hUni = (float)members[0]->h0;
         DBuf<double4> tp, tv, ts;
         DBuf<double> trh;
         if (nd > 0) {
@@ -1362,12 +1812,7 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         d.velOut = s.vel[s.Vv ^ 1].p;
         d.velfOut = s.velf[s.Vv ^ 1].p;
         d.posqOut = s.posq[s.P ^ 1].p;
-        if (s.precision == DEMSPH_PRECISION_FP64)
-            k_sph_accel<double><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
-        else
-            k_sph_accel<float><<<grid_for(s.N(), kSphPerBlock), kSphBlock, 0, s.s>>>(d, 0.0, 0.0, 0);
-        g_launches += 1;
-        DEMSPH_LAUNCH_CHECK();
+        s.launch_accel(d, 0.0, 0.0, 0, false);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
     });
 }
@@ -1711,6 +2156,71 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
                 b[w] = col[nb[which == 2 ? (size_t)k * rows + t : (size_t)t * K + k]];
                 w++;
             }
+        }
+    });
+}
+
+// ------------------------------------------------ coupled DEM balls ----
+int demsph_sph_couple_balls(demsph_sph_t h, demsph_dem_t dem, long n, const int* balls, double spacing,
+                            double smoothingLength, double soundSpeed, double viscosity, double density) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!dem) throw Status(DEMSPH_ERR_INVALID, "null DEM scene handle");
+        h->sc.add_bodies(dem, n, balls, spacing, smoothingLength, soundSpeed, viscosity, density);
+    });
+}
+int demsph_sph_couple_step(demsph_sph_t h, demsph_dem_t dem, long n, int demSubsteps) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        h->sc.coupled_run(dem, n, demSubsteps);
+    });
+}
+int demsph_sph_num_markers(demsph_sph_t h, long* n, long* bodies) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (n) *n = h->sc.nM;
+        if (bodies) *bodies = h->sc.nBody;
+    });
+}
+int demsph_sph_get_markers(demsph_sph_t h, double* pos, double* vel, double* normal, double* force, int* ball) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        const int nm = s.nM;
+        if (nm == 0) return;
+        std::vector<double4> p, v, nr, f;
+        std::vector<int> slot;
+        s.mpos.download(p, s.s); s.mvel.download(v, s.s); s.mnorm.download(nr, s.s); s.mforce.download(f, s.s);
+        s.mid.download(slot, s.s);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (int t = 0; t < nm; t++) {
+            const int k = slot[t];
+            if (k < 0 || k >= nm) throw Status(DEMSPH_ERR_INVALID, "marker order corrupted");
+            if (pos) sst3(pos, k, xyz(p[t]));
+            if (vel) sst3(vel, k, xyz(v[t]));
+            if (normal) sst3(normal, k, xyz(nr[t]));
+        }
+        for (int k = 0; k < nm; k++) {
+            if (force) sst3(force, k, xyz(f[k]));
+            if (ball) ball[k] = s.hMb[k];
+        }
+    });
+}
+int demsph_sph_get_coupling(demsph_sph_t h, int* ball, double* force, double* torque) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.coupledDem) return;
+        const DemBodies B = dem_bodies(s.coupledDem);
+        std::vector<double4> F(B.n), T(B.n);
+        DEMSPH_CUDA(cudaMemcpyAsync(F.data(), B.force, B.n * sizeof(double4), cudaMemcpyDeviceToHost, s.s));
+        DEMSPH_CUDA(cudaMemcpyAsync(T.data(), B.torque, B.n * sizeof(double4), cudaMemcpyDeviceToHost, s.s));
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        for (int b = 0; b < s.nBody; b++) {
+            const int i = s.hBall[b];
+            if (ball) ball[b] = i;
+            if (force) sst3(force, b, xyz(F[i]));
+            if (torque) sst3(torque, b, xyz(T[i]));
         }
     });
 }

@@ -440,6 +440,79 @@ def sph_column(n, sound_speed, dt, dx=0.01, layers=3):
                     minb=tuple(lo), maxb=tuple(hi), dt=dt)
 
 
+@dataclass
+class CoupledScene:
+    """A fluid scene, a DEM scene and the balls coupled particle by particle."""
+    name: str
+    sph: SPHScene
+    dem: DEMScene
+    balls: np.ndarray            # DEM indices of the coupled balls
+    marker_spacing: float
+    marker_h: float
+    dem_substeps: int = 1
+    steps: int = 100
+
+
+def balls_in_tank(nx=24, ny=24, depth=24, dx=0.01, layers=3, balls=((0.5, 0.5, 0.5, 4.0, 500.0),),
+                  ball_velocity=None, headroom=12, dem_substeps=2, gravity=(0.0, 0.0, -9.81), walls=True,
+                  E=1e7, nu=0.3, restitution=0.5, mu=0.3, steps=100):
+    """DEM balls immersed in a tank of still water: an nx x ny x depth
+    lattice of fluid (spacing dx) in a tank with `layers` dummy layers on the
+    floor and the four sides (open top, `headroom` cells above the water), and
+    balls given as (x, y, z as fractions of the water block, radius in dx,
+    density).  Fluid particles closer than radius + dx/2 to a ball centre are
+    removed.  The DEM scene has the balls over a 2-triangle floor plane at
+    the tank floor (Hertz-Mindlin, E, nu, restitution, mu); its time step is
+    the fluid's divided by dem_substeps.  Fluid h = 1.3 dx, c0 = 10 sqrt(2 g H),
+    dt = 0.25 h / (c0 + 2 sqrt(g H)); markers use dx and h.  walls=False
+    drops the dummies and the floor (a free block, for momentum checks)."""
+    H = depth * dx
+    g = max(9.81, abs(gravity[2]))
+    c0 = 10.0 * math.sqrt(2 * g * H)
+    h = 1.3 * dx
+    dt = 0.25 * h / (c0 + 2.0 * math.sqrt(g * H))
+    gx = (np.arange(nx) + 0.5) * dx
+    gy = (np.arange(ny) + 0.5) * dx
+    gz = (np.arange(depth) + 0.5) * dx
+    z, y, x = np.meshgrid(gz, gy, gx, indexing="ij")
+    fluid = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    block = np.array([nx * dx, ny * dx, H])
+    bpos = np.array([[b[0] * block[0], b[1] * block[1], b[2] * block[2]] for b in balls], float)
+    brad = np.array([b[3] * dx for b in balls], float)
+    bden = np.array([b[4] for b in balls], float)
+    keep = np.ones(len(fluid), bool)
+    for c, r in zip(bpos, brad):
+        keep &= np.linalg.norm(fluid - c, axis=1) >= r + 0.5 * dx
+    fluid = fluid[keep]
+    tank = (nx * dx, ny * dx, (depth + headroom) * dx)
+    tw = layers * dx
+    lo = np.array([0.0, 0, 0]) - tw
+    hi = np.array(tank, float) + tw
+    if walls:
+        ax = [np.arange(-layers, int(round(t / dx)) + layers) * dx + 0.5 * dx for t in tank]
+        zz, yy, xx = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+        d0 = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+        side = ((d0[:, 0] < 0) | (d0[:, 1] < 0) | (d0[:, 2] < 0) | (d0[:, 0] > tank[0]) | (d0[:, 1] > tank[1]))
+        dummy = d0[side]
+    else:
+        dummy = np.zeros((0, 3))
+    sph = SPHScene(name="balls_in_tank_fluid", fluid=fluid, dummy=dummy, spacing=dx, sound_speed=c0,
+                   minb=tuple(lo), maxb=tuple(hi), gravity=tuple(gravity), dt=dt, steps=steps)
+    Es, Gs = hertz_params(E, nu)
+    k = len(bpos)
+    wl = []
+    if walls:
+        verts = np.array([[lo[0], lo[1], 0.0], [hi[0], lo[1], 0.0], [hi[0], hi[1], 0.0], [lo[0], hi[1], 0.0]])
+        wl = [dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0), material=0)]
+    vel = None if ball_velocity is None else np.asarray(ball_velocity, float).reshape(k, 3)
+    dem = DEMScene(name="balls_in_tank_balls", position=bpos, radius=brad, density=bden,
+                   material=np.zeros(k, np.int32), velocity=vel,
+                   hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)], walls=wl,
+                   minb=tuple(lo), maxb=tuple(hi), gravity=tuple(gravity), dt=dt / dem_substeps, steps=steps)
+    return CoupledScene(name="balls_in_tank", sph=sph, dem=dem, balls=np.arange(k, dtype=np.int32),
+                        marker_spacing=dx, marker_h=h, dem_substeps=dem_substeps, steps=steps)
+
+
 # ---------------------------------------------------------------------------
 # Loading into the solvers
 # ---------------------------------------------------------------------------
@@ -495,3 +568,15 @@ def build_sph(scene: SPHScene, precision="fp64", stream=None, initialize=True):
     if initialize:
         s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
     return s
+
+
+def build_coupled(scene: CoupledScene, precision="fp64", stream=None):
+    """(WCSPHSolver, DEMSolver, DEMSPHCoupling) of a coupled scene, initialised."""
+    from .solvers import DEMSPHCoupling
+
+    f = build_sph(scene.sph, precision, stream)
+    d = build_dem(scene.dem, precision, stream)
+    c = DEMSPHCoupling(f, d)
+    sp = scene.sph
+    c.addBalls(scene.balls, scene.marker_spacing, scene.marker_h, sp.sound_speed, sp.viscosity, sp.density)
+    return f, d, c

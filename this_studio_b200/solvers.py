@@ -553,3 +553,56 @@ class WCSPHSolver:
         a, b = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32)
         call("demsph_sph_get_pairs", self._h, int(which), _ip(a), _ip(b))
         return a, b
+
+
+class DEMSPHCoupling:
+    """Particle-level two-way coupling of DEM balls and a WCSPH fluid.
+
+    The reference couples balls to a fluid only through the buoyancy-drag
+    plane of DEMSolver.setBuoyancyDrag (externalForceTorque.cu:66-133).  Here
+    each coupled ball is sampled by markers -- moving boundary particles on
+    shells inside its surface -- that act on the fluid exactly as the
+    reference's dummy particles do (WCSPHIntegrationKernel.cu:110-143,
+    240-270), with the ball's rigid velocity and an outward normal; the ball
+    receives minus the sum of m_a times its markers' terms in the fluid
+    accelerations as force, and offset x force as torque.
+
+    Both solvers must be initialised; the DEM time step times demSubsteps
+    must equal the fluid's.
+    """
+
+    def __init__(self, sph: WCSPHSolver, dem: DEMSolver):
+        self.sph = sph
+        self.dem = dem
+
+    def addBalls(self, balls, spacing, smoothingLength, soundSpeed, viscosity, density):
+        """Couples DEM balls `balls` (indices) with markers of the given
+        spacing, h, sound speed, viscosity and rest density."""
+        b = _i32(np.atleast_1d(balls))
+        call("demsph_sph_couple_balls", self.sph._h, self.dem._h, len(b), _ip(b), float(spacing),
+             float(smoothingLength), float(soundSpeed), float(viscosity), float(density))
+
+    def step(self, numSteps=1, demSubsteps=1):
+        call("demsph_sph_couple_step", self.sph._h, self.dem._h, int(numSteps), int(demSubsteps))
+
+    def numMarkers(self):
+        n, b = C.c_long(), C.c_long()
+        call("demsph_sph_num_markers", self.sph._h, C.byref(n), C.byref(b))
+        return n.value, b.value
+
+    def getMarkers(self):
+        """Per marker (body order): position, velocity, normal, last reaction, ball."""
+        n, _ = self.numMarkers()
+        out = {"position": np.zeros((n, 3)), "velocity": np.zeros((n, 3)), "normal": np.zeros((n, 3)),
+               "force": np.zeros((n, 3)), "ball": np.zeros(n, np.int32)}
+        call("demsph_sph_get_markers", self.sph._h, _dp(out["position"]), _dp(out["velocity"]),
+             _dp(out["normal"]), _dp(out["force"]), _ip(out["ball"]))
+        return out
+
+    def getForces(self):
+        """(ball indices, force (n, 3), torque (n, 3)) on the coupled balls."""
+        _, nb = self.numMarkers()
+        ball = np.zeros(nb, np.int32)
+        F, T = np.zeros((nb, 3)), np.zeros((nb, 3))
+        call("demsph_sph_get_coupling", self.sph._h, _ip(ball), _dp(F), _dp(T))
+        return ball, F, T
