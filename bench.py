@@ -180,6 +180,40 @@ def dem_bounce(torch, steps, warmup, flush):
             "note": "4,096 spheres; launch-bound at this size (see DESIGN.md)"}
 
 
+def coupled_tank(torch, steps, warmup, flush):
+    """Particle-level DEM-SPH coupling: eight DEM balls (r = 6 dx, densities
+    500-2500) in a 64 x 64 x 48 tank of still water at dx = 0.01, two DEM
+    substeps per fluid step, mixed precision; the same fluid stepped alone
+    (markers held) for the coupling's overhead."""
+    from this_studio_b200 import workloads
+
+    sc = workloads.coupled_tank_scene()
+    from this_studio_b200 import scenes
+
+    f, d, c = scenes.build_coupled(sc, "mixed")
+    c.step(max(warmup, 10), sc.dem_substeps)
+    block = 10  # one captured block of coupled steps per timed call
+    def run(fn):
+        times = []
+        torch.cuda.synchronize()
+        for _ in range(max(1, steps // block)):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return float(sum(times)) / (len(times) * block)
+    ms = run(lambda: c.step(block, sc.dem_substeps))
+    ms_fluid = run(lambda: f.step(block))
+    nm, nb = c.numMarkers()
+    nf = sc.sph.fluid.shape[0]
+    return {"workload": "coupled_tank_200k", "value": nf / (ms / 1e3), "unit": METRIC, "ms_per_step": ms,
+            "fluid_alone_ms_per_step": ms_fluid, "fluid_particles": nf, "dummy_particles": sc.sph.dummy.shape[0],
+            "balls": nb, "markers": nm, "dem_substeps": sc.dem_substeps, "precision": "mixed", "steps": steps}
+
+
 def served_stream(torch, num, seed=5, rate=30.0, steps=500, chunk=100):
     """The serving / batching stream (seeded Poisson arrivals of DEM drops and
     WCSPH dam breaks, particle counts log-uniform over 1k-200k, polydisperse
@@ -286,6 +320,7 @@ def native(args, rank, world, dist):
     del s3
     other_value = nf / (float(sum(t3)) / len(t3) / 1e3)
     dem = dem_bounce(torch, min(args.steps, 200), args.warmup, flush)
+    coupled = coupled_tank(torch, min(args.steps, 100), args.warmup, flush)
     del flush
     stream = served_stream(torch, args.stream) if (args.stream > 0 and rank == 0 and world == 1) else None
 
@@ -301,6 +336,7 @@ def native(args, rank, world, dist):
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "value_" + other: other_value,
         "dem": dem,
+        "coupled": coupled,
         "stream": stream,
         "gpu_launches": int(launches),
         "clocks": clk,

@@ -259,6 +259,7 @@ struct DevStatus {
     int need_aux;      // largest per-row count for the secondary list
     int bad_index;     // nonzero: a remapped index fell outside its array
     int need_mark;     // largest per-row count for the fluid-marker list
+    int need_mrev;     // largest per-row count for the marker-fluid list
 };
 
 }  // namespace demsph

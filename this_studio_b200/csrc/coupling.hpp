@@ -28,8 +28,20 @@ DemBodies dem_bodies(demsph_dem_t h);
 // stream, the DEM launches on s until dem_block_end, and its dynamic state
 // is saved for a replay.
 void dem_block_begin(demsph_dem_t h, cudaStream_t s);
-// n DEM steps (DEMSolver::solve's loop body) on the block's stream.
-void dem_block_steps(demsph_dem_t h, int n);
+// n DEM steps (DEMSolver::solve's loop body) issued on stream s (the
+// block's stream, or the stream capturing it).
+void dem_block_steps(demsph_dem_t h, int n, cudaStream_t s);
+// For capturing coupled steps in a CUDA graph: whether the DEM step can be
+// replayed (no time-dependent kernel arguments), its step counter and clock
+// (saved around a capture, advanced after a replay), the key of its
+// ping-pong buffer state, and a counter of its graph resets (a change means
+// its buffers or kernel arguments changed).
+bool dem_graphable(demsph_dem_t h);
+void dem_clock(demsph_dem_t h, long* iStep, double* time);
+void dem_set_clock(demsph_dem_t h, long iStep, double time);
+void dem_advance_clock(demsph_dem_t h, long steps);
+int dem_graph_key(demsph_dem_t h);
+long dem_graph_epoch(demsph_dem_t h);
 // Ends the block (synchronising its stream).  Returns false when a DEM
 // list overflowed: the lists were regrown and the DEM state restored to the
 // block's start, and the block must be replayed.

@@ -1496,10 +1496,34 @@ void dem_block_begin(demsph_dem_t h, cudaStream_t s) {
     if (!sc.ghosts.empty()) DEMSPH_CUDA(cudaMemsetAsync(sc.gstatus.p, 0, sizeof(DevStatus), s));
 }
 
-void dem_block_steps(demsph_dem_t h, int n) {
+void dem_block_steps(demsph_dem_t h, int n, cudaStream_t s) {
     DemScene& sc = h->sc;
-    for (int k = 0; k < n; k++) sc.step_once();
+    const cudaStream_t keep = sc.s;
+    sc.s = s;
+    try {
+        for (int k = 0; k < n; k++) sc.step_once();
+    } catch (...) {
+        sc.s = keep;
+        throw;
+    }
+    sc.s = keep;
 }
+
+bool dem_graphable(demsph_dem_t h) { return h->sc.graphable(); }
+void dem_clock(demsph_dem_t h, long* iStep, double* time) {
+    *iStep = h->sc.iStep;
+    *time = h->sc.time;
+}
+void dem_set_clock(demsph_dem_t h, long iStep, double time) {
+    h->sc.iStep = iStep;
+    h->sc.time = time;
+}
+void dem_advance_clock(demsph_dem_t h, long steps) {
+    h->sc.iStep += steps;
+    h->sc.time += steps * h->sc.dt;
+}
+int dem_graph_key(demsph_dem_t h) { return h->sc.index_key(); }
+long dem_graph_epoch(demsph_dem_t h) { return h->sc.graph.epoch; }
 
 bool dem_block_end(demsph_dem_t h) {
     DemScene& sc = h->sc;

@@ -131,7 +131,11 @@ struct StepGraph {
 // a different index state would use the wrong buffers.
 struct GraphSet {
     std::map<int, std::unique_ptr<StepGraph>> byKey;
-    void reset() { byKey.clear(); }
+    long epoch = 0;  // counts resets: graphs built on this scene's buffers elsewhere check it
+    void reset() {
+        byKey.clear();
+        epoch++;
+    }
     StepGraph& at(int key) {
         auto& p = byKey[key];
         if (!p) p = std::make_unique<StepGraph>();

@@ -94,6 +94,9 @@ struct SphDev {
     const int* mid;
     int* nbM;
     int* cntM;
+    int KR;          // the transposed list: fluid partners of each marker slot
+    int* nbR;
+    int* cntR;
     double4* mforce;
     double4* macc;   // per fluid particle: the markers' terms in its acceleration
     double* mdrho;   // and in its density change (before 2 rho_i)
@@ -270,19 +273,35 @@ __global__ void k_sph_marker_gather(int nm, const int* __restrict__ sorted, cons
 // Coupling force and torque of each coupled ball: the sum of its markers'
 // reactions (body order, markers [start[b], start[b+1])), and of offset x
 // reaction, written at the ball's index.
-__global__ void k_sph_body_force(int nb, const int* __restrict__ start, const int* __restrict__ ball,
-                                 const double4* __restrict__ mforce, const double4* __restrict__ moff,
-                                 double4* __restrict__ force, double4* __restrict__ torque) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+// One block per ball: each thread sums a strided share of the markers, then
+// a fixed-order tree in shared memory (the same sums every run).
+constexpr int kBodyBlock = 128;
+__global__ void __launch_bounds__(kBodyBlock) k_sph_body_force(const int* __restrict__ start,
+                                                               const int* __restrict__ ball,
+                                                               const double4* __restrict__ mforce,
+                                                               const double4* __restrict__ moff,
+                                                               double4* __restrict__ force,
+                                                               double4* __restrict__ torque) {
+    __shared__ double sh[6][kBodyBlock];
+    const int b = blockIdx.x, tid = threadIdx.x;
     double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
-    for (int k = start[b]; k < start[b + 1]; k++) {
+    for (int k = start[b] + tid; k < start[b + 1]; k += kBodyBlock) {
         const double3 f = xyz(mforce[k]);
         F += f;
         T += cross(xyz(moff[k]), f);
     }
-    force[ball[b]] = d4(F, 0);
-    torque[ball[b]] = d4(T, 0);
+    sh[0][tid] = F.x; sh[1][tid] = F.y; sh[2][tid] = F.z;
+    sh[3][tid] = T.x; sh[4][tid] = T.y; sh[5][tid] = T.z;
+    __syncthreads();
+    for (int h = kBodyBlock / 2; h > 0; h >>= 1) {
+        if (tid < h)
+            for (int c = 0; c < 6; c++) sh[c][tid] += sh[c][tid + h];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        force[ball[b]] = make_double4(sh[0][0], sh[1][0], sh[2][0], 0);
+        torque[ball[b]] = make_double4(sh[3][0], sh[4][0], sh[5][0], 0);
+    }
 }
 // Puts the dummies into cell order (sorted[t] = caller index of slot t).
 __global__ void k_sph_dummy_gather(int nd, const int* __restrict__ sorted, const double4* __restrict__ tp,
@@ -511,6 +530,27 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     if (kMarkers)
         cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM, d.N,
                                       d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
+}
+
+// The transposed fluid-marker list: for each marker slot, the fluid
+// particles within the list cutoff, one warp per marker cell (the fluid
+// list build with the roles swapped; the FP64 test is symmetric, so the
+// pairs are exactly those of the fluid rows).
+template <bool kUniformH, int kShape>
+__global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
+    k_sph_marker_lists(SphDev d, int ncell) {
+    constexpr int kListWarps = kListShapes[kShape].warps, kStage = kListShapes[kShape].stage;
+    __shared__ float4 sPos[kListWarps][kStage];
+    __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
+    const int w = threadIdx.x >> 5;
+    const int cell = blockIdx.x * kListWarps + w;
+    if (cell >= ncell) return;
+    const int ps = d.mStart[cell], pe = d.mStart[cell + 1];
+    if (ps == pe) return;
+    ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
+    Stencil st = stencil_of(xyz(d.mpos[ps]), d.g);
+    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.mpos, d.mposf, d.pos, d.posf, d.eps, false, d.KR, d.NM,
+                                  d.nbR, d.cntR, &d.status->need_mrev, &d.status->overflow, sg);
 }
 
 // Calls f(j) for this lane's share of particle i's neighbours: from the ELL
@@ -853,11 +893,11 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_marker_pass(SphDev d, int den
 }
 
 // Reaction of the fluid on the markers: for marker t, minus the sum over
-// the fluid particles a in its list rows of m_a times marker t's term in a's
-// acceleration, evaluated by the same function from the same state as the
-// accel pass (so the pair set and the terms are the fluid's own).  Four
-// lanes walk the fluid cells of the marker's stencil; the result, times w,
-// is written (add = 0) or added (add = 1) at the marker's body-order index.
+// the fluid particles a whose list rows hold t of m_a times marker t's term
+// in a's acceleration, evaluated by the same function from the same state as
+// the fluid's pass (so the pair set and the terms are the fluid's own).  Four
+// lanes share the marker's transposed list row; the result, times w, is
+// written (add = 0) or added (add = 1) at the marker's body-order index.
 template <class R>
 __global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double w, int add) {
     const int t = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
@@ -870,22 +910,31 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double
     const BView mv = marker_view(d);
     const VR g = cvt<R>(d.gravity);
     double3 F = mk3(0, 0, 0);
-    Stencil st = stencil_of(rm, d.g);
-    for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
-        for (int a = b + sub; a < e; a += kQuad) {
-            // the pair set of the lists: the cutoff test on the build-time positions
-            const double4 la = d.lpos[a];
-            const double cut = 2.0 * fmax(la.w, pm.w);
-            const double3 r = xyz(la) - rm;
-            if ((cut * cut - dot(r, r)) < 0.) continue;
-            const double4 pa = d.pos[a];
-            const double4 va = d.vel[a];
-            const FluidOwn<R> o = fluid_own<R>(d, a, pa, va, d.st[a]);
-            VR acc = v3r<R>(0, 0, 0);
-            boundary_acc<R>(d, o, mv, t, g, acc);
-            F -= va.w * up(acc);
-        }
-    });
+    auto term = [&](int a) {
+        const double4 va = d.vel[a];
+        const FluidOwn<R> o = fluid_own<R>(d, a, d.pos[a], va, d.st[a]);
+        VR acc = v3r<R>(0, 0, 0);
+        boundary_acc<R>(d, o, mv, t, g, acc);
+        F -= va.w * up(acc);
+    };
+    const int cnt = d.cntR[t];
+    if (cnt >= 0) {
+        // the transposed list (k_sph_marker_lists): the fluid rows' pair set
+        const int* __restrict__ row = d.nbR + (size_t)t * d.KR;
+        for (int k = sub; k < cnt; k += kQuad) term(__ldg(row + k));
+    } else {
+        // an overflowed row: the same pairs from the cell stencil, with the
+        // cutoff test on the build-time positions
+        Stencil st = stencil_of(rm, d.g);
+        for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
+            for (int a = b + sub; a < e; a += kQuad) {
+                const double4 la = d.lpos[a];
+                const double cut = 2.0 * fmax(la.w, pm.w);
+                const double3 r = xyz(la) - rm;
+                if ((cut * cut - dot(r, r)) >= 0.) term(a);
+            }
+        });
+    }
     F.x = quad_sum(F.x, gm);
     F.y = quad_sum(F.y, gm);
     F.z = quad_sum(F.z, gm);
@@ -1041,7 +1090,7 @@ struct SphScene {
     // [hBStart[b], hBStart[b+1]) of the body-order arrays.  The markers are
     // placed from the balls' state at the start of each coupled step and stay
     // where they are when the fluid is stepped alone.
-    int nM = 0, KM = 48, nBody = 0;
+    int nM = 0, KM = 48, KR = 96, nBody = 0;
     std::vector<int> hBall, hBStart{0}, hMb;
     std::vector<double4> hMoff, hMrec;  // offset (x, y, z, h); (c, nu, rho0, m)
     demsph_dem_t coupledDem = nullptr;
@@ -1050,10 +1099,17 @@ struct SphScene {
     DBuf<double> mdrho;
     DBuf<float4> mposf, mvelf, mstf, mnormf;
     DBuf<int4> mposq;
-    DBuf<int> nbM, cntM;
+    DBuf<int> nbM, cntM, nbR, cntR;
     CellTable mCells;
     DemBodies bodies{};
     bool coupling = false;  // inside a coupled block: place markers, compute reactions
+    // Graphs of kCoupledSteps coupled steps, keyed by both scenes' buffer
+    // state; dropped when either scene drops its own graphs (buffers or
+    // kernel arguments changed) or the DEM substep count changes.
+    static constexpr int kCoupledSteps = 10;
+    GraphSet cgraph;
+    long cgSphEpoch = -1, cgDemEpoch = -1;
+    int cgSub = 0;
 
     SphDev dev() {
         SphDev d{};
@@ -1076,6 +1132,7 @@ struct SphScene {
         d.mpos = mpos.p; d.mvel = mvel.p; d.mst = mst.p; d.mnorm = mnorm.p;
         d.mposf = mposf.p; d.mvelf = mvelf.p; d.mstf = mstf.p; d.mnormf = mnormf.p; d.mposq = mposq.p;
         d.mid = mid.p; d.nbM = nbM.p; d.cntM = cntM.p; d.mforce = mforce.p;
+        d.KR = KR; d.nbR = nbR.p; d.cntR = cntR.p;
         d.macc = macc.p; d.mdrho = mdrho.p;
         return d;
     }
@@ -1090,6 +1147,8 @@ struct SphScene {
         if (nM > 0) {
             nbM.alloc(n * KM, s, false);
             cntM.alloc(n, s, true);
+            nbR.alloc((size_t)nM * KR, s, false);
+            cntR.alloc(nM, s, true);
         }
     }
 
@@ -1106,6 +1165,11 @@ struct SphScene {
         if (nM > 0) {
             if (uniformH) k_sph_lists_cell<true, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
             else k_sph_lists_cell<false, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+            if (coupling) {  // the transposed rows the reaction reads
+                if (uniformH) k_sph_marker_lists<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+                else k_sph_marker_lists<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+                g_launches += 1;
+            }
         } else {
             if (uniformH) k_sph_lists_cell<true, S, false><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
             else k_sph_lists_cell<false, S, false><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
@@ -1280,6 +1344,7 @@ struct SphScene {
         if (st2.need_pairs > KF) KF = st2.need_pairs + st2.need_pairs / 4 + 1;
         if (st2.need_aux > KD) KD = st2.need_aux + st2.need_aux / 4 + 1;
         if (st2.need_mark > KM) KM = st2.need_mark + st2.need_mark / 4 + 1;
+        if (st2.need_mrev > KR) KR = st2.need_mrev + st2.need_mrev / 4 + 1;
         alloc_lists();
         haveLists = false;  // rebuilt by the next neighbour search
     }
@@ -1412,6 +1477,16 @@ struct SphScene {
         const DemBodies B = dem_bodies(dem);
         if (std::fabs(B.dt * demSub - dt) > 1e-9 * dt)
             throw Status(DEMSPH_ERR_INVALID, "DEM time step times substeps differs from the fluid time step");
+        // one coupled step, issued on s (the scene stream, or a capture stream)
+        auto one = [&] {
+            iStep++;
+            time += dt;
+            step_body();
+            k_sph_body_force<<<nBody, kBodyBlock, 0, s>>>(bStart.p, bBall.p, mforce.p, moff.p, B.force, B.torque);
+            g_launches += 1;
+            DEMSPH_LAUNCH_CHECK();
+            dem_block_steps(dem, demSub, s);
+        };
         for (int attempt = 0; attempt < 8; attempt++) {
             Snap sn;
             take(sn);
@@ -1419,15 +1494,51 @@ struct SphScene {
             dem_block_begin(dem, s);
             bodies = B;
             coupling = true;
-            for (long k = 0; k < n; k++) {
-                iStep++;
-                time += dt;
-                step_body();
-                k_sph_body_force<<<grid_for(nBody, 128), 128, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p, moff.p,
-                                                                      B.force, B.torque);
-                g_launches += 1;
-                DEMSPH_LAUNCH_CHECK();
-                dem_block_steps(dem, demSub);
+            long k = 0;
+            try {
+                if (useGraphs && dem_graphable(dem)) {
+                    // blocks of kCoupledSteps coupled steps start where a DEM
+                    // re-sort just happened, so that each block holds the same
+                    // launches (an even number of fluid steps and of DEM
+                    // re-sorts: every ping-pong index is back to its parity)
+                    for (long di; k < n; k++) {
+                        double dtm;
+                        dem_clock(dem, &di, &dtm);
+                        if (di % 5 == 0) break;
+                        one();
+                    }
+                    if (cgSphEpoch != graph.epoch || cgDemEpoch != dem_graph_epoch(dem) || cgSub != demSub) {
+                        cgraph.reset();
+                        cgSphEpoch = graph.epoch;
+                        cgDemEpoch = dem_graph_epoch(dem);
+                        cgSub = demSub;
+                    }
+                    for (; k + kCoupledSteps <= n; k += kCoupledSteps) {
+                        StepGraph& gr = cgraph.at(index_key() | dem_graph_key(dem) << 6);
+                        if (!gr.ready()) {
+                            const long i0 = iStep;
+                            const double t0 = time;
+                            long di;
+                            double dtm;
+                            dem_clock(dem, &di, &dtm);
+                            gr.capture(kCoupledSteps, s, [&] {
+                                for (int j = 0; j < kCoupledSteps; j++) one();
+                            });
+                            iStep = i0;
+                            time = t0;
+                            dem_set_clock(dem, di, dtm);
+                        }
+                        gr.launch(s);
+                        iStep += kCoupledSteps;
+                        time += kCoupledSteps * dt;
+                        dem_advance_clock(dem, (long)kCoupledSteps * demSub);
+                    }
+                }
+                for (; k < n; k++) one();
+            } catch (...) {
+                coupling = false;
+                dem_block_end(dem);
+                throw;
             }
             coupling = false;
             const bool ok = dem_block_end(dem);

@@ -7,6 +7,9 @@ sph_dam_break_128k  WCSPH dam break, 40 x 40 x 80 fluid at dx = 0.01 (128,000)
 sph_dam_break_1m    the same tank at dx = 0.005: 80 x 80 x 160 fluid (1,024,000)
 dem_drop_4096       4,096 Hertz-Mindlin spheres dropped onto a plane
 dem_drop_1m         about 10^6 polydisperse spheres dropped onto a plane
+coupled_tank_200k   eight DEM balls (r = 6 dx) in a 64 x 64 x 48 tank of water
+                    at dx = 0.01 (about 190,000 fluid particles), coupled
+                    particle by particle, two DEM substeps per fluid step
 """
 from __future__ import annotations
 
@@ -15,7 +18,18 @@ import argparse
 from . import scenes
 
 
+COUPLED_BALLS = ((0.25, 0.25, 0.35, 6.0, 2500.0), (0.75, 0.25, 0.35, 6.0, 500.0), (0.25, 0.75, 0.35, 6.0, 1200.0),
+                 (0.75, 0.75, 0.35, 6.0, 800.0), (0.25, 0.25, 0.75, 6.0, 2500.0), (0.75, 0.25, 0.75, 6.0, 500.0),
+                 (0.25, 0.75, 0.75, 6.0, 1200.0), (0.75, 0.75, 0.75, 6.0, 800.0))
+
+
+def coupled_tank_scene():
+    return scenes.balls_in_tank(nx=64, ny=64, depth=48, balls=COUPLED_BALLS, dem_substeps=2)
+
+
 def build(name, precision="mixed"):
+    if name == "coupled_tank_200k":
+        return scenes.build_coupled(coupled_tank_scene(), precision)[2]
     if name == "sph_dam_break_128k":
         return scenes.build_sph(scenes.sph_dam_break(), precision)
     if name == "sph_dam_break_1m":
@@ -35,10 +49,17 @@ def main():
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel directly")
     a = ap.parse_args()
     s = build(a.name, a.precision)
-    if a.no_graphs:
-        s.setGraphs(False)
-    s.step(a.steps)
-    s.stepIndex()
+    if a.name.startswith("coupled"):
+        if a.no_graphs:
+            s.sph.setGraphs(False)
+            s.dem.setGraphs(False)
+        s.step(a.steps, 2)
+        s.sph.stepIndex()
+    else:
+        if a.no_graphs:
+            s.setGraphs(False)
+        s.step(a.steps)
+        s.stepIndex()
     print(f"{a.name}: {a.steps} steps done")
 
 
