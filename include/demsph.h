@@ -314,6 +314,21 @@ int demsph_sph_assemble(demsph_sph_t s, int count, const demsph_sph_member_t* me
  * DEMSPH_VTU_DUMMIES) in the reference's layout. */
 int demsph_sph_write_vtu(demsph_sph_t s, const char* dir, long frame, int what);
 
+/* Skin lists (no counterpart in the reference, which rebuilds its lists every
+ * step: WCSPHSolver::neighborSearch, WCSPHSolver.h:150-285).  The fluid's
+ * neighbour rows hold every candidate within the cutoff plus a skin of
+ * `fraction` x 2 h_max at their last rebuild; a step rebuilds them (cell sort,
+ * reorder, list build) only when some particle has drifted half the skin, and
+ * its first momentum pass keeps the pairs that pass the reference's exact
+ * cutoff test on that step's positions, so every step uses the reference's
+ * pair set.  Default 0.05; 0 rebuilds exact lists every step.  Before
+ * initialisation the value also sizes the grid's cells (2 h_max (1 +
+ * fraction)); afterwards it may only be lowered.  Scenes with coupled balls
+ * rebuild every step.  skin_stats: the fraction in use (0 when off) and the
+ * rebuilds so far. */
+int demsph_sph_set_skin(demsph_sph_t s, double fraction);
+int demsph_sph_skin_stats(demsph_sph_t s, double* fraction, long* rebuilds);
+
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);
 int demsph_sph_step_index(demsph_sph_t s, long* step, double* time);

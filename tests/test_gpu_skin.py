@@ -1,0 +1,74 @@
+"""Skin lists: a fluid step that reuses rows built with a skin and keeps the
+pairs within the exact cutoff uses the reference's per-step pair set.
+Checked step by step against scenes that rebuild exact lists every step, in
+both precisions, with the rebuilds counted; graph replay against direct
+launches; the setting's limits."""
+import numpy as np
+import pytest
+
+from this_studio_b200 import DemsphError, scenes
+from this_studio_b200.solvers import WCSPHSolver
+
+from .helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _build(sc, prec, skin):
+    s = WCSPHSolver()
+    s.setSkin(skin)
+    s.addSPHs(sc.fluid, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    s.addDummies(sc.dummy, None, sc.sound_speed, sc.spacing, sc.density, sc.viscosity)
+    s.initialize(sc.minb, sc.maxb, sc.gravity, sc.dt, prec)
+    return s
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_skin_steps_use_the_exact_pair_set(gpu, prec):
+    sc = scenes.dam_break_reference()
+    a = _build(sc, prec, 0.05)
+    b = _build(sc, prec, 0.0)
+    assert a.skinStats()[0] == pytest.approx(0.05)
+    assert b.skinStats()[0] == 0.0
+    for k in range(40):
+        a.step(1)
+        b.step(1)
+        for w in (0, 1):
+            pa, pb = a.getPairs(w), b.getPairs(w)
+            assert len(pa[0]) == len(pb[0]), (k, w)
+            np.testing.assert_array_equal(pa[0], pb[0])
+            np.testing.assert_array_equal(pa[1], pb[1])
+    fa, fb = a.getSPH(), b.getSPH()
+    e = rel_err(fa["position"] - sc.fluid, fb["position"] - sc.fluid)
+    ev = rel_err(fa["velocity"], fb["velocity"])
+    rebuilds = a.skinStats()[1]
+    print(f"{prec}: 40 steps, {rebuilds} skin rebuilds; displacement {e:.2e}, velocity {ev:.2e} vs exact lists")
+    assert 1 <= rebuilds < 40
+    assert e < (1e-12 if prec == "fp64" else 1e-6) and ev < (1e-11 if prec == "fp64" else 1e-5)
+
+
+def test_skin_graph_replay_matches_direct_launches(gpu):
+    """The gated rebuild inside captured steps gives the same bits as direct launches."""
+    sc = scenes.dam_break_reference()
+    out = []
+    for graphs in (True, False):
+        s = _build(sc, "mixed", 0.05)
+        s.setGraphs(graphs)
+        s.step(37)
+        out.append((s.getSPH(), s.skinStats()[1]))
+    (sa, ra), (sb, rb) = out
+    assert ra == rb
+    for k in ("position", "velocity", "density", "pressure"):
+        np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_skin_setting(gpu):
+    sc = scenes.dam_break_reference()
+    s = _build(sc, "fp64", 0.1)
+    with pytest.raises(DemsphError):
+        s.setSkin(0.2)  # above what the grid was built for
+    s.setSkin(0.05)
+    s.step(5)
+    s.setSkin(0.0)
+    s.step(5)
+    assert s.skinStats()[0] == 0.0

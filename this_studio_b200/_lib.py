@@ -89,6 +89,8 @@ SIGNATURES = {
     "demsph_sph_profile_steps": [_vp, _long, _d],
     "demsph_sph_tune": [_vp, _int, _i, _d],
     "demsph_sph_set_graphs": [_vp, _int],
+    "demsph_sph_set_skin": [_vp, _dbl],
+    "demsph_sph_skin_stats": [_vp, _d, _l],
     "demsph_sph_write_vtu": [_vp, C.c_char_p, _long, _int],
     "demsph_sph_num_list_shapes": [],
     "demsph_sph_set_list_shape": [_vp, _int],

@@ -19,10 +19,13 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 // Histogram: key[i] = clamped cell key of object i; cnt[key]++.  With
 // outsideOnly, objects inside the domain get key -1 and stay out of the table
 // (calculateDummyHash, neighborSearchKernel.cu:29-55).
+// A non-null gate makes every kernel of a build return at once while *gate is
+// zero, so a build can sit in a captured step and run only when the device
+// decides to (the skin lists of the fluid).
 static __global__ void k_cell_count(const double4* __restrict__ p, int n, GridDesc g, int* __restrict__ key,
-                             int* __restrict__ cnt, int outsideOnly) {
+                             int* __restrict__ cnt, int outsideOnly, const int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate == 0)) return;
     double4 q = p[i];
     if (outsideOnly && q.x >= g.mn.x && q.x < g.mx.x && q.y >= g.mn.y && q.y < g.mx.y && q.z >= g.mn.z &&
         q.z < g.mx.z) {
@@ -38,7 +41,8 @@ static __global__ void k_cell_count(const double4* __restrict__ p, int n, GridDe
 // the tile total, and writes the scanned values (out[n] = grand total).
 static __global__ void __launch_bounds__(kScanBlock) k_scan_tile(const int* __restrict__ in, int* __restrict__ out, int n,
                                                           const int* __restrict__ tileOffset,
-                                                          int* __restrict__ tileSum) {
+                                                          int* __restrict__ tileSum, const int* __restrict__ gate) {
+    if (gate && *gate == 0) return;
     __shared__ int warpSums[kScanBlock / 32];
     int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -82,9 +86,9 @@ static __global__ void __launch_bounds__(kScanBlock) k_scan_tile(const int* __re
 // Scatter into cell order: the atomic decrement returns the counters to zero
 // for the next rebuild, so no memset is needed between rebuilds.
 static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const int* __restrict__ start, int* __restrict__ cnt,
-                               int* __restrict__ sorted) {
+                               int* __restrict__ sorted, const int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate == 0)) return;
     int k = key[i];
     if (k < 0) return;
     int slot = start[k] + atomicSub(cnt + k, 1) - 1;
@@ -97,9 +101,10 @@ static __global__ void k_cell_scatter(const int* __restrict__ key, int n, const 
 // cell costs O(members) per thread instead of a serial insertion sort.
 static __global__ void k_cell_rank(int n, const int* __restrict__ key, const int* __restrict__ start,
                                    const int* __restrict__ unordered, int* __restrict__ sorted,
-                                   const int* __restrict__ orderKey, int ncell) {
+                                   const int* __restrict__ orderKey, int ncell, const int* __restrict__ gate) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || s >= start[ncell]) return;  // start[ncell] = objects in the table
+    if (s >= n || (gate && *gate == 0)) return;
+    if (s >= start[ncell]) return;  // start[ncell] = objects in the table
     int v = unordered[s];
     int c = key[v];
     int b = start[c], e = start[c + 1];
@@ -147,33 +152,36 @@ struct CellTable {
         }
     }
     // Exclusive scan of in[0..n) into out[0..n], recursing over tile sums.
-    void scan(const int* in, int* out, int n, int level, cudaStream_t s) {
+    void scan(const int* in, int* out, int n, int level, cudaStream_t s, const int* gate) {
         if (n <= kScanTile) {
-            k_scan_tile<<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, nullptr);
+            k_scan_tile<<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, nullptr, gate);
             launches++;
             return;
         }
         int nt = (n + kScanTile - 1) / kScanTile;
         int* sums = scanTmp[2 * level]->p;
         int* offs = scanTmp[2 * level + 1]->p;
-        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, nullptr, n, nullptr, sums);
+        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, nullptr, n, nullptr, sums, gate);
         launches++;
-        scan(sums, offs, nt, level + 1, s);
-        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, out, n, offs, nullptr);
+        scan(sums, offs, nt, level + 1, s, gate);
+        k_scan_tile<<<nt, kScanBlock, 0, s>>>(in, out, n, offs, nullptr, gate);
         launches++;
     }
     // Sorts objects p[0..n) (positions in .xyz) into cells.
     // outsideOnly: only objects outside the domain enter the table.
-    void build(const double4* p, int n, cudaStream_t s, const int* orderKey = nullptr, bool outsideOnly = false) {
+    // gate: device word; the build happens only where it is nonzero.
+    void build(const double4* p, int n, cudaStream_t s, const int* orderKey = nullptr, bool outsideOnly = false,
+               const int* gate = nullptr) {
         launches = 0;
         if (n > 0) {
-            k_cell_count<<<grid_for(n, 256), 256, 0, s>>>(p, n, g, key.p, cnt.p, outsideOnly ? 1 : 0);
+            k_cell_count<<<grid_for(n, 256), 256, 0, s>>>(p, n, g, key.p, cnt.p, outsideOnly ? 1 : 0, gate);
             launches++;
         }
-        scan(cnt.p, start.p, ncell, 0, s);
+        scan(cnt.p, start.p, ncell, 0, s, gate);
         if (n > 0) {
-            k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, unordered.p);
-            k_cell_rank<<<grid_for(n, 256), 256, 0, s>>>(n, key.p, start.p, unordered.p, sorted.p, orderKey, ncell);
+            k_cell_scatter<<<grid_for(n, 256), 256, 0, s>>>(key.p, n, start.p, cnt.p, unordered.p, gate);
+            k_cell_rank<<<grid_for(n, 256), 256, 0, s>>>(n, key.p, start.p, unordered.p, sorted.p, orderKey, ncell,
+                                                         gate);
             launches += 2;
         }
         DEMSPH_LAUNCH_CHECK();

@@ -199,21 +199,21 @@ static inline bool grid_set(GridDesc& g, double3 mn, double3 mx, double cell) {
     return true;
 }
 // calculateGridPosition (neighborSearchKernel.cuh:4-9): truncation toward zero.
-__device__ __forceinline__ int3 cell_of(double3 p, const GridDesc& g) {
+__host__ __device__ __forceinline__ int3 cell_of(double3 p, const GridDesc& g) {
     return make_int3(int((p.x - g.mn.x) / g.cs.x), int((p.y - g.mn.y) / g.cs.y), int((p.z - g.mn.z) / g.cs.z));
 }
-__device__ __forceinline__ int key_of(int3 c, const GridDesc& g) { return c.z * g.ny * g.nx + c.y * g.nx + c.x; }
+__host__ __device__ __forceinline__ int key_of(int3 c, const GridDesc& g) { return c.z * g.ny * g.nx + c.y * g.nx + c.x; }
 // calculateHash kernel (neighborSearchKernel.cu:6-27): clamp into the domain first.
-__device__ __forceinline__ int clamped_key(double3 p, const GridDesc& g) {
+__host__ __device__ __forceinline__ int clamped_key(double3 p, const GridDesc& g) {
     if (p.x < g.mn.x) p.x = g.mn.x; else if (p.x >= g.mx.x) p.x = g.mx.x - 0.5 * g.cs.x;
     if (p.y < g.mn.y) p.y = g.mn.y; else if (p.y >= g.mx.y) p.y = g.mx.y - 0.5 * g.cs.y;
     if (p.z < g.mn.z) p.z = g.mn.z; else if (p.z >= g.mx.z) p.z = g.mx.z - 0.5 * g.cs.z;
     int3 c = cell_of(p, g);
     // A coordinate within an ulp below the max face can round up to index n
     // (and NaN converts to an arbitrary int); keep the key inside the table.
-    c.x = min(max(c.x, 0), g.nx - 1);
-    c.y = min(max(c.y, 0), g.ny - 1);
-    c.z = min(max(c.z, 0), g.nz - 1);
+    c.x = c.x < 0 ? 0 : (c.x > g.nx - 1 ? g.nx - 1 : c.x);
+    c.y = c.y < 0 ? 0 : (c.y > g.ny - 1 ? g.ny - 1 : c.y);
+    c.z = c.z < 0 ? 0 : (c.z > g.nz - 1 ? g.nz - 1 : c.z);
     return key_of(c, g);
 }
 // The 27-cell stencil with the reference's index clamping

@@ -76,6 +76,19 @@ struct SphDev {
     int* cntF;
     int* nbD;
     int* cntD;
+    // Skin lists: rows of every candidate within the cutoff plus a skin at
+    // the last rebuild, rebuilt only when some particle has drifted half the
+    // skin; the first momentum pass of each step evaluates them with the
+    // exact cutoff test and writes the pairs it kept into nbF / nbD (the
+    // reference's per-step pair set) for the step's later passes.
+    float skin;        // added to the cutoff by the list build (0: exact lists)
+    const int* gate;   // device word: nonzero when this step rebuilds
+    int* nbV;
+    int* cntV;
+    int* nbVD;
+    int* cntVD;
+    const double4* xb;  // positions at the last rebuild
+    unsigned* maxd2;    // largest squared drifts since the rebuild (float bits)
     // Moving boundary particles ("markers") that sample the DEM balls coupled
     // to the fluid, in this step's cell order, with the dummies' record
     // layout; mid maps a slot to the marker's index in body order, where
@@ -224,6 +237,68 @@ __global__ void k_sph_place(int n, int start, double3 off, const double4* __rest
     extra2[start + t] = extra[t];
     if (zero2) zero2[start + t] = 0.0;
 }
+// Skin-list rebuild of a step: copies the records the gated permute wrote
+// into the scratch halves of the ping-pong pairs back into the current
+// halves (so the host's buffer indices do not depend on the device's
+// decision) and records the rebuild positions.
+__global__ void k_sph_copy_back(int n, const int* __restrict__ gate, const double4* __restrict__ pos2,
+                                const double4* __restrict__ vel2, const double4* __restrict__ st2,
+                                const double* __restrict__ rho02, const double* __restrict__ drho2,
+                                const int* __restrict__ id2, const float4* __restrict__ velf2,
+                                const float4* __restrict__ stf2, const int4* __restrict__ posq2,
+                                double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ st,
+                                double* __restrict__ rho0, double* __restrict__ drho, int* __restrict__ id,
+                                float4* __restrict__ velf, float4* __restrict__ stf, int4* __restrict__ posq,
+                                double4* __restrict__ xb) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || *gate == 0) return;
+    const double4 p = pos2[t];
+    pos[t] = p;
+    xb[t] = p;
+    vel[t] = vel2[t];
+    st[t] = st2[t];
+    rho0[t] = rho02[t];
+    drho[t] = drho2[t];
+    id[t] = id2[t];
+    velf[t] = velf2[t];
+    stf[t] = stf2[t];
+    posq[t] = posq2[t];
+}
+
+// Skin-list state of a scene, on the device.
+constexpr int kSkinSlots = 256;
+struct SkinState {
+    int rebuild;                 // this step rebuilds (read by the gated kernels)
+    int force;                   // set by the host after any change of the particle state
+    int rebuilds;                // rebuilds so far (statistics)
+    int pad;
+    unsigned maxd2[kSkinSlots];  // largest squared drifts since the rebuild, as float bits
+};
+// Start of a step (one block of kSkinSlots threads): rebuild when forced or
+// when some particle has drifted more than half the skin since the last
+// rebuild (then no pair within the cutoff now was beyond cutoff + skin at
+// the rebuild).
+__global__ void __launch_bounds__(kSkinSlots) k_sph_skin_decide(SkinState* st, float half2) {
+    __shared__ unsigned m[kSkinSlots];
+    const int t = threadIdx.x;
+    m[t] = st->maxd2[t];
+    __syncthreads();
+    for (int h = kSkinSlots / 2; h > 0; h >>= 1) {
+        if (t < h) m[t] = max(m[t], m[t + h]);
+        __syncthreads();
+    }
+    const bool r = st->force != 0 || m[0] > __float_as_uint(half2);  // unsigned: a NaN drift rebuilds
+    __syncthreads();
+    if (r) st->maxd2[t] = 0u;
+    if (t == 0) {
+        st->rebuild = r ? 1 : 0;
+        if (r) {
+            st->force = 0;
+            st->rebuilds++;
+        }
+    }
+}
+
 // World position of marker k (body order): its ball's centre plus the
 // marker's offset, with h in w.
 __global__ void k_sph_marker_place(int nm, const int* __restrict__ mb, const double4* __restrict__ moff,
@@ -328,9 +403,10 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
                               const int* __restrict__ id, double4* __restrict__ pos2, double4* __restrict__ vel2,
                               double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
                               int* __restrict__ id2, float4* __restrict__ posf, float4* __restrict__ velf2,
-                              float4* __restrict__ stf2, int4* __restrict__ posq2, double3 origin, double invq) {
+                              float4* __restrict__ stf2, int4* __restrict__ posq2, double3 origin, double invq,
+                              const int* __restrict__ gate) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    if (t >= n || (gate && *gate == 0)) return;
     int o = sorted[t];
     double4 p = pos[o];
     pos2[t] = p;
@@ -399,10 +475,10 @@ struct ListStage {
 // One own particle against one staged batch: hit / band flags for this lane.
 template <bool kUniformH>
 __device__ __forceinline__ void list_test(const float4& pf, const float4& q, float loI, float hiI, float eps,
-                                          bool& in, bool& band) {
+                                          float skin, bool& in, bool& band) {
     float lo = loI, hi = hiI;
     if (!kUniformH && q.w > pf.w) {
-        const float cut = 2.0f * q.w, c2 = cut * cut, bd = list_band(cut, eps);
+        const float cut = 2.0f * q.w + skin, c2 = cut * cut, bd = list_band(cut, eps);
         lo = c2 - bd;
         hi = c2 + bd;
     }
@@ -426,7 +502,7 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
                                            const float4* __restrict__ ownf, const double4* __restrict__ other,
                                            const float4* __restrict__ otherf, float eps, bool same, int K, int N,
                                            int* __restrict__ nb, int* __restrict__ cnt, int* needMax, int* overflow,
-                                           const ListStage<kUniformH>& sg) {
+                                           const ListStage<kUniformH>& sg, float skin = 0.0f) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int total = 0;
@@ -453,7 +529,7 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
             const int i1 = min(i0 + 1, pe - 1);
             const bool two = i0 + 1 < pe;
             const float4 pa = ownf[i0], pb = ownf[i1];
-            const float cA = 2.0f * pa.w, cB = 2.0f * pb.w;
+            const float cA = 2.0f * pa.w + skin, cB = 2.0f * pb.w + skin;
             const float bA = list_band(cA, eps), bB = list_band(cB, eps);
             const float loA = cA * cA - bA, hiA = cA * cA + bA, loB = cB * cB - bB, hiB = cB * cB + bB;
             int na = ch == 0 ? 0 : cnt[i0];
@@ -463,8 +539,13 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
                 const float4 q = sg.pos[v];
                 const int j = sg.index(v, q);
                 bool inA, bandA, inB, bandB;
-                list_test<kUniformH>(pa, q, loA, hiA, eps, inA, bandA);
-                list_test<kUniformH>(pb, q, loB, hiB, eps, inB, bandB);
+                list_test<kUniformH>(pa, q, loA, hiA, eps, skin, inA, bandA);
+                list_test<kUniformH>(pb, q, loB, hiB, eps, skin, inB, bandB);
+                if (skin > 0.0f) {  // a skin row only has to hold every pair within the cutoff
+                    inA = inA || bandA;
+                    inB = inB || bandB;
+                    bandA = bandB = false;
+                }
                 if (same) {
                     if (j == i0) inA = bandA = false;
                     if (j == i1) inB = bandB = false;
@@ -513,7 +594,7 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
     const int w = threadIdx.x >> 5;
     const int cell = blockIdx.x * kListWarps + w;
-    if (cell >= ncell) return;
+    if (cell >= ncell || (d.gate && *d.gate == 0)) return;
     const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
     if (ps == pe) return;
     ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
@@ -521,10 +602,10 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     const double4 p0 = d.pos[ps];
     Stencil st = stencil_of(xyz(p0), d.g);
     cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N,
-                                  d.nbF, d.cntF, &d.status->need_pairs, &d.status->overflow, sg);
+                                  d.nbF, d.cntF, &d.status->need_pairs, &d.status->overflow, sg, d.skin);
     if (d.ND > 0)
         cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false, d.KD, d.N,
-                              d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg);
+                              d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg, d.skin);
     else
         for (int i = ps + (threadIdx.x & 31); i < pe; i += 32) d.cntD[i] = 0;
     if (kMarkers)
@@ -559,6 +640,16 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
 // against `other`.  With pi and `other` the positions the lists were built
 // from this yields the list's pair set; the fluid passes after the step's
 // drift pass the drifted positions (see k_sph_accel).
+// A row's count word: a count c >= 0 of a dense row (lane `sub` of the quad
+// takes entries sub, sub + 4, ... below c), or, with kLaneRows set, four lane
+// counts of 7 bits (lane `sub` takes entries sub, sub + 4, ... of its own
+// count: the rows the first pass on skin lists writes), or -1 (overflowed).
+constexpr int kLaneRows = 1 << 30;
+__host__ __device__ __forceinline__ int lane_count(int cnt, int sub) {
+    if (cnt >= kLaneRows) return (cnt >> (7 * sub)) & 127;
+    return cnt > sub ? (cnt - sub + 3) >> 2 : 0;
+}
+
 template <class F>
 __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ nb, int K, int i, int self,
                                                const double4 pi, const GridDesc& g,
@@ -569,14 +660,15 @@ __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ 
         // two neighbours per iteration, their row entries loaded one
         // iteration ahead so the index load is off the gather's critical path
         const int* __restrict__ row = nb + (size_t)i * K;
+        const int kend = sub + kQuad * lane_count(cnt, sub);
         int k = sub;
-        int j0 = k < cnt ? __ldg(row + k) : -1;
-        int j1 = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
-        for (; k < cnt; k += 2 * kQuad) {
+        int j0 = k < kend ? __ldg(row + k) : -1;
+        int j1 = k + kQuad < kend ? __ldg(row + k + kQuad) : -1;
+        for (; k < kend; k += 2 * kQuad) {
             const int a = j0, b = j1;
             const int kn = k + 2 * kQuad;
-            j0 = kn < cnt ? __ldg(row + kn) : -1;
-            j1 = kn + kQuad < cnt ? __ldg(row + kn + kQuad) : -1;
+            j0 = kn < kend ? __ldg(row + kn) : -1;
+            j1 = kn + kQuad < kend ? __ldg(row + kn + kQuad) : -1;
             f(a);
             if (b >= 0) f(b);
         }
@@ -684,12 +776,11 @@ __device__ __forceinline__ FluidOwn<R> fluid_own(const SphDev& d, int i, const d
 // mirrored normal velocity and the hydrostatically extrapolated pressure
 // PR = PL + rho_i max(0, -g . r_ij), rho_j = PR / c_j^2 + rho0_j.
 template <class R>
-__device__ __forceinline__ void boundary_acc(const SphDev& d, const FluidOwn<R>& o, const BView& bv, int j,
-                                             const V<R>& g, V<R>& acc) {
+__device__ __forceinline__ void boundary_acc_r(const SphDev& d, const FluidOwn<R>& o, const BView& bv, int j,
+                                               const V<R>& rij, R hj, const V<R>& g, V<R>& acc) {
     using VR = V<R>;
-    VR rij, nw, vj;
-    R hj, cj, nuj, rho0j, mj;
-    pair_r<R>(o.op, bv.pos, bv.posq, d.q, j, rij, hj);
+    VR nw, vj;
+    R cj, nuj, rho0j, mj;
     load_dummy<R>(bv, j, nw, vj, mj, cj, nuj, rho0j);
     R UL = dot(-nw, o.vi);
     R UR = -UL + (R)2.0 * dot(-nw, vj);
@@ -708,6 +799,118 @@ __device__ __forceinline__ void boundary_acc(const SphDev& d, const FluidOwn<R>&
     acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
     R nuij = (R)0.5 * (o.nui + nuj);
     acc += (R)2.0 * nuij * dot(rij * inv_r, dW) * (o.vi - vj) * mj * inv_rr;
+}
+template <class R>
+__device__ __forceinline__ void boundary_acc(const SphDev& d, const FluidOwn<R>& o, const BView& bv, int j,
+                                             const V<R>& g, V<R>& acc) {
+    V<R> rij;
+    R hj;
+    pair_r<R>(o.op, bv.pos, bv.posq, d.q, j, rij, hj);
+    boundary_acc_r<R>(d, o, bv, j, rij, hj, g, acc);
+}
+
+// Fluid-fluid term of updateWCSPHAccelerationKernel
+// (WCSPHIntegrationKernel.cu:70-109) given r_ij and h_j, accumulated into acc.
+template <class R>
+__device__ __forceinline__ void fluid_acc_r(const SphDev& d, const FluidOwn<R>& o, int j, const V<R>& rij, R hj,
+                                            V<R>& acc) {
+    using VR = V<R>;
+    VR vj;
+    R rhoj, PR, cj, nuj, mj;
+    load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
+    R r2 = dot(rij, rij);
+    // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
+    // reference's normalize does (myVec.h:112-128)
+    R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
+    R r = r2 * inv_r;
+    VR e = rij * (-inv_r);
+    R UL = dot(o.vi, e), UR = dot(vj, e);
+    VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
+    R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
+    R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
+    R Ps = (R)0.5 * (o.PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
+    R inv_rr = div_r((R)1.0, o.rhoi * rhoj);
+    acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
+    R nuij = (R)0.5 * (o.nui + nuj);
+    // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
+    acc += (R)2.0 * nuij * dot(-e, dW) * (o.vi - vj) * mj * inv_rr;
+}
+template <class R>
+__device__ __forceinline__ void fluid_acc(const SphDev& d, const FluidOwn<R>& o, int j, V<R>& acc) {
+    V<R> rij;
+    R hj;
+    pair_r<R>(o.op, d.pos, d.posq, d.q, j, rij, hj);
+    fluid_acc_r<R>(d, o, j, rij, hj, acc);
+}
+
+// The reference list's cutoff test (countSPHInteractionsKernel,
+// SPHNeighborSearchKernel.cu:6-60): (cut^2 - |r|^2) >= 0, cut = 2 max(h_i, h_j),
+// on the FP64 positions, given the pass's r_ij and h_j.  In FP64 that r_ij is
+// the reference's.  The mixed passes test the FP32 square of the fixed-point
+// difference (the pair term's own |r|^2) and take the FP64 test only in a
+// band of 2e-6 cut^2 around the cutoff, which covers that square's rounding
+// (< 5e-7 relative) and the positions' quantisation (< 3e-8 relative).
+template <class R>
+__device__ __forceinline__ bool cutoff_r(const V<R>& rij, R hj, const double4& pi, const double4* __restrict__ other,
+                                         int j) {
+    if constexpr (std::is_same<R, float>::value) {
+        const float d2 = dot(rij, rij);
+        const float cut = 2.0f * fmaxf((float)pi.w, hj);
+        const float c2 = cut * cut, band = 2.0e-6f * c2;
+        if (d2 < c2 - band) return true;
+        if (d2 > c2 + band) return false;
+        const double4 pj = other[j];
+        const double cd = 2.0 * fmax(pi.w, pj.w);
+        const double3 r = xyz(pi) - xyz(pj);
+        return (cd * cd - dot(r, r)) >= 0.;
+    } else {
+        const double cd = 2.0 * fmax(pi.w, hj);
+        return (cd * cd - dot(rij, rij)) >= 0.;
+    }
+}
+
+// One skin row of particle i in the first pass of a step: fn(j) tests the
+// exact cutoff, adds the pair's term when it holds, and returns the test.
+// Each lane of the quad takes entries sub, sub + 4, ... of the skin row and
+// writes the ones it keeps to sub, sub + 4, ... of the exact row nbOut (in
+// place of its own candidates, so never past them); cntOut gets the four
+// lane counts (kLaneRows), which the step's later passes read.  A skin row
+// that overflowed its capacity (cnt < 0) is replaced by the cell-stencil
+// walk, and the exact row is marked overflowed (-1: the later passes walk as
+// well); so is a row with more than 127 pairs in one lane.
+template <class F>
+__device__ __forceinline__ void skin_loop(int cnt, const int* __restrict__ nbV, int K, int i, int* __restrict__ nbOut,
+                                          int* __restrict__ cntOut, const double4& pi, const GridDesc& g,
+                                          const int* __restrict__ cellStart, const double4* __restrict__ other,
+                                          int self, F&& fn) {
+    const int sub = threadIdx.x & 3;
+    if (cnt < 0) {
+        if (sub == 0) cntOut[i] = -1;
+        Stencil st = stencil_of(xyz(pi), g);
+        for_stencil_rows(st, g, cellStart, [&](int b, int e) {
+            for (int j = b + sub; j < e; j += kQuad)
+                if (j != self) fn(j);
+        });
+        return;
+    }
+    const int* __restrict__ row = nbV + (size_t)i * K;
+    int* __restrict__ out = nbOut + (size_t)i * K;
+    int w = 0;  // pairs this lane kept
+    int k = sub;
+    int j0 = k < cnt ? __ldg(row + k) : -1;
+    int j1 = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
+    for (; k < cnt; k += 2 * kQuad) {
+        const int a = j0, b = j1;
+        const int kn = k + 2 * kQuad;
+        j0 = kn < cnt ? __ldg(row + kn) : -1;
+        j1 = kn + kQuad < cnt ? __ldg(row + kn + kQuad) : -1;
+        if (fn(a)) out[sub + kQuad * w++] = a;
+        if (b >= 0 && fn(b)) out[sub + kQuad * w++] = b;
+    }
+    const unsigned gm = quad_mask();
+    const int over = quad_sum(w > 127 ? 1 : 0, gm);
+    const int packed = quad_sum(w << (7 * sub), gm);
+    if (sub == 0) cntOut[i] = over ? -1 : (kLaneRows | packed);
 }
 
 // Fluid-boundary term of updateWCSPHDensityChangeKernel
@@ -742,7 +945,12 @@ constexpr int kAccelBlocks = std::is_same<R, float>::value ? 6 : 4;
 template <class R>
 constexpr int kDensityBlocks = std::is_same<R, float>::value ? 8 : 5;
 
-template <class R, bool kMarkers>
+// kSkin: the first pass of a step on skin lists (first = 1).  The quad walks
+// the particle's skin rows, keeps the pairs within the exact cutoff (their
+// terms are the pass's sum, and they are written as this step's exact rows
+// for the continuity and second momentum passes), and the pass records the
+// particle's drift from its rebuild position.
+template <class R, bool kMarkers, bool kSkin = false>
 __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
@@ -754,33 +962,35 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
     const double4 vi4 = d.vel[i];
     const FluidOwn<R> o = fluid_own<R>(d, i, pi4, vi4, d.st[i]);
     VR acc = v3r<R>(0, 0, 0);
-    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-        VR rij, vj;
-        R hj, rhoj, PR, cj, nuj, mj;
-        pair_r<R>(o.op, d.pos, d.posq, d.q, j, rij, hj);
-        load_fluid<R>(d, j, vj, mj, rhoj, PR, cj, nuj);
-        R r2 = dot(rij, rij);
-        // -normalize(r_ij) and |r_ij| from one reciprocal square root, as the
-        // reference's normalize does (myVec.h:112-128)
-        R inv_r = r2 < (R)1.0e-20 ? (R)0 : rsqrt_r(r2);
-        R r = r2 * inv_r;
-        VR e = rij * (-inv_r);
-        R UL = dot(o.vi, e), UR = dot(vj, e);
-        VR dW = gradw_fast<R>(r, inv_r, o.hk, hj) * rij;
-        R cbar = (R)0.5 * (o.ci + cj), rbar = (R)0.5 * (o.rhoi + rhoj);
-        R beta = fmin((R)3.0 * fmax(UL - UR, (R)0.0), cbar);
-        R Ps = (R)0.5 * (o.PL + PR) + (R)0.5 * beta * rbar * (UL - UR);
-        R inv_rr = div_r((R)1.0, o.rhoi * rhoj);
-        acc -= (R)2.0 * mj * (Ps * inv_rr) * dW;
-        R nuij = (R)0.5 * (o.nui + nuj);
-        // Q5: r_hat . gradW without 1/r, as the reference (WCSPHIntegrationKernel.cu:108)
-        acc += (R)2.0 * nuij * dot(-e, dW) * (o.vi - vj) * mj * inv_rr;
-    });
     const VR g = cvt<R>(d.gravity);
-    if (d.ND > 0) {
-        const BView dv = dummy_view(d);
-        quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos,
-                       [&](int j) { boundary_acc<R>(d, o, dv, j, g, acc); });
+    if constexpr (kSkin) {
+        skin_loop(d.cntV[i], d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
+            VR rij;
+            R hj;
+            pair_r<R>(o.op, d.pos, d.posq, d.q, j, rij, hj);
+            if (!cutoff_r<R>(rij, hj, pi4, d.pos, j)) return false;
+            fluid_acc_r<R>(d, o, j, rij, hj, acc);
+            return true;
+        });
+        if (d.ND > 0) {
+            const BView dv = dummy_view(d);
+            skin_loop(d.cntVD[i], d.nbVD, d.KD, i, d.nbD, d.cntD, pi4, d.g, d.dStart, d.dpos, -1, [&](int j) {
+                VR rij;
+                R hj;
+                pair_r<R>(o.op, d.dpos, d.dposq, d.q, j, rij, hj);
+                if (!cutoff_r<R>(rij, hj, pi4, d.dpos, j)) return false;
+                boundary_acc_r<R>(d, o, dv, j, rij, hj, g, acc);
+                return true;
+            });
+        }
+    } else {
+        quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos,
+                       [&](int j) { fluid_acc<R>(d, o, j, acc); });
+        if (d.ND > 0) {
+            const BView dv = dummy_view(d);
+            quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos,
+                           [&](int j) { boundary_acc<R>(d, o, dv, j, g, acc); });
+        }
     }
     double3 a = up(acc);
     a.x = quad_sum(a.x, gm);
@@ -798,6 +1008,12 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
         const double4 pn = d4(ri + dt * v, pi4.w);
         d.posOut[i] = pn;
         d.posqOut[i] = fixq(pn, d.g.mn, d.invq);
+        if constexpr (kSkin) {
+            // drift since the rebuild, into one of kSkinSlots maxima (spread so
+            // that the atomics of different blocks do not queue on one address)
+            const double3 dd = xyz(pn) - xyz(d.xb[i]);
+            atomicMax(d.maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
+        }
     }
 }
 
@@ -1080,6 +1296,25 @@ struct SphScene {
     DBuf<DevStatus> status;
     bool haveLists = false;
 
+    // Skin lists (fluid scenes without markers): rows hold every candidate
+    // within cutoff + skin at the last rebuild; a step rebuilds them (cell
+    // sort, reorder, list build, all gated on the device) only when some
+    // particle has drifted half the skin, and its first momentum pass keeps
+    // the pairs within the exact cutoff.  The grid's cells are
+    // 2 h_max (1 + skinMax) wide so that the 27-cell stencil covers the skin.
+    float skinMax = 0.05f;   // fraction of 2 h_max the grid allows (fixed at initialisation)
+    float skinFrac = 0.05f;  // fraction in use (0: exact lists every step)
+    double hmaxGrid = 0;
+    DBuf<int> nbV, cntV, nbVD, cntVD;
+    DBuf<double4> xb;
+    DBuf<SkinState> skinState;
+    bool skin_on() const { return skinFrac > 0 && nM == 0; }
+    float skin_abs() const { return (float)(2.0 * hmaxGrid * skinFrac); }
+    // The next step rebuilds the skin lists (after any host-side change).
+    void skin_force() {
+        if (skinState.p) DEMSPH_CUDA(cudaMemsetAsync(&skinState.p->force, 1, 1, s));
+    }
+
     int nF = 0, nD = 0;  // fluid / dummy counts (the host sets before initialisation)
     int N() const { return nF; }
     int ND() const { return nD; }
@@ -1134,6 +1369,9 @@ struct SphScene {
         d.mid = mid.p; d.nbM = nbM.p; d.cntM = cntM.p; d.mforce = mforce.p;
         d.KR = KR; d.nbR = nbR.p; d.cntR = cntR.p;
         d.macc = macc.p; d.mdrho = mdrho.p;
+        d.skin = 0.0f; d.gate = nullptr;
+        d.nbV = nbV.p; d.cntV = cntV.p; d.nbVD = nbVD.p; d.cntVD = cntVD.p;
+        d.xb = xb.p; d.maxd2 = skinState.p ? skinState.p->maxd2 : nullptr;
         return d;
     }
 
@@ -1149,6 +1387,15 @@ struct SphScene {
             cntM.alloc(n, s, true);
             nbR.alloc((size_t)nM * KR, s, false);
             cntR.alloc(nM, s, true);
+        }
+        if (skinMax > 0) {
+            nbV.alloc(n * KF, s, false);
+            cntV.alloc(n, s, true);
+            nbVD.alloc(n * std::max(KD, 1), s, false);
+            cntVD.alloc(n, s, true);
+            if (xb.n < n) xb.alloc(n, s, true);
+            if (!skinState.p) skinState.alloc(1, s, true);
+            skin_force();
         }
     }
 
@@ -1184,14 +1431,22 @@ struct SphScene {
         }
     }
     // Moves the fluid records (and their FP32 shadows) into this step's cell order.
-    void permute() {
+    void permute(const int* gate = nullptr) {
         const int n = N();
         k_sph_permute<<<grid_for(n, 256), 256, 0, s>>>(n, fCells.sorted.p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p,
                                                        drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
                                                        rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p,
                                                        velf[Vv ^ 1].p, stf[S ^ 1].p, posq[P ^ 1].p, fCells.g.mn,
-                                                       invq);
-        P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+                                                       invq, gate);
+        if (gate) {  // a device-side decision: copy back instead of flipping the indices
+            k_sph_copy_back<<<grid_for(n, 256), 256, 0, s>>>(
+                n, gate, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p, rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p,
+                velf[Vv ^ 1].p, stf[S ^ 1].p, posq[P ^ 1].p, pos[P].p, vel[Vv].p, st[S].p, rho0[R0].p, drho[D].p,
+                id[ID].p, velf[Vv].p, stf[S].p, posq[P].p, xb.p);
+            g_launches += 1;
+        } else {
+            P ^= 1; Vv ^= 1; S ^= 1; R0 ^= 1; D ^= 1; ID ^= 1;
+        }
         L = P;
     }
     // Rewrites the fluid shadows after a host-side change of the records.
@@ -1201,6 +1456,7 @@ struct SphScene {
         k_sph_fix<<<grid_for(n, 256), 256, 0, s>>>(n, pos[P].p, fCells.g.mn, invq, posq[P].p);
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
+        skin_force();
     }
     // Markers from the coupled balls' current state, in cell order.
     void place_markers() {
@@ -1223,6 +1479,45 @@ struct SphScene {
         g_launches += 2;
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
+        skin_force();  // the particles moved in memory: the skin rows are stale
+    }
+    // The step's rebuild of the skin lists, gated on the device's decision.
+    void skin_rebuild() {
+        const int n = N();
+        k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
+        const int* gate = &skinState.p->rebuild;
+        fCells.build(pos[P].p, n, s, id[ID].p, false, gate);
+        g_launches += 1 + fCells.launches;
+        permute(gate);
+        launch_lists(skin_view(gate));
+        g_launches += 2;
+        DEMSPH_LAUNCH_CHECK();
+        haveLists = true;
+    }
+    // The device view the skin-list build writes through.
+    SphDev skin_view(const int* gate) {
+        SphDev d = dev();
+        d.skin = skin_abs();
+        d.gate = gate;
+        d.nbF = nbV.p; d.cntF = cntV.p; d.nbD = nbVD.p; d.cntD = cntVD.p;
+        return d;
+    }
+    // The first momentum pass of a step on the skin lists.
+    void accel_skin() {
+        SphDev d = dev();
+        d.posOut = pos[P ^ 1].p;
+        d.velOut = vel[Vv ^ 1].p;
+        d.velfOut = velf[Vv ^ 1].p;
+        d.posqOut = posq[P ^ 1].p;
+        const unsigned grid = grid_for(N(), kSphPerBlock);
+        if (precision == DEMSPH_PRECISION_FP64)
+            k_sph_accel<double, false, true><<<grid, kSphBlock, 0, s>>>(d, 0.5 * dt, dt, 1);
+        else
+            k_sph_accel<float, false, true><<<grid, kSphBlock, 0, s>>>(d, 0.5 * dt, dt, 1);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        P ^= 1;
+        Vv ^= 1;
     }
     // The momentum pass (k_sph_accel) on the state d reads, preceded, when
     // there are markers, by their terms (k_sph_marker_pass) and, inside a
@@ -1284,8 +1579,13 @@ struct SphScene {
     }
     // One pass of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621).
     void step_body() {
-        neighbor_search();
-        accel(1);
+        if (skin_on()) {
+            skin_rebuild();
+            accel_skin();
+        } else {
+            neighbor_search();
+            accel(1);
+        }
         density();
         accel(0);
     }
@@ -1309,16 +1609,31 @@ struct SphScene {
         time += dt;
         const int n = N();
         DEMSPH_CUDA(cudaEventRecord(ev[0], s));
-        fCells.build(pos[P].p, n, s, id[ID].p);
-        g_launches += fCells.launches;
-        DEMSPH_CUDA(cudaEventRecord(ev[1], s));
-        permute();
-        SphDev d = dev();
-        launch_lists(d);
-        g_launches += 2;
-        haveLists = true;
-        DEMSPH_CUDA(cudaEventRecord(ev[2], s));
-        accel(1);
+        if (skin_on()) {
+            // 0 decision + gated cell sort, 1 gated reorder + skin lists, 2 first pass on the skin rows
+            k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
+            const int* gate = &skinState.p->rebuild;
+            fCells.build(pos[P].p, n, s, id[ID].p, false, gate);
+            g_launches += 1 + fCells.launches;
+            DEMSPH_CUDA(cudaEventRecord(ev[1], s));
+            permute(gate);
+            launch_lists(skin_view(gate));
+            g_launches += 2;
+            haveLists = true;
+            DEMSPH_CUDA(cudaEventRecord(ev[2], s));
+            accel_skin();
+        } else {
+            fCells.build(pos[P].p, n, s, id[ID].p);
+            g_launches += fCells.launches;
+            DEMSPH_CUDA(cudaEventRecord(ev[1], s));
+            permute();
+            SphDev d = dev();
+            launch_lists(d);
+            g_launches += 2;
+            haveLists = true;
+            DEMSPH_CUDA(cudaEventRecord(ev[2], s));
+            accel(1);
+        }
         DEMSPH_CUDA(cudaEventRecord(ev[3], s));
         density();
         DEMSPH_CUDA(cudaEventRecord(ev[4], s));
@@ -1377,6 +1692,7 @@ struct SphScene {
         for (size_t k = 0; k < sn.bufs.size(); k++)
             DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
         iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID; L = sn.L;
+        skin_force();
     }
     // Steps without a state snapshot: a list row that overflows its capacity
     // is walked from the cell table by the passes (same neighbours), so an
@@ -1603,7 +1919,8 @@ struct SphScene {
         gravity = g;
         dt = timeStep;
         uniformH = uni;
-        const double cell = 2.0 * hmax;
+        hmaxGrid = hmax;
+        const double cell = 2.0 * hmax * (1.0 + skinMax);
         GridDesc gd{};
         if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
         status.alloc(1, s, true);
@@ -1678,6 +1995,7 @@ struct SphScene {
         for (int attempt = 0; attempt < 8; attempt++) {
             clear_status();
             neighbor_search();
+            if (skinMax > 0 && skinFrac > 0) launch_lists(skin_view(nullptr));  // the skin rows are longer
             DevStatus st2 = read_status();
             if (!st2.overflow) break;
             grow(st2);
@@ -2001,6 +2319,35 @@ int demsph_sph_set_graphs(demsph_sph_t h, int enable) {
         h->sc.graph.reset();
     });
 }
+int demsph_sph_set_skin(demsph_sph_t h, double fraction) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!(fraction >= 0) || fraction > 1.0) throw Status(DEMSPH_ERR_INVALID, "skin fraction must be in [0, 1]");
+        if (s.ready && fraction > s.skinMax)
+            throw Status(DEMSPH_ERR_INVALID, "skin above the one the grid was built for");
+        if (!s.ready) s.skinMax = (float)fraction;
+        s.skinFrac = (float)fraction;
+        s.graph.reset();  // the captured launches carry the skin
+        s.skin_force();
+    });
+}
+int demsph_sph_skin_stats(demsph_sph_t h, double* fraction, long* rebuilds) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (fraction) *fraction = s.skin_on() ? s.skinFrac : 0.0;
+        if (rebuilds) {
+            *rebuilds = 0;
+            if (s.skinState.p) {
+                SkinState st{};
+                DEMSPH_CUDA(cudaMemcpyAsync(&st, s.skinState.p, sizeof st, cudaMemcpyDeviceToHost, s.s));
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+                *rebuilds = st.rebuilds;
+            }
+        }
+    });
+}
 int demsph_sph_set_list_shape(demsph_sph_t h, int shape) {
     return guarded([&] {
         SPH_CHECK(h);
@@ -2227,7 +2574,9 @@ int demsph_sph_num_pairs(demsph_sph_t h, int which, long* n) {
         long t = 0;
         for (int c : cnt) {
             if (c < 0) throw Status(DEMSPH_ERR_OVERFLOW, "a list row overflowed; call neighborSearch to rebuild");
-            t += c;
+            if (which == 2) t += c;
+            else
+                for (int sub = 0; sub < kQuad; sub++) t += lane_count(c, sub);
         }
         *n = t;
     });
@@ -2252,19 +2601,41 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
         }
         std::vector<int> didv;
         s.did.download(didv, s.s);
+        // the neighbours' positions when the lists were built
+        std::vector<double4> colPos;
+        if (which == 0) s.pos[s.L].download(colPos, s.s);
+        else s.dpos.download(colPos, s.s);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         const std::vector<int>& col = (which == 0) ? rowId : didv;
+        // The reference's row order: its stencil visits cells in ascending key
+        // on a grid of 2 h_max cells, each cell in ascending original index.
+        // This library's cells are wider (they cover the skin of the skin
+        // lists), so each row is put into that order here.
+        GridDesc gref{};
+        grid_set(gref, s.fCells.g.mn, s.fCells.g.mx, 2.0 * s.hmaxGrid);
+        std::vector<long long> colKey(colPos.size());
+        for (size_t j = 0; j < colPos.size(); j++)
+            colKey[j] = (long long)clamped_key(xyz(colPos[j]), gref) * (1LL << 31) + col[j];
         // rows emitted in the caller's original order
         std::vector<int> rowOf(rows);
         for (int t = 0; t < rows; t++) rowOf[rowId[t]] = t;
         for (int c : cnt)
             if (c < 0) throw Status(DEMSPH_ERR_OVERFLOW, "a list row overflowed; call neighborSearch to rebuild");
         long w = 0;
+        std::vector<int> slots;
         for (int o = 0; o < rows; o++) {
             int t = rowOf[o];
-            for (int k = 0; k < cnt[t]; k++) {
+            slots.clear();
+            if (which == 2) {
+                for (int k = 0; k < cnt[t]; k++) slots.push_back(nb[(size_t)k * rows + t]);
+            } else {
+                for (int sub = 0; sub < kQuad; sub++)
+                    for (int m = 0; m < lane_count(cnt[t], sub); m++) slots.push_back(nb[(size_t)t * K + sub + kQuad * m]);
+            }
+            std::sort(slots.begin(), slots.end(), [&](int x, int y) { return colKey[x] < colKey[y]; });
+            for (int j : slots) {
                 a[w] = o;
-                b[w] = col[nb[which == 2 ? (size_t)k * rows + t : (size_t)t * K + k]];
+                b[w] = col[j];
                 w++;
             }
         }

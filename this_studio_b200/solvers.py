@@ -535,6 +535,17 @@ class WCSPHSolver:
         call("demsph_sph_tune", self._h, int(trials), C.byref(ch), _dp(ms))
         return ch.value, ms
 
+    def setSkin(self, fraction):
+        """Skin of the neighbour rows as a fraction of 2 h_max (0: exact lists
+        rebuilt every step); before initialize() it also sizes the grid."""
+        call("demsph_sph_set_skin", self._h, float(fraction))
+
+    def skinStats(self):
+        """(fraction in use, rebuilds so far)."""
+        f, r = C.c_double(), C.c_long()
+        call("demsph_sph_skin_stats", self._h, C.byref(f), C.byref(r))
+        return f.value, r.value
+
     def setListShape(self, shape):
         call("demsph_sph_set_list_shape", self._h, int(shape))
 
