@@ -226,9 +226,11 @@ def served_stream(torch, num, seed=5, rate=30.0, steps=500, chunk=100):
     n_max = 200_000
     c0, dt = serve.stream_params(n_max)
     mk = lambda: serve.make_stream(num, seed=seed, n_min=1000, n_max=n_max, rate=rate, steps=steps)
-    # warm-up: module loads and memory pools
-    serve.SceneServer(hbm_budget=4e9, chunk=10, sph_c0=c0, sph_dt=dt).run(
-        serve.make_stream(4, seed=1, n_min=1000, n_max=4000, rate=1e4, steps=20))
+    # warm-up on a stream of the same sizes (another seed): kernel loads, graph
+    # executables and the memory pool grown to the stream's working set, as in
+    # a server that has been running
+    serve.SceneServer(hbm_budget=60e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt).run(
+        serve.make_stream(24, seed=1, n_min=1000, n_max=n_max, rate=1e3, steps=100))
     reqs = mk()
     ps = serve.particle_steps(reqs, c0, dt)
     srv = serve.SceneServer(hbm_budget=60e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt)
