@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--stress", type=int, default=1,
+                    help="1: also time the bonded beam + clumps and the coupled ice sheet (about 40 s more)")
     ap.add_argument("--stream", type=int, default=64,
                     help="scenes in the served-stream measurement (0: skip it)")
     return ap.parse_args()
@@ -214,6 +216,55 @@ def coupled_tank(torch, steps, warmup, flush):
             "balls": nb, "markers": nm, "dem_substeps": sc.dem_substeps, "precision": "mixed", "steps": steps}
 
 
+def beam_clumps(torch, steps):
+    """The bonded beam plus clumps stress scene: a 20 x 20 x 400 bonded beam of
+    r = 1 mm spheres (parallel bonds on the face contacts, one end clamped,
+    seeded tip load) beside 20,000 three-sphere clumps, dt = 1e-7, mixed
+    precision.  Particles counted: moving spheres and pebbles."""
+    from this_studio_b200 import scenes
+
+    sc = scenes.bonded_beam_clumps()
+    s = scenes.build_dem(sc, "mixed")
+    s.step(20)
+    n = int((~sc.fixed).sum()) + 3 * len(sc.clumps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    s.step(steps)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nb = int(s.getBondedInteraction()["isBonded"].size)
+    return {"workload": "bonded_beam_clumps_220k", "value": n / (ms / 1e3), "unit": METRIC, "ms_per_step": ms,
+            "moving_particles": n, "bonds": nb, "clumps": len(sc.clumps), "precision": "mixed", "steps": steps}
+
+
+def ice_sheet(torch, steps):
+    """The coupled ice-sheet stress scene: about 1M bonded r = 2 mm spheres
+    moving into a 20,000-triangle cylinder, floating on 2M WCSPH particles
+    (dx = 4 mm, 3M floor dummies), coupled particle by particle (one marker per
+    ball), one DEM step per fluid step, mixed precision.  Particles counted:
+    balls + fluid."""
+    from this_studio_b200 import scenes
+
+    sc = scenes.ice_sheet_on_water()
+    f, d, c = scenes.build_coupled(sc, "mixed")
+    c.step(10, sc.dem_substeps)
+    n = sc.dem.position.shape[0] + sc.sph.fluid.shape[0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    c.step(steps, sc.dem_substeps)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nm, nb = c.numMarkers()
+    return {"workload": "ice_sheet_coupled_3m", "value": n / (ms / 1e3), "unit": METRIC, "ms_per_step": ms,
+            "balls": int(sc.dem.position.shape[0]), "fluid_particles": int(sc.sph.fluid.shape[0]),
+            "dummy_particles": int(sc.sph.dummy.shape[0]), "markers": nm, "triangles": 20000,
+            "dem_substeps": sc.dem_substeps, "precision": "mixed", "steps": steps}
+
+
 def served_stream(torch, num, seed=5, rate=30.0, steps=500, chunk=100):
     """The serving / batching stream (seeded Poisson arrivals of DEM drops and
     WCSPH dam breaks, particle counts log-uniform over 1k-200k, polydisperse
@@ -324,6 +375,8 @@ def native(args, rank, world, dist):
     dem = dem_bounce(torch, min(args.steps, 200), args.warmup, flush)
     coupled = coupled_tank(torch, min(args.steps, 100), args.warmup, flush)
     del flush
+    beam = beam_clumps(torch, min(args.steps, 200)) if args.stress else None
+    ice = ice_sheet(torch, min(args.steps, 40)) if args.stress else None
     stream = served_stream(torch, args.stream) if (args.stream > 0 and rank == 0 and world == 1) else None
 
     line = {
@@ -339,6 +392,8 @@ def native(args, rank, world, dist):
         "value_" + other: other_value,
         "dem": dem,
         "coupled": coupled,
+        "beam_clumps": beam,
+        "ice_sheet": ice,
         "stream": stream,
         "gpu_launches": int(launches),
         "clocks": clk,

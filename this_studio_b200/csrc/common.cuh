@@ -224,9 +224,16 @@ __host__ __device__ __forceinline__ int clamped_key(double3 p, const GridDesc& g
 struct Stencil {
     int3 c, s, e;
 };
-__device__ __forceinline__ Stencil stencil_of(double3 p, const GridDesc& g) {
+__device__ __forceinline__ Stencil stencil_of_cell3(int3 c, const GridDesc& g);
+__device__ __forceinline__ Stencil stencil_of(double3 p, const GridDesc& g) { return stencil_of_cell3(cell_of(p, g), g); }
+// The stencil of cell `key` (the cell an object was sorted into, wherever it
+// has moved since).
+__device__ __forceinline__ Stencil stencil_of_cell(int key, const GridDesc& g) {
+    return stencil_of_cell3(make_int3(key % g.nx, (key / g.nx) % g.ny, key / (g.nx * g.ny)), g);
+}
+__device__ __forceinline__ Stencil stencil_of_cell3(int3 c, const GridDesc& g) {
     Stencil st;
-    st.c = cell_of(p, g);
+    st.c = c;
     st.s = make_int3(-1, -1, -1);
     st.e = make_int3(1, 1, 1);
     if (st.c.x <= 0) { st.c.x = 0; st.s.x = 0; }

@@ -70,6 +70,7 @@ struct SphDev {
     float q;
     double invq;
     const float4* posf;   // fluid (x, y, z) - grid min and h, FP32, this step's order
+    float4* posfOut;      // the same after the first pass's drift (skin lists with markers)
     const float4* dposf;  // dummies, same form
     float eps;            // bound on |float coordinate - exact coordinate|
     int* nbF;
@@ -348,34 +349,35 @@ __global__ void k_sph_marker_gather(int nm, const int* __restrict__ sorted, cons
 // Coupling force and torque of each coupled ball: the sum of its markers'
 // reactions (body order, markers [start[b], start[b+1])), and of offset x
 // reaction, written at the ball's index.
-// One block per ball: each thread sums a strided share of the markers, then
-// a fixed-order tree in shared memory (the same sums every run).
-constexpr int kBodyBlock = 128;
-__global__ void __launch_bounds__(kBodyBlock) k_sph_body_force(const int* __restrict__ start,
+// One warp per ball: each lane sums a strided share of the ball's markers,
+// then a fixed butterfly over the warp (the same sums every run).
+constexpr int kBodyBlock = 256;
+__global__ void __launch_bounds__(kBodyBlock) k_sph_body_force(int nb, const int* __restrict__ start,
                                                                const int* __restrict__ ball,
                                                                const double4* __restrict__ mforce,
                                                                const double4* __restrict__ moff,
                                                                double4* __restrict__ force,
                                                                double4* __restrict__ torque) {
-    __shared__ double sh[6][kBodyBlock];
-    const int b = blockIdx.x, tid = threadIdx.x;
+    const int b = blockIdx.x * (kBodyBlock / 32) + (threadIdx.x >> 5);
+    if (b >= nb) return;  // whole warps
+    const int lane = threadIdx.x & 31;
     double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
-    for (int k = start[b] + tid; k < start[b + 1]; k += kBodyBlock) {
+    for (int k = start[b] + lane; k < start[b + 1]; k += 32) {
         const double3 f = xyz(mforce[k]);
         F += f;
         T += cross(xyz(moff[k]), f);
     }
-    sh[0][tid] = F.x; sh[1][tid] = F.y; sh[2][tid] = F.z;
-    sh[3][tid] = T.x; sh[4][tid] = T.y; sh[5][tid] = T.z;
-    __syncthreads();
-    for (int h = kBodyBlock / 2; h > 0; h >>= 1) {
-        if (tid < h)
-            for (int c = 0; c < 6; c++) sh[c][tid] += sh[c][tid + h];
-        __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) {
+        F.x += __shfl_xor_sync(0xffffffffu, F.x, o);
+        F.y += __shfl_xor_sync(0xffffffffu, F.y, o);
+        F.z += __shfl_xor_sync(0xffffffffu, F.z, o);
+        T.x += __shfl_xor_sync(0xffffffffu, T.x, o);
+        T.y += __shfl_xor_sync(0xffffffffu, T.y, o);
+        T.z += __shfl_xor_sync(0xffffffffu, T.z, o);
     }
-    if (tid == 0) {
-        force[ball[b]] = make_double4(sh[0][0], sh[1][0], sh[2][0], 0);
-        torque[ball[b]] = make_double4(sh[3][0], sh[4][0], sh[5][0], 0);
+    if (lane == 0) {
+        force[ball[b]] = d4(F, 0);
+        torque[ball[b]] = d4(T, 0);
     }
 }
 // Puts the dummies into cell order (sorted[t] = caller index of slot t).
@@ -632,6 +634,28 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     Stencil st = stencil_of(xyz(d.mpos[ps]), d.g);
     cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.mpos, d.mposf, d.pos, d.posf, d.eps, false, d.KR, d.NM,
                                   d.nbR, d.cntR, &d.status->need_mrev, &d.status->overflow, sg);
+}
+
+// The fluid-marker rows of a step on skin lists: k_sph_lists_cell's marker
+// row alone, every step (the markers move), over the fluid cells of the last
+// rebuild with each cell's own stencil (the cells are 2 h_max (1 + skin)
+// wide and a particle drifts less than half the skin, so the stencil still
+// covers every marker within its cutoff) and the fluid's drifted positions.
+template <bool kUniformH, int kShape>
+__global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
+    k_sph_marker_rows(SphDev d, int ncell) {
+    constexpr int kListWarps = kListShapes[kShape].warps, kStage = kListShapes[kShape].stage;
+    __shared__ float4 sPos[kListWarps][kStage];
+    __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
+    const int w = threadIdx.x >> 5;
+    const int cell = blockIdx.x * kListWarps + w;
+    if (cell >= ncell) return;
+    const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
+    if (ps == pe) return;
+    ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
+    Stencil st = stencil_of_cell(cell, d.g);
+    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM, d.N,
+                                  d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
 }
 
 // Calls f(j) for this lane's share of particle i's neighbours: from the ELL
@@ -1013,6 +1037,10 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
             // that the atomics of different blocks do not queue on one address)
             const double3 dd = xyz(pn) - xyz(d.xb[i]);
             atomicMax(d.maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
+            // the marker rows of the next step test the drifted positions
+            if (kMarkers)
+                d.posfOut[i] = make_float4((float)(pn.x - d.g.mn.x), (float)(pn.y - d.g.mn.y),
+                                           (float)(pn.z - d.g.mn.z), (float)pn.w);
         }
     }
 }
@@ -1308,7 +1336,7 @@ struct SphScene {
     DBuf<int> nbV, cntV, nbVD, cntVD;
     DBuf<double4> xb;
     DBuf<SkinState> skinState;
-    bool skin_on() const { return skinFrac > 0 && nM == 0; }
+    bool skin_on() const { return skinFrac > 0; }
     float skin_abs() const { return (float)(2.0 * hmaxGrid * skinFrac); }
     // The next step rebuilds the skin lists (after any host-side change).
     void skin_force() {
@@ -1406,10 +1434,10 @@ struct SphScene {
     bool uniformH = false;
     int listShape = 0;  // index into kListShapes (autotuned)
     template <int S>
-    void launch_lists_shape(const SphDev& d) {
+    void launch_lists_shape(const SphDev& d, bool withMarkers) {
         constexpr int W = kListShapes[S].warps;
         const unsigned grid = grid_for(fCells.ncell, W);
-        if (nM > 0) {
+        if (withMarkers && nM > 0) {
             if (uniformH) k_sph_lists_cell<true, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
             else k_sph_lists_cell<false, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
             if (coupling) {  // the transposed rows the reaction reads
@@ -1422,12 +1450,37 @@ struct SphScene {
             else k_sph_lists_cell<false, S, false><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
         }
     }
-    void launch_lists(const SphDev& d) {
+    // withMarkers: the fluid-marker rows (and, inside a coupled step, the
+    // transposed rows) come out of the same build (exact lists every step).
+    void launch_lists(const SphDev& d, bool withMarkers = true) {
         switch (listShape) {
-            case 0: launch_lists_shape<0>(d); break;
-            case 1: launch_lists_shape<1>(d); break;
-            case 2: launch_lists_shape<2>(d); break;
-            default: launch_lists_shape<3>(d); break;
+            case 0: launch_lists_shape<0>(d, withMarkers); break;
+            case 1: launch_lists_shape<1>(d, withMarkers); break;
+            case 2: launch_lists_shape<2>(d, withMarkers); break;
+            default: launch_lists_shape<3>(d, withMarkers); break;
+        }
+    }
+    // Skin lists with markers: this step's fluid-marker rows and, inside a
+    // coupled step, the transposed rows, after the (gated) skin rebuild.
+    template <int S>
+    void launch_marker_rows_shape(const SphDev& d) {
+        constexpr int W = kListShapes[S].warps;
+        const unsigned grid = grid_for(fCells.ncell, W);
+        if (uniformH) k_sph_marker_rows<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        else k_sph_marker_rows<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+        g_launches += 1;
+        if (coupling) {
+            if (uniformH) k_sph_marker_lists<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+            else k_sph_marker_lists<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
+            g_launches += 1;
+        }
+    }
+    void launch_marker_rows(const SphDev& d) {
+        switch (listShape) {
+            case 0: launch_marker_rows_shape<0>(d); break;
+            case 1: launch_marker_rows_shape<1>(d); break;
+            case 2: launch_marker_rows_shape<2>(d); break;
+            default: launch_marker_rows_shape<3>(d); break;
         }
     }
     // Moves the fluid records (and their FP32 shadows) into this step's cell order.
@@ -1483,14 +1536,23 @@ struct SphScene {
     }
     // The step's rebuild of the skin lists, gated on the device's decision.
     void skin_rebuild() {
-        const int n = N();
+        skin_rebuild_sort();
+        skin_rebuild_lists();
+    }
+    // The decision and the gated cell sort (markers placed first in a coupled step).
+    void skin_rebuild_sort() {
+        if (coupling && nM > 0) place_markers();
         k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
-        const int* gate = &skinState.p->rebuild;
-        fCells.build(pos[P].p, n, s, id[ID].p, false, gate);
+        fCells.build(pos[P].p, N(), s, id[ID].p, false, &skinState.p->rebuild);
         g_launches += 1 + fCells.launches;
+    }
+    // The gated reorder and skin-list build, then this step's marker rows.
+    void skin_rebuild_lists() {
+        const int* gate = &skinState.p->rebuild;
         permute(gate);
-        launch_lists(skin_view(gate));
+        launch_lists(skin_view(gate), false);
         g_launches += 2;
+        if (nM > 0) launch_marker_rows(dev());
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
     }
@@ -1509,13 +1571,8 @@ struct SphScene {
         d.velOut = vel[Vv ^ 1].p;
         d.velfOut = velf[Vv ^ 1].p;
         d.posqOut = posq[P ^ 1].p;
-        const unsigned grid = grid_for(N(), kSphPerBlock);
-        if (precision == DEMSPH_PRECISION_FP64)
-            k_sph_accel<double, false, true><<<grid, kSphBlock, 0, s>>>(d, 0.5 * dt, dt, 1);
-        else
-            k_sph_accel<float, false, true><<<grid, kSphBlock, 0, s>>>(d, 0.5 * dt, dt, 1);
-        g_launches += 1;
-        DEMSPH_LAUNCH_CHECK();
+        d.posfOut = posf.p;
+        launch_accel(d, 0.5 * dt, dt, 1, coupling, true);
         P ^= 1;
         Vv ^= 1;
     }
@@ -1523,7 +1580,8 @@ struct SphScene {
     // there are markers, by their terms (k_sph_marker_pass) and, inside a
     // coupled step, by the reaction on them (half of it from each of a
     // step's two passes: first = 1 writes, first = 0 adds).
-    void launch_accel(const SphDev& d, double hdt, double tstep, int first, bool reaction) {
+    // skin: the first pass of a step on skin lists (first = 1).
+    void launch_accel(const SphDev& d, double hdt, double tstep, int first, bool reaction, bool skin = false) {
         const int n = N();
         const unsigned grid = grid_for(n, kSphPerBlock);
         const bool fp64 = precision == DEMSPH_PRECISION_FP64;
@@ -1536,12 +1594,22 @@ struct SphScene {
             }
             if (fp64) k_sph_marker_pass<double><<<grid, kSphBlock, 0, s>>>(d, 0);
             else k_sph_marker_pass<float><<<grid, kSphBlock, 0, s>>>(d, 0);
-            if (fp64) k_sph_accel<double, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
-            else k_sph_accel<float, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            if (skin) {
+                if (fp64) k_sph_accel<double, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+                else k_sph_accel<float, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            } else {
+                if (fp64) k_sph_accel<double, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+                else k_sph_accel<float, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            }
             g_launches += 2;
         } else {
-            if (fp64) k_sph_accel<double, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
-            else k_sph_accel<float, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            if (skin) {
+                if (fp64) k_sph_accel<double, false, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+                else k_sph_accel<float, false, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            } else {
+                if (fp64) k_sph_accel<double, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+                else k_sph_accel<float, false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            }
             g_launches += 1;
         }
         DEMSPH_LAUNCH_CHECK();
@@ -1611,15 +1679,9 @@ struct SphScene {
         DEMSPH_CUDA(cudaEventRecord(ev[0], s));
         if (skin_on()) {
             // 0 decision + gated cell sort, 1 gated reorder + skin lists, 2 first pass on the skin rows
-            k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
-            const int* gate = &skinState.p->rebuild;
-            fCells.build(pos[P].p, n, s, id[ID].p, false, gate);
-            g_launches += 1 + fCells.launches;
+            skin_rebuild_sort();
             DEMSPH_CUDA(cudaEventRecord(ev[1], s));
-            permute(gate);
-            launch_lists(skin_view(gate));
-            g_launches += 2;
-            haveLists = true;
+            skin_rebuild_lists();
             DEMSPH_CUDA(cudaEventRecord(ev[2], s));
             accel_skin();
         } else {
@@ -1798,7 +1860,8 @@ struct SphScene {
             iStep++;
             time += dt;
             step_body();
-            k_sph_body_force<<<nBody, kBodyBlock, 0, s>>>(bStart.p, bBall.p, mforce.p, moff.p, B.force, B.torque);
+            k_sph_body_force<<<grid_for(nBody, kBodyBlock / 32), kBodyBlock, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p,
+                                                                                   moff.p, B.force, B.torque);
             g_launches += 1;
             DEMSPH_LAUNCH_CHECK();
             dem_block_steps(dem, demSub, s);
@@ -1995,7 +2058,7 @@ struct SphScene {
         for (int attempt = 0; attempt < 8; attempt++) {
             clear_status();
             neighbor_search();
-            if (skinMax > 0 && skinFrac > 0) launch_lists(skin_view(nullptr));  // the skin rows are longer
+            if (skinMax > 0 && skinFrac > 0) launch_lists(skin_view(nullptr), false);  // the skin rows are longer
             DevStatus st2 = read_status();
             if (!st2.overflow) break;
             grow(st2);

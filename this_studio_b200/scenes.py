@@ -417,6 +417,135 @@ def dem_drop_poly(n, seed, sigma=0.2, ratio=3.0, r0=0.005, density=2500.0, E=1e8
                     minb=tuple(lo), maxb=tuple(hi), dt=dt)
 
 
+def bonded_beam_clumps(nx=400, ny=20, nz=20, r=0.001, n_clumps=20_000, seed=11, density=7800.0, E=2.0e11,
+                       nu=0.3, restitution=0.5, mu=0.3, tip_load=0.05, dt=1.0e-7, steps=1000):
+    """The bonded cantilever beam plus clumps of the DEM stress test: nx x ny x nz
+    spheres of radius r on a cubic lattice of pitch 2r (the beam along x),
+    parallel bonds on the initial face contacts (normal stiffness 1e12 Pa/m
+    and shear stiffness 4e11 Pa/m, i.e. E_b = 1e12 x 2r and k_n/k_s = 2.5; normal
+    and shear strengths 5e6 Pa, breakable, gamma = 1, no friction term), the
+    x = 0 layer clamped (fixed balls), a seeded random constant load on the tip
+    layer; beside the beam n_clumps rigid 3-sphere clumps (collinear pebbles of
+    radius r at 1.5 r spacing, seeded orientations) over a 2-triangle floor,
+    falling under gravity.  Hertz-Mindlin contact (E, nu, restitution, mu)."""
+    rng = np.random.default_rng(seed)
+    gx = (np.arange(nx) + 0.5) * 2 * r
+    gy = (np.arange(ny) + 0.5) * 2 * r
+    gz = (np.arange(nz) + 0.5) * 2 * r + 0.02
+    x, y, z = np.meshgrid(gx, gy, gz, indexing="ij")
+    beam = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)  # x-major: the first ny*nz are the x = 0 layer
+    nb = beam.shape[0]
+    fixed = np.zeros(nb, bool)
+    fixed[: ny * nz] = True
+    Es, Gs = hertz_params(E, nu)
+    # clumps on a lattice beside the beam (y > beam), each inside a 6r cube
+    side = int(math.ceil(n_clumps ** (1.0 / 3.0)))
+    pitch = 6.0 * r
+    clumps = []
+    y0 = ny * 2 * r + 4 * r
+    m = 3.0 * 4.0 / 3.0 * math.pi * r ** 3 * density
+    I0 = 0.4 * (m / 3.0) * r * r
+    for k in range(n_clumps):
+        i, j, l = k % side, (k // side) % side, k // (side * side)
+        c = np.array([(i + 0.5) * pitch, y0 + (j + 0.5) * pitch, 0.004 + (l + 0.5) * pitch])
+        ax = rng.normal(size=3)
+        ax /= np.linalg.norm(ax)
+        pts = c + np.outer([-1.0, 0.0, 1.0], ax) * 1.5 * r
+        # inertia of three spheres about the centroid: 3 x sphere + 2 x (m/3)(1.5r)^2 off the axis
+        off = 2.0 * (m / 3.0) * (1.5 * r) ** 2
+        Iax = 3 * I0
+        Iperp = 3 * I0 + off
+        Ifull = Iperp * np.eye(3) + (Iax - Iperp) * np.outer(ax, ax)
+        clumps.append(dict(point=pts, radius=[r, r, r], centroid=c, velocity=(0.0, 0.0, 0.0),
+                           angularVelocity=(0.0, 0.0, 0.0), mass=m,
+                           inertia=(Ifull[0, 0], Ifull[1, 1], Ifull[2, 2], Ifull[0, 1], Ifull[0, 2], Ifull[1, 2]),
+                           material=0))
+    L = max(nx * 2 * r, side * pitch)
+    lo = np.array([-4 * r, -4 * r, 0.0])
+    hi = np.array([L + 4 * r, y0 + side * pitch + 4 * r, max(0.02 + nz * 2 * r, 0.004 + side * pitch) + 8 * r])
+    verts = np.array([[lo[0], lo[1], 0.002], [hi[0], lo[1], 0.002], [hi[0], hi[1], 0.002], [lo[0], hi[1], 0.002]])
+    sc = DEMScene(name="bonded_beam_clumps", position=beam, radius=np.full(nb, r), density=np.full(nb, density),
+                  material=np.zeros(nb, np.int32), fixed=fixed,
+                  hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)],
+                  bonded=[(0, 0, 1.0, 1.0e12 * 2 * r, 2.5, 5.0e6, 5.0e6, 0.0)],
+                  clumps=clumps,
+                  walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0),
+                              material=0)],
+                  minb=tuple(lo), maxb=tuple(hi), dt=dt, steps=steps)
+    sc.bond_initial_contacts = True
+    load = np.zeros((nb, 3))
+    tip = np.arange(nb - ny * nz, nb)
+    d = rng.normal(size=(tip.size, 3))
+    load[tip] = tip_load * d / np.linalg.norm(d, axis=1, keepdims=True)
+    sc.constant_force = load
+    return sc
+
+
+def ice_sheet_on_water(n_side=930, r=0.002, jitter=0.05, dx=0.004, water_layers=2, fluid=2_000_000, layers=3, seed=13,
+                       density=917.0, E=9.0e9, nu=0.3, speed=0.5, cyl_segments=(100, 100), dem_dt=2.0e-7,
+                       dem_substeps=1, steps=100):
+    """The coupled ice-cylinder stress scene: a hexagonally packed sheet of about
+    n_side^2 bonded spheres (radius r with seeded +-jitter, density 917,
+    Hertz-Mindlin with E = 9e9) moving at `speed` in -x towards a fixed
+    cylinder mesh (n_around x n_height segments: 20,000 triangles by
+    default), floating on a WCSPH water layer of `water_layers` lattice layers
+    at spacing dx under the sheet and ahead of it, about `fluid` particles,
+    over `layers` dummy layers of floor; the sheet's balls are coupled
+    to the water particle by particle (one marker each when r <= 3 dx / 4).
+    The fluid step is dem_dt x dem_substeps (far below its own CFL limit; the
+    bond stiffness sets the step).  Returns a CoupledScene."""
+    rng = np.random.default_rng(seed)
+    pitch = 2 * r
+    rows = int(round(n_side / (math.sqrt(3) / 2)))
+    cols = n_side
+    W, H = cols * pitch, rows * pitch * math.sqrt(3) / 2
+    j = np.arange(rows)
+    i = np.arange(cols)
+    ii, jj = np.meshgrid(i, j, indexing="xy")
+    px = (ii + 0.5 + 0.5 * (jj % 2)) * pitch
+    py = (jj + 0.5) * pitch * math.sqrt(3) / 2
+    zw = water_layers * dx  # water surface
+    pz = np.full(px.shape, zw)  # centres at the surface: half submerged
+    pos = np.stack([px.ravel(), py.ravel(), pz.ravel()], axis=1)
+    n = pos.shape[0]
+    rad = r * (1.0 + rng.uniform(-jitter, jitter, n))
+    # the water: a lattice under the sheet, extended ahead of it (-x) to about `fluid` particles
+    nyw = int(H / dx)
+    nxw = max(int(W / dx), int(round(fluid / (water_layers * nyw))))
+    margin = nxw * dx - W
+    Ly = H
+    gx = (np.arange(nxw) + 0.5) * dx - margin
+    gy = (np.arange(nyw) + 0.5) * dx
+    gz = (np.arange(water_layers) + 0.5) * dx
+    zz, yy, xx = np.meshgrid(gz, gy, gx, indexing="ij")
+    fluid = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    tw = layers * dx
+    lo = np.array([-margin, 0.0, 0.0]) - tw
+    hi = np.array([W, Ly, zw + 8 * r + 4 * dx]) + tw
+    ax = [np.arange(int(round((h0 - l0) / dx))) * dx + l0 + 0.5 * dx for l0, h0 in zip(lo, hi)]
+    dz = ax[2][ax[2] < 0]
+    zz, yy, xx = np.meshgrid(dz, ax[1], ax[0], indexing="ij")
+    floor = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    g = 9.81
+    c0 = 10.0 * math.sqrt(2 * g * zw)
+    h = 1.3 * dx
+    sph = SPHScene(name="ice_sheet_water", fluid=fluid, dummy=floor, spacing=dx, sound_speed=c0, density=1000.0,
+                   minb=tuple(lo), maxb=tuple(hi), gravity=(0.0, 0.0, -g), dt=dem_dt * dem_substeps, steps=steps)
+    Es, Gs = hertz_params(E, nu)
+    n_around, n_height = cyl_segments
+    cyl_r = 0.05 * H  # ahead of the sheet's leading (-x) edge
+    mesh = cylinder_mesh((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), cyl_r, 0.1, n_around, n_height, caps=False)
+    dem = DEMScene(name="ice_sheet", position=pos, radius=rad, density=np.full(n, density),
+                   material=np.zeros(n, np.int32), velocity=np.tile([-speed, 0.0, 0.0], (n, 1)),
+                   hertz=[(0, 0, Es, Gs, 0.3, 0.0, 0.0, 0.2, 0.0, 0.0), (0, 1, Es, Gs, 0.3, 0.0, 0.0, 0.2, 0.0, 0.0)],
+                   bonded=[(0, 0, 1.0, E, 2.6, 0.5e6, 0.5e6, 0.1)],
+                   walls=[dict(mesh, position=(-(cyl_r + 4 * r), 0.5 * H, zw - 0.05), material=1)],
+                   minb=tuple(lo), maxb=tuple(hi), gravity=(0.0, 0.0, -g), dt=dem_dt, steps=steps)
+    dem.bond_initial_contacts = True
+    return CoupledScene(name="ice_sheet_on_water", sph=sph, dem=dem, balls=np.arange(n, dtype=np.int32),
+                        marker_spacing=dx, marker_h=h, dem_substeps=dem_substeps, steps=steps)
+
+
 def sph_column(n, sound_speed, dt, dx=0.01, layers=3):
     """A dam break with about n fluid particles: a nx x nx x 2nx column at the
     left end of a tank four columns long and 1.25 columns high, three dummy
@@ -549,6 +678,8 @@ def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
             s.setMeshWallMotion(k, w["velocity"], w.get("angularVelocity", (0, 0, 0)))
     if scene.buoyancy is not None:
         s.setBuoyancyDrag(*scene.buoyancy)
+    if getattr(scene, "constant_force", None) is not None:
+        s.setConstantForce(scene.constant_force)
     if scene.periodic is not None:
         s.setPeriodicBoundary(*scene.periodic)
     if initialize:

@@ -7,6 +7,12 @@ sph_dam_break_128k  WCSPH dam break, 40 x 40 x 80 fluid at dx = 0.01 (128,000)
 sph_dam_break_1m    the same tank at dx = 0.005: 80 x 80 x 160 fluid (1,024,000)
 dem_drop_4096       4,096 Hertz-Mindlin spheres dropped onto a plane
 dem_drop_1m         about 10^6 polydisperse spheres dropped onto a plane
+bonded_beam_clumps  a 20 x 20 x 400 bonded beam of r = 1 mm spheres (about 464k
+                    parallel bonds, one end clamped, random tip load) beside
+                    20,000 three-sphere clumps, dt = 1e-7
+ice_sheet_coupled   about 1M bonded r = 2 mm spheres (ice, E = 9e9) moving into a
+                    20,000-triangle cylinder, floating on 2M WCSPH particles at
+                    dx = 4 mm, coupled particle by particle
 coupled_tank_200k   eight DEM balls (r = 6 dx) in a 64 x 64 x 48 tank of water
                     at dx = 0.01 (about 190,000 fluid particles), coupled
                     particle by particle, two DEM substeps per fluid step
@@ -30,6 +36,10 @@ def coupled_tank_scene():
 def build(name, precision="mixed"):
     if name == "coupled_tank_200k":
         return scenes.build_coupled(coupled_tank_scene(), precision)[2]
+    if name == "bonded_beam_clumps":
+        return scenes.build_dem(scenes.bonded_beam_clumps(), precision)
+    if name == "ice_sheet_coupled":
+        return scenes.build_coupled(scenes.ice_sheet_on_water(), precision)[2]
     if name == "sph_dam_break_128k":
         return scenes.build_sph(scenes.sph_dam_break(), precision)
     if name == "sph_dam_break_1m":
@@ -49,11 +59,11 @@ def main():
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel directly")
     a = ap.parse_args()
     s = build(a.name, a.precision)
-    if a.name.startswith("coupled"):
+    if a.name.startswith("coupled") or a.name.startswith("ice_sheet"):
         if a.no_graphs:
             s.sph.setGraphs(False)
             s.dem.setGraphs(False)
-        s.step(a.steps, 2)
+        s.step(a.steps, 2 if a.name.startswith("coupled") else 1)
         s.sph.stepIndex()
     else:
         if a.no_graphs:
