@@ -965,7 +965,7 @@ __device__ __forceinline__ void boundary_drho(const SphDev& d, const FluidOwn<R>
 // Resident blocks per SM the passes' register budgets are fitted to (FP32 /
 // FP64 arithmetic): what the measured-fastest register allocations gave.
 template <class R>
-constexpr int kAccelBlocks = std::is_same<R, float>::value ? 6 : 4;
+constexpr int kAccelBlocks = std::is_same<R, float>::value ? 7 : 4;
 template <class R>
 constexpr int kDensityBlocks = std::is_same<R, float>::value ? 8 : 5;
 
