@@ -238,6 +238,28 @@ __global__ void k_sph_place(int n, int start, double3 off, const double4* __rest
     extra2[start + t] = extra[t];
     if (zero2) zero2[start + t] = 0.0;
 }
+// getSPH on the device: the fluid records back into the caller's order
+// (slot t holds caller index id[t]), in the host arrays' layout (3 doubles
+// per vector), so each requested field is one contiguous copy to the host.
+__global__ void k_sph_unpermute(int n, const int* __restrict__ id, const double4* __restrict__ pos,
+                                const double4* __restrict__ vel, const double4* __restrict__ acc,
+                                const double4* __restrict__ st, const double* __restrict__ drho,
+                                double* __restrict__ oPos, double* __restrict__ oVel, double* __restrict__ oAcc,
+                                double* __restrict__ oRho, double* __restrict__ oP, double* __restrict__ oDrho) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long o = id[t];
+    if (oPos) { const double4 a = pos[t]; oPos[3 * o] = a.x; oPos[3 * o + 1] = a.y; oPos[3 * o + 2] = a.z; }
+    if (oVel) { const double4 a = vel[t]; oVel[3 * o] = a.x; oVel[3 * o + 1] = a.y; oVel[3 * o + 2] = a.z; }
+    if (oAcc) { const double4 a = acc[t]; oAcc[3 * o] = a.x; oAcc[3 * o + 1] = a.y; oAcc[3 * o + 2] = a.z; }
+    if (oRho || oP) {
+        const double4 q = st[t];
+        if (oRho) oRho[o] = q.x;
+        if (oP) oP[o] = q.y;
+    }
+    if (oDrho) oDrho[o] = drho[t];
+}
+
 // Skin-list rebuild of a step: copies the records the gated permute wrote
 // into the scratch halves of the ping-pong pairs back into the current
 // halves (so the host's buffer indices do not depend on the device's
@@ -2053,16 +2075,17 @@ struct SphScene {
             g_launches += dCells.launches;
         }
         // size the neighbour lists on the initial configuration (sorting the
-        // fluid into cell order, which any later step does anyway)
+        // fluid into cell order, which any later step does anyway): one build
+        // with no room in the rows records the longest row of each list
+        KF = 0;
+        KD = 0;
         alloc_lists();
-        for (int attempt = 0; attempt < 8; attempt++) {
-            clear_status();
-            neighbor_search();
-            if (skinMax > 0 && skinFrac > 0) launch_lists(skin_view(nullptr), false);  // the skin rows are longer
-            DevStatus st2 = read_status();
-            if (!st2.overflow) break;
-            grow(st2);
-        }
+        clear_status();
+        neighbor_search();
+        if (skinMax > 0 && skinFrac > 0) launch_lists(skin_view(nullptr), false);  // the skin rows are longer
+        const DevStatus st2 = read_status();
+        KF = std::max(st2.need_pairs, 1);
+        KD = std::max(st2.need_aux, 1);
         // a little headroom for compression during the run
         KF = KF + KF / 8;
         KD = KD + KD / 8;
@@ -2111,18 +2134,20 @@ int demsph_sph_destroy(demsph_sph_t h) {
 // addSPH / addDummy (WCSPHSolver.h:520-560): h = 1.3 spacing, m = spacing^3 rho.
 static void add_particles(SphScene::HostSet& t, long n, const double* pos, const double* vel, const double* c,
                           const double* spacing, const double* dens, const double* visc) {
-    t.pos.reserve(t.pos.size() + n); t.vel.reserve(t.vel.size() + n); t.st.reserve(t.st.size() + n);
-    t.rho0.reserve(t.rho0.size() + n); t.drho.reserve(t.drho.size() + n);
+    const size_t b = t.pos.size();
+    t.pos.resize(b + n); t.vel.resize(b + n); t.st.resize(b + n); t.rho0.resize(b + n); t.drho.resize(b + n, 0.0);
+    size_t k = b;
     for (long i = 0; i < n; i++) {
-        double rho = dens[i], cc = c[i], sp = spacing[i];
+        const double rho = dens[i], cc = c[i], sp = spacing[i];
         if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
-        double m = sp * sp * sp * rho;
-        t.pos.push_back(d4(sld3(pos, i), 1.3 * sp));
-        t.vel.push_back(d4(vel ? sld3(vel, i) : mk3(0, 0, 0), m));
-        t.st.push_back(make_double4(rho, 0.0, cc, visc[i]));
-        t.rho0.push_back(rho);
-        t.drho.push_back(0.0);
+        const double m = sp * sp * sp * rho;
+        t.pos[k] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 1.3 * sp);
+        t.vel[k] = vel ? make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], m) : make_double4(0, 0, 0, m);
+        t.st[k] = make_double4(rho, 0.0, cc, visc[i]);
+        t.rho0[k] = rho;
+        k++;
     }
+    t.pos.resize(k); t.vel.resize(k); t.st.resize(k); t.rho0.resize(k); t.drho.resize(k);
 }
 int demsph_sph_add(demsph_sph_t h, int dummy, long n, const double* pos, const double* vel, const double* c,
                    const double* spacing, const double* dens, const double* visc) {
@@ -2504,25 +2529,41 @@ int demsph_sph_get(demsph_sph_t h, int dummy, double* pos, double* vel, double* 
             }
             return;
         }
-        int n = s.N();
-        std::vector<double4> P4, V4, S4, A4;
-        std::vector<double> DR;
-        std::vector<int> IDp, IDv, IDs, IDd;
-        s.pos[s.P].download(P4, s.s); s.vel[s.Vv].download(V4, s.s); s.st[s.S].download(S4, s.s);
-        s.drho[s.D].download(DR, s.s); s.acc.download(A4, s.s);
-        s.id[s.ID].download(IDp, s.s);
-        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
-        // all fields share the order of the last permutation
-        for (int t = 0; t < n; t++) {
-            int o = IDp[t];
-            if (pos) sst3(pos, o, xyz(P4[t]));
-            if (vel) sst3(vel, o, xyz(V4[t]));
-            if (accel) sst3(accel, o, xyz(A4[t]));
-            if (rho) rho[o] = S4[t].x;
-            if (p) p[o] = S4[t].y;
-            if (drho) drho[o] = DR[t];
-            if (normal) sst3(normal, o, mk3(0, 0, 0));
+        const int n = s.N();
+        // all fields share the order of the last permutation: put them back into
+        // the caller's order on the device, then one copy per field
+        const size_t w3 = (size_t)3 * n;
+        const size_t words = (pos ? w3 : 0) + (vel ? w3 : 0) + (accel ? w3 : 0) + (rho ? n : 0) + (p ? n : 0) +
+                             (drho ? n : 0);
+        if (words > 0) {
+            DBuf<double> out;
+            out.alloc(words, s.s, false);
+            double* q = out.p;
+            auto take = [&](double* host, size_t len) -> double* {
+                if (!host) return nullptr;
+                double* d = q;
+                q += len;
+                return d;
+            };
+            double* dPos = take(pos, w3);
+            double* dVel = take(vel, w3);
+            double* dAcc = take(accel, w3);
+            double* dRho = take(rho, n);
+            double* dP = take(p, n);
+            double* dDr = take(drho, n);
+            k_sph_unpermute<<<grid_for(n, 256), 256, 0, s.s>>>(n, s.id[s.ID].p, s.pos[s.P].p, s.vel[s.Vv].p, s.acc.p,
+                                                              s.st[s.S].p, s.drho[s.D].p, dPos, dVel, dAcc, dRho, dP,
+                                                              dDr);
+            g_launches += 1;
+            DEMSPH_LAUNCH_CHECK();
+            auto back = [&](double* host, const double* dev, size_t len) {
+                if (host) DEMSPH_CUDA(cudaMemcpyAsync(host, dev, len * sizeof(double), cudaMemcpyDeviceToHost, s.s));
+            };
+            back(pos, dPos, w3); back(vel, dVel, w3); back(accel, dAcc, w3);
+            back(rho, dRho, n); back(p, dP, n); back(drho, dDr, n);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         }
+        if (normal) std::fill(normal, normal + w3, 0.0);
     });
 }
 // outputWCSPHVTU / outputDummyVTU (WCSPHSolver.h:360-520): <dir>/SPH_NNNN.vtu

@@ -435,7 +435,7 @@ class WCSPHSolver:
     def _add(self, dummy, position, velocity, soundSpeed, spacing, density, viscosity):
         p = _f64(position, (-1, 3))
         n = p.shape[0]
-        v = _f64(np.zeros((n, 3)) if velocity is None else velocity, (n, 3))
+        v = None if velocity is None else _f64(velocity, (n, 3))
         b = lambda x: _f64(np.broadcast_to(x, (n,)))
         call("demsph_sph_add", self._h, int(dummy), n, _dp(p), _dp(v), _dp(b(soundSpeed)), _dp(b(spacing)),
              _dp(b(density)), _dp(b(viscosity)))
@@ -493,9 +493,9 @@ class WCSPHSolver:
 
     def _get(self, dummy):
         n = self.num(dummy)
-        out = {"position": np.zeros((n, 3)), "velocity": np.zeros((n, 3)), "acceleration": np.zeros((n, 3)),
-               "density": np.zeros(n), "pressure": np.zeros(n), "densityChange": np.zeros(n),
-               "normal": np.zeros((n, 3))}
+        out = {"position": np.empty((n, 3)), "velocity": np.empty((n, 3)), "acceleration": np.empty((n, 3)),
+               "density": np.empty(n), "pressure": np.empty(n), "densityChange": np.empty(n),
+               "normal": np.empty((n, 3))}
         call("demsph_sph_get", self._h, int(dummy), _dp(out["position"]), _dp(out["velocity"]),
              _dp(out["acceleration"]), _dp(out["density"]), _dp(out["pressure"]), _dp(out["densityChange"]),
              _dp(out["normal"]))
