@@ -327,6 +327,11 @@ int demsph_sph_write_vtu(demsph_sph_t s, const char* dir, long frame, int what);
  * rebuild every step.  skin_stats: the fraction in use (0 when off) and the
  * rebuilds so far. */
 int demsph_sph_set_skin(demsph_sph_t s, double fraction);
+/* Autotunes the skin (and with it the share of steps that rebuild lists and
+ * the length of the rows): times `steps` steps with no skin, half the grid's
+ * skin and the grid's skin, each from the same saved state (restored after),
+ * and keeps the fastest.  msPerStep (3 doubles, or NULL) gets the times. */
+int demsph_sph_tune_skin(demsph_sph_t s, int steps, double* chosen, double* msPerStep);
 int demsph_sph_skin_stats(demsph_sph_t s, double* fraction, long* rebuilds);
 
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);

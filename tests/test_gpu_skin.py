@@ -72,3 +72,31 @@ def test_skin_setting(gpu):
     s.setSkin(0.0)
     s.step(5)
     assert s.skinStats()[0] == 0.0
+
+
+def test_tune_skin_restores_the_state(gpu):
+    """The skin tuner times steps from a saved state and puts it back: the
+    scene after tuning steps on as one that was never tuned (to rounding, as
+    the skin sets the order in which pairs are summed), in mixed precision,
+    whose FP32 and fixed-point copies must follow the restored records."""
+    sc = scenes.dam_break_reference()
+    a = _build(sc, "mixed", 0.05)
+    b = _build(sc, "mixed", 0.05)
+    a.step(10)
+    b.step(10)
+    before = a.getSPH()
+    chosen, ms = a.tuneSkin(8)
+    assert chosen in (0.0, pytest.approx(0.025), pytest.approx(0.05))
+    assert all(m > 0 for m in ms)
+    assert a.stepIndex()[0] == 10
+    np.testing.assert_array_equal(a.getSPH()["position"], before["position"])
+    a.step(20)
+    b.step(20)
+    for w in (0, 1):
+        pa, pb = a.getPairs(w), b.getPairs(w)
+        np.testing.assert_array_equal(pa[0], pb[0])
+        np.testing.assert_array_equal(pa[1], pb[1])
+    fa, fb = a.getSPH(), b.getSPH()
+    e = rel_err(fa["position"] - sc.fluid, fb["position"] - sc.fluid)
+    print(f"tuned skin {chosen} ({', '.join(f'{m:.3f}' for m in ms)} ms/step); displacement vs untuned {e:.2e}")
+    assert e < 1e-6

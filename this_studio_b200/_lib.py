@@ -90,6 +90,7 @@ SIGNATURES = {
     "demsph_sph_tune": [_vp, _int, _i, _d],
     "demsph_sph_set_graphs": [_vp, _int],
     "demsph_sph_set_skin": [_vp, _dbl],
+    "demsph_sph_tune_skin": [_vp, _int, _d, _d],
     "demsph_sph_skin_stats": [_vp, _d, _l],
     "demsph_sph_write_vtu": [_vp, C.c_char_p, _long, _int],
     "demsph_sph_num_list_shapes": [],

@@ -1776,7 +1776,7 @@ struct SphScene {
         for (size_t k = 0; k < sn.bufs.size(); k++)
             DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
         iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID; L = sn.L;
-        skin_force();
+        refresh_shadows();  // the FP32 / fixed-point copies follow the restored records (and force a skin rebuild)
     }
     // Steps without a state snapshot: a list row that overflows its capacity
     // is walked from the cell table by the passes (same neighbours), so an
@@ -2397,6 +2397,50 @@ int demsph_sph_tune(demsph_sph_t h, int trials, int* chosen, double* msPerShape)
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
         if (chosen) *chosen = best;
         (void)keep;
+    });
+}
+int demsph_sph_tune_skin(demsph_sph_t h, int steps, double* chosen, double* msPerStep) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (steps < 2) throw Status(DEMSPH_ERR_INVALID, "steps must be at least 2");
+        // no skin, half the grid's skin, the grid's skin: each timed over the
+        // same steps from the same saved state
+        const double cand[3] = {0.0, 0.5 * s.skinMax, (double)s.skinMax};
+        const int nc = s.skinMax > 0 ? 3 : 1;
+        SphScene::Snap sn;
+        s.take(sn);
+        cudaEvent_t e0, e1;
+        DEMSPH_CUDA(cudaEventCreate(&e0));
+        DEMSPH_CUDA(cudaEventCreate(&e1));
+        double bestMs = 1e300, best = s.skinFrac;
+        for (int k = 0; k < nc; k++) {
+            s.skinFrac = (float)cand[k];
+            s.graph.reset();
+            s.skin_force();
+            s.run(2);  // captures the step graphs, rebuilds the lists
+            DEMSPH_CUDA(cudaEventRecord(e0, s.s));
+            s.run(steps);
+            DEMSPH_CUDA(cudaEventRecord(e1, s.s));
+            DEMSPH_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            DEMSPH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double per = ms / steps;
+            if (msPerStep) msPerStep[k] = per;
+            if (per < bestMs) {
+                bestMs = per;
+                best = cand[k];
+            }
+            s.restore(sn);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        s.skinFrac = (float)best;
+        s.graph.reset();
+        s.skin_force();
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        if (chosen) *chosen = best;
     });
 }
 int demsph_sph_num_list_shapes(void) { return kNumListShapes; }

@@ -540,6 +540,15 @@ class WCSPHSolver:
         rebuilt every step); before initialize() it also sizes the grid."""
         call("demsph_sph_set_skin", self._h, float(fraction))
 
+    def tuneSkin(self, steps=20):
+        """Times `steps` steps with no skin, half the grid's and the grid's
+        skin from the same state (restored after) and keeps the fastest;
+        returns (chosen fraction, [ms per step for each])."""
+        c = C.c_double()
+        ms = np.zeros(3)
+        call("demsph_sph_tune_skin", self._h, int(steps), C.byref(c), _dp(ms))
+        return c.value, list(ms)
+
     def skinStats(self):
         """(fraction in use, rebuilds so far)."""
         f, r = C.c_double(), C.c_long()
