@@ -348,9 +348,12 @@ def native(args, rank, world, dist):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = mom_bytes / (mom_ms / 1e3) / 1e9
     traffic = None
+    inst = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("k_sph_accel_bytes_per_launch")
+        tj = json.load(open(tpath))
+        traffic = tj.get("k_sph_accel_bytes_per_launch")
+        inst = tj.get("k_sph_accel_warp_instructions_per_launch")
 
     # end to end through the public API: upload, K steps, read back
     torch.cuda.synchronize()
@@ -404,6 +407,14 @@ def native(args, rank, world, dist):
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": mom_bytes, "ms_per_launch": mom_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s"},
+        # the bound the SPH passes actually sit at: warp-instruction issue
+        # (4 per SM per clock: 148 SMs at the sampled SM clock); instructions per
+        # launch from the committed ncu capture, time live
+        "issue_roofline": None if not inst else {
+            "kernel": "k_sph_accel", "achieved": inst / (mom_ms / 1e3), "unit": "warp-instructions/s",
+            "peak": 4 * 148 * (clk.get("sm_mhz") or 1965.0) * 1e6,
+            "frac": inst / (mom_ms / 1e3) / (4 * 148 * (clk.get("sm_mhz") or 1965.0) * 1e6),
+            "instructions_per_launch": inst, "source": "profiles/traffic.json (ncu smsp__inst_executed.sum)"},
         "phase_ms": {"cell_sort": ph[0], "reorder_lists": ph[1], "momentum_1": ph[2], "continuity_eos": ph[3],
                      "momentum_2": ph[4]},
     }
