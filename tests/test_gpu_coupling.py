@@ -161,3 +161,38 @@ def test_graph_replay_matches_direct_launches(gpu, prec):
     assert np.array_equal(ba["angularVelocity"], bb["angularVelocity"])
     assert np.array_equal(ca[1], cb[1]) and np.array_equal(ca[2], cb[2])
     assert f.stepIndex()[0] == 30 and d.stepIndex()[0] == 30 * sc.dem_substeps
+
+
+def test_balls_float_near_their_flotation_height(gpu):
+    """Physical check of the coupling (it has no reference counterpart): two
+    balls of density 500 and 800 released in still water bob and settle
+    (about six bobbing periods, 24,000 steps); their mean heights over the
+    last third sit within 0.5 R of the static flotation height of a sphere
+    (submerged cap volume = its mass / rho_water, the reference's
+    waterSurfaceHeightForStaticSphere) above the water level raised by the
+    balls' displaced volume, and the denser ball sits lower by the analytic
+    difference to within 0.25 R."""
+    balls = ((0.3, 0.5, 0.85, 4.0, 500.0), (0.7, 0.5, 0.85, 4.0, 800.0))
+    sc = scenes.balls_in_tank(nx=40, ny=32, depth=24, balls=balls, dem_substeps=1)
+    f, d, c = scenes.build_coupled(sc, "mixed")
+    rho, p, drho = hydrostatic(sc)
+    f.setSPH(density=rho, pressure=p, densityChange=drho)
+    R = sc.dem.radius
+    H = sc.sph.fluid[:, 2].max() + 0.5 * sc.sph.spacing
+    area = (40 * sc.sph.spacing) * (32 * sc.sph.spacing)
+    expect = []
+    for r, (_, _, _, _, rho_b) in zip(R, balls):
+        h = scenes.static_sphere_water_level(r, rho_b, 1000.0)  # water plane above the centre
+        expect.append(H - h)
+    rise = sum(rb / 1000.0 * 4.0 / 3.0 * np.pi * r ** 3 for r, (_, _, _, _, rb) in zip(R, balls)) / area
+    expect = np.array(expect) + rise
+    zs = []
+    for _ in range(60):
+        c.step(400, 1)
+        zs.append(d.getBall()["position"][:, 2].copy())
+    zs = np.array(zs)
+    mean = zs[40:].mean(axis=0)
+    print(f"settled centres {mean}, static flotation {expect} (R {R[0]:.3f}); "
+          f"offsets {(mean - expect) / R} R; difference {mean[0] - mean[1]:.4f} vs {expect[0] - expect[1]:.4f}")
+    assert np.all(np.abs(mean - expect) < 0.5 * R)
+    assert abs((mean[0] - mean[1]) - (expect[0] - expect[1])) < 0.25 * R[0]
