@@ -8,6 +8,10 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <memory>
+#include <thread>
+#include <utility>
+#include <algorithm>
 
 #include "../../include/demsph.h"
 
@@ -62,6 +66,49 @@ static inline int guarded(F&& f) {
 
 // ---------------------------------------------------------- device buffer --
 // Owns a device allocation made with cudaMallocAsync on the owner's stream.
+// std::allocator that leaves trivially constructible elements uninitialised
+// on resize, so host staging arrays are first touched by the (parallel) code
+// that fills them rather than by a serial zero fill.
+template <class T>
+struct DefaultInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInitAlloc<U>;
+    };
+    DefaultInitAlloc() = default;
+    template <class U>
+    DefaultInitAlloc(const DefaultInitAlloc<U>&) {}
+    template <class U>
+    void construct(U* p) {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args) {
+        ::new ((void*)p) U(std::forward<Args>(args)...);
+    }
+};
+template <class T>
+using HostVec = std::vector<T, DefaultInitAlloc<T>>;
+
+// Runs f(begin, end) over [0, n) in up to `threads` host threads (one when n
+// is small).
+template <class F>
+static void host_parallel(long n, F&& f, int threads = 8) {
+    const long minChunk = 32768;
+    int k = (int)std::min<long>(threads, std::max<long>(1, n / minChunk));
+    if (k <= 1) {
+        f(0L, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const long step = (n + k - 1) / k;
+    for (int t = 0; t < k; t++) {
+        const long b = t * step, e = std::min(n, b + step);
+        if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -96,7 +143,8 @@ struct DBuf {
         n = count;
         s = stream;
     }
-    void upload(const std::vector<T>& h, cudaStream_t stream) {
+    template <class A>
+    void upload(const std::vector<T, A>& h, cudaStream_t stream) {
         alloc(h.size(), stream, false);
         if (!h.empty()) DEMSPH_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     }

@@ -1317,8 +1317,8 @@ struct SphScene {
     bool ready = false;
     // host staging: fluid and dummy particles in caller order
     struct HostSet {
-        std::vector<double4> pos, vel, st;  // st = (rho, p, c, nu)
-        std::vector<double> rho0, drho;
+        HostVec<double4> pos, vel, st;  // st = (rho, p, c, nu)
+        HostVec<double> rho0, drho;
         size_t size() const { return pos.size(); }
     } hf, hd;
     double3 gravity{0, 0, 0};
@@ -1970,7 +1970,7 @@ struct SphScene {
         init_grid(mn, mx, g, timeStep, prec, hmax, uni);
         hUni = h0;
         const int n = N(), nd = ND();
-        auto up4 = [&](DBuf<double4>& b, const std::vector<double4>& h) {
+        auto up4 = [&](DBuf<double4>& b, const HostVec<double4>& h) {
             DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
         };
         up4(pos[0], hf.pos); up4(vel[0], hf.vel); up4(st[0], hf.st);
@@ -2132,22 +2132,49 @@ int demsph_sph_destroy(demsph_sph_t h) {
     });
 }
 // addSPH / addDummy (WCSPHSolver.h:520-560): h = 1.3 spacing, m = spacing^3 rho.
+// addSPH / addDummy (WCSPHSolver.h:523-541) for n particles: records in
+// the caller's order, skipping those with density or sound speed <= 0 as the
+// reference does.  Filled by several host threads (each first-touching its
+// own part of the new arrays): count the kept particles per chunk, then write.
 static void add_particles(SphScene::HostSet& t, long n, const double* pos, const double* vel, const double* c,
                           const double* spacing, const double* dens, const double* visc) {
-    const size_t b = t.pos.size();
-    t.pos.resize(b + n); t.vel.resize(b + n); t.st.resize(b + n); t.rho0.resize(b + n); t.drho.resize(b + n, 0.0);
-    size_t k = b;
-    for (long i = 0; i < n; i++) {
-        const double rho = dens[i], cc = c[i], sp = spacing[i];
-        if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
-        const double m = sp * sp * sp * rho;
-        t.pos[k] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 1.3 * sp);
-        t.vel[k] = vel ? make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], m) : make_double4(0, 0, 0, m);
-        t.st[k] = make_double4(rho, 0.0, cc, visc[i]);
-        t.rho0[k] = rho;
-        k++;
+    if (n <= 0) return;
+    const int kThreads = 8;
+    const long step = (n + kThreads - 1) / kThreads;
+    std::vector<long> kept(kThreads + 1, 0);
+    host_parallel(kThreads, [&](long a, long b) {
+        for (long ch = a; ch < b; ch++) {
+            long cnt = 0;
+            for (long i = ch * step; i < std::min(n, (ch + 1) * step); i++) cnt += (dens[i] > 0. && c[i] > 0.);
+            kept[ch + 1] = cnt;
+        }
+    }, 1);
+    for (int ch = 0; ch < kThreads; ch++) kept[ch + 1] += kept[ch];
+    const size_t b0 = t.pos.size(), m = (size_t)kept[kThreads];
+    t.pos.resize(b0 + m); t.vel.resize(b0 + m); t.st.resize(b0 + m); t.rho0.resize(b0 + m); t.drho.resize(b0 + m);
+    std::vector<std::thread> pool;
+    for (int ch = 0; ch < kThreads; ch++) {
+        const long lo = ch * step, hi = std::min(n, (ch + 1) * step);
+        if (lo >= hi) continue;
+        auto fill = [&, lo, hi, ch] {
+            size_t k = b0 + kept[ch];
+            for (long i = lo; i < hi; i++) {
+                const double rho = dens[i], cc = c[i], sp = spacing[i];
+                if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
+                const double mass = sp * sp * sp * rho;
+                t.pos[k] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 1.3 * sp);
+                t.vel[k] = vel ? make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], mass)
+                               : make_double4(0, 0, 0, mass);
+                t.st[k] = make_double4(rho, 0.0, cc, visc[i]);
+                t.rho0[k] = rho;
+                t.drho[k] = 0.0;
+                k++;
+            }
+        };
+        if (n < 65536) fill();
+        else pool.emplace_back(fill);
     }
-    t.pos.resize(k); t.vel.resize(k); t.st.resize(k); t.rho0.resize(k); t.drho.resize(k);
+    for (auto& th : pool) th.join();
 }
 int demsph_sph_add(demsph_sph_t h, int dummy, long n, const double* pos, const double* vel, const double* c,
                    const double* spacing, const double* dens, const double* visc) {
