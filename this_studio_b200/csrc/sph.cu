@@ -112,8 +112,6 @@ struct SphDev {
     int* nbR;
     int* cntR;
     double4* mforce;
-    double4* macc;   // per fluid particle: the markers' terms in its acceleration
-    double* mdrho;   // and in its density change (before 2 rho_i)
     double3 gravity;
     DevStatus* status;
 };
@@ -371,8 +369,24 @@ __global__ void k_sph_marker_gather(int nm, const int* __restrict__ sorted, cons
 // Coupling force and torque of each coupled ball: the sum of its markers'
 // reactions (body order, markers [start[b], start[b+1])), and of offset x
 // reaction, written at the ball's index.
-// One warp per ball: each lane sums a strided share of the ball's markers,
-// then a fixed butterfly over the warp (the same sums every run).
+// Balls with at most a few markers each (small balls: one marker at the
+// centre): one thread per ball, the markers in order.
+__global__ void k_sph_body_force_thread(int nb, const int* __restrict__ start, const int* __restrict__ ball,
+                                        const double4* __restrict__ mforce, const double4* __restrict__ moff,
+                                        double4* __restrict__ force, double4* __restrict__ torque) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
+    for (int k = start[b]; k < start[b + 1]; k++) {
+        const double3 f = xyz(mforce[k]);
+        F += f;
+        T += cross(xyz(moff[k]), f);
+    }
+    force[ball[b]] = d4(F, 0);
+    torque[ball[b]] = d4(T, 0);
+}
+// Larger balls: one warp per ball, each lane sums a strided share of the
+// ball's markers, then a fixed butterfly over the warp (the same sums every run).
 constexpr int kBodyBlock = 256;
 __global__ void __launch_bounds__(kBodyBlock) k_sph_body_force(int nb, const int* __restrict__ start,
                                                                const int* __restrict__ ball,
@@ -1038,12 +1052,20 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
                            [&](int j) { boundary_acc<R>(d, o, dv, j, g, acc); });
         }
     }
+    if constexpr (kMarkers) {
+        // the markers' terms, from this step's fluid-marker rows; an overflowed
+        // row walks the marker cells at the rows' build positions, so the pairs
+        // are exactly the ones the reaction on the markers uses
+        const BView mv = marker_view(d);
+        const int cM = d.cntM[i];
+        quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
+                       [&](int j) { boundary_acc<R>(d, o, mv, j, g, acc); });
+    }
     double3 a = up(acc);
     a.x = quad_sum(a.x, gm);
     a.y = quad_sum(a.y, gm);
     a.z = quad_sum(a.z, gm);
     if (sub != 0) return;
-    if (kMarkers) a += xyz(d.macc[i]);  // the markers' terms (k_sph_marker_pass)
     a += d.gravity;
     d.acc[i] = d4(a, 0);
     double3 v = xyz(vi4) + hdt * a;
@@ -1102,9 +1124,14 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
         quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos,
                        [&](int j) { boundary_drho<R>(d, o, dv, j, g, dRho); });
     }
+    if constexpr (kMarkers) {
+        const BView mv = marker_view(d);
+        const int cM = d.cntM[i];
+        quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
+                       [&](int j) { boundary_drho<R>(d, o, mv, j, g, dRho); });
+    }
     double dsum = quad_sum((double)dRho, gm);
     if (sub != 0) return;
-    if (kMarkers) dsum += d.mdrho[i];  // the markers' terms (k_sph_marker_pass)
     double dr = dsum * (2.0 * (double)o.rhoi);
     double ch = d.drho[i] + dr * dt;
     d.drho[i] = ch;
@@ -1113,49 +1140,6 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
     const double4 so = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
     d.stOut[i] = so;
     d.stfOut[i] = f4(so);
-}
-
-// The markers' terms in each fluid particle's acceleration (density = 0,
-// into macc) or density change (density = 1, into mdrho, before the factor
-// 2 rho_i), from the fluid-marker lists; the momentum and continuity passes
-// add them to their sums.  Kept out of those passes so their code stays as
-// small as without markers.
-template <class R>
-__global__ void __launch_bounds__(kSphBlock) k_sph_marker_pass(SphDev d, int density) {
-    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
-    if (i >= d.N) return;
-    const int sub = threadIdx.x & 3;
-    const unsigned gm = quad_mask();
-    using VR = V<R>;
-    const int cnt = d.cntM[i];
-    if (cnt == 0) {
-        if (sub == 0) {
-            if (density) d.mdrho[i] = 0.0;
-            else d.macc[i] = make_double4(0, 0, 0, 0);
-        }
-        return;
-    }
-    const double4 pi4 = d.pos[i];
-    const double4 li4 = d.lpos[i];  // the list-build positions: the lists' pair set on an overflowed row
-    const FluidOwn<R> o = fluid_own<R>(d, i, pi4, d.vel[i], d.st[i]);
-    const VR g = cvt<R>(d.gravity);
-    const BView mv = marker_view(d);
-    if (density) {
-        R dRho = (R)0;
-        quad_neighbors(cnt, d.nbM, d.KM, i, -1, li4, d.g, d.mStart, d.mpos,
-                       [&](int j) { boundary_drho<R>(d, o, mv, j, g, dRho); });
-        const double s = quad_sum((double)dRho, gm);
-        if (sub == 0) d.mdrho[i] = s;
-    } else {
-        VR acc = v3r<R>(0, 0, 0);
-        quad_neighbors(cnt, d.nbM, d.KM, i, -1, li4, d.g, d.mStart, d.mpos,
-                       [&](int j) { boundary_acc<R>(d, o, mv, j, g, acc); });
-        double3 a = up(acc);
-        a.x = quad_sum(a.x, gm);
-        a.y = quad_sum(a.y, gm);
-        a.z = quad_sum(a.z, gm);
-        if (sub == 0) d.macc[i] = d4(a, 0);
-    }
 }
 
 // Reaction of the fluid on the markers: for marker t, minus the sum over
@@ -1377,11 +1361,11 @@ struct SphScene {
     // where they are when the fluid is stepped alone.
     int nM = 0, KM = 48, KR = 96, nBody = 0;
     std::vector<int> hBall, hBStart{0}, hMb;
+    int maxMarkersPerBody = 0;
     std::vector<double4> hMoff, hMrec;  // offset (x, y, z, h); (c, nu, rho0, m)
     demsph_dem_t coupledDem = nullptr;
     DBuf<int> mb, mid, bBall, bStart;
-    DBuf<double4> moff, mrec, mtmp, mpos, mvel, mst, mnorm, mforce, macc;
-    DBuf<double> mdrho;
+    DBuf<double4> moff, mrec, mtmp, mpos, mvel, mst, mnorm, mforce;
     DBuf<float4> mposf, mvelf, mstf, mnormf;
     DBuf<int4> mposq;
     DBuf<int> nbM, cntM, nbR, cntR;
@@ -1418,7 +1402,6 @@ struct SphScene {
         d.mposf = mposf.p; d.mvelf = mvelf.p; d.mstf = mstf.p; d.mnormf = mnormf.p; d.mposq = mposq.p;
         d.mid = mid.p; d.nbM = nbM.p; d.cntM = cntM.p; d.mforce = mforce.p;
         d.KR = KR; d.nbR = nbR.p; d.cntR = cntR.p;
-        d.macc = macc.p; d.mdrho = mdrho.p;
         d.skin = 0.0f; d.gate = nullptr;
         d.nbV = nbV.p; d.cntV = cntV.p; d.nbVD = nbVD.p; d.cntVD = cntVD.p;
         d.xb = xb.p; d.maxd2 = skinState.p ? skinState.p->maxd2 : nullptr;
@@ -1598,10 +1581,10 @@ struct SphScene {
         P ^= 1;
         Vv ^= 1;
     }
-    // The momentum pass (k_sph_accel) on the state d reads, preceded, when
-    // there are markers, by their terms (k_sph_marker_pass) and, inside a
-    // coupled step, by the reaction on them (half of it from each of a
-    // step's two passes: first = 1 writes, first = 0 adds).
+    // The momentum pass (k_sph_accel) on the state d reads (with the markers'
+    // terms when there are markers), preceded inside a coupled step by the
+    // reaction on the markers (half of it from each of a step's two passes:
+    // first = 1 writes, first = 0 adds).
     // skin: the first pass of a step on skin lists (first = 1).
     void launch_accel(const SphDev& d, double hdt, double tstep, int first, bool reaction, bool skin = false) {
         const int n = N();
@@ -1614,8 +1597,6 @@ struct SphScene {
                 else k_sph_marker_force<float><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
                 g_launches += 1;
             }
-            if (fp64) k_sph_marker_pass<double><<<grid, kSphBlock, 0, s>>>(d, 0);
-            else k_sph_marker_pass<float><<<grid, kSphBlock, 0, s>>>(d, 0);
             if (skin) {
                 if (fp64) k_sph_accel<double, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
                 else k_sph_accel<float, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
@@ -1623,7 +1604,7 @@ struct SphScene {
                 if (fp64) k_sph_accel<double, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
                 else k_sph_accel<float, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
             }
-            g_launches += 2;
+            g_launches += 1;
         } else {
             if (skin) {
                 if (fp64) k_sph_accel<double, false, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
@@ -1654,11 +1635,9 @@ struct SphScene {
         const unsigned grid = grid_for(n, kSphPerBlock);
         const bool fp64 = precision == DEMSPH_PRECISION_FP64;
         if (nM > 0) {
-            if (fp64) k_sph_marker_pass<double><<<grid, kSphBlock, 0, s>>>(d, 1);
-            else k_sph_marker_pass<float><<<grid, kSphBlock, 0, s>>>(d, 1);
             if (fp64) k_sph_density<double, true><<<grid, kSphBlock, 0, s>>>(d, dt);
             else k_sph_density<float, true><<<grid, kSphBlock, 0, s>>>(d, dt);
-            g_launches += 2;
+            g_launches += 1;
         } else {
             if (fp64) k_sph_density<double, false><<<grid, kSphBlock, 0, s>>>(d, dt);
             else k_sph_density<float, false><<<grid, kSphBlock, 0, s>>>(d, dt);
@@ -1839,6 +1818,7 @@ struct SphScene {
             }
             hBall.push_back(b);
             hBStart.push_back((int)hMb.size());
+            maxMarkersPerBody = std::max(maxMarkersPerBody, (int)off.size());
         }
         if (hMb.size() > (size_t)INT_MAX / 2) throw Status(DEMSPH_ERR_INVALID, "too many markers");
         coupledDem = dem;
@@ -1851,8 +1831,6 @@ struct SphScene {
         mnorm.alloc(nM, s, false); mposf.alloc(nM, s, false); mvelf.alloc(nM, s, false); mstf.alloc(nM, s, false);
         mnormf.alloc(nM, s, false); mposq.alloc(nM, s, false); mid.alloc(nM, s, false);
         mforce.alloc(nM, s, true);
-        macc.alloc(N(), s, true);
-        mdrho.alloc(N(), s, true);
         mCells.setup(g, nM, s);
         alloc_lists();  // resets the graphs
         bodies = B;
@@ -1882,8 +1860,13 @@ struct SphScene {
             iStep++;
             time += dt;
             step_body();
-            k_sph_body_force<<<grid_for(nBody, kBodyBlock / 32), kBodyBlock, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p,
-                                                                                   moff.p, B.force, B.torque);
+            if (maxMarkersPerBody <= 8)
+                k_sph_body_force_thread<<<grid_for(nBody, 256), 256, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p, moff.p,
+                                                                             B.force, B.torque);
+            else
+                k_sph_body_force<<<grid_for(nBody, kBodyBlock / 32), kBodyBlock, 0, s>>>(nBody, bStart.p, bBall.p,
+                                                                                       mforce.p, moff.p, B.force,
+                                                                                       B.torque);
             g_launches += 1;
             DEMSPH_LAUNCH_CHECK();
             dem_block_steps(dem, demSub, s);
