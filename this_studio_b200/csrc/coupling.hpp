@@ -46,7 +46,5 @@ long dem_graph_epoch(demsph_dem_t h);
 // list overflowed: the lists were regrown and the DEM state restored to the
 // block's start, and the block must be replayed.
 bool dem_block_end(demsph_dem_t h);
-// Drops the DEM's captured step graphs (their kernels hold old buffers).
-void dem_reset_graphs(demsph_dem_t h);
 
 }  // namespace demsph

@@ -1546,7 +1546,6 @@ bool dem_block_end(demsph_dem_t h) {
     return ok;
 }
 
-void dem_reset_graphs(demsph_dem_t h) { h->sc.graph.reset(); }
 
 }  // namespace demsph
 
