@@ -80,6 +80,7 @@ struct DemDev {
     double4* bF;
     double4* bTA;
     double4* bTB;
+    int* bpair;  // 1 when the bond's balls are a pair of the current list
     const int* bincStart;
     const int* binc;
     // mesh walls
@@ -306,11 +307,7 @@ __global__ void k_dem_bonds(DemDev d, double dt) {
     double3 rc = rj + (pj4.w - 0.5 * delta) * n;
     // The reference takes r_c and n from the matching contact pair when one
     // exists; that pair computed them with these same expressions.
-    bool found = false;
-    int c = d.pcnt[i];
-    for (int k = 0; k < c; k++) {
-        if (d.pj[(size_t)k * d.N + i] == j) { found = true; break; }
-    }
+    const bool found = d.bpair[b] != 0;
     d.bpoint[b] = d4(rc, 0);
     d.bnormal[b] = d4(n, 0);
     double3 wi = xyz(d.angv[i]), wj = xyz(d.angv[j]);
@@ -338,20 +335,164 @@ __global__ void k_dem_bonds(DemDev d, double dt) {
     }
 }
 
-// Per-ball finish of one force evaluation:
-//  * B-side pair sum (sumObjectPointingForceTorqueFromInteractionKernel,
-//    contactKernel.cu:683-714) and bond contributions;
-//  * mesh-wall contact: candidate triangles by AABB over the triangle grid
-//    with spring carry (count/writeBallTriangleInteractionsKernel,
-//    ballNeighborSearchKernel.cu:153-338), edge/vertex de-duplication
-//    (updateBallTriangleContact, contactKernel.cu:261-418) and the wall law
-//    (calBallWallContactForceTorqueKernel, contactKernel.cu:420-533);
-//  * the external force hook (externalForceTorque.cu);
-//  * optionally the half-kick (+ drift) of ballIntegrationKernel.cu:30-56,112-121.
+// Whether each bond's balls (A, B) are a pair of the current list: the
+// per-bond search of A's row in calBondedForceTorqueKernel
+// (contactKernel.cu:595-611), done once per list rebuild instead of in every
+// force evaluation (the list only changes at a rebuild).
+__global__ void k_dem_bond_pairs(DemDev d) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.nBond) return;
+    const int2 ab = d.bab[b];
+    const int c = d.pcnt[ab.x];
+    int found = 0;
+    for (int k = 0; k < c; k++) {
+        if (d.pj[(size_t)k * d.N + ab.x] == ab.y) { found = 1; break; }
+    }
+    d.bpair[b] = found;
+}
+
+// Mesh-wall contacts of one force evaluation, per ball: candidate triangles
+// by AABB over the triangle grid with spring carry
+// (count/writeBallTriangleInteractionsKernel, ballNeighborSearchKernel.cu:153-338),
+// edge/vertex de-duplication (updateBallTriangleContact, contactKernel.cu:261-418)
+// and the wall law (calBallWallContactForceTorqueKernel, contactKernel.cu:420-533),
+// added into the ball's A-side accumulators before k_dem_finalize sums them.
+// (A kernel of its own: the candidate arrays and the law would otherwise set
+// the register budget of every ball's finish.)
 constexpr int kMaxTriPerBall = 32;
 template <class R>
-__global__ void __launch_bounds__(128) k_dem_finalize(DemDev d, double dtWall, double extTime, int ext, int integ,
-                                                      double hdt) {
+__global__ void __launch_bounds__(128) k_dem_walls(DemDev d, double dtWall) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    const int i = d.order[t];
+    const double4 p4 = d.pos[i];
+    const double3 ri = xyz(p4);
+    double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
+    bool any = false;
+    // candidate triangles in the reference's stencil order
+    int tri[kMaxTriPerBall];
+    int cnt = 0;
+    Stencil st = stencil_of(ri, d.tg);
+    const double r2 = p4.w * p4.w;
+    for_stencil_rows(st, d.tg, d.triCellStart, [&](int b, int e) {
+        for (int k = b; k < e; k++) {
+            int tj = d.triOrder[k];
+            int4 tv = d.tris[tj];
+            double3 a = xyz(d.vglobal[tv.x]), bb = xyz(d.vglobal[tv.y]), c = xyz(d.vglobal[tv.z]);
+            double cx = fmin(fmax(ri.x, fmin(a.x, fmin(bb.x, c.x))), fmax(a.x, fmax(bb.x, c.x)));
+            double cy = fmin(fmax(ri.y, fmin(a.y, fmin(bb.y, c.y))), fmax(a.y, fmax(bb.y, c.y)));
+            double cz = fmin(fmax(ri.z, fmin(a.z, fmin(bb.z, c.z))), fmax(a.z, fmax(bb.z, c.z)));
+            double dx = ri.x - cx, dy = ri.y - cy, dz = ri.z - cz;
+            if (dx * dx + dy * dy + dz * dz <= r2) {
+                if (cnt < d.KT && cnt < kMaxTriPerBall) tri[cnt] = tj;
+                cnt++;
+            }
+        }
+    });
+    if (cnt > d.KT || cnt > kMaxTriPerBall) {
+        atomicMax(&d.status->need_aux, cnt);
+        atomicExch(&d.status->overflow, 1);
+        cnt = min(d.KT, kMaxTriPerBall);
+    }
+    // springs: carry from this ball's previous candidate row
+    double3 sS[kMaxTriPerBall], sR[kMaxTriPerBall], sT[kMaxTriPerBall];
+    double3 cp[kMaxTriPerBall];
+    int type[kMaxTriPerBall];
+    const int oc = d.wcntOld ? d.wcntOld[i] : 0;
+    for (int c = 0; c < cnt; c++) {
+        sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
+        for (int q = 0; q < oc; q++) {
+            size_t os = (size_t)q * d.N + i;
+            if (d.wtjOld[os] == tri[c]) {
+                sS[c] = xyz(d.wSOld[os]);
+                if (d.roll) sR[c] = xyz(d.wROld[os]);
+                if (d.tors) sT[c] = xyz(d.wTOld[os]);
+                break;
+            }
+        }
+        int4 tv = d.tris[tri[c]];
+        cp[c] = mk3(0, 0, 0);
+        type[c] = classify_sphere_triangle(ri, p4.w, xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]),
+                                           xyz(d.vglobal[tv.z]), cp[c]);
+    }
+    // de-duplication, sequential as in the reference thread
+    unsigned cancel = 0;
+    for (int c = 0; c < cnt; c++) {
+        if (type[c] == kCtNone) {
+            sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
+            cancel |= 1u << c;
+            continue;
+        }
+        if (type[c] == kCtFace) continue;
+        for (int c1 = 0; c1 < cnt; c1++) {
+            if (c1 == c) continue;
+            int t1 = type[c1];
+            bool copy = false;
+            if (t1 == kCtNone) continue;
+            if (t1 == kCtFace) {
+                int4 tv = d.tris[tri[c1]];
+                double3 q0 = xyz(d.vglobal[tv.x]), q1 = xyz(d.vglobal[tv.y]), q2 = xyz(d.vglobal[tv.z]);
+                if (len2(cross(cp[c] - q0, q1 - q0)) < 1.e-20) copy = true;
+                else if (len2(cross(cp[c] - q1, q2 - q1)) < 1.e-20) copy = true;
+                else if (len2(cross(cp[c] - q0, q2 - q0)) < 1.e-20) copy = true;
+            } else if (t1 == kCtEdge) {
+                if (type[c] == t1) { if (c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true; }
+                else if (len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
+            } else {
+                if (type[c] == t1 && c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
+            }
+            if (copy) {
+                sS[c] = sS[c1]; sR[c] = sR[c1]; sT[c] = sT[c1];
+                cancel |= 1u << c;
+                break;
+            }
+        }
+    }
+    // wall law (fixed balls skip it, as calBallWallContactForceTorqueKernel returns early)
+    const double4 v4 = cnt ? d.vel[i] : make_double4(0, 0, 0, 0);
+    if (cnt && !(v4.w < 1.e-20)) {
+        const double3 vi = xyz(v4), wi = xyz(d.angv[i]);
+        const double m = 1. / v4.w;
+        const int mi = d.mat[i];
+        for (int c = 0; c < cnt; c++) {
+            if (cancel & (1u << c)) continue;
+            int wj = d.tris[tri[c]].w;
+            double3 n = normalize(ri - cp[c]);
+            double delta = p4.w - len(ri - cp[c]);
+            double3 rj = xyz(d.wpos[wj]), vj = xyz(d.wvel[wj]), wwj = xyz(d.wangv[wj]);
+            double3 vc = vi + cross(wi, cp[c] - ri) - (vj + cross(wwj, cp[c] - rj));
+            double3 wij = wi - wwj;
+            const MatPair mp = d.mats[pair_param_index(mi, d.wmat[wj], d.nMat, d.cap)];
+            V<R> Fc, Tc;
+            contact_law<R>(mp, Fc, Tc, sS[c], sR[c], sT[c], vc, wij, n, delta, m, p4.w, dtWall, d.roll, d.tors);
+            double3 Fd = up(Fc);
+            F += Fd;
+            T += up(Tc) + cross(cp[c] - ri, Fd);
+            any = true;
+        }
+    }
+    for (int c = 0; c < cnt; c++) {
+        size_t s = (size_t)c * d.N + i;
+        d.wtj[s] = tri[c];
+        d.wS[s] = d4(sS[c], 0);
+        if (d.roll) d.wR[s] = d4(sR[c], 0);
+        if (d.tors) d.wT[s] = d4(sT[c], 0);
+    }
+    d.wcnt[i] = cnt;
+    if (any) {
+        d.forceA[i] = d4(xyz(d.forceA[i]) + F, 0);
+        d.torqueA[i] = d4(xyz(d.torqueA[i]) + T, 0);
+    }
+}
+
+// Per-ball finish of one force evaluation:
+//  * the A-side sums (pairs, periodic ghosts, mesh walls), the B-side pair
+//    sum (sumObjectPointingForceTorqueFromInteractionKernel,
+//    contactKernel.cu:683-714) and bond contributions;
+//  * the external force hook (externalForceTorque.cu);
+//  * optionally the half-kick (+ drift) of ballIntegrationKernel.cu:30-56,112-121.
+template <class R>
+__global__ void __launch_bounds__(128, 8) k_dem_finalize(DemDev d, double extTime, int ext, int integ, double hdt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= d.N) return;
     const int i = d.order[t];
@@ -373,116 +514,6 @@ __global__ void __launch_bounds__(128) k_dem_finalize(DemDev d, double dtWall, d
     const double4 p4 = d.pos[i];
     const double3 ri = xyz(p4);
     const double4 v4 = d.vel[i];
-    if (d.nTri) {
-        // candidate triangles in the reference's stencil order
-        int tri[kMaxTriPerBall];
-        int cnt = 0;
-        Stencil st = stencil_of(ri, d.tg);
-        const double r2 = p4.w * p4.w;
-        for_stencil_rows(st, d.tg, d.triCellStart, [&](int b, int e) {
-            for (int k = b; k < e; k++) {
-                int tj = d.triOrder[k];
-                int4 tv = d.tris[tj];
-                double3 a = xyz(d.vglobal[tv.x]), bb = xyz(d.vglobal[tv.y]), c = xyz(d.vglobal[tv.z]);
-                double cx = fmin(fmax(ri.x, fmin(a.x, fmin(bb.x, c.x))), fmax(a.x, fmax(bb.x, c.x)));
-                double cy = fmin(fmax(ri.y, fmin(a.y, fmin(bb.y, c.y))), fmax(a.y, fmax(bb.y, c.y)));
-                double cz = fmin(fmax(ri.z, fmin(a.z, fmin(bb.z, c.z))), fmax(a.z, fmax(bb.z, c.z)));
-                double dx = ri.x - cx, dy = ri.y - cy, dz = ri.z - cz;
-                if (dx * dx + dy * dy + dz * dz <= r2) {
-                    if (cnt < d.KT && cnt < kMaxTriPerBall) tri[cnt] = tj;
-                    cnt++;
-                }
-            }
-        });
-        if (cnt > d.KT || cnt > kMaxTriPerBall) {
-            atomicMax(&d.status->need_aux, cnt);
-            atomicExch(&d.status->overflow, 1);
-            cnt = min(d.KT, kMaxTriPerBall);
-        }
-        // springs: carry from this ball's previous candidate row
-        double3 sS[kMaxTriPerBall], sR[kMaxTriPerBall], sT[kMaxTriPerBall];
-        double3 cp[kMaxTriPerBall];
-        int type[kMaxTriPerBall];
-        const int oc = d.wcntOld ? d.wcntOld[i] : 0;
-        for (int c = 0; c < cnt; c++) {
-            sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
-            for (int q = 0; q < oc; q++) {
-                size_t os = (size_t)q * d.N + i;
-                if (d.wtjOld[os] == tri[c]) {
-                    sS[c] = xyz(d.wSOld[os]);
-                    if (d.roll) sR[c] = xyz(d.wROld[os]);
-                    if (d.tors) sT[c] = xyz(d.wTOld[os]);
-                    break;
-                }
-            }
-            int4 tv = d.tris[tri[c]];
-            cp[c] = mk3(0, 0, 0);
-            type[c] = classify_sphere_triangle(ri, p4.w, xyz(d.vglobal[tv.x]), xyz(d.vglobal[tv.y]),
-                                               xyz(d.vglobal[tv.z]), cp[c]);
-        }
-        // de-duplication, sequential as in the reference thread
-        unsigned cancel = 0;
-        for (int c = 0; c < cnt; c++) {
-            if (type[c] == kCtNone) {
-                sS[c] = sR[c] = sT[c] = mk3(0, 0, 0);
-                cancel |= 1u << c;
-                continue;
-            }
-            if (type[c] == kCtFace) continue;
-            for (int c1 = 0; c1 < cnt; c1++) {
-                if (c1 == c) continue;
-                int t1 = type[c1];
-                bool copy = false;
-                if (t1 == kCtNone) continue;
-                if (t1 == kCtFace) {
-                    int4 tv = d.tris[tri[c1]];
-                    double3 q0 = xyz(d.vglobal[tv.x]), q1 = xyz(d.vglobal[tv.y]), q2 = xyz(d.vglobal[tv.z]);
-                    if (len2(cross(cp[c] - q0, q1 - q0)) < 1.e-20) copy = true;
-                    else if (len2(cross(cp[c] - q1, q2 - q1)) < 1.e-20) copy = true;
-                    else if (len2(cross(cp[c] - q0, q2 - q0)) < 1.e-20) copy = true;
-                } else if (t1 == kCtEdge) {
-                    if (type[c] == t1) { if (c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true; }
-                    else if (len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
-                } else {
-                    if (type[c] == t1 && c1 < c && len2(cp[c] - cp[c1]) < 1.e-20) copy = true;
-                }
-                if (copy) {
-                    sS[c] = sS[c1]; sR[c] = sR[c1]; sT[c] = sT[c1];
-                    cancel |= 1u << c;
-                    break;
-                }
-            }
-        }
-        // wall law (fixed balls skip it, as calBallWallContactForceTorqueKernel returns early)
-        if (!(v4.w < 1.e-20)) {
-            const double3 vi = xyz(v4), wi = xyz(d.angv[i]);
-            const double m = 1. / v4.w;
-            const int mi = d.mat[i];
-            for (int c = 0; c < cnt; c++) {
-                if (cancel & (1u << c)) continue;
-                int wj = d.tris[tri[c]].w;
-                double3 n = normalize(ri - cp[c]);
-                double delta = p4.w - len(ri - cp[c]);
-                double3 rj = xyz(d.wpos[wj]), vj = xyz(d.wvel[wj]), wwj = xyz(d.wangv[wj]);
-                double3 vc = vi + cross(wi, cp[c] - ri) - (vj + cross(wwj, cp[c] - rj));
-                double3 wij = wi - wwj;
-                const MatPair mp = d.mats[pair_param_index(mi, d.wmat[wj], d.nMat, d.cap)];
-                V<R> Fc, Tc;
-                contact_law<R>(mp, Fc, Tc, sS[c], sR[c], sT[c], vc, wij, n, delta, m, p4.w, dtWall, d.roll, d.tors);
-                double3 Fd = up(Fc);
-                F += Fd;
-                T += up(Tc) + cross(cp[c] - ri, Fd);
-            }
-        }
-        for (int c = 0; c < cnt; c++) {
-            size_t s = (size_t)c * d.N + i;
-            d.wtj[s] = tri[c];
-            d.wS[s] = d4(sS[c], 0);
-            if (d.roll) d.wR[s] = d4(sR[c], 0);
-            if (d.tors) d.wT[s] = d4(sT[c], 0);
-        }
-        d.wcnt[i] = cnt;
-    }
     if (ext) {
         // launchAddConstantForce (externalForceTorque.cu:4-24)
         if (d.fconst) {
@@ -795,6 +826,8 @@ struct DemScene {
     DBuf<double4> bpoint, bnormal, bFs, bTb, bF, bTA, bTB;
     DBuf<double> bFn, bTt, bsmax, btmax;
     DBuf<int> bincStart, binc;
+    DBuf<int> bpair;
+    bool bondPairsStale = true;  // bpair does not describe the current pair list
     DBuf<double4> wpos, wvel, wangv, wq, vlocal, vglobal, tcenter;
     DBuf<int> wmat, vwall;
     DBuf<int4> tris;
@@ -859,6 +892,7 @@ struct DemScene {
         d.pF = pF.p; d.pTB = pTB.p; d.rcnt = rcnt.p; d.rslot = rslot.p;
         d.bab = bab.p; d.bok = bok.p; d.bpoint = bpoint.p; d.bnormal = bnormal.p; d.bFs = bFs.p; d.bTb = bTb.p;
         d.bFn = bFn.p; d.bTt = bTt.p; d.bsmax = bsmax.p; d.btmax = btmax.p; d.bF = bF.p; d.bTA = bTA.p; d.bTB = bTB.p;
+        d.bpair = bpair.p;
         d.bincStart = bincStart.p; d.binc = binc.p;
         d.wpos = wpos.p; d.wvel = wvel.p; d.wangv = wangv.p; d.wq = wq.p; d.wmat = wmat.p;
         d.vlocal = vlocal.p; d.vglobal = vglobal.p; d.vwall = vwall.p; d.tris = tris.p; d.tcenter = tcenter.p;
@@ -959,6 +993,8 @@ struct DemScene {
         }
         bincStart.upload(cnt, s);
         binc.upload(inc, s);
+        bpair.alloc(std::max(nb, 1), s, true);
+        bondPairsStale = true;
     }
 
     void alloc_pairs() {
@@ -990,6 +1026,7 @@ struct DemScene {
     // Capacity growth keeps the k*N + A layout, so the first planes stay valid.
     void grow(int needPairs, int needRev, int needTri) {
         if (needPairs > K || needRev > KR || needTri > KT) graph.reset();
+        bondPairsStale = true;
         size_t n = (size_t)N();
         if (needPairs > K) {
             int nk = needPairs + needPairs / 4 + 1;
@@ -1150,6 +1187,7 @@ struct DemScene {
         launch_count(4);
         DEMSPH_LAUNCH_CHECK();
         havePairs = true;
+        bondPairsStale = true;
     }
     void tri_grid() {
         if (hTris.empty()) return;
@@ -1167,6 +1205,11 @@ struct DemScene {
         launch_count(1);
         if (ghostPass && !ghosts.empty()) ghost_passes(dt);
         if (d.nBond) {
+            if (bondPairsStale) {
+                k_dem_bond_pairs<<<grid_for(d.nBond, 256), 256, 0, s>>>(d);
+                launch_count(1);
+                bondPairsStale = false;
+            }
             k_dem_bonds<<<grid_for(d.nBond, 128), 128, 0, s>>>(d, dt);
             launch_count(1);
         }
@@ -1178,12 +1221,17 @@ struct DemScene {
         } else {
             d.nTri = 0;
         }
+        if (doWalls) {
+            if (precision == DEMSPH_PRECISION_FP64) k_dem_walls<double><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall);
+            else k_dem_walls<float><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall);
+            launch_count(1);
+        }
         bool clumps = !hCpos.empty();
         int fin = clumps ? 0 : integ;
         if (precision == DEMSPH_PRECISION_FP64)
-            k_dem_finalize<double><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall, extTime, ext ? 1 : 0, fin, hdt);
+            k_dem_finalize<double><<<grid_for(n, 128), 128, 0, s>>>(d, extTime, ext ? 1 : 0, fin, hdt);
         else
-            k_dem_finalize<float><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall, extTime, ext ? 1 : 0, fin, hdt);
+            k_dem_finalize<float><<<grid_for(n, 128), 128, 0, s>>>(d, extTime, ext ? 1 : 0, fin, hdt);
         launch_count(1);
         if (doWalls) {
             haveWallRows = true;
@@ -1299,6 +1347,7 @@ struct DemScene {
         }
         iStep = sn.iStep; time = sn.time; cur = sn.cur; wcur = sn.wcur; havePairs = sn.havePairs;
         haveWallRows = sn.haveWallRows;
+        bondPairsStale = true;
         for (size_t g = 0; g < ghosts.size() && g < sn.ghost.size(); g++) {
             ghosts[g]->cur = sn.ghost[g].first;
             ghosts[g]->have = sn.ghost[g].second;
