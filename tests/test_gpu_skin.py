@@ -100,3 +100,30 @@ def test_tune_skin_restores_the_state(gpu):
     e = rel_err(fa["position"] - sc.fluid, fb["position"] - sc.fluid)
     print(f"tuned skin {chosen} ({', '.join(f'{m:.3f}' for m in ms)} ms/step); displacement vs untuned {e:.2e}")
     assert e < 1e-6
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_coupled_skin_steps_match_exact_lists(gpu, prec):
+    """Coupled steps on skin rows (the fluid-marker rows and their transposed
+    rows are rebuilt with the fluid's, when a fluid particle or a marker has
+    drifted half the skin) against the same steps on exact lists rebuilt
+    every step: fast balls make the markers' drift force most rebuilds."""
+    sc = scenes.balls_in_tank(nx=16, ny=16, depth=16, balls=((0.5, 0.5, 0.45, 4.0, 1200.0), (0.25, 0.3, 0.7, 2.5, 600.0)),
+                              ball_velocity=[[1.5, 0.0, -1.0], [0.0, 2.0, 0.5]])
+    runs = []
+    for skin in (0.05, 0.0):
+        f, d, cpl = scenes.build_coupled(sc, prec)
+        f.setSkin(skin)
+        cpl.step(7, sc.dem_substeps)
+        cpl.step(33, sc.dem_substeps)
+        runs.append((f.getSPH(), d.getBall(), cpl.getForces(), f.skinStats()[1]))
+    (fa, ba, ca, ra), (fb, bb, cb, rb) = runs
+    e = rel_err(fa["position"] - sc.sph.fluid, fb["position"] - sc.sph.fluid)
+    ev = rel_err(fa["velocity"], fb["velocity"])
+    eb = rel_err(ba["position"] - sc.dem.position, bb["position"] - sc.dem.position)
+    ef = rel_err(ca[1], cb[1])
+    print(f"{prec}: 40 coupled steps, {ra} skin rebuilds; fluid displacement {e:.2e}, velocity {ev:.2e}, "
+          f"ball displacement {eb:.2e}, ball force {ef:.2e} vs exact lists")
+    assert 8 <= ra < 40
+    tol = 1e-10 if prec == "fp64" else 2e-5
+    assert e < tol and ev < tol and eb < tol and ef < 10 * tol

@@ -156,6 +156,14 @@ struct DBuf {
 };
 
 static inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+// SMs of the current device (asked once per device and host thread).
+static inline int device_sms() {
+    thread_local int dev = -1, sms = 1;
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return sms;
+    if (d != dev && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d) == cudaSuccess) dev = d;
+    return sms > 0 ? sms : 1;
+}
 
 // Zero-fill as a kernel: inside captured step loops every node is a kernel,
 // so a pooled graph of the same shape can be updated to another scene's

@@ -96,6 +96,7 @@ struct DemDev {
     double4* tcenter;
     const int* triOrder;
     const int* triCellStart;
+    double4* wbox;  // [min, max] corners of the mesh vertices' box
     int* wtj;
     int* wcnt;
     double4* wS;
@@ -351,6 +352,34 @@ __global__ void k_dem_bond_pairs(DemDev d) {
     d.bpair[b] = found;
 }
 
+// The box of all mesh vertices (a triangle's box lies inside it): a ball
+// farther than its radius from it has no candidate triangle.
+constexpr int kBoxThreads = 256;
+__global__ void __launch_bounds__(kBoxThreads) k_dem_wall_box(DemDev d) {
+    __shared__ double3 lo[kBoxThreads], hi[kBoxThreads];
+    const int t = threadIdx.x;
+    double3 a = mk3(1e300, 1e300, 1e300), b = mk3(-1e300, -1e300, -1e300);
+    for (int v = t; v < d.nVert; v += kBoxThreads) {
+        const double3 p = xyz(d.vglobal[v]);
+        a = mk3(fmin(a.x, p.x), fmin(a.y, p.y), fmin(a.z, p.z));
+        b = mk3(fmax(b.x, p.x), fmax(b.y, p.y), fmax(b.z, p.z));
+    }
+    lo[t] = a;
+    hi[t] = b;
+    __syncthreads();
+    for (int h = kBoxThreads / 2; h > 0; h >>= 1) {
+        if (t < h) {
+            lo[t] = mk3(fmin(lo[t].x, lo[t + h].x), fmin(lo[t].y, lo[t + h].y), fmin(lo[t].z, lo[t + h].z));
+            hi[t] = mk3(fmax(hi[t].x, hi[t + h].x), fmax(hi[t].y, hi[t + h].y), fmax(hi[t].z, hi[t + h].z));
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        d.wbox[0] = d4(lo[0], 0);
+        d.wbox[1] = d4(hi[0], 0);
+    }
+}
+
 // Mesh-wall contacts of one force evaluation, per ball: candidate triangles
 // by AABB over the triangle grid with spring carry
 // (count/writeBallTriangleInteractionsKernel, ballNeighborSearchKernel.cu:153-338),
@@ -367,6 +396,18 @@ __global__ void __launch_bounds__(128) k_dem_walls(DemDev d, double dtWall) {
     const int i = d.order[t];
     const double4 p4 = d.pos[i];
     const double3 ri = xyz(p4);
+    {
+        // outside the mesh box by more than r (with a relative margin that
+        // covers rounding): no triangle passes the candidate test below
+        const double3 lo = xyz(d.wbox[0]), hi = xyz(d.wbox[1]);
+        const double cx = fmin(fmax(ri.x, lo.x), hi.x), cy = fmin(fmax(ri.y, lo.y), hi.y),
+                     cz = fmin(fmax(ri.z, lo.z), hi.z);
+        const double dx = ri.x - cx, dy = ri.y - cy, dz = ri.z - cz;
+        if (dx * dx + dy * dy + dz * dz > 1.000001 * p4.w * p4.w) {
+            d.wcnt[i] = 0;
+            return;
+        }
+    }
     double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
     bool any = false;
     // candidate triangles in the reference's stencil order
@@ -829,6 +870,7 @@ struct DemScene {
     DBuf<int> bpair;
     bool bondPairsStale = true;  // bpair does not describe the current pair list
     DBuf<double4> wpos, wvel, wangv, wq, vlocal, vglobal, tcenter;
+    DBuf<double4> wbox;
     DBuf<int> wmat, vwall;
     DBuf<int4> tris;
     DBuf<int> wtj[2], wcnt[2];
@@ -896,7 +938,7 @@ struct DemScene {
         d.bincStart = bincStart.p; d.binc = binc.p;
         d.wpos = wpos.p; d.wvel = wvel.p; d.wangv = wangv.p; d.wq = wq.p; d.wmat = wmat.p;
         d.vlocal = vlocal.p; d.vglobal = vglobal.p; d.vwall = vwall.p; d.tris = tris.p; d.tcenter = tcenter.p;
-        d.triOrder = triCells.sorted.p; d.triCellStart = triCells.start.p;
+        d.triOrder = triCells.sorted.p; d.triCellStart = triCells.start.p; d.wbox = wbox.p;
         int wo = wcur ^ 1;
         d.wtj = wtj[wcur].p; d.wcnt = wcnt[wcur].p; d.wS = wS[wcur].p; d.wR = wR[wcur].p; d.wT = wT[wcur].p;
         if (haveWallRows) {
@@ -1192,7 +1234,10 @@ struct DemScene {
     void tri_grid() {
         if (hTris.empty()) return;
         triCells.build(tcenter.p, (int)hTris.size(), s);
-        launch_count(triCells.launches);
+        if (wbox.n < 2) wbox.alloc(2, s, false);
+        DemDev d = dev(false);
+        k_dem_wall_box<<<1, kBoxThreads, 0, s>>>(d);
+        launch_count(1 + triCells.launches);
     }
     // calculateBallContactForceTorque(dt) [+ addTriangleContactForceTorque(dtWall)]
     // [+ external hook at extTime] [+ half-step integration]

@@ -70,7 +70,6 @@ struct SphDev {
     float q;
     double invq;
     const float4* posf;   // fluid (x, y, z) - grid min and h, FP32, this step's order
-    float4* posfOut;      // the same after the first pass's drift (skin lists with markers)
     const float4* dposf;  // dummies, same form
     float eps;            // bound on |float coordinate - exact coordinate|
     int* nbF;
@@ -111,6 +110,13 @@ struct SphDev {
     int KR;          // the transposed list: fluid partners of each marker slot
     int* nbR;
     int* cntR;
+    // Skin rows of the fluid-marker pairs (fluid rows and transposed rows),
+    // built at a skin rebuild; a step's first momentum pass and first
+    // reaction keep the pairs within the exact cutoff into nbM / nbR.
+    int* nbMV;
+    int* cntMV;
+    int* nbRV;
+    int* cntRV;
     double4* mforce;
     double3 gravity;
     DevStatus* status;
@@ -322,12 +328,21 @@ __global__ void __launch_bounds__(kSkinSlots) k_sph_skin_decide(SkinState* st, f
 
 // World position of marker k (body order): its ball's centre plus the
 // marker's offset, with h in w.
+// With skin lists (maxd2 set) each marker's drift from its position at the
+// last rebuild (xbM, body order) goes into the fluid's drift maxima, so
+// that the rebuild decision covers both sides of a fluid-marker pair.
 __global__ void k_sph_marker_place(int nm, const int* __restrict__ mb, const double4* __restrict__ moff,
-                                   const double4* __restrict__ bpos, double4* __restrict__ tmp) {
+                                   const double4* __restrict__ bpos, double4* __restrict__ tmp,
+                                   const double4* __restrict__ xbM, unsigned* __restrict__ maxd2) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nm) return;
     const double4 o = moff[k];
-    tmp[k] = d4(xyz(bpos[mb[k]]) + xyz(o), o.w);
+    const double3 p = xyz(bpos[mb[k]]) + xyz(o);
+    tmp[k] = d4(p, o.w);
+    if (maxd2) {
+        const double3 dd = p - xyz(xbM[k]);
+        atomicMax(maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
+    }
 }
 // Puts the markers into cell order (sorted[t] = body-order index of slot t)
 // with their ball's rigid-body velocity v + omega x offset, the outward
@@ -342,11 +357,13 @@ __global__ void k_sph_marker_gather(int nm, const int* __restrict__ sorted, cons
                                     double4* __restrict__ mvel, double4* __restrict__ mst,
                                     double4* __restrict__ mnorm, float4* __restrict__ mposf,
                                     float4* __restrict__ mvelf, float4* __restrict__ mstf,
-                                    float4* __restrict__ mnormf, int4* __restrict__ mposq, int* __restrict__ mid) {
+                                    float4* __restrict__ mnormf, int4* __restrict__ mposq, int* __restrict__ mid,
+                                    const int* __restrict__ gate, double4* __restrict__ xbM) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nm) return;
     const int k = sorted[t];
     const double4 p = tmp[k];
+    if (xbM && *gate) xbM[k] = p;  // a skin rebuild: the drift is measured from here
     const int b = mb[k];
     const double3 off = xyz(moff[k]);
     const double3 v = xyz(bvel[b]) + cross(xyz(bangv[b]), off);
@@ -464,8 +481,11 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
 // kernels (SPHNeighborSearchKernel.cu:6-228) in one pass: j != i,
 // |r_ij| <= 2 max(h_i, h_j), rows in the reference's stencil order.
 //
-// Built one warp per cell.  All particles of a cell share the cell's 27-cell
-// stencil (the reference clamps positions and cell indices the same way for
+// Built one warp per cell (the warps stride over the cells with a grid of a
+// few blocks per SM, so that a launch gated off by the skin decision, or the
+// empty cells of a mostly empty domain, cost little).  All particles of a
+// cell share the cell's 27-cell stencil (the reference clamps positions and
+// cell indices the same way for
 // every particle of a cell), so the warp stages the stencil's candidates --
 // nine rows of three contiguous cells, in row order -- once in shared memory
 // (coalesced loads), then sweeps them for each of the cell's particles in
@@ -631,30 +651,33 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     __shared__ float4 sPos[kListWarps][kStage];
     __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
     const int w = threadIdx.x >> 5;
-    const int cell = blockIdx.x * kListWarps + w;
-    if (cell >= ncell || (d.gate && *d.gate == 0)) return;
-    const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
-    if (ps == pe) return;
+    if (d.gate && *d.gate == 0) return;
     ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
-    // stencil of the cell: the one every particle of the cell computes
-    const double4 p0 = d.pos[ps];
-    Stencil st = stencil_of(xyz(p0), d.g);
-    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N,
-                                  d.nbF, d.cntF, &d.status->need_pairs, &d.status->overflow, sg, d.skin);
-    if (d.ND > 0)
-        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false, d.KD, d.N,
-                              d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg, d.skin);
-    else
-        for (int i = ps + (threadIdx.x & 31); i < pe; i += 32) d.cntD[i] = 0;
-    if (kMarkers)
-        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM, d.N,
-                                      d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
+    for (int cell = blockIdx.x * kListWarps + w; cell < ncell; cell += gridDim.x * kListWarps) {
+        const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
+        if (ps == pe) continue;
+        // stencil of the cell: the one every particle of the cell computes
+        const double4 p0 = d.pos[ps];
+        Stencil st = stencil_of(xyz(p0), d.g);
+        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.pos, d.posf, d.pos, d.posf, d.eps, true, d.KF, d.N,
+                                      d.nbF, d.cntF, &d.status->need_pairs, &d.status->overflow, sg, d.skin);
+        if (d.ND > 0)
+            cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.dStart, d.pos, d.posf, d.dpos, d.dposf, d.eps, false,
+                                          d.KD, d.N, d.nbD, d.cntD, &d.status->need_aux, &d.status->overflow, sg,
+                                          d.skin);
+        else
+            for (int i = ps + (threadIdx.x & 31); i < pe; i += 32) d.cntD[i] = 0;
+        if (kMarkers)
+            cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false,
+                                          d.KM, d.N, d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
+    }
 }
 
 // The transposed fluid-marker list: for each marker slot, the fluid
 // particles within the list cutoff, one warp per marker cell (the fluid
 // list build with the roles swapped; the FP64 test is symmetric, so the
-// pairs are exactly those of the fluid rows).
+// pairs are exactly those of the fluid rows).  With skin lists (d.skin > 0,
+// gated on the rebuild decision) the rows are skin rows.
 template <bool kUniformH, int kShape>
 __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
     k_sph_marker_lists(SphDev d, int ncell) {
@@ -662,21 +685,19 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     __shared__ float4 sPos[kListWarps][kStage];
     __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
     const int w = threadIdx.x >> 5;
-    const int cell = blockIdx.x * kListWarps + w;
-    if (cell >= ncell) return;
-    const int ps = d.mStart[cell], pe = d.mStart[cell + 1];
-    if (ps == pe) return;
+    if (d.gate && *d.gate == 0) return;
     ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
-    Stencil st = stencil_of(xyz(d.mpos[ps]), d.g);
-    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.mpos, d.mposf, d.pos, d.posf, d.eps, false, d.KR, d.NM,
-                                  d.nbR, d.cntR, &d.status->need_mrev, &d.status->overflow, sg);
+    for (int cell = blockIdx.x * kListWarps + w; cell < ncell; cell += gridDim.x * kListWarps) {
+        const int ps = d.mStart[cell], pe = d.mStart[cell + 1];
+        if (ps == pe) continue;
+        Stencil st = stencil_of(xyz(d.mpos[ps]), d.g);
+        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.fStart, d.mpos, d.mposf, d.pos, d.posf, d.eps, false, d.KR,
+                                      d.NM, d.nbR, d.cntR, &d.status->need_mrev, &d.status->overflow, sg, d.skin);
+    }
 }
 
-// The fluid-marker rows of a step on skin lists: k_sph_lists_cell's marker
-// row alone, every step (the markers move), over the fluid cells of the last
-// rebuild with each cell's own stencil (the cells are 2 h_max (1 + skin)
-// wide and a particle drifts less than half the skin, so the stencil still
-// covers every marker within its cutoff) and the fluid's drifted positions.
+// The fluid-marker skin rows: k_sph_lists_cell's marker row alone, at a skin
+// rebuild (gated), within the cutoff plus the skin.
 template <bool kUniformH, int kShape>
 __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kShape].minBlocks)
     k_sph_marker_rows(SphDev d, int ncell) {
@@ -684,14 +705,15 @@ __global__ void __launch_bounds__(32 * kListShapes[kShape].warps, kListShapes[kS
     __shared__ float4 sPos[kListWarps][kStage];
     __shared__ int sIdx[kUniformH ? 1 : kListWarps][kUniformH ? 1 : kStage];
     const int w = threadIdx.x >> 5;
-    const int cell = blockIdx.x * kListWarps + w;
-    if (cell >= ncell) return;
-    const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
-    if (ps == pe) return;
+    if (d.gate && *d.gate == 0) return;
     ListStage<kUniformH> sg{sPos[w], kUniformH ? nullptr : sIdx[kUniformH ? 0 : w]};
-    Stencil st = stencil_of_cell(cell, d.g);
-    cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM, d.N,
-                                  d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg);
+    for (int cell = blockIdx.x * kListWarps + w; cell < ncell; cell += gridDim.x * kListWarps) {
+        const int ps = d.fStart[cell], pe = d.fStart[cell + 1];
+        if (ps == pe) continue;
+        Stencil st = stencil_of_cell(cell, d.g);
+        cell_lists<kUniformH, kStage>(ps, pe, st, d.g, d.mStart, d.pos, d.posf, d.mpos, d.mposf, d.eps, false, d.KM,
+                                      d.N, d.nbM, d.cntM, &d.status->need_mark, &d.status->overflow, sg, d.skin);
+    }
 }
 
 // Calls f(j) for this lane's share of particle i's neighbours: from the ELL
@@ -910,19 +932,27 @@ __device__ __forceinline__ void fluid_acc(const SphDev& d, const FluidOwn<R>& o,
 // difference (the pair term's own |r|^2) and take the FP64 test only in a
 // band of 2e-6 cut^2 around the cutoff, which covers that square's rounding
 // (< 5e-7 relative) and the positions' quantisation (< 3e-8 relative).
+// pi_of() gives the FP64 position of i when the band needs it (the reaction
+// on the markers loads it only then); the fluid passes pass what they hold.
+template <class PI>
+__device__ __forceinline__ bool cutoff_f(const float3& rij, float hi, float hj, PI&& pi_of,
+                                         const double4* __restrict__ other, int j) {
+    const float d2 = dot(rij, rij);
+    const float cut = 2.0f * fmaxf(hi, hj);
+    const float c2 = cut * cut, band = 2.0e-6f * c2;
+    if (d2 < c2 - band) return true;
+    if (d2 > c2 + band) return false;
+    const double4 pi = pi_of();
+    const double4 pj = other[j];
+    const double cd = 2.0 * fmax(pi.w, pj.w);
+    const double3 r = xyz(pi) - xyz(pj);
+    return (cd * cd - dot(r, r)) >= 0.;
+}
 template <class R>
 __device__ __forceinline__ bool cutoff_r(const V<R>& rij, R hj, const double4& pi, const double4* __restrict__ other,
                                          int j) {
     if constexpr (std::is_same<R, float>::value) {
-        const float d2 = dot(rij, rij);
-        const float cut = 2.0f * fmaxf((float)pi.w, hj);
-        const float c2 = cut * cut, band = 2.0e-6f * c2;
-        if (d2 < c2 - band) return true;
-        if (d2 > c2 + band) return false;
-        const double4 pj = other[j];
-        const double cd = 2.0 * fmax(pi.w, pj.w);
-        const double3 r = xyz(pi) - xyz(pj);
-        return (cd * cd - dot(r, r)) >= 0.;
+        return cutoff_f(rij, (float)pi.w, hj, [&] { return pi; }, other, j);
     } else {
         const double cd = 2.0 * fmax(pi.w, hj);
         return (cd * cd - dot(rij, rij)) >= 0.;
@@ -1053,13 +1083,28 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
         }
     }
     if constexpr (kMarkers) {
-        // the markers' terms, from this step's fluid-marker rows; an overflowed
-        // row walks the marker cells at the rows' build positions, so the pairs
-        // are exactly the ones the reaction on the markers uses
         const BView mv = marker_view(d);
-        const int cM = d.cntM[i];
-        quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
-                       [&](int j) { boundary_acc<R>(d, o, mv, j, g, acc); });
+        if constexpr (kSkin) {
+            // the fluid-marker skin row, with the same exact test the reaction
+            // on the markers applies to its transposed row (cutoff_r from the
+            // fluid's side of the pair, on the same positions)
+            skin_loop(d.cntMV[i], d.nbMV, d.KM, i, d.nbM, d.cntM, pi4, d.g, d.mStart, d.mpos, -1, [&](int j) {
+                VR rij;
+                R hj;
+                pair_r<R>(o.op, mv.pos, mv.posq, d.q, j, rij, hj);
+                if (!cutoff_r<R>(rij, hj, pi4, d.mpos, j)) return false;
+                boundary_acc_r<R>(d, o, mv, j, rij, hj, g, acc);
+                return true;
+            });
+        } else {
+            // the markers' terms, from this step's fluid-marker rows; an
+            // overflowed row walks the marker cells at the rows' build
+            // positions, so the pairs are exactly the ones the reaction on
+            // the markers uses
+            const int cM = d.cntM[i];
+            quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
+                           [&](int j) { boundary_acc<R>(d, o, mv, j, g, acc); });
+        }
     }
     double3 a = up(acc);
     a.x = quad_sum(a.x, gm);
@@ -1081,10 +1126,6 @@ __global__ void __launch_bounds__(kSphBlock, kAccelBlocks<R>) k_sph_accel(SphDev
             // that the atomics of different blocks do not queue on one address)
             const double3 dd = xyz(pn) - xyz(d.xb[i]);
             atomicMax(d.maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
-            // the marker rows of the next step test the drifted positions
-            if (kMarkers)
-                d.posfOut[i] = make_float4((float)(pn.x - d.g.mn.x), (float)(pn.y - d.g.mn.y),
-                                           (float)(pn.z - d.g.mn.z), (float)pn.w);
         }
     }
 }
@@ -1148,7 +1189,11 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
 // the fluid's pass (so the pair set and the terms are the fluid's own).  Four
 // lanes share the marker's transposed list row; the result, times w, is
 // written (add = 0) or added (add = 1) at the marker's body-order index.
-template <class R>
+// kSkinRows: the first reaction of a step on skin lists walks the transposed
+// skin row, keeps the pairs the fluid's first pass keeps (cutoff_r from the
+// fluid's side, on the same positions: the test is the pass's own) and
+// writes them as this step's transposed rows for the second reaction.
+template <class R, bool kSkinRows>
 __global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double w, int add) {
     const int t = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (t >= d.NM) return;
@@ -1160,30 +1205,62 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double
     const BView mv = marker_view(d);
     const VR g = cvt<R>(d.gravity);
     double3 F = mk3(0, 0, 0);
-    auto term = [&](int a) {
-        const double4 va = d.vel[a];
-        const FluidOwn<R> o = fluid_own<R>(d, a, d.pos[a], va, d.st[a]);
+    // the pair (a, t) from the fluid's side: false when outside the exact
+    // cutoff (tested only for skin rows), else its term is added
+    auto term = [&](int a, bool test) {
         VR acc = v3r<R>(0, 0, 0);
-        boundary_acc<R>(d, o, mv, t, g, acc);
-        F -= va.w * up(acc);
+        if constexpr (std::is_same<R, float>::value) {
+            // the FP32 shadows hold what fluid_own rounds the FP64 records to;
+            // the mass is the shadow's FP32 rounding (relative 6e-8)
+            const int4 qa = d.posq[a];
+            const float ha = __int_as_float(qa.w);
+            const OwnPos<float> op{mk3(0, 0, 0), qa};
+            float3 rij;
+            float hj;
+            pair_r<float>(op, mv.pos, mv.posq, d.q, t, rij, hj);
+            if (test && !cutoff_f(rij, ha, hj, [&] { return d.pos[a]; }, d.mpos, t)) return false;
+            const float4 va = d.velf[a], sa = d.stf[a];
+            const FluidOwn<float> o{op, make_float3(va.x, va.y, va.z), sa.x, sa.y, sa.z, sa.w, hconst<float>(ha)};
+            boundary_acc_r<R>(d, o, mv, t, rij, hj, g, acc);
+            F -= (double)va.w * up(acc);
+        } else {
+            const double4 pa = d.pos[a];
+            const OwnPos<double> op{xyz(pa), make_int4(0, 0, 0, 0)};
+            double3 rij;
+            double hj;
+            pair_r<double>(op, mv.pos, mv.posq, d.q, t, rij, hj);
+            if (test && !cutoff_r<double>(rij, hj, pa, d.mpos, t)) return false;
+            const double4 va = d.vel[a];
+            const FluidOwn<R> o = fluid_own<R>(d, a, pa, va, d.st[a]);
+            boundary_acc_r<R>(d, o, mv, t, rij, hj, g, acc);
+            F -= va.w * up(acc);
+        }
+        return true;
     };
-    const int cnt = d.cntR[t];
-    if (cnt >= 0) {
-        // the transposed list (k_sph_marker_lists): the fluid rows' pair set
-        const int* __restrict__ row = d.nbR + (size_t)t * d.KR;
-        for (int k = sub; k < cnt; k += kQuad) term(__ldg(row + k));
+    if constexpr (kSkinRows) {
+        skin_loop(d.cntRV[t], d.nbRV, d.KR, t, d.nbR, d.cntR, pm, d.g, d.fStart, d.pos, -1,
+                  [&](int a) { return term(a, true); });
     } else {
-        // an overflowed row: the same pairs from the cell stencil, with the
-        // cutoff test on the build-time positions
-        Stencil st = stencil_of(rm, d.g);
-        for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
-            for (int a = b + sub; a < e; a += kQuad) {
-                const double4 la = d.lpos[a];
-                const double cut = 2.0 * fmax(la.w, pm.w);
-                const double3 r = xyz(la) - rm;
-                if ((cut * cut - dot(r, r)) >= 0.) term(a);
-            }
-        });
+        const int cnt = d.cntR[t];
+        if (cnt >= 0) {
+            // the transposed list (k_sph_marker_lists, or the first reaction's
+            // exact rows on skin lists): the fluid rows' pair set
+            const int* __restrict__ row = d.nbR + (size_t)t * d.KR;
+            const int c = lane_count(cnt, sub);
+            for (int k = 0; k < c; k++) term(__ldg(row + sub + kQuad * k), false);
+        } else {
+            // an overflowed row: the same pairs from the cell stencil, with the
+            // cutoff test on the build-time positions
+            Stencil st = stencil_of(rm, d.g);
+            for_stencil_rows(st, d.g, d.fStart, [&](int b, int e) {
+                for (int a = b + sub; a < e; a += kQuad) {
+                    const double4 la = d.lpos[a];
+                    const double cut = 2.0 * fmax(la.w, pm.w);
+                    const double3 r = xyz(la) - rm;
+                    if ((cut * cut - dot(r, r)) >= 0.) term(a, false);
+                }
+            });
+        }
     }
     F.x = quad_sum(F.x, gm);
     F.y = quad_sum(F.y, gm);
@@ -1369,6 +1446,8 @@ struct SphScene {
     DBuf<float4> mposf, mvelf, mstf, mnormf;
     DBuf<int4> mposq;
     DBuf<int> nbM, cntM, nbR, cntR;
+    DBuf<int> nbMV, cntMV, nbRV, cntRV;  // skin rows of the fluid-marker pairs
+    DBuf<double4> xbM;                   // marker positions at the last skin rebuild (body order)
     CellTable mCells;
     DemBodies bodies{};
     bool coupling = false;  // inside a coupled block: place markers, compute reactions
@@ -1402,6 +1481,7 @@ struct SphScene {
         d.mposf = mposf.p; d.mvelf = mvelf.p; d.mstf = mstf.p; d.mnormf = mnormf.p; d.mposq = mposq.p;
         d.mid = mid.p; d.nbM = nbM.p; d.cntM = cntM.p; d.mforce = mforce.p;
         d.KR = KR; d.nbR = nbR.p; d.cntR = cntR.p;
+        d.nbMV = nbMV.p; d.cntMV = cntMV.p; d.nbRV = nbRV.p; d.cntRV = cntRV.p;
         d.skin = 0.0f; d.gate = nullptr;
         d.nbV = nbV.p; d.cntV = cntV.p; d.nbVD = nbVD.p; d.cntVD = cntVD.p;
         d.xb = xb.p; d.maxd2 = skinState.p ? skinState.p->maxd2 : nullptr;
@@ -1427,6 +1507,13 @@ struct SphScene {
             nbVD.alloc(n * std::max(KD, 1), s, false);
             cntVD.alloc(n, s, true);
             if (xb.n < n) xb.alloc(n, s, true);
+            if (nM > 0) {
+                nbMV.alloc(n * KM, s, false);
+                cntMV.alloc(n, s, true);
+                nbRV.alloc((size_t)nM * KR, s, false);
+                cntRV.alloc(nM, s, true);
+                if (xbM.n < (size_t)nM) xbM.alloc(nM, s, true);
+            }
             if (!skinState.p) skinState.alloc(1, s, true);
             skin_force();
         }
@@ -1438,10 +1525,17 @@ struct SphScene {
     // candidate index in the staged record
     bool uniformH = false;
     int listShape = 0;  // index into kListShapes (autotuned)
+    // Blocks of a list build over ncell cells: one warp per cell up to eight
+    // waves of the shape's resident blocks, the warps striding beyond.
+    template <int kShape>
+    static unsigned list_grid(int ncell) {
+        const unsigned cap = (unsigned)(device_sms() * kListShapes[kShape].minBlocks * 8);
+        return std::min(grid_for(ncell, kListShapes[kShape].warps), cap);
+    }
     template <int S>
     void launch_lists_shape(const SphDev& d, bool withMarkers) {
         constexpr int W = kListShapes[S].warps;
-        const unsigned grid = grid_for(fCells.ncell, W);
+        const unsigned grid = list_grid<S>(fCells.ncell);
         if (withMarkers && nM > 0) {
             if (uniformH) k_sph_lists_cell<true, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
             else k_sph_lists_cell<false, S, true><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
@@ -1465,20 +1559,18 @@ struct SphScene {
             default: launch_lists_shape<3>(d, withMarkers); break;
         }
     }
-    // Skin lists with markers: this step's fluid-marker rows and, inside a
-    // coupled step, the transposed rows, after the (gated) skin rebuild.
+    // Skin lists with markers: the fluid-marker skin rows and the transposed
+    // skin rows, at a (gated) skin rebuild.
     template <int S>
     void launch_marker_rows_shape(const SphDev& d) {
         constexpr int W = kListShapes[S].warps;
-        const unsigned grid = grid_for(fCells.ncell, W);
+        const unsigned grid = list_grid<S>(fCells.ncell);
         if (uniformH) k_sph_marker_rows<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
         else k_sph_marker_rows<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
-        g_launches += 1;
-        if (coupling) {
-            if (uniformH) k_sph_marker_lists<true, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
-            else k_sph_marker_lists<false, S><<<grid, 32 * W, 0, s>>>(d, fCells.ncell);
-            g_launches += 1;
-        }
+        const unsigned mgrid = list_grid<S>(mCells.ncell);
+        if (uniformH) k_sph_marker_lists<true, S><<<mgrid, 32 * W, 0, s>>>(d, mCells.ncell);
+        else k_sph_marker_lists<false, S><<<mgrid, 32 * W, 0, s>>>(d, mCells.ncell);
+        g_launches += 2;
     }
     void launch_marker_rows(const SphDev& d) {
         switch (listShape) {
@@ -1518,12 +1610,26 @@ struct SphScene {
     }
     // Markers from the coupled balls' current state, in cell order.
     void place_markers() {
-        k_sph_marker_place<<<grid_for(nM, 256), 256, 0, s>>>(nM, mb.p, moff.p, bodies.pos, mtmp.p);
-        mCells.build(mtmp.p, nM, s);
+        marker_place(false);
+        marker_sort(nullptr);
+    }
+    // The markers' positions in body order; with skin lists (drift) each
+    // marker's drift since the last rebuild joins the rebuild decision.
+    void marker_place(bool drift) {
+        k_sph_marker_place<<<grid_for(nM, 256), 256, 0, s>>>(nM, mb.p, moff.p, bodies.pos, mtmp.p, xbM.p,
+                                                             drift ? skinState.p->maxd2 : nullptr);
+        g_launches += 1;
+    }
+    // Cell sort (gated on a skin rebuild: otherwise the slots keep the order
+    // of the last rebuild, which the skin rows index) and the records in slot
+    // order; a skin rebuild also re-anchors the drift.
+    void marker_sort(const int* gate) {
+        mCells.build(mtmp.p, nM, s, nullptr, false, gate);
         k_sph_marker_gather<<<grid_for(nM, 256), 256, 0, s>>>(
             nM, mCells.sorted.p, mtmp.p, mb.p, moff.p, mrec.p, bodies.vel, bodies.angv, fCells.g.mn, invq, mpos.p,
-            mvel.p, mst.p, mnorm.p, mposf.p, mvelf.p, mstf.p, mnormf.p, mposq.p, mid.p);
-        g_launches += 2 + mCells.launches;
+            mvel.p, mst.p, mnorm.p, mposf.p, mvelf.p, mstf.p, mnormf.p, mposq.p, mid.p, gate,
+            gate ? xbM.p : nullptr);
+        g_launches += 1 + mCells.launches;
         DEMSPH_LAUNCH_CHECK();
     }
     void neighbor_search() {
@@ -1544,20 +1650,29 @@ struct SphScene {
         skin_rebuild_sort();
         skin_rebuild_lists();
     }
-    // The decision and the gated cell sort (markers placed first in a coupled step).
+    // The decision and the gated cell sorts (in a coupled step the markers
+    // are placed first: their drift joins the decision).
     void skin_rebuild_sort() {
-        if (coupling && nM > 0) place_markers();
+        const int* gate = &skinState.p->rebuild;
+        const bool move = coupling && nM > 0;
+        if (move) marker_place(true);
         k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
-        fCells.build(pos[P].p, N(), s, id[ID].p, false, &skinState.p->rebuild);
+        if (move) marker_sort(gate);
+        fCells.build(pos[P].p, N(), s, id[ID].p, false, gate);
         g_launches += 1 + fCells.launches;
     }
-    // The gated reorder and skin-list build, then this step's marker rows.
+    // The gated reorder and skin-list build (with markers: the fluid-marker
+    // skin rows and their transposed rows too).
     void skin_rebuild_lists() {
         const int* gate = &skinState.p->rebuild;
         permute(gate);
         launch_lists(skin_view(gate), false);
         g_launches += 2;
-        if (nM > 0) launch_marker_rows(dev());
+        if (nM > 0) {
+            SphDev d = skin_view(gate);
+            d.nbM = nbMV.p; d.cntM = cntMV.p; d.nbR = nbRV.p; d.cntR = cntRV.p;
+            launch_marker_rows(d);
+        }
         DEMSPH_LAUNCH_CHECK();
         haveLists = true;
     }
@@ -1576,7 +1691,6 @@ struct SphScene {
         d.velOut = vel[Vv ^ 1].p;
         d.velfOut = velf[Vv ^ 1].p;
         d.posqOut = posq[P ^ 1].p;
-        d.posfOut = posf.p;
         launch_accel(d, 0.5 * dt, dt, 1, coupling, true);
         P ^= 1;
         Vv ^= 1;
@@ -1593,8 +1707,13 @@ struct SphScene {
         if (nM > 0) {
             if (reaction) {
                 const unsigned mg = grid_for(nM, kSphPerBlock);
-                if (fp64) k_sph_marker_force<double><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
-                else k_sph_marker_force<float><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
+                if (skin) {
+                    if (fp64) k_sph_marker_force<double, true><<<mg, kSphBlock, 0, s>>>(d, 0.5, 0);
+                    else k_sph_marker_force<float, true><<<mg, kSphBlock, 0, s>>>(d, 0.5, 0);
+                } else {
+                    if (fp64) k_sph_marker_force<double, false><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
+                    else k_sph_marker_force<float, false><<<mg, kSphBlock, 0, s>>>(d, 0.5, first ? 0 : 1);
+                }
                 g_launches += 1;
             }
             if (skin) {
@@ -1875,6 +1994,9 @@ struct SphScene {
             Snap sn;
             take(sn);
             clear_status();
+            // the markers' drift is measured from the rebuild that placed them:
+            // steps of the fluid alone may have rebuilt without them
+            skin_force();
             dem_block_begin(dem, s);
             bodies = B;
             coupling = true;
