@@ -1193,8 +1193,10 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
 // skin row, keeps the pairs the fluid's first pass keeps (cutoff_r from the
 // fluid's side, on the same positions: the test is the pass's own) and
 // writes them as this step's transposed rows for the second reaction.
+template <class R>
+constexpr int kMarkerForceBlocks = std::is_same<R, float>::value ? 8 : 4;
 template <class R, bool kSkinRows>
-__global__ void __launch_bounds__(kSphBlock) k_sph_marker_force(SphDev d, double w, int add) {
+__global__ void __launch_bounds__(kSphBlock, kMarkerForceBlocks<R>) k_sph_marker_force(SphDev d, double w, int add) {
     const int t = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (t >= d.NM) return;
     const int sub = threadIdx.x & 3;
