@@ -60,11 +60,13 @@ const char* demsph_version(void);
 /* Number of CUDA kernels this library has launched since load (instrumentation). */
 long long demsph_kernel_launches(void);
 /* No counterpart in the reference.  Scene buffers come from the current
- * device's default stream-ordered memory pool; by default the pool hands
- * freed memory back to the driver at every synchronisation.  This keeps up to
- * `bytes` of freed memory in this process's pool instead, so a loop that
- * destroys and re-creates scenes (the batched and served forms) reuses it
- * without re-mapping.  Affects only this process. */
+ * device's default stream-ordered memory pool, whose stock setting hands
+ * freed memory back to the driver at every synchronisation (re-mapping it on
+ * the next allocation costs milliseconds per scene, and more on a busy GPU).
+ * The first scene created on a device sets the pool to keep up to 8 GiB of
+ * freed memory in this process; this call sets another limit (0: the stock
+ * behaviour), and a limit set here is never overridden.  Affects only this
+ * process. */
 int demsph_retain_device_memory(unsigned long long bytes);
 
 /* ======================================================================= */

@@ -156,6 +156,9 @@ struct DBuf {
 };
 
 static inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+// Keeps up to 8 GiB of freed memory in the current device's default pool,
+// once per device, unless the caller set a limit (demsph_retain_device_memory).
+void default_pool_retention();
 // SMs of the current device (asked once per device and host thread).
 static inline int device_sms() {
     thread_local int dev = -1, sms = 1;

@@ -1648,6 +1648,7 @@ extern "C" {
 int demsph_dem_create(demsph_dem_t* out, void* stream) {
     return guarded([&] {
         if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        default_pool_retention();
         auto* h = new demsph_dem_scene();
         h->sc.s = (cudaStream_t)stream;
         *out = h;

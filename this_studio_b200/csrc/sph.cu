@@ -2225,6 +2225,7 @@ extern "C" {
 int demsph_sph_create(demsph_sph_t* out, void* stream) {
     return guarded([&] {
         if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        default_pool_retention();
         auto* h = new demsph_sph_scene();
         h->sc.s = (cudaStream_t)stream;
         *out = h;
