@@ -179,7 +179,7 @@ def dem_bounce(torch, steps, warmup, flush):
     ms = float(sum(times)) / (len(times) * block)
     return {"workload": "dem_bounce_4096", "value": sc.position.shape[0] / (ms / 1e3), "unit": METRIC,
             "ms_per_step": ms, "precision": "mixed", "steps": steps,
-            "note": "4,096 spheres; launch-bound at this size (see DESIGN.md)"}
+            "note": "4,096 spheres: each kernel runs 4,096 threads, bound by the latency of their dependent loads"}
 
 
 def coupled_tank(torch, steps, warmup, flush):
