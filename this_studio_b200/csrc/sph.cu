@@ -433,6 +433,47 @@ __global__ void __launch_bounds__(kBodyBlock) k_sph_body_force(int nb, const int
         torque[ball[b]] = d4(T, 0);
     }
 }
+// The same with one block per ball, for balls with hundreds of markers: each
+// thread sums a strided share, then a fixed-order tree over the warps.
+__global__ void __launch_bounds__(kBodyBlock) k_sph_body_force_block(const int* __restrict__ start,
+                                                                     const int* __restrict__ ball,
+                                                                     const double4* __restrict__ mforce,
+                                                                     const double4* __restrict__ moff,
+                                                                     double4* __restrict__ force,
+                                                                     double4* __restrict__ torque) {
+    __shared__ double sh[kBodyBlock / 32][6];
+    const int b = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double3 F = mk3(0, 0, 0), T = mk3(0, 0, 0);
+    for (int k = start[b] + threadIdx.x; k < start[b + 1]; k += kBodyBlock) {
+        const double3 f = xyz(mforce[k]);
+        F += f;
+        T += cross(xyz(moff[k]), f);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        F.x += __shfl_xor_sync(0xffffffffu, F.x, o);
+        F.y += __shfl_xor_sync(0xffffffffu, F.y, o);
+        F.z += __shfl_xor_sync(0xffffffffu, F.z, o);
+        T.x += __shfl_xor_sync(0xffffffffu, T.x, o);
+        T.y += __shfl_xor_sync(0xffffffffu, T.y, o);
+        T.z += __shfl_xor_sync(0xffffffffu, T.z, o);
+    }
+    if (lane == 0) {
+        sh[w][0] = F.x; sh[w][1] = F.y; sh[w][2] = F.z;
+        sh[w][3] = T.x; sh[w][4] = T.y; sh[w][5] = T.z;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        F = mk3(0, 0, 0);
+        T = mk3(0, 0, 0);
+        for (int v = 0; v < kBodyBlock / 32; v++) {
+            F += mk3(sh[v][0], sh[v][1], sh[v][2]);
+            T += mk3(sh[v][3], sh[v][4], sh[v][5]);
+        }
+        force[ball[b]] = d4(F, 0);
+        torque[ball[b]] = d4(T, 0);
+    }
+}
 // Puts the dummies into cell order (sorted[t] = caller index of slot t).
 __global__ void k_sph_dummy_gather(int nd, const int* __restrict__ sorted, const double4* __restrict__ tp,
                                    const double4* __restrict__ tv, const double4* __restrict__ ts,
@@ -1984,6 +2025,9 @@ struct SphScene {
             if (maxMarkersPerBody <= 8)
                 k_sph_body_force_thread<<<grid_for(nBody, 256), 256, 0, s>>>(nBody, bStart.p, bBall.p, mforce.p, moff.p,
                                                                              B.force, B.torque);
+            else if (maxMarkersPerBody > 256)
+                k_sph_body_force_block<<<nBody, kBodyBlock, 0, s>>>(bStart.p, bBall.p, mforce.p, moff.p, B.force,
+                                                                    B.torque);
             else
                 k_sph_body_force<<<grid_for(nBody, kBodyBlock / 32), kBodyBlock, 0, s>>>(nBody, bStart.p, bBall.p,
                                                                                        mforce.p, moff.p, B.force,
