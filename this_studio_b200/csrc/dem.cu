@@ -234,10 +234,7 @@ __global__ void k_dem_reverse_order(DemDev d) {
 // (contactKernel.cu:657-681).  The pair force and the B-side torque
 // contribution -(T_c + (r_c - r_B) x F_c) are stored for the B side.
 template <class R>
-__global__ void __launch_bounds__(128, 4) k_dem_pair_forces(DemDev d, double dt) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= d.N) return;
-    const int A = d.qorder[t];
+__device__ __forceinline__ void pair_forces_ball(const DemDev& d, int A, double dt) {
     const double4 pa = d.pos[A];
     const double3 ra = xyz(pa);
     const double4 va4 = d.vel[A];
@@ -279,6 +276,11 @@ __global__ void __launch_bounds__(128, 4) k_dem_pair_forces(DemDev d, double dt)
     }
     d.forceA[A] = d4(FA, 0);
     d.torqueA[A] = d4(TA, 0);
+}
+template <class R>
+__global__ void __launch_bounds__(128, 4) k_dem_pair_forces(DemDev d, double dt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < d.N) pair_forces_ball<R>(d, d.qorder[t], dt);
 }
 
 // calBondedForceTorqueKernel (contactKernel.cu:535-655).  Instead of adding
@@ -390,10 +392,7 @@ __global__ void __launch_bounds__(kBoxThreads) k_dem_wall_box(DemDev d) {
 // the register budget of every ball's finish.)
 constexpr int kMaxTriPerBall = 32;
 template <class R>
-__global__ void __launch_bounds__(128) k_dem_walls(DemDev d, double dtWall) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= d.N) return;
-    const int i = d.order[t];
+__device__ __forceinline__ void walls_ball(const DemDev& d, int i, double dtWall) {
     const double4 p4 = d.pos[i];
     const double3 ri = xyz(p4);
     {
@@ -524,6 +523,23 @@ __global__ void __launch_bounds__(128) k_dem_walls(DemDev d, double dtWall) {
         d.forceA[i] = d4(xyz(d.forceA[i]) + F, 0);
         d.torqueA[i] = d4(xyz(d.torqueA[i]) + T, 0);
     }
+}
+template <class R>
+__global__ void __launch_bounds__(128) k_dem_walls(DemDev d, double dtWall) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < d.N) walls_ball<R>(d, d.order[t], dtWall);
+}
+// Small scenes, whose steps are bound by the latency of each launch's chain
+// of loads: a ball's pair forces and then its wall contacts in one thread
+// (the wall terms are added to the A-side sums the pair forces just wrote, as
+// the separate kernels do, so the result is the same).
+template <class R>
+__global__ void __launch_bounds__(128) k_dem_pair_walls(DemDev d, double dt, double dtWall) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    const int A = d.qorder[t];
+    pair_forces_ball<R>(d, A, dt);
+    walls_ball<R>(d, A, dtWall);
 }
 
 // Per-ball finish of one force evaluation:
@@ -886,6 +902,7 @@ struct DemScene {
     cudaStream_t blockOwn = 0;
     bool inBlock = false;
     DBuf<DevStatus> status;
+    static constexpr int kMergedWallBalls = 65536;  // up to this size k_dem_pair_walls
 
     // Periodic boundaries (setPeriodicBoundary, DEMSolver.h:1944-1959): one
     // ghost set per active direction, passed in the reference's order X, Y,
@@ -1245,8 +1262,20 @@ struct DemScene {
                     bool ghostPass = false) {
         DemDev d = dev(false);
         const int n = N();
-        if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
-        else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        // small scenes without periodic ghosts: wall contacts in the pair kernel
+        const bool merged = walls && !hTris.empty() && n <= kMergedWallBalls && ghosts.empty();
+        if (merged) {
+            if (wallsMove || !haveWallRows) tri_grid();
+            wcur ^= 1;
+            d = dev(false);
+            if (precision == DEMSPH_PRECISION_FP64)
+                k_dem_pair_walls<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt, dtWall);
+            else
+                k_dem_pair_walls<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt, dtWall);
+        } else {
+            if (precision == DEMSPH_PRECISION_FP64) k_dem_pair_forces<double><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+            else k_dem_pair_forces<float><<<grid_for(n, 128), 128, 0, s>>>(d, dt);
+        }
         launch_count(1);
         if (ghostPass && !ghosts.empty()) ghost_passes(dt);
         if (d.nBond) {
@@ -1259,14 +1288,14 @@ struct DemScene {
             launch_count(1);
         }
         bool doWalls = walls && !hTris.empty();
-        if (doWalls) {
+        if (doWalls && !merged) {
             if (wallsMove || !haveWallRows) tri_grid();
             wcur ^= 1;
             d = dev(false);
-        } else {
+        } else if (!doWalls) {
             d.nTri = 0;
         }
-        if (doWalls) {
+        if (doWalls && !merged) {
             if (precision == DEMSPH_PRECISION_FP64) k_dem_walls<double><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall);
             else k_dem_walls<float><<<grid_for(n, 128), 128, 0, s>>>(d, dtWall);
             launch_count(1);
