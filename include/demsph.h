@@ -323,10 +323,11 @@ int demsph_sph_write_vtu(demsph_sph_t s, const char* dir, long frame, int what);
  * reorder, list build) only when some particle has drifted half the skin, and
  * its first momentum pass keeps the pairs that pass the reference's exact
  * cutoff test on that step's positions, so every step uses the reference's
- * pair set.  Default 0.05; 0 rebuilds exact lists every step.  Before
+ * pair set.  Default 0.04; 0 rebuilds exact lists every step.  Before
  * initialisation the value also sizes the grid's cells (2 h_max (1 +
- * fraction)); afterwards it may only be lowered.  Scenes with coupled balls
- * rebuild every step.  skin_stats: the fraction in use (0 when off) and the
+ * fraction)); afterwards it may only be lowered.  With coupled balls the
+ * fluid-marker rows are skin rows too, and a marker's drift joins the
+ * rebuild decision.  skin_stats: the fraction in use (0 when off) and the
  * rebuilds so far. */
 int demsph_sph_set_skin(demsph_sph_t s, double fraction);
 /* Autotunes the skin (and with it the share of steps that rebuild lists and

@@ -1456,8 +1456,8 @@ struct SphScene {
     // particle has drifted half the skin, and its first momentum pass keeps
     // the pairs within the exact cutoff.  The grid's cells are
     // 2 h_max (1 + skinMax) wide so that the 27-cell stencil covers the skin.
-    float skinMax = 0.05f;   // fraction of 2 h_max the grid allows (fixed at initialisation)
-    float skinFrac = 0.05f;  // fraction in use (0: exact lists every step)
+    float skinMax = 0.04f;   // fraction of 2 h_max the grid allows (fixed at initialisation)
+    float skinFrac = 0.04f;  // fraction in use (0: exact lists every step)
     double hmaxGrid = 0;
     DBuf<int> nbV, cntV, nbVD, cntVD;
     DBuf<double4> xb;
@@ -2635,7 +2635,7 @@ int demsph_sph_set_skin(demsph_sph_t h, double fraction) {
         SPH_CHECK(h);
         SphScene& s = h->sc;
         if (!(fraction >= 0) || fraction > 1.0) throw Status(DEMSPH_ERR_INVALID, "skin fraction must be in [0, 1]");
-        if (s.ready && fraction > s.skinMax)
+        if (s.ready && (float)fraction > s.skinMax)  // the grid's value is stored as FP32
             throw Status(DEMSPH_ERR_INVALID, "skin above the one the grid was built for");
         if (!s.ready) s.skinMax = (float)fraction;
         s.skinFrac = (float)fraction;
