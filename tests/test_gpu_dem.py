@@ -194,3 +194,51 @@ def test_launch_counter_moves(gpu):
     k0 = tsb.kernel_launches()
     s.step(5)
     assert tsb.kernel_launches() > k0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_wall_contacts_at_the_mesh_box_edge(gpu, oracle_lib, prec):
+    """Balls beside the edges and corners of a square plane wall, at
+    distances just inside and just outside their radius from it: those
+    within reach touch an edge or a vertex, the others are skipped before the
+    triangle walk by the mesh-box test.  Pair sets and states against the
+    oracle, which walks every triangle."""
+    r, L = 0.005, 0.1
+    d = np.array([0.5, 0.9, 0.999, 1.001, 1.5]) * r
+    corners = np.array([[L, L], [0, 0], [L, 0], [0, L]])
+    p = []
+    for k, e in enumerate(d):
+        y = 0.1 * L + 0.15 * L * k  # 15 mm apart along each edge: no two balls touch
+        p += [[L + e, y, 0.0], [-e, y + 0.05 * L, 0.0], [y, L + e, 0.0],  # beside three edges
+              [y + 0.02 * L, 0.5 * L, e], [y + 0.02 * L, 0.75 * L, -e]]   # above / below the face
+        if k < 4:  # beside a corner, outwards along its diagonal
+            c = corners[k]
+            out = np.sign(c - 0.5 * L)
+            p.append([c[0] + out[0] * e / np.sqrt(2), c[1] + out[1] * e / np.sqrt(2), 0.0])
+    p = np.array(p)
+    n = len(p)
+    rng = np.random.default_rng(2)
+    v = rng.uniform(-0.05, 0.05, size=(n, 3))
+    Es, Gs = scenes.hertz_params(1e8, 0.3)
+    verts = np.array([[0, 0, 0], [L, 0, 0], [L, L, 0], [0, L, 0]], float)
+    sc = scenes.DEMScene(name="box_edge", position=p, radius=np.full(n, r), density=np.full(n, 2500.0),
+                         material=np.zeros(n, np.int32), velocity=v,
+                         hertz=[(0, 0, Es, Gs, 0.8, 0.0, 0.0, 0.3, 0.0, 0.0)],
+                         walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0),
+                                     material=0)],
+                         minb=(-0.02, -0.02, -0.02), maxb=(L + 0.02, L + 0.02, 0.02), gravity=(0.0, 0.0, 0.0),
+                         dt=1e-5, steps=20)
+    o = oracle_dem(sc)
+    g = build_dem(sc, prec)
+    for k, steps in enumerate((1, sc.steps - 1)):
+        o.step(steps)
+        g.step(steps)
+        wo, wg = o.pairs(1), g.getPairs(1)
+        assert np.array_equal(np.sort(pair_keys(wg["objectPointed"], wg["objectPointing"])),
+                              np.sort(pair_keys(wo["a"], wo["b"])))
+        if k == 0:  # every ball within reach (18 of them) is a candidate after the first step
+            assert len({int(b) for b in wg["objectPointed"]}) >= 15
+    bo, bg = o.balls(), g.getBall()
+    e = rel_err(bg["velocity"], bo["vel"])
+    print(f"{prec}: {len(wg['objectPointed'])} wall pairs after {sc.steps} steps, velocity rel err {e:.2e}")
+    assert e < 1e3 * TOL[prec]
