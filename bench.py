@@ -359,17 +359,25 @@ def native(args, rank, world, dist):
         traffic = tj.get("k_sph_accel_bytes_per_launch")
         inst = tj.get("k_sph_accel_warp_instructions_per_launch")
 
-    # end to end through the public API: upload, K steps, read back
-    torch.cuda.synchronize()
-    h0 = time.perf_counter()
-    s2 = build_sph(sc, args.precision)
-    s2.step(args.steps)
-    out = s2.getSPH()
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - h0
+    # end to end through the public API: upload, K steps, read back.  Three
+    # complete runs (each scene destroyed after its read-back), the median
+    # reported: the first one also pays for mapping fresh device memory, which
+    # on a shared GPU has varied from 10 ms to 300 ms; the later ones reuse
+    # the memory the library's pool keeps (its default).
+    runs_s = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        s2 = build_sph(sc, args.precision)
+        s2.step(args.steps)
+        out = s2.getSPH()
+        torch.cuda.synchronize()
+        runs_s.append(time.perf_counter() - h0)
+        del s2
+        torch.cuda.synchronize()
+    e2e_s = sorted(runs_s)[1]
     h2d = (nf + nd) * (3 * 8 * 2 + 4 * 8)  # positions, velocities, 4 scalars per particle
     d2h = sum(v.nbytes for v in out.values()) + 16 * args.steps  # final state + per-step status word
-    del s2
     e2e = nf * args.steps * world / e2e_s
 
     # the other precision and the DEM workload, for reference next to the headline
@@ -417,7 +425,8 @@ def native(args, rank, world, dist):
         "clocks": clk,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
-                "what": "build scene from host arrays, initialise, K steps, read state back"},
+                "what": "build scene from host arrays, initialise, K steps, read state back; median of 3 runs",
+                "runs_s": runs_s, "first_run_value": nf * args.steps * world / runs_s[0]},
         "roofline": {"bound": "hbm", "kernel": "k_sph_accel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": mom_bytes, "ms_per_launch": mom_ms,
