@@ -157,7 +157,7 @@ def timed_steps(torch, solver, steps, flush):
 
 
 def dem_bounce(torch, steps, warmup, flush):
-    """The plain DEM bounce of BASELINE config 1: 4,096 Hertz-Mindlin spheres
+    """The plain DEM elastic bounce: 4,096 Hertz-Mindlin spheres
     (r 5 mm, rho 2500, 16^3 lattice at 12 mm, +-0.5 mm seeded jitter) dropping
     onto a 2-triangle plane, dt = 1e-5, mixed precision."""
     from this_studio_b200 import scenes
