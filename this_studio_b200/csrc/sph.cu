@@ -11,6 +11,8 @@
 //          and neighbour gathers stay in L1/L2.
 //   dummy  pos | vel | st (c,nu,rho0,-) | normal : double4, sorted once.
 //   lists  ELL, row-major: nb[i*K + k] = k-th neighbour of fluid i.
+#include <array>
+#include <map>
 #include <algorithm>
 #include <climits>
 #include <atomic>
@@ -1936,10 +1938,28 @@ struct SphScene {
                 time += 2 * dt;
             }
         }
+        // a single step (step(1), or the odd one): a one-step graph per
+        // ping-pong state, with the host's indices set to the state it leaves
+        for (; k < n && useGraphs; k++) {
+            const int key = index_key() | kOneStepKey;
+            StepGraph& gr = graph.at(key);
+            if (!gr.ready()) {
+                gr.capture(1, s, [&] { step_body(); });  // moves the host's indices on
+                oneStepAfter[key] = {P, Vv, S, R0, D, ID, L};
+            } else {
+                const auto& a = oneStepAfter.at(key);
+                P = a[0]; Vv = a[1]; S = a[2]; R0 = a[3]; D = a[4]; ID = a[5]; L = a[6];
+            }
+            gr.launch(s);
+            iStep += 1;
+            time += dt;
+        }
         for (; k < n; k++) step_once();
         DevStatus st2 = read_status();
         if (st2.overflow) grow(st2);
     }
+    static constexpr int kOneStepKey = 1 << 10;
+    std::map<int, std::array<int, 7>> oneStepAfter;  // one-step graph key -> indices after the step
 
     // ------------------------------------------------ coupled DEM balls ----
     // Samples balls[0..n) of the DEM scene (radii read from its device
