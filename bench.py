@@ -444,7 +444,89 @@ def native(args, rank, world, dist):
     }
     if rank == 0:
         line["cpu_baseline"] = cpu_baseline(sc)
+        if world == 1:
+            fl = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+            mine = {"sph": total_ms / args.steps, "dem": dem["ms_per_step"],
+                    "beam": beam_only(torch, min(args.steps, 20), fl) if args.stress else None}
+            line["reference_cuda"] = reference_cuda_baseline(torch, sc, min(args.steps, 50), args.warmup, fl, mine)
+            del fl
     return line
+
+
+def _event_steps(torch, fn, steps, block, flush):
+    """Mean ms per step of `steps` steps run `block` at a time, each block
+    bracketed by CUDA events on the current stream, L2 flushed before it."""
+    times = []
+    torch.cuda.synchronize()
+    for _ in range(max(1, steps // block)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn(block)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(sum(times)) / (len(times) * block)
+
+
+def reference_cuda_baseline(torch, sc, steps, warmup, flush, mine_ms):
+    """Baseline leg: the reference's own CUDA kernels (DEMSPH/kernel/*.cu built
+    from its sources for sm_100a with its Release flags, oracle/Makefile.ref)
+    driven as its solvers drive them (oracle/ref_harness: WCSPHSolver::solve's
+    step, DEMSolver's loop_ball_wall), FP64 as the reference computes, on the
+    same workloads as this library's lines, same L2 flush, CUDA events.  The
+    reference reads its pair counts back to the host in every neighbour
+    search, as its solvers do; that is part of its step.  DEM rows: the
+    4,096-sphere bounce and the bonded beam without the clumps (the
+    reference's clump force gather reads past its clump array,
+    ballIntegrationKernel.cu:20, so clumps are not run on it)."""
+    from oracle import ref_harness
+    from this_studio_b200 import scenes
+
+    if not ref_harness.available():
+        return {"unavailable": "oracle/_ref/libdemsph_ref.so not built (no reference checkout at build time)"}
+    out = {"what": "the reference's CUDA kernels built from its sources (sm_100a, -O3), FP64, its launch geometry"}
+    r = ref_harness.RefSPH(sc, torch)
+    r.step(max(warmup, 3))
+    ms = _event_steps(torch, r.step, steps, 1, flush)
+    nf = sc.fluid.shape[0]
+    out["sph"] = {"workload": WORKLOAD, "ms_per_step": ms, "value": nf / (ms / 1e3), "unit": METRIC,
+                  "this_library_ms_per_step": mine_ms["sph"], "speedup": ms / mine_ms["sph"]}
+    del r
+    dem = scenes.dem_drop()
+    r = ref_harness.RefDEM(dem, torch)
+    r.initialize()
+    r.step(max(warmup, 5))
+    ms = _event_steps(torch, r.step, min(steps * 5, 200), 10, flush)
+    out["dem_bounce"] = {"workload": "dem_bounce_4096", "ms_per_step": ms, "value": 4096 / (ms / 1e3),
+                         "unit": METRIC, "this_library_ms_per_step": mine_ms["dem"],
+                         "speedup": ms / mine_ms["dem"]}
+    del r
+    if mine_ms.get("beam") is not None:
+        beam = scenes.bonded_beam_clumps(n_clumps=0)
+        r = ref_harness.RefDEM(beam, torch)
+        r.initialize()
+        r.step(5)
+        ms = _event_steps(torch, r.step, min(steps, 20), 5, flush)
+        nmov = int((~beam.fixed).sum())
+        out["bonded_beam"] = {"workload": "bonded_beam_160k", "ms_per_step": ms, "value": nmov / (ms / 1e3),
+                              "unit": METRIC, "bonds": r.nb, "this_library_ms_per_step": mine_ms["beam"],
+                              "speedup": ms / mine_ms["beam"]}
+        del r
+    torch.cuda.empty_cache()
+    return out
+
+
+def beam_only(torch, steps, flush):
+    """The bonded beam of the beam + clumps scene alone (160,000 spheres, the
+    x = 0 layer clamped, 462,840 bonds), the workload the reference's own
+    kernels are timed on; mixed precision."""
+    from this_studio_b200 import scenes
+
+    sc = scenes.bonded_beam_clumps(n_clumps=0)
+    s = scenes.build_dem(sc, "mixed")
+    s.step(5)
+    return _event_steps(torch, s.step, steps, 5, flush)
 
 
 def cpu_baseline(sc, steps=2):

@@ -31,6 +31,11 @@
 
 #include <stddef.h>
 
+/* CUDA's stream handle (cudaStream_t is struct CUstream_st*) and double3,
+ * named without including the CUDA headers */
+struct CUstream_st;
+struct double3;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -68,6 +73,15 @@ long long demsph_kernel_launches(void);
  * behaviour), and a limit set here is never overridden.  Affects only this
  * process. */
 int demsph_retain_device_memory(unsigned long long bytes);
+/* No counterpart in the reference (its HostDeviceArray1D calls the CUDA
+ * runtime directly, myHostDeviceArray.h:99-186).  Device memory for callers
+ * that do not link the CUDA runtime themselves, such as the header-only C++
+ * facade's HostDeviceArray1D: stream-ordered allocation from the current
+ * device's default pool, its release, and a copy (kind 0 host to device, 1
+ * device to host, 2 device to device) that returns once the copy is done. */
+int demsph_device_alloc(void** ptr, size_t bytes, void* stream);
+int demsph_device_free(void* ptr, void* stream);
+int demsph_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
 
 /* ======================================================================= */
 /* DEM: spheres, clumps, triangle-mesh walls, contact + parallel bonds      */
@@ -126,6 +140,46 @@ int demsph_dem_set_global_damping(demsph_dem_t s, double dampingCoefficient);
 int demsph_dem_set_buoyancy_drag(demsph_dem_t s, double fluidDensity, double dragCoefficient, const double* gravity,
                                  const double* fluidVelocity, double waterLevel);
 
+/* DEMSolver::addExternalForceTorque (virtual, DEMSolver.h:1372), as a
+ * callback: when set, every force evaluation of a step (two per step, the
+ * reference's calls at DEMSolver.h:1464,1470 and in the periodic loops)
+ * calls fn(user, iStep, time) after the contact, bond and wall forces and
+ * the configured hooks above are summed, and before the half-step
+ * integration; iStep is 1-based and time is t - dt/2, then t, as in the
+ * reference.  Around the call the ball state sits in arrays of the
+ * reference's layout (demsph_dem_hook_arrays); whatever the callback's
+ * kernels write there (force and torque, or also position, velocity,
+ * angular velocity, radius, inverse mass) is taken back before the
+ * integration.  The callback's device work must be ordered on the scene's
+ * stream or on the legacy default stream (stream 0), as the reference's
+ * hooks launch on stream 0.  It runs on the host thread that called
+ * demsph_dem_step; it may call demsph_dem_hook_arrays, demsph_dem_num_balls
+ * and demsph_dem_set_external_hook (to remove itself) but no other function
+ * of this scene.  A scene with a callback
+ * launches every kernel directly (no CUDA graphs), and steps replayed after
+ * a list overflow call it again.  fn = NULL removes it.
+ *
+ * demsph_dem_hook_arrays: device pointers to those arrays (3 doubles per
+ * ball for position, velocity, angularVelocity, force, torque; one double per
+ * ball for radius and inverseMass; the scene's int materialID and clumpID;
+ * n balls), allocated on first request.  Their contents are current only
+ * while a callback runs. */
+typedef void (*demsph_dem_hook_fn)(void* user, long iStep, double time);
+typedef struct demsph_ball_arrays {
+    double* position;
+    double* velocity;
+    double* angularVelocity;
+    double* force;
+    double* torque;
+    double* radius;
+    double* inverseMass;
+    int* materialID;
+    int* clumpID;
+    long n;
+} demsph_ball_arrays;
+int demsph_dem_set_external_hook(demsph_dem_t s, demsph_dem_hook_fn fn, void* user);
+int demsph_dem_hook_arrays(demsph_dem_t s, demsph_ball_arrays* out);
+
 /* The initialisation part of DEMSolver::solve (DEMSolver.h:1961-1997):
  * upload, grids (cell = 2 r_max; triangle cell >= 2 circumradius),
  * neighbour search, one force evaluation with dt = 0.  precision is
@@ -157,11 +211,22 @@ int demsph_dem_set_graphs(demsph_dem_t s, int enable);
 /* Protected step pieces of DEMSolver, exposed for parity checks:
  * neighborSearch (DEMSolver.h:698-777) and calculateBallContactForceTorque
  * (:599-695) followed, when walls & 1, by addTriangleContactForceTorque(dtWall)
- * (:428-597) and, when walls & 2, by the periodic ghost passes
- * addDummyContactForceTorque(dt) (:279-426). */
+ * (:428-597), when walls & 2, by the periodic ghost passes
+ * addDummyContactForceTorque(dt) (:279-426), and when walls & 4, by the
+ * external forces (the configured hooks and a callback) at the scene's
+ * current time, as addExternalForceTorque (:1372) after a force evaluation. */
 int demsph_dem_neighbor_search(demsph_dem_t s);
 int demsph_dem_eval_forces(demsph_dem_t s, double dt, int walls, double dtWall);
 
+/* No counterpart in the reference (which has no diagnostics).  FP64
+ * conservation diagnostics of the current state, summed on the device in a
+ * fixed order (the same bits for the same state), 12 doubles: linear
+ * momentum (3), angular momentum about the origin (3, x cross m v plus I w),
+ * translational and rotational kinetic energy, mass -- over the moving
+ * bodies (free spheres and clumps; pebbles count through their clump) --
+ * and the sum of the ball forces of the last force evaluation (3; contact
+ * and bond forces cancel pairwise). */
+int demsph_dem_diagnostics(demsph_dem_t s, double* out);
 int demsph_dem_num_balls(demsph_dem_t s, long* n);
 int demsph_dem_num_pairs(demsph_dem_t s, int which /*0 ball-ball, 1 ball-triangle*/, long* n);
 int demsph_dem_num_bonds(demsph_dem_t s, long* n);
@@ -217,6 +282,14 @@ int demsph_dem_assemble_balls(demsph_dem_t s, int count, const demsph_dem_member
 int demsph_dem_get_bonds(demsph_dem_t s, int* objectPointed, int* objectPointing, int* isBonded, double* normalForce,
                          double* torsionTorque, double* shearForce, double* bendingTorque, double* normal,
                          double* point);
+/* Writes the bond state, in the order demsph_dem_get_bonds returns it (n =
+ * the number of bonds); any array may be NULL to keep that field.  No
+ * counterpart in the reference, whose bond arrays callers write through
+ * getBondedInteraction() (DEMSolver.h:1547): used to start a force
+ * evaluation from a given bond state. */
+int demsph_dem_set_bonds(demsph_dem_t s, long n, const int* isBonded, const double* normalForce,
+                         const double* torsionTorque, const double* shearForce, const double* bendingTorque,
+                         const double* normal, const double* point);
 /* getClump (DEMSolver.h:1543) */
 /* outputBallVTU / outputMeshWallVTU / outputBallInteractionVTU /
  * outputBondedInteractionVTU / outputBallTriangleInteractionVTU
@@ -337,6 +410,11 @@ int demsph_sph_set_skin(demsph_sph_t s, double fraction);
 int demsph_sph_tune_skin(demsph_sph_t s, int steps, double* chosen, double* msPerStep);
 int demsph_sph_skin_stats(demsph_sph_t s, double* fraction, long* rebuilds);
 
+/* No counterpart in the reference.  FP64 conservation diagnostics of the
+ * fluid, summed on the device in a fixed order, 8 doubles: mass, momentum
+ * (3), kinetic energy, potential energy -sum m g.x, sum of the density
+ * changes Delta rho, volume sum m / rho. */
+int demsph_sph_diagnostics(demsph_sph_t s, double* out);
 int demsph_sph_num(demsph_sph_t s, int dummy, long* n);
 int demsph_sph_num_pairs(demsph_sph_t s, int which /*0 fluid-fluid, 1 fluid-dummy, 2 dummy-dummy*/, long* n);
 int demsph_sph_step_index(demsph_sph_t s, long* step, double* time);
@@ -417,13 +495,36 @@ void buildPrefixSum(int* prefixSum, int* count, const size_t size, struct CUstre
  * where a cudaMalloc (which may synchronise the device, or fail under memory
  * pressure) is not allowed.  It calls no allocator: its scratch is a fixed
  * array inside the library, sized for DEMSPH_NOALLOC_MAX_KEYS keys (3.3 MB,
- * held on every GPU that loads the library until the process exits).  The
- * first call on a device looks up that array's device address; make that
- * first call before any stream capture.  All calls share the one array, so
+ * held on every GPU that loads the library until the process exits).  Each
+ * call looks up that array's device address on the current device; the
+ * first lookup on a device may load the library's module, so make the first
+ * call on a device before any stream capture.  All calls share the one array, so
  * calls that overlap on the GPU (other streams, other host threads) race;
  * calls ordered on one stream are safe.  Returns DEMSPH_OK,
  * DEMSPH_ERR_INVALID when hashListSize > DEMSPH_NOALLOC_MAX_KEYS (with a
  * message in demsph_last_error), or DEMSPH_ERR_CUDA. */
+/* The reference's user-force launchers with its exact signatures
+ * (DEMSPH/externalForceTorque.h:6-36; `struct double3` is CUDA's double3):
+ * on ball arrays of the reference's layout, such as those an external-force
+ * callback receives (demsph_dem_hook_arrays).  They return void like the
+ * reference; a failure is recorded for demsph_last_error().  gridD / blockD
+ * are ignored.
+ * launchAddConstantForce: force[i] += force_external[i] (externalForceTorque.cu:4-24).
+ * launchAddGlobalDampingForceTorque: force[i] -= c |force[i]| v_i / |v_i|,
+ *   torque[i] -= c |torque[i]| w_i / |w_i| (:26-57).
+ * launchAddBuoyancyDrag: buoyancy of the part of each ball below the plane
+ *   z = waterLevel plus quadratic drag against fluidVelocity; balls with
+ *   inverseMass <= 0 are skipped (:59-160). */
+void launchAddConstantForce(struct double3* force, const struct double3* force_external, const size_t num,
+                            const size_t gridD, const size_t blockD, struct CUstream_st* stream);
+void launchAddGlobalDampingForceTorque(struct double3* force, struct double3* torque, const struct double3* velocity,
+                                       const struct double3* angularVelocity, const double dampCoeff, const size_t num,
+                                       const size_t gridD, const size_t blockD, struct CUstream_st* stream);
+void launchAddBuoyancyDrag(struct double3* force, struct double3* position, struct double3* velocity, double* radius,
+                           double* inverseMass, const double rhoFluid, const double Cd, const struct double3 gravity,
+                           const struct double3 fluidVelocity, const double waterLevel, const size_t numBall,
+                           const size_t gridD, const size_t blockD, struct CUstream_st* stream);
+
 #define DEMSPH_NOALLOC_MAX_KEYS 262144
 int demsph_build_hash_start_end_noalloc(int* start, int* end, int* hashIndex, int* hashValue, size_t startEndSize,
                                         size_t hashListSize, struct CUstream_st* stream);

@@ -2,18 +2,25 @@
 // and method names (DEMSolver, DEMSPH/kernel/DEMSolver.h:144-2078;
 // WCSPHSolver, DEMSPH/kernel/WCSPHSolver.h:18-635), header-only.
 //
-// Differences from the reference: failures throw demsph::Error instead of
-// exiting; the virtual hooks are configuration
-// (setConstantForce / setGlobalDamping / setBuoyancyDrag, and
-// addBondedInteraction after initialize() for bonded initial contacts).
+// The reference's virtual hooks are virtual here too: a subclass overriding
+// addExternalForceTorque(iStep, time) has it called after each force
+// evaluation of a step (DEMSolver.h:1372, called at :1464,1470), with
+// getBall() giving the ball arrays in the reference's layout for the
+// reference's launchers (launchAddConstantForce and the others, declared in
+// demsph.h); addInitialCondition() is called once after initialisation
+// (DEMSolver.h:1998).  The same forces can also be configured without a
+// subclass (setConstantForce / setGlobalDamping / setBuoyancyDrag).
+// Failures throw demsph::Error instead of exiting.
 #pragma once
 #include <driver_types.h>
 #include <vector_functions.h>
 #include <vector_types.h>
 
 #include <array>
+#include <exception>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../demsph.h"
@@ -60,10 +67,129 @@ inline void runFrames(long total, size_t numFrame, Step step, Write write) {
     }
 }
 
+// A device array with a host staging copy, as the reference's
+// HostDeviceArray1D (myHostDeviceArray.h:99-186) that hook code uses to pass
+// its own per-ball data to a launcher: setHost / pushHost, then
+// copyHostToDevice, then d_ptr on the device.  Memory comes from the
+// library (stream-ordered allocation), so no CUDA runtime link is needed.
+template <class T>
+class HostDeviceArray1D {
+public:
+    T* d_ptr = nullptr;
+
+    HostDeviceArray1D() = default;
+    ~HostDeviceArray1D() { release(); }
+    HostDeviceArray1D(const HostDeviceArray1D&) = delete;
+    HostDeviceArray1D& operator=(const HostDeviceArray1D&) = delete;
+    HostDeviceArray1D(HostDeviceArray1D&& o) noexcept { *this = std::move(o); }
+    HostDeviceArray1D& operator=(HostDeviceArray1D&& o) noexcept {
+        if (this != &o) {
+            release();
+            d_ptr = o.d_ptr; n_ = o.n_; s_ = o.s_; host_ = std::move(o.host_);
+            o.d_ptr = nullptr; o.n_ = 0;
+        }
+        return *this;
+    }
+
+    size_t hostSize() const { return host_.size(); }
+    size_t deviceSize() const { return n_; }
+    void setHost(const std::vector<T>& h) { host_ = h; }
+    void pushHost(const T& v) { host_.push_back(v); }
+    const std::vector<T>& hostRef() const { return host_; }
+    void allocateDevice(size_t n, cudaStream_t s, bool zeroFill = true) {
+        release();
+        s_ = s;
+        check(demsph_device_alloc((void**)&d_ptr, n * sizeof(T), (void*)s), "HostDeviceArray1D::allocateDevice");
+        n_ = n;
+        if (zeroFill && n) {
+            std::vector<T> z(n, T{});
+            check(demsph_memcpy(d_ptr, z.data(), n * sizeof(T), 0, (void*)s), "HostDeviceArray1D::allocateDevice");
+        }
+    }
+    void copyHostToDevice(cudaStream_t s) {
+        if (n_ != host_.size()) allocateDevice(host_.size(), s, false);
+        if (n_) check(demsph_memcpy(d_ptr, host_.data(), n_ * sizeof(T), 0, (void*)s), "copyHostToDevice");
+    }
+    void copyDeviceToHost(cudaStream_t s) {
+        host_.resize(n_);
+        if (n_) check(demsph_memcpy(host_.data(), d_ptr, n_ * sizeof(T), 1, (void*)s), "copyDeviceToHost");
+    }
+    std::vector<T> getHostCopy() {
+        copyDeviceToHost(s_);
+        return host_;
+    }
+
+private:
+    void release() {
+        if (d_ptr) demsph_device_free(d_ptr, (void*)s_);
+        d_ptr = nullptr;
+        n_ = 0;
+    }
+    size_t n_ = 0;
+    cudaStream_t s_ = nullptr;
+    std::vector<T> host_;
+};
+
+// What DEMSolver::getBall() returns (the reference's ball_, particle.h):
+// device pointers to the ball arrays in the reference's layout, current
+// while addExternalForceTorque runs, the launch geometry of the reference
+// (blockDim = min(maximumThread, n), gridDim to cover n), and host copies.
+class BallArrays {
+public:
+    explicit BallArrays(demsph_dem_t h) : h_(h) {}
+    double3* position() { return (double3*)arrays().position; }
+    double3* velocity() { return (double3*)arrays().velocity; }
+    double3* angularVelocity() { return (double3*)arrays().angularVelocity; }
+    double3* force() { return (double3*)arrays().force; }
+    double3* torque() { return (double3*)arrays().torque; }
+    double* radius() { return arrays().radius; }
+    double* inverseMass() { return arrays().inverseMass; }
+    int* materialID() { return arrays().materialID; }
+    int* clumpID() { return arrays().clumpID; }
+    size_t deviceSize() const {
+        long n = 0;
+        check(demsph_dem_num_balls(h_, &n), "getBall");
+        return (size_t)n;
+    }
+    size_t hostSize() const { return deviceSize(); }
+    size_t blockDim() const {
+        size_t n = deviceSize();
+        size_t b = n < maxThread_ ? n : maxThread_;
+        return b ? b : 1;
+    }
+    size_t gridDim() const { return (deviceSize() + blockDim() - 1) / blockDim(); }
+    std::vector<double3> positionHostCopy() { return copy(0); }
+    std::vector<double3> velocityHostCopy() { return copy(1); }
+    std::vector<double3> angularVelocityHostCopy() { return copy(2); }
+    std::vector<double3> forceHostCopy() { return copy(3); }
+    std::vector<double3> torqueHostCopy() { return copy(4); }
+    size_t maxThread_ = 256;
+
+private:
+    demsph_ball_arrays arrays() {
+        demsph_ball_arrays a{};
+        check(demsph_dem_hook_arrays(h_, &a), "getBall");
+        return a;
+    }
+    std::vector<double3> copy(int which) {
+        std::vector<double3> v(deviceSize());
+        double* p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        if (!v.empty()) {
+            p[which] = &v[0].x;
+            check(demsph_dem_get_balls(h_, p[0], p[1], p[2], p[3], p[4]), "getBall");
+        }
+        return v;
+    }
+    demsph_dem_t h_;
+};
+
 class DEMSolver {
 public:
-    explicit DEMSolver(cudaStream_t s = nullptr) { check(demsph_dem_create(&h_, (void*)s), "DEMSolver"); }
-    ~DEMSolver() { demsph_dem_destroy(h_); }
+    explicit DEMSolver(cudaStream_t s = nullptr) {
+        check(demsph_dem_create(&h_, (void*)s), "DEMSolver");
+        ball_ = BallArrays(h_);
+    }
+    virtual ~DEMSolver() { demsph_dem_destroy(h_); }
     DEMSolver(const DEMSolver&) = delete;
     DEMSolver& operator=(const DEMSolver&) = delete;
 
@@ -120,15 +246,29 @@ public:
     void setBuoyancyDrag(double rho, double Cd, double3 g, double3 u, double level) {
         check(demsph_dem_set_buoyancy_drag(h_, rho, Cd, &g.x, &u.x, level), "setBuoyancyDrag");
     }
-    void initialize(double3 mn, double3 mx, double3 g, double dt, int precision = DEMSPH_PRECISION_MIXED) {
+    // The precision solve() initialises with (DEMSPH_PRECISION_*; mixed by default).
+    void setPrecision(int precision) { precision_ = precision; }
+    void initialize(double3 mn, double3 mx, double3 g, double dt, int precision) {
         check(demsph_dem_initialize(h_, &mn.x, &mx.x, &g.x, dt, precision), "initialize");
     }
-    void step(long n) { check(demsph_dem_step(h_, n), "step"); }
-    // DEMSolver::solve (DEMSolver.h:1961-2049); VTU frames in `dir` (none when empty).
+    void initialize(double3 mn, double3 mx, double3 g, double dt) { initialize(mn, mx, g, dt, precision_); }
+    void step(long n) {
+        const int rc = demsph_dem_step(h_, n);
+        rethrowHookError();
+        check(rc, "step");
+    }
+    // DEMSolver::solve (DEMSolver.h:1961-2049): initialisation (upload,
+    // grids, neighbour search, one force evaluation with dt = 0), then
+    // addInitialCondition(), then the step loop with addExternalForceTorque
+    // after each force evaluation; VTU frames in `dir` on the reference's
+    // cadence (none when `dir` is empty).
     void solve(double3 mn, double3 mx, double3 g, double dt, double maximumTime, size_t numFrame,
                const std::string& dir, size_t deviceID = 0, size_t maximumThread = 256) {
-        (void)deviceID; (void)maximumThread;
+        (void)deviceID;
+        ball_.maxThread_ = maximumThread ? maximumThread : 256;
         initialize(mn, mx, g, dt);
+        addInitialCondition();
+        check(demsph_dem_set_external_hook(h_, &DEMSolver::hookTrampoline, this), "solve");
         const long total = solveSteps(dt, maximumTime);
         if (dir.empty()) {
             step(total);
@@ -139,6 +279,8 @@ public:
         runFrames(total, numFrame, [&](long n) { step(n); },
                   [&](long f) { check(demsph_dem_write_vtu(h_, dir.c_str(), f, what), "writeVTU"); });
     }
+    // ball_ (DEMSolver::getBall, DEMSolver.h:1541)
+    BallArrays& getBall() { return ball_; }
     std::vector<double3> getBallPosition() {
         std::vector<double3> p(numBalls_);
         check(demsph_dem_get_balls(h_, &p[0].x, nullptr, nullptr, nullptr, nullptr), "getBall");
@@ -148,7 +290,38 @@ public:
     std::vector<int> getBallPairPointing() { return pairs(0).second; }
     demsph_dem_t handle() { return h_; }
 
+protected:
+    // DEMSolver::addExternalForceTorque (virtual, DEMSolver.h:1372): called
+    // after each force evaluation of a step, at time t - dt/2 and t.  This
+    // default adds nothing and takes the callback away, so a solver that
+    // does not override it steps as one without hooks (CUDA graphs on).
+    virtual void addExternalForceTorque(const size_t iStep, const double time) {
+        (void)iStep;
+        (void)time;
+        demsph_dem_set_external_hook(h_, nullptr, nullptr);
+    }
+    // DEMSolver::addInitialCondition (virtual, DEMSolver.h:1536), called once
+    // after initialisation; returns whether it changed the scene.
+    virtual bool addInitialCondition() { return false; }
+
 private:
+    static void hookTrampoline(void* self, long iStep, double time) {
+        DEMSolver* s = static_cast<DEMSolver*>(self);
+        if (s->hookError_) return;
+        try {
+            s->addExternalForceTorque((size_t)iStep, time);
+        } catch (...) {
+            s->hookError_ = std::current_exception();
+            demsph_dem_set_external_hook(s->h_, nullptr, nullptr);
+        }
+    }
+    void rethrowHookError() {
+        if (hookError_) {
+            std::exception_ptr e = hookError_;
+            hookError_ = nullptr;
+            std::rethrow_exception(e);
+        }
+    }
     std::pair<std::vector<int>, std::vector<int>> pairs(int which) {
         long n = 0;
         check(demsph_dem_num_pairs(h_, which, &n), "numPairs");
@@ -158,6 +331,9 @@ private:
         return {a, b};
     }
     demsph_dem_t h_ = nullptr;
+    BallArrays ball_{nullptr};
+    std::exception_ptr hookError_;
+    int precision_ = DEMSPH_PRECISION_MIXED;
     long numBalls_ = 0;
     int walls_ = 0;
 };
@@ -165,7 +341,7 @@ private:
 class WCSPHSolver {
 public:
     explicit WCSPHSolver(cudaStream_t s = nullptr) { check(demsph_sph_create(&h_, (void*)s), "WCSPHSolver"); }
-    ~WCSPHSolver() { demsph_sph_destroy(h_); }
+    virtual ~WCSPHSolver() { demsph_sph_destroy(h_); }
     WCSPHSolver(const WCSPHSolver&) = delete;
     WCSPHSolver& operator=(const WCSPHSolver&) = delete;
 

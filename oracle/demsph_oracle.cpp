@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <unordered_set>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1561,13 +1562,15 @@ void oracle_dem_set_wall_motion(void* h, int wall, const double* vel, const doub
 // DEMSolver.h:93-135 (bondedInteraction::add)
 void oracle_dem_add_bonds(void* h, long n, const int* a0, const int* b0, const double* posHost, long npos) {
     DEM& s = *(DEM*)h;
+    // bondedInteraction::add (DEMSolver.h:93-135) skips a pair that is already
+    // bonded; its linear search is a set lookup here (same result)
+    std::unordered_set<long long> have;
+    for (size_t j = 0; j < s.bA.size(); j++) have.insert(((long long)s.bA[j] << 32) | (unsigned)s.bB[j]);
     for (long k = 0; k < n; k++) {
         int i0 = a0[k], i1 = b0[k];
         if (i0 < 0 || i1 < 0 || i0 >= npos || i1 >= npos || i0 == i1) continue;
         int a = std::min(i0, i1), b = std::max(i0, i1);
-        bool found = false;
-        for (size_t j = 0; j < s.bA.size(); j++) if (s.bA[j] == a && s.bB[j] == b) { found = true; break; }
-        if (found) continue;
+        if (!have.insert(((long long)a << 32) | (unsigned)b).second) continue;
         V3 pa = ld3(posHost, a), pb = ld3(posHost, b);
         s.bA.push_back(a); s.bB.push_back(b); s.bOk.push_back(1);
         s.bPoint.push_back(0.5 * (pa + pb)); s.bNormal.push_back(normalize(pa - pb));

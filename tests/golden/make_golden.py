@@ -80,4 +80,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: first argument, else DEMSPH_REFERENCE, else
+    # where it is mounted in the build container
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEMSPH_REFERENCE", "/root/reference"))

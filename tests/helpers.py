@@ -60,6 +60,17 @@ def rel_err(x, ref):
     return d / n if n > 0 else d
 
 
+def torque_err(T, T64, F64, radius):
+    """||T - T64|| / max(||T64||, ||F64|| * mean radius): the torque error
+    measured against the larger of the torque itself and the torque scale of
+    the forces (force times lever arm), so that torques that vanish to
+    rounding (a sphere pressed straight onto a plane) are not divided by
+    their own rounding noise."""
+    scale = max(np.linalg.norm(T64), np.linalg.norm(F64) * float(np.mean(radius)))
+    d = np.linalg.norm(np.asarray(T) - np.asarray(T64))
+    return d / scale if scale > 0 else d
+
+
 def oracle_coupled(scene):
     """(OracleSPH, OracleDEM) of a CoupledScene with its balls coupled."""
     f = oracle_sph(scene.sph)

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared():
     hdr = open(os.path.join(ROOT, "include", "demsph.h")).read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
-    return sorted(set(re.findall(r"\b(demsph_\w+|buildHashStartEnd|buildPrefixSum)\s*\(", hdr)))
+    return sorted(set(re.findall(r"\b(demsph_\w+|buildHashStartEnd|buildPrefixSum|launchAdd\w+)\s*\(", hdr)))
 
 
 def test_library_exports_every_declared_symbol():

@@ -68,8 +68,11 @@ def test_one_coupled_step_matches_oracle(gpu, oracle_lib, prec, tol):
         assert e < tol
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 2e-4)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
 def test_coupled_trajectory_matches_oracle(gpu, oracle_lib, prec, tol):
+    """Twenty coupled steps: displacements, ball velocities and the last
+    step's force on the balls within the target's 1e-5 (mixed) of the FP64
+    oracle."""
     sc = _scene()
     o_f, o_d, g_f, g_d, cpl = _pair(sc, prec)
     o_f.couple_step(o_d, 20, sc.dem_substeps)
@@ -85,7 +88,7 @@ def test_coupled_trajectory_matches_oracle(gpu, oracle_lib, prec, tol):
     ef = rel_err(Fg, Fo)
     print(f"{prec}, 20 coupled steps: fluid displacement {ep:.2e} ball displacement {ebp:.2e} "
           f"ball vel {ebv:.2e} force {ef:.2e}")
-    assert ep < tol and ebp < tol and ebv < tol and ef < 10 * tol
+    assert ep < tol and ebp < tol and ebv < tol and ef < tol
 
 
 def test_fluid_steps_alone_keep_markers(gpu, oracle_lib):

@@ -56,7 +56,8 @@ def test_accel_from_identical_state(gpu, oracle_lib, dam, prec):
     gvec = np.array(dam.gravity)
     ei = rel_err(ag - gvec, ao - gvec)
     print(f"{prec}: accel rel err {e:.3e} (interaction part {ei:.3e})")
-    assert e < (1e-11 if prec == "fp64" else 2e-4)
+    tol = 1e-11 if prec == "fp64" else 1e-5  # mixed: the target's relative force error
+    assert e < tol and ei < tol
 
 
 def test_short_trajectory_vs_oracle(gpu, oracle_lib, dam):

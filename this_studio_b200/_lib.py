@@ -31,8 +31,38 @@ _int = C.c_int
 _dbl = C.c_double
 _long = C.c_long
 
+
+class Double3(C.Structure):
+    """CUDA's double3, passed by value."""
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class BallArrays(C.Structure):
+    """demsph_ball_arrays: device pointers to the ball arrays in the
+    reference's layout, filled by demsph_dem_hook_arrays."""
+    _fields_ = [("position", C.c_void_p), ("velocity", C.c_void_p), ("angularVelocity", C.c_void_p),
+                ("force", C.c_void_p), ("torque", C.c_void_p), ("radius", C.c_void_p),
+                ("inverseMass", C.c_void_p), ("materialID", C.c_void_p), ("clumpID", C.c_void_p),
+                ("n", C.c_long)]
+
+
+# demsph_dem_hook_fn: void (*)(void* user, long iStep, double time)
+HOOK_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_long, C.c_double)
+_sz = C.c_size_t
+
 # name -> argument types (all return int unless listed in _RESTYPE)
 SIGNATURES = {
+    "demsph_device_alloc": [_pvp, _sz, _vp],
+    "demsph_device_free": [_vp, _vp],
+    "demsph_memcpy": [_vp, _vp, _sz, _int, _vp],
+    "demsph_dem_set_external_hook": [_vp, HOOK_FN, _vp],
+    "demsph_dem_hook_arrays": [_vp, C.POINTER(BallArrays)],
+    "demsph_dem_set_bonds": [_vp, _long, _i, _d, _d, _d, _d, _d, _d],
+    "demsph_dem_diagnostics": [_vp, _d],
+    "demsph_sph_diagnostics": [_vp, _d],
+    "launchAddConstantForce": [_vp, _vp, _sz, _sz, _sz, _vp],
+    "launchAddGlobalDampingForceTorque": [_vp, _vp, _vp, _vp, _dbl, _sz, _sz, _sz, _vp],
+    "launchAddBuoyancyDrag": [_vp, _vp, _vp, _vp, _vp, _dbl, _dbl, Double3, Double3, _dbl, _sz, _sz, _sz, _vp],
     "demsph_last_error": [],
     "demsph_version": [],
     "demsph_kernel_launches": [],
@@ -123,6 +153,9 @@ _RESTYPE = {
     "demsph_kernel_launches": C.c_longlong,
     "buildHashStartEnd": None,
     "buildPrefixSum": None,
+    "launchAddConstantForce": None,
+    "launchAddGlobalDampingForceTorque": None,
+    "launchAddBuoyancyDrag": None,
 }
 
 _lib = None

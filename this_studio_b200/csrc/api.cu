@@ -60,4 +60,31 @@ int demsph_retain_device_memory(unsigned long long bytes) {
     });
 }
 
+int demsph_device_alloc(void** ptr, size_t bytes, void* stream) {
+    return demsph::guarded([&] {
+        if (!ptr) throw demsph::Status(DEMSPH_ERR_INVALID, "null output pointer");
+        *ptr = nullptr;
+        if (bytes == 0) return;
+        DEMSPH_CUDA(cudaMallocAsync(ptr, bytes, (cudaStream_t)stream));
+    });
+}
+
+int demsph_device_free(void* ptr, void* stream) {
+    return demsph::guarded([&] {
+        if (ptr) DEMSPH_CUDA(cudaFreeAsync(ptr, (cudaStream_t)stream));
+    });
+}
+
+int demsph_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+    return demsph::guarded([&] {
+        if (bytes == 0) return;
+        if (!dst || !src) throw demsph::Status(DEMSPH_ERR_INVALID, "null pointer");
+        cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice
+                                     : (kind == 1 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+        if (kind < 0 || kind > 2) throw demsph::Status(DEMSPH_ERR_INVALID, "memcpy kind must be 0, 1 or 2");
+        DEMSPH_CUDA(cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream));
+        DEMSPH_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    });
+}
+
 }  // extern "C"

@@ -14,7 +14,6 @@
 // for demsph_last_error().
 #include <atomic>
 #include <climits>
-#include <mutex>
 
 #include "radix.cuh"
 
@@ -71,22 +70,16 @@ void hash_sort_start_end(int* start, int* end, int* hashIndex, int* hashValue, i
 // calls that overlap on the GPU share it and race.
 static __device__ __align__(256) int g_hash_sort_scratch[hash_sort_scratch_words(DEMSPH_NOALLOC_MAX_KEYS)];
 
-// Device address of the array for the current device, looked up once per
-// device on the first call (host code cannot use the symbol itself).
+// Device address of the array on the current device.  Host code cannot use
+// the symbol itself (in host code it names a host-side stand-in), so the
+// address is looked up on every call: the lookup is cheap after the first
+// one on a device (which may load the module), and a cached pointer would go
+// stale if the device's primary context were reset and the module reloaded.
 static int* noalloc_scratch() {
-    static std::mutex mu;
-    static int* ptr[64] = {};
-    int dev = 0;
-    DEMSPH_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw Status(DEMSPH_ERR_INVALID, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(mu);
-    if (!ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_hash_sort_scratch);
-        if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress of the sort scratch array failed");
-        ptr[dev] = (int*)p;
-    }
-    return ptr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_hash_sort_scratch);
+    if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress of the sort scratch array failed");
+    return (int*)p;
 }
 
 }  // namespace demsph

@@ -26,6 +26,8 @@
 #include "vtu.hpp"
 #include "dem_physics.cuh"
 #include "coupling.hpp"
+#include "external.cuh"
+#include "diag.cuh"
 
 namespace demsph {
 
@@ -590,29 +592,10 @@ __global__ void __launch_bounds__(128, 8) k_dem_finalize(DemDev d, double extTim
         }
         // addBuoyancyDragKernel (externalForceTorque.cu:66-133)
         if (d.buoy && !(v4.w <= 0.0)) {
-            double r = p4.w;
-            double dd = d.blevel - ri.z;
-            double Vsub;
-            if (dd <= -r) Vsub = 0.0;
-            else if (dd >= r) Vsub = (4.0 / 3.0) * kPi * r * r * r;
-            else { double h = dd + r; Vsub = (kPi * h * h * (3.0 * r - h)) / 3.0; }
-            if (Vsub > 0.0) {
-                double3 Fb = mk3(-d.brho * Vsub * d.bg3.x, -d.brho * Vsub * d.bg3.y, -d.brho * Vsub * d.bg3.z);
-                double Vs = (4.0 / 3.0) * kPi * r * r * r;
-                double alpha = (Vs > 1.e-30) ? (Vsub / Vs) : 0.0;
-                double3 vr = xyz(v4) - d.bu;
-                double v2 = dot(vr, vr);
-                double3 Fdr = mk3(0, 0, 0);
-                if (v2 > 1.e-30 && d.bcd > 0.0) {
-                    double vm = sqrt(v2);
-                    double Aeff = alpha * (kPi * r * r);
-                    double kk = 0.5 * d.brho * d.bcd * Aeff * vm;
-                    Fdr = mk3(-kk * vr.x, -kk * vr.y, -kk * vr.z);
-                }
-                F.x += Fb.x + Fdr.x;
-                F.y += Fb.y + Fdr.y;
-                F.z += Fb.z + Fdr.z;
-            }
+            double3 Fbd = buoyancy_drag(ri, xyz(v4), p4.w, d.brho, d.bcd, d.bg3, d.bu, d.blevel);
+            F.x += Fbd.x;
+            F.y += Fbd.y;
+            F.z += Fbd.z;
         }
     }
     d.force[i] = d4(F, 0);
@@ -699,6 +682,92 @@ __global__ void k_dem_integrate(DemDev d, double hdt, int first) {
         d.pos[i] = d4(xyz(p) + (2.0 * hdt) * v, p.w);
     }
 }
+// The ball arrays in the reference's layout (ball_ of particle.h: double3
+// position, velocity, angular velocity, force, torque; double radius and
+// inverse mass), written before an addExternalForceTorque callback and read
+// back after it, so the callback's kernels see and change the state as the
+// reference's hooks do.
+struct HookArrays {
+    double3* pos;
+    double3* vel;
+    double3* angv;
+    double3* force;
+    double3* torque;
+    double* rad;
+    double* invm;
+};
+__global__ void k_dem_hook_out(DemDev d, HookArrays h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const double4 p = d.pos[i], v = d.vel[i];
+    h.pos[i] = xyz(p);
+    h.rad[i] = p.w;
+    h.vel[i] = xyz(v);
+    h.invm[i] = v.w;
+    h.angv[i] = xyz(d.angv[i]);
+    h.force[i] = xyz(d.force[i]);
+    h.torque[i] = xyz(d.torque[i]);
+}
+__global__ void k_dem_hook_in(DemDev d, HookArrays h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    d.pos[i] = d4(h.pos[i], h.rad[i]);
+    d.vel[i] = d4(h.vel[i], h.invm[i]);
+    d.angv[i] = d4(h.angv[i], 0);
+    d.force[i] = d4(h.force[i], 0);
+    d.torque[i] = d4(h.torque[i], 0);
+}
+// FP64 conservation diagnostics of a DEM scene, per object (the balls, then
+// the clumps), summed by diag_reduce:
+//   0-2  linear momentum  sum m v            (moving bodies: free spheres and
+//   3-5  angular momentum sum x x m v + I w   clumps; pebbles count through
+//   6    translational kinetic energy         their clump; fixed balls, with
+//   7    rotational kinetic energy            inverse mass 0, not at all)
+//   8    mass
+//   9-11 sum of the ball forces of the last force evaluation (all balls: the
+//        contact and bond forces cancel pairwise, so this is the sum of the
+//        external and wall forces)
+struct DemDiagTerm {
+    DemDev d;
+    __device__ void operator()(int i, double* v) const {
+#pragma unroll
+        for (int k = 0; k < 12; k++) v[k] = 0.0;
+        double3 x, u, w, L;
+        double m;
+        if (i < d.N) {
+            const double3 F = xyz(d.force[i]);
+            v[9] = F.x; v[10] = F.y; v[11] = F.z;
+            const double4 v4 = d.vel[i];
+            if (!(v4.w > 0.0) || d.clump[i] >= 0) return;
+            const double4 p4 = d.pos[i];
+            m = 1.0 / v4.w;
+            x = xyz(p4); u = xyz(v4); w = xyz(d.angv[i]);
+            L = (0.4 * m * p4.w * p4.w) * w;
+        } else {
+            const int c = i - d.N;
+            const double im = d.cinvm[c];
+            if (!(im > 1.e-20)) return;
+            m = 1.0 / im;
+            x = xyz(d.cpos[c]); u = xyz(d.cvel[c]); w = xyz(d.cangv[c]);
+            // world inverse inertia R I^-1 R^T by columns, then I_world w by Cramer's rule
+            const double4 q = d.cq[c], Ia = d.cinvIa[c], Ib = d.cinvIb[c];
+            const double3 c0 = rot_inv_inertia_apply(q, Ia, Ib, mk3(1, 0, 0));
+            const double3 c1 = rot_inv_inertia_apply(q, Ia, Ib, mk3(0, 1, 0));
+            const double3 c2 = rot_inv_inertia_apply(q, Ia, Ib, mk3(0, 0, 1));
+            const double det = dot(c0, cross(c1, c2));
+            L = (fabs(det) > 0.0) ? mk3(dot(w, cross(c1, c2)), dot(c0, cross(w, c2)), dot(c0, cross(c1, w))) / det
+                                  : mk3(0, 0, 0);
+        }
+        const double3 P = m * u;
+        const double3 Lx = cross(x, P) + L;
+        v[0] = P.x; v[1] = P.y; v[2] = P.z;
+        v[3] = Lx.x; v[4] = Lx.y; v[5] = Lx.z;
+        v[6] = 0.5 * m * dot(u, u);
+        v[7] = 0.5 * dot(w, L);
+        v[8] = m;
+    }
+};
+
 // wallPositionIntegrationKernel + wallOrientationIntegrationKernel (wallIntegrationKernel.cu:3-23)
 __global__ void k_dem_wall_move(DemDev d, double dt) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -902,6 +971,7 @@ struct DemScene {
     cudaStream_t blockOwn = 0;
     bool inBlock = false;
     DBuf<DevStatus> status;
+    DBuf<double> diagScratch;
     static constexpr int kMergedWallBalls = 65536;  // up to this size k_dem_pair_walls
 
     // Periodic boundaries (setPeriodicBoundary, DEMSolver.h:1944-1959): one
@@ -1301,7 +1371,8 @@ struct DemScene {
             launch_count(1);
         }
         bool clumps = !hCpos.empty();
-        int fin = clumps ? 0 : integ;
+        const bool hook = ext && hookFn != nullptr;
+        int fin = (clumps || hook) ? 0 : integ;
         if (precision == DEMSPH_PRECISION_FP64)
             k_dem_finalize<double><<<grid_for(n, 128), 128, 0, s>>>(d, extTime, ext ? 1 : 0, fin, hdt);
         else
@@ -1316,12 +1387,58 @@ struct DemScene {
                 launch_count(3);
             }
         }
-        if (clumps && integ) {
-            k_dem_clumps<<<grid_for(d.nClump, 128), 128, 0, s>>>(d, hdt, integ == 1);
-            k_dem_pebbles<<<grid_for(n, 256), 256, 0, s>>>(d);
+        if (hook) run_hook(extTime);
+        if ((clumps || hook) && integ) {
+            if (clumps) {
+                k_dem_clumps<<<grid_for(d.nClump, 128), 128, 0, s>>>(d, hdt, integ == 1);
+                k_dem_pebbles<<<grid_for(n, 256), 256, 0, s>>>(d);
+                launch_count(2);
+            }
             k_dem_integrate<<<grid_for(n, 256), 256, 0, s>>>(d, hdt, integ == 1);
-            launch_count(3);
+            launch_count(1);
         }
+        DEMSPH_LAUNCH_CHECK();
+    }
+
+    // addExternalForceTorque (virtual, DEMSolver.h:1372; called after each
+    // force evaluation of a step, :1464,1470): a caller's callback between
+    // the force evaluation and the half-step integration.  The ball state is
+    // copied into arrays of the reference's layout before the call and read
+    // back after it; the callback's device work must be ordered on the
+    // scene's stream or the legacy default stream.
+    demsph_dem_hook_fn hookFn = nullptr;
+    void* hookUser = nullptr;
+    DBuf<double3> hkPos, hkVel, hkAngv, hkForce, hkTorque;
+    DBuf<double> hkRad, hkInvm;
+    HookArrays hook_arrays() {
+        const size_t n = (size_t)N();
+        if (hkPos.n < n) {
+            hkPos.alloc(n, s, true); hkVel.alloc(n, s, true); hkAngv.alloc(n, s, true);
+            hkForce.alloc(n, s, true); hkTorque.alloc(n, s, true);
+            hkRad.alloc(n, s, true); hkInvm.alloc(n, s, true);
+        }
+        return HookArrays{hkPos.p, hkVel.p, hkAngv.p, hkForce.p, hkTorque.p, hkRad.p, hkInvm.p};
+    }
+    static void order_after(cudaStream_t waiter, cudaStream_t done) {
+        cudaEvent_t ev;
+        DEMSPH_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        DEMSPH_CUDA(cudaEventRecord(ev, done));
+        DEMSPH_CUDA(cudaStreamWaitEvent(waiter, ev, 0));
+        DEMSPH_CUDA(cudaEventDestroy(ev));
+    }
+    void run_hook(double t) {
+        const HookArrays h = hook_arrays();
+        DemDev d = dev(false);
+        k_dem_hook_out<<<grid_for(N(), 256), 256, 0, s>>>(d, h);
+        launch_count(1);
+        DEMSPH_LAUNCH_CHECK();
+        const bool legacy = (s == 0 || s == cudaStreamLegacy);
+        if (!legacy) order_after(cudaStreamLegacy, s);
+        demsph_dem_hook_fn fn = hookFn;
+        if (fn) fn(hookUser, iStep, t);
+        if (!legacy) order_after(s, cudaStreamLegacy);
+        k_dem_hook_in<<<grid_for(N(), 256), 256, 0, s>>>(d, h);
+        launch_count(1);
         DEMSPH_LAUNCH_CHECK();
     }
     // One pass of loop_ball / loop_ball_wall (DEMSolver.h:1376-1485).
@@ -1346,7 +1463,7 @@ struct DemScene {
         for (size_t g = 0; g < ghosts.size(); g++) k |= (ghosts[g]->cur | (ghosts[g]->have ? 2 : 0)) << (2 + 2 * g);
         return k;
     }
-    bool graphable() const { return useGraphs && !(framp > 0) && ready; }
+    bool graphable() const { return useGraphs && !(framp > 0) && ready && !hookFn; }
 
     DevStatus read_status() {
         DevStatus h{};
@@ -1980,6 +2097,34 @@ int demsph_dem_set_buoyancy_drag(demsph_dem_t h, double rho, double cd, const do
         s.buoy = 1; s.brho = rho; s.bcd = cd; s.bg3 = ld3(g, 0); s.bu = ld3(u, 0); s.blevel = lvl;
     });
 }
+int demsph_dem_set_external_hook(demsph_dem_t h, demsph_dem_hook_fn fn, void* user) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.inBlock) throw Status(DEMSPH_ERR_INVALID, "set_external_hook inside a coupled block");
+        s.hookFn = fn;
+        s.hookUser = fn ? user : nullptr;
+    });
+}
+int demsph_dem_hook_arrays(demsph_dem_t h, demsph_ball_arrays* out) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        const HookArrays a = s.hook_arrays();
+        out->position = (double*)a.pos;
+        out->velocity = (double*)a.vel;
+        out->angularVelocity = (double*)a.angv;
+        out->force = (double*)a.force;
+        out->torque = (double*)a.torque;
+        out->radius = a.rad;
+        out->inverseMass = a.invm;
+        out->materialID = s.mat.p;
+        out->clumpID = s.clump.p;
+        out->n = s.N();
+    });
+}
 int demsph_dem_reserve(demsph_dem_t h, int pairsPerBall, int reversePerBall, int trianglesPerBall) {
     return guarded([&] {
         SCENE_CHECK(h);
@@ -2048,7 +2193,7 @@ int demsph_dem_eval_forces(demsph_dem_t h, double dt, int walls, double dtWall) 
         DemScene& s = h->sc;
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         s.graph.reset();  // the ghost passes flip list buffers outside a graph
-        s.force_eval(dt, (walls & 1) != 0, dtWall, false, 0.0, 0, 0.0, (walls & 2) != 0);
+        s.force_eval(dt, (walls & 1) != 0, dtWall, (walls & 4) != 0, s.time, 0, 0.0, (walls & 2) != 0);
         DEMSPH_CUDA(cudaStreamSynchronize(s.s));
     });
 }
@@ -2347,6 +2492,52 @@ int demsph_dem_get_bonds(demsph_dem_t h, int* a, int* b, int* ok, double* fn, do
             if (normal) st3(normal, k, xyz(NO[k]));
             if (point) st3(point, k, xyz(PO[k]));
         }
+    });
+}
+int demsph_dem_diagnostics(demsph_dem_t h, double* out) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        DemDiagTerm t{s.dev(false)};
+        diag_reduce<12>(t, s.N() + (int)s.hCpos.size(), out, s.diagScratch, s.s);
+    });
+}
+int demsph_dem_set_bonds(demsph_dem_t h, long n, const int* ok, const double* fn, const double* tt, const double* fs,
+                         const double* tb, const double* normal, const double* point) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        const long nb = (long)s.hBab.size();
+        if (n != nb) throw Status(DEMSPH_ERR_INVALID, "set_bonds: n must equal the number of bonds");
+        if (nb == 0) return;
+        s.graph.reset();  // buffers change under captured launches
+        if (ok) {
+            std::vector<int> v(ok, ok + nb);
+            s.bok.upload(v, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        }
+        auto scalars = [&](DBuf<double>& b, const double* src) {
+            if (!src) return;
+            std::vector<double> v(src, src + nb);
+            b.upload(v, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        };
+        auto vectors = [&](DBuf<double4>& b, const double* src) {
+            if (!src) return;
+            std::vector<double4> v(nb);
+            for (long k = 0; k < nb; k++) v[k] = d4(ld3(src, k), 0);
+            b.upload(v, s.s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        };
+        scalars(s.bFn, fn);
+        scalars(s.bTt, tt);
+        vectors(s.bFs, fs);
+        vectors(s.bTb, tb);
+        vectors(s.bnormal, normal);
+        vectors(s.bpoint, point);
     });
 }
 // ------------------------------------------------------------ VTU frames --

@@ -39,7 +39,10 @@ static __global__ void __launch_bounds__(kRxThreads) k_rx_hist(const unsigned* _
 // Exclusive scan of one 4096-element tile (1024 threads x 4 items); with a
 // tile offset it finishes a multi-tile scan, with tileSum it produces the
 // per-tile totals of the first level.
-static __global__ void __launch_bounds__(1024) k_rx_scan(const int* __restrict__ in, int* __restrict__ out, int n,
+// `in` and `out` may be the same array (the sort scans its histogram in
+// place): each thread reads its four words before the first barrier and
+// writes them after the last, so they carry no __restrict__.
+static __global__ void __launch_bounds__(1024) k_rx_scan(const int* in, int* out, int n,
                                                          const int* __restrict__ tileOffset, int* __restrict__ tileSum,
                                                          int inclusive) {
     __shared__ int ws[32];

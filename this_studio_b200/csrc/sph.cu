@@ -24,6 +24,7 @@
 #include "coupling.hpp"
 #include "graph.cuh"
 #include "vtu.hpp"
+#include "diag.cuh"
 
 namespace demsph {
 
@@ -1417,6 +1418,28 @@ static void marker_offsets(double R, double dx, double h, std::vector<double3>& 
     if (out.empty()) out.push_back(mk3(0, 0, 0));
 }
 
+// FP64 conservation diagnostics of the fluid, per particle, summed by
+// diag_reduce: 0 mass, 1-3 momentum sum m v, 4 kinetic energy, 5 potential
+// energy -sum m g.x, 6 sum of the density changes (Delta rho), 7 volume
+// sum m / rho.
+struct SphDiagTerm {
+    const double4* pos;
+    const double4* vel;
+    const double4* st;
+    const double* drho;
+    double3 g;
+    __device__ void operator()(int i, double* v) const {
+        const double4 p = pos[i], u = vel[i];
+        const double m = u.w;
+        v[0] = m;
+        v[1] = m * u.x; v[2] = m * u.y; v[3] = m * u.z;
+        v[4] = 0.5 * m * (u.x * u.x + u.y * u.y + u.z * u.z);
+        v[5] = -m * (g.x * p.x + g.y * p.y + g.z * p.z);
+        v[6] = drho[i];
+        v[7] = m / st[i].x;
+    }
+};
+
 struct SphScene {
     cudaStream_t s = 0;
     int precision = DEMSPH_PRECISION_FP64;
@@ -1450,6 +1473,7 @@ struct SphScene {
     DBuf<int> did;
     DBuf<int> nbF, cntF, nbD, cntD, nbDD, cntDD;
     DBuf<DevStatus> status;
+    DBuf<double> diagScratch;
     bool haveLists = false;
 
     // Skin lists (fluid scenes without markers): rows hold every candidate
@@ -2661,6 +2685,16 @@ int demsph_sph_set_skin(demsph_sph_t h, double fraction) {
         s.skinFrac = (float)fraction;
         s.graph.reset();  // the captured launches carry the skin
         s.skin_force();
+    });
+}
+int demsph_sph_diagnostics(demsph_sph_t h, double* out) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        SphDiagTerm t{s.pos[s.P].p, s.vel[s.Vv].p, s.st[s.S].p, s.drho[s.D].p, s.gravity};
+        diag_reduce<8>(t, s.N(), out, s.diagScratch, s.s);
     });
 }
 int demsph_sph_skin_stats(demsph_sph_t h, double* fraction, long* rebuilds) {

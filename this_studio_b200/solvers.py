@@ -260,9 +260,32 @@ class DEMSolver:
     def calculateBallContactForceTorque(self, timeStep):
         call("demsph_dem_eval_forces", self._h, float(timeStep), 0, 0.0)
 
-    def evalForces(self, timeStep, walls=False, wallTimeStep=0.0, periodic=False):
-        flags = (1 if walls else 0) | (2 if periodic else 0)
+    def evalForces(self, timeStep, walls=False, wallTimeStep=0.0, periodic=False, external=False):
+        """One force evaluation (calculateBallContactForceTorque, DEMSolver.h:
+        599-695) with, optionally, the wall contacts (addTriangleContact-
+        ForceTorque(wallTimeStep)), the periodic ghost passes and the external
+        forces (the configured hooks and a callback, at the scene's time)."""
+        flags = (1 if walls else 0) | (2 if periodic else 0) | (4 if external else 0)
         call("demsph_dem_eval_forces", self._h, float(timeStep), flags, float(wallTimeStep))
+
+    def setExternalHook(self, fn):
+        """addExternalForceTorque (virtual, DEMSolver.h:1372) as a Python
+        callable fn(iStep, time), called after each force evaluation of a
+        step; inside it, hookArrays() gives the ball arrays in the reference's
+        layout for launchers such as launchAddConstantForce.  None removes it."""
+        if fn is None:
+            self._hook = None
+            call("demsph_dem_set_external_hook", self._h, _lib.HOOK_FN(), None)
+            return
+        self._hook = _lib.HOOK_FN(lambda user, iStep, time: fn(int(iStep), float(time)))
+        call("demsph_dem_set_external_hook", self._h, self._hook, None)
+
+    def hookArrays(self):
+        """demsph_dem_hook_arrays: the device pointers an external-force
+        callback works on (current only while it runs)."""
+        a = _lib.BallArrays()
+        call("demsph_dem_hook_arrays", self._h, C.byref(a))
+        return a
 
     # ------------------------------------------------------------ getters --
     def _n(self, fn, *a):
@@ -357,6 +380,25 @@ class DEMSolver:
              _ip(out["isBonded"]), _dp(out["normalForce"]), _dp(out["torsionTorque"]), _dp(out["shearForce"]),
              _dp(out["bendingTorque"]), _dp(out["normal"]), _dp(out["point"]))
         return out
+
+    def diagnostics(self):
+        """demsph_dem_diagnostics: FP64 momentum, angular momentum, kinetic
+        energies and mass of the moving bodies, and the summed ball force."""
+        out = np.zeros(12)
+        call("demsph_dem_diagnostics", self._h, _dp(out))
+        return {"momentum": out[0:3], "angularMomentum": out[3:6], "kineticEnergy": out[6],
+                "rotationalEnergy": out[7], "mass": out[8], "forceSum": out[9:12]}
+
+    def setBondedInteraction(self, isBonded=None, normalForce=None, torsionTorque=None, shearForce=None,
+                             bendingTorque=None, normal=None, point=None):
+        """Writes the bond state (getBondedInteraction's order; None keeps a field)."""
+        n = self._n("demsph_dem_num_bonds")
+        i = lambda x: None if x is None else _i32(x)
+        d1 = lambda x: None if x is None else _f64(x, (n,))
+        d3 = lambda x: None if x is None else _f64(x, (n, 3))
+        ok = i(isBonded)
+        call("demsph_dem_set_bonds", self._h, n, _ip(ok), _dp(d1(normalForce)), _dp(d1(torsionTorque)),
+             _dp(d3(shearForce)), _dp(d3(bendingTorque)), _dp(d3(normal)), _dp(d3(point)))
 
     def getClump(self):
         n = self._n("demsph_dem_num_clumps")
@@ -500,6 +542,14 @@ class WCSPHSolver:
              _dp(out["acceleration"]), _dp(out["density"]), _dp(out["pressure"]), _dp(out["densityChange"]),
              _dp(out["normal"]))
         return out
+
+    def diagnostics(self):
+        """demsph_sph_diagnostics: FP64 mass, momentum, kinetic and potential
+        energy, summed density change and volume of the fluid."""
+        out = np.zeros(8)
+        call("demsph_sph_diagnostics", self._h, _dp(out))
+        return {"mass": out[0], "momentum": out[1:4], "kineticEnergy": out[4], "potentialEnergy": out[5],
+                "densityChangeSum": out[6], "volume": out[7]}
 
     def getSPH(self):
         return self._get(False)
