@@ -59,6 +59,8 @@ typedef struct demsph_dem_scene* demsph_dem_t;
 typedef struct demsph_dem_member* demsph_dem_member_t;
 typedef struct demsph_sph_scene* demsph_sph_t;
 typedef struct demsph_sph_member* demsph_sph_member_t;
+typedef struct demsph_dem_snapshot* demsph_dem_snapshot_t;
+typedef struct demsph_sph_snapshot* demsph_sph_snapshot_t;
 
 const char* demsph_last_error(void);
 const char* demsph_version(void);
@@ -218,6 +220,17 @@ int demsph_dem_set_graphs(demsph_dem_t s, int enable);
 int demsph_dem_neighbor_search(demsph_dem_t s);
 int demsph_dem_eval_forces(demsph_dem_t s, double dt, int walls, double dtWall);
 
+/* No counterpart in the reference (which keeps its state in host-device
+ * arrays that a caller copies by hand).  A device copy of a scene's
+ * dynamic state -- balls, clumps, walls, pair and triangle rows with their
+ * springs, bonds, periodic ghost lists, the step counter -- and its
+ * restoration into the same scene, for checkpoints kept in device memory,
+ * what-if branches and replays: steps from a restored state repeat the steps
+ * after the snapshot bit for bit.  A snapshot holds device memory until
+ * destroyed; it restores only into the scene it was taken from. */
+int demsph_dem_snapshot(demsph_dem_t s, demsph_dem_snapshot_t* out);
+int demsph_dem_restore(demsph_dem_t s, demsph_dem_snapshot_t snapshot);
+int demsph_dem_snapshot_destroy(demsph_dem_snapshot_t snapshot);
 /* No counterpart in the reference (which has no diagnostics).  FP64
  * conservation diagnostics of the current state, summed on the device in a
  * fixed order (the same bits for the same state), 12 doubles: linear
@@ -410,6 +423,22 @@ int demsph_sph_set_skin(demsph_sph_t s, double fraction);
 int demsph_sph_tune_skin(demsph_sph_t s, int steps, double* chosen, double* msPerStep);
 int demsph_sph_skin_stats(demsph_sph_t s, double* fraction, long* rebuilds);
 
+/* No counterpart in the reference.  The fluid's state (positions,
+ * velocities, density, pressure, density change, order, the step counter)
+ * copied on the device and restored into the same scene; the neighbour
+ * lists are rebuilt at the next step, which then repeats the steps after
+ * the snapshot bit for bit.  A snapshot restores only into its own scene. */
+int demsph_sph_snapshot(demsph_sph_t s, demsph_sph_snapshot_t* out);
+int demsph_sph_restore(demsph_sph_t s, demsph_sph_snapshot_t snapshot);
+int demsph_sph_snapshot_destroy(demsph_sph_snapshot_t snapshot);
+/* No counterpart in the reference.  In mixed precision, a scene whose fluid
+ * particles share h, m, c and nu and whose dummies share m, c, nu and rest
+ * density (with the fluid's h) runs momentum and continuity passes
+ * specialised for it (constants hoisted, terms regrouped; same pairs, same
+ * formulas); enable = 0 keeps the general passes.  uniform_kernels reports
+ * whether the specialised passes are in use. */
+int demsph_sph_set_uniform_kernels(demsph_sph_t s, int enable);
+int demsph_sph_uniform_kernels(demsph_sph_t s, int* active);
 /* No counterpart in the reference.  FP64 conservation diagnostics of the
  * fluid, summed on the device in a fixed order, 8 doubles: mass, momentum
  * (3), kinetic energy, potential energy -sum m g.x, sum of the density

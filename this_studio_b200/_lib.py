@@ -60,6 +60,14 @@ SIGNATURES = {
     "demsph_dem_set_bonds": [_vp, _long, _i, _d, _d, _d, _d, _d, _d],
     "demsph_dem_diagnostics": [_vp, _d],
     "demsph_sph_diagnostics": [_vp, _d],
+    "demsph_sph_set_uniform_kernels": [_vp, _int],
+    "demsph_dem_snapshot": [_vp, _pvp],
+    "demsph_dem_restore": [_vp, _vp],
+    "demsph_dem_snapshot_destroy": [_vp],
+    "demsph_sph_snapshot": [_vp, _pvp],
+    "demsph_sph_restore": [_vp, _vp],
+    "demsph_sph_snapshot_destroy": [_vp],
+    "demsph_sph_uniform_kernels": [_vp, _i],
     "launchAddConstantForce": [_vp, _vp, _sz, _sz, _sz, _vp],
     "launchAddGlobalDampingForceTorque": [_vp, _vp, _vp, _vp, _dbl, _sz, _sz, _sz, _vp],
     "launchAddBuoyancyDrag": [_vp, _vp, _vp, _vp, _vp, _dbl, _dbl, Double3, Double3, _dbl, _sz, _sz, _sz, _vp],

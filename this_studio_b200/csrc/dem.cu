@@ -2494,6 +2494,48 @@ int demsph_dem_get_bonds(demsph_dem_t h, int* a, int* b, int* ok, double* fn, do
         }
     });
 }
+struct demsph_dem_snapshot {
+    demsph_dem_t scene = nullptr;
+    DemScene::Snap snap;
+};
+int demsph_dem_snapshot(demsph_dem_t h, demsph_dem_snapshot_t* out) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        DemScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        if (s.inBlock) throw Status(DEMSPH_ERR_INVALID, "snapshot inside a coupled block");
+        auto* sn = new struct demsph_dem_snapshot();
+        sn->scene = h;
+        try {
+            s.take(sn->snap);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        } catch (...) {
+            delete sn;
+            throw;
+        }
+        *out = sn;
+    });
+}
+int demsph_dem_restore(demsph_dem_t h, demsph_dem_snapshot_t sn) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        if (!sn) throw Status(DEMSPH_ERR_INVALID, "null snapshot");
+        if (sn->scene != h) throw Status(DEMSPH_ERR_INVALID, "the snapshot belongs to another scene");
+        DemScene& s = h->sc;
+        if (s.inBlock) throw Status(DEMSPH_ERR_INVALID, "restore inside a coupled block");
+        s.restore(sn->snap);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_dem_snapshot_destroy(demsph_dem_snapshot_t sn) {
+    return guarded([&] {
+        if (!sn) return;
+        cudaStream_t st = sn->scene ? sn->scene->sc.s : 0;
+        delete sn;
+        DEMSPH_CUDA(cudaStreamSynchronize(st));
+    });
+}
 int demsph_dem_diagnostics(demsph_dem_t h, double* out) {
     return guarded([&] {
         SCENE_CHECK(h);

@@ -30,6 +30,29 @@ namespace demsph {
 
 extern std::atomic<long long> g_launches;
 
+// Constants of the mixed-precision passes specialised for scenes whose fluid
+// particles share h, m, c and nu and whose dummies share m, c, nu and rho0
+// (with the fluid's h): every benchmark scene, and the reference's examples.
+// Lengths in the pair terms stay in position quanta (r' = r / q, the exact
+// integer difference of the fixed-point positions), so no per-pair rescaling
+// is needed: grad W = K dq(q_n) r'/|r'| with K = 21 / (16 pi h^4) and
+// q_n = |r'| q / h.
+struct UniK {
+    float invhq;   // q / h
+    float K;       // 21 / (16 pi h^4)
+    float c2q;     // (2 h / q)^2, the cutoff in quanta squared
+    float cF;      // fluid sound speed
+    float mF2;     // 2 m (fluid)
+    float bF;      // 2 nu m (fluid-fluid viscosity factor)
+    float mF, mD;  // particle masses (continuity)
+    float mD2;     // 2 m_dummy
+    float bD;      // 2 (nu + nu_dummy) / 2 m_dummy
+    float cbarD;   // (c + c_dummy) / 2
+    float invcD2;  // 1 / c_dummy^2
+    float rho0D;   // dummy rest density
+    float3 gq;     // gravity times q
+};
+
 struct SphDev {
     int N, ND, KF, KD;
     GridDesc g;
@@ -123,6 +146,7 @@ struct SphDev {
     double4* mforce;
     double3 gravity;
     DevStatus* status;
+    UniK uk;  // set when the scene qualifies for the specialised passes
 };
 
 // A boundary set (dummies or markers) as the fluid passes read it.
@@ -212,6 +236,28 @@ __device__ __forceinline__ float fixdiff(int a, int b, float q) {
 __global__ void k_sph_fix(int n, const double4* __restrict__ pos, double3 o, double invq, int4* __restrict__ posq) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) posq[t] = fixq(pos[t], o, invq);
+}
+// Packed fluid shadows (scenes on the uniform-constant passes, whose h and m
+// are the scene's constants): the fixed-point position carries rho in w and
+// the FP32 velocity carries p in w, so a neighbour is two 16-byte gathers.
+__device__ __forceinline__ int4 fixq_rho(double4 p, double4 st, double3 o, double invq) {
+    int4 a = fixq(p, o, invq);
+    a.w = __float_as_int((float)st.x);
+    return a;
+}
+__device__ __forceinline__ float4 velf_p(double4 v, double4 st) {
+    return make_float4((float)v.x, (float)v.y, (float)v.z, (float)st.y);
+}
+// Sets the w components of the fluid shadows for the packed (rho, p) or the
+// general (h, m) layout.
+__global__ void k_sph_pack(int n, const double4* __restrict__ pos, const double4* __restrict__ vel,
+                           const double4* __restrict__ st, int4* __restrict__ posq, float4* __restrict__ velf,
+                           int packed) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double4 q = st[t];
+    posq[t].w = __float_as_int(packed ? (float)q.x : (float)pos[t].w);
+    velf[t].w = packed ? (float)q.y : (float)vel[t].w;
 }
 
 // Rewrites the FP32 shadows from the FP64 records (after a host-side change).
@@ -503,18 +549,18 @@ __global__ void k_sph_permute(int n, const int* __restrict__ sorted, const doubl
                               double4* __restrict__ st2, double* __restrict__ rho02, double* __restrict__ drho2,
                               int* __restrict__ id2, float4* __restrict__ posf, float4* __restrict__ velf2,
                               float4* __restrict__ stf2, int4* __restrict__ posq2, double3 origin, double invq,
-                              const int* __restrict__ gate) {
+                              const int* __restrict__ gate, int packed) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n || (gate && *gate == 0)) return;
     int o = sorted[t];
     double4 p = pos[o];
     pos2[t] = p;
-    posq2[t] = fixq(p, origin, invq);
-    posf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
     const double4 v = vel[o], q = st[o];
+    posq2[t] = packed ? fixq_rho(p, q, origin, invq) : fixq(p, origin, invq);
+    posf[t] = make_float4((float)(p.x - origin.x), (float)(p.y - origin.y), (float)(p.z - origin.z), (float)p.w);
     vel2[t] = v;
     st2[t] = q;
-    velf2[t] = f4(v);
+    velf2[t] = packed ? velf_p(v, q) : f4(v);
     stf2[t] = f4(q);
     rho02[t] = rho0[o];
     drho2[t] = drho[o];
@@ -1227,6 +1273,210 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
     d.stfOut[i] = f4(so);
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision passes for scenes with uniform particle constants (UniK),
+// without markers.  Same pair sets, same formulas as k_sph_accel /
+// k_sph_density (updateWCSPHAccelerationKernel and
+// updateWCSPHDensityChangeKernel, WCSPHIntegrationKernel.cu:42-282), with
+// the constants hoisted and the terms regrouped:
+//   grad W_ij = K dq r'/|r'|,  dq = 2 t^3 (t - 1 - 2 q_n),  t = max(1 - q_n/2, 0);
+//   U_L - U_R = -(v_i - v_j) . r'/|r'|;
+//   r_hat . grad W = K dq (the reference's viscosity factor, Q5);
+//   momentum:   a_i += s [2 nu m (v_i - v_j) - 2 m P* r'/|r'|],  s = K dq / (rho_i rho_j);
+//   continuity: (v_i - v*) . grad W = K dq [(v_i - v_j) . r'/|r'| + (P_L - P_R) / (rho_bar c_bar)] / 2.
+// The fluid shadows are packed (k_sph_pack): the fixed-point position
+// carries rho in w and the FP32 velocity carries p, so a fluid neighbour is
+// two 16-byte gathers (the general passes gather a third record, the FP32
+// state); a dummy is three (position, velocity, normal).  Each pass writes
+// the packed shadows of the records it writes; the continuity pass, which
+// changes rho and p, writes the next position / velocity buffers.
+
+struct PairGeom {
+    float3 r;   // r_i - r_j in quanta
+    float inv_r;
+    float Kdq;  // K dq(q_n)
+};
+__device__ __forceinline__ PairGeom pair_geom(const int4& qi, const int4& qj, const UniK& u) {
+    PairGeom p;
+    p.r = make_float3((float)(int)((unsigned)qi.x - (unsigned)qj.x), (float)(int)((unsigned)qi.y - (unsigned)qj.y),
+                      (float)(int)((unsigned)qi.z - (unsigned)qj.z));
+    const float r2 = dot(p.r, p.r);
+    p.inv_r = rsqrtf(fmaxf(r2, 1e-30f));
+    const float qn = r2 * p.inv_r * u.invhq;
+    const float t = fmaxf(1.0f - 0.5f * qn, 0.0f);
+    const float t3 = t * t * t;
+    p.Kdq = u.K * (2.0f * t3 * (t - 1.0f - 2.0f * qn));
+    return p;
+}
+// The reference's cutoff test for a skin candidate, from the quanta
+// difference: FP32 outside a band of 2e-6 cut^2, the FP64 test on the FP64
+// positions inside it (as cutoff_f).
+__device__ __forceinline__ bool cutoff_u(const float3& r, const UniK& u, const double4& pi,
+                                         const double4* __restrict__ other, int j) {
+    const float d2 = dot(r, r);
+    const float band = 2.0e-6f * u.c2q;
+    if (d2 < u.c2q - band) return true;
+    if (d2 > u.c2q + band) return false;
+    const double4 pj = other[j];
+    const double cd = 2.0 * fmax(pi.w, pj.w);
+    const double3 dr = xyz(pi) - xyz(pj);
+    return (cd * cd - dot(dr, dr)) >= 0.;
+}
+
+struct OwnU {
+    int4 q;
+    float3 v;
+    float rho, PL;
+};
+// vj = (v_j, p_j), rhoj from the packed shadows
+__device__ __forceinline__ void acc_fluid_u(const OwnU& o, const PairGeom& p, const float4& vj, float rhoj,
+                                            const UniK& u, float3& acc) {
+    const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
+    const float dU = -dot(dv, p.r) * p.inv_r;
+    const float beta = fminf(3.0f * fmaxf(dU, 0.0f), u.cF);
+    const float Ps = 0.5f * (o.PL + vj.w) + 0.5f * beta * (0.5f * (o.rho + rhoj)) * dU;
+    const float s = p.Kdq * __fdividef(1.0f, o.rho * rhoj);
+    const float sw = s * u.mF2 * Ps * p.inv_r;
+    const float sb = s * u.bF;
+    acc += sb * dv - sw * p.r;
+}
+// The dummy's extrapolated pressure and density (WCSPHIntegrationKernel.cu:
+// 110-143): P_R = P_L + rho_i max(-g . r_ij, 0), rho_j = P_R / c_j^2 + rho0_j.
+__device__ __forceinline__ void dummy_state_u(const OwnU& o, const PairGeom& p, const UniK& u, float& PR, float& rhoj) {
+    const float grj = fmaxf(-dot(u.gq, p.r), 0.0f);
+    PR = o.PL + o.rho * grj;
+    rhoj = PR * u.invcD2 + u.rho0D;
+}
+__device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, const float4& vj, const float4& nj,
+                                            const UniK& u, float3& acc) {
+    const float3 vd = make_float3(vj.x, vj.y, vj.z), nw = make_float3(nj.x, nj.y, nj.z);
+    const float UL = -dot(nw, o.v);
+    const float UR = -UL - 2.0f * dot(nw, vd);
+    float PR, rhoj;
+    dummy_state_u(o, p, u, PR, rhoj);
+    const float dU = UL - UR;
+    const float beta = fminf(3.0f * fmaxf(dU, 0.0f), u.cbarD);
+    const float Ps = 0.5f * (o.PL + PR) + 0.5f * beta * (0.5f * (o.rho + rhoj)) * dU;
+    const float s = p.Kdq * __fdividef(1.0f, o.rho * rhoj);
+    const float sw = s * u.mD2 * Ps * p.inv_r;
+    const float sb = s * u.bD;
+    acc += sb * (o.v - vd) - sw * p.r;
+}
+
+template <bool kSkin>
+__global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
+    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
+    if (i >= d.N) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
+    const UniK& u = d.uk;
+    const double4 pi4 = d.pos[i];
+    const double4 vi4 = d.vel[i];
+    const double4 s4 = d.st[i];
+    const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    if constexpr (kSkin) {
+        skin_loop(d.cntV[i], d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
+            const int4 qj = d.posq[j];
+            const PairGeom p = pair_geom(o.q, qj, u);
+            if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
+            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+            return true;
+        });
+        if (d.ND > 0) {
+            skin_loop(d.cntVD[i], d.nbVD, d.KD, i, d.nbD, d.cntD, pi4, d.g, d.dStart, d.dpos, -1, [&](int j) {
+                const PairGeom p = pair_geom(o.q, d.dposq[j], u);
+                if (!cutoff_u(p.r, u, pi4, d.dpos, j)) return false;
+                acc_dummy_u(o, p, d.dvelf[j], d.dnormf[j], u, acc);
+                return true;
+            });
+        }
+    } else {
+        quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+            const int4 qj = d.posq[j];
+            const PairGeom p = pair_geom(o.q, qj, u);
+            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+        });
+        if (d.ND > 0) {
+            quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
+                const PairGeom p = pair_geom(o.q, d.dposq[j], u);
+                acc_dummy_u(o, p, d.dvelf[j], d.dnormf[j], u, acc);
+            });
+        }
+    }
+    double3 a = up(acc);
+    a.x = quad_sum(a.x, gm);
+    a.y = quad_sum(a.y, gm);
+    a.z = quad_sum(a.z, gm);
+    if (sub != 0) return;
+    a += d.gravity;
+    d.acc[i] = d4(a, 0);
+    const double3 v = xyz(vi4) + hdt * a;
+    const double4 v4 = d4(v, vi4.w);
+    d.velOut[i] = v4;
+    d.velfOut[i] = velf_p(v4, s4);
+    if (first) {
+        const double4 pn = d4(xyz(pi4) + dt * v, pi4.w);
+        d.posOut[i] = pn;
+        d.posqOut[i] = fixq_rho(pn, s4, d.g.mn, d.invq);
+        if constexpr (kSkin) {
+            const double3 dd = xyz(pn) - xyz(d.xb[i]);
+            atomicMax(d.maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double dt) {
+    const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
+    if (i >= d.N) return;
+    const int sub = threadIdx.x & 3;
+    const unsigned gm = quad_mask();
+    const UniK& u = d.uk;
+    const double4 pi4 = d.pos[i];
+    const double4 vi4 = d.vel[i];
+    const double4 s4 = d.st[i];
+    const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
+    float sumF = 0.f, sumD = 0.f;  // sum of (1 / rho_j) (v_i - v*) . grad W / (1/2), per kind of neighbour
+    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+        const int4 qj = d.posq[j];
+        const PairGeom p = pair_geom(o.q, qj, u);
+        const float4 vj = d.velf[j];  // (v_j, p_j)
+        const float rhoj = __int_as_float(qj.w);
+        const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
+        const float rbar = 0.5f * (o.rho + rhoj);
+        const float X = __fdividef(o.PL - vj.w, rbar * u.cF);
+        sumF += __fdividef(p.Kdq * (dot(dv, p.r) * p.inv_r + X), rhoj);
+    });
+    if (d.ND > 0) {
+        quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
+            const PairGeom p = pair_geom(o.q, d.dposq[j], u);
+            const float4 vj = d.dvelf[j];
+            float PR, rhoj;
+            dummy_state_u(o, p, u, PR, rhoj);
+            const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
+            const float rbar = 0.5f * (o.rho + rhoj);
+            const float X = __fdividef(o.PL - PR, rbar * u.cbarD);
+            sumD += __fdividef(p.Kdq * (dot(dv, p.r) * p.inv_r + X), rhoj);
+        });
+    }
+    const double dsum = quad_sum(0.5 * ((double)u.mF * (double)sumF + (double)u.mD * (double)sumD), gm);
+    if (sub != 0) return;
+    const double dr = dsum * (2.0 * (double)o.rho);
+    double ch = d.drho[i] + dr * dt;
+    d.drho[i] = ch;
+    const double r0 = d.rho0[i];
+    if (ch < -0.1 * r0) ch = -0.1 * r0;
+    const double4 so = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
+    d.stOut[i] = so;
+    d.stfOut[i] = f4(so);
+    // the next position / velocity buffers: the same records, their packed
+    // shadows with the new rho and p
+    d.posOut[i] = pi4;
+    d.velOut[i] = vi4;
+    d.posqOut[i] = make_int4(o.q.x, o.q.y, o.q.z, __float_as_int((float)so.x));
+    d.velfOut[i] = velf_p(vi4, so);
+}
+
 // Reaction of the fluid on the markers: for marker t, minus the sum over
 // the fluid particles a whose list rows hold t of m_a times marker t's term
 // in a's acceleration, evaluated by the same function from the same state as
@@ -1499,6 +1749,55 @@ struct SphScene {
     int N() const { return nF; }
     int ND() const { return nD; }
     float hUni = 0;      // the common h when uniformH
+    // Uniform particle constants (fluid h, m, c, nu; dummy m, c, nu, rho0,
+    // dummy h = fluid h): the mixed-precision passes then run
+    // k_sph_accel_u / k_sph_density_u.  uniKernels = false keeps the general
+    // passes (for comparisons).
+    struct Uniform {
+        bool on = false;
+        double h = 0, mF = 0, cF = 0, nuF = 0, mD = 0, cD = 0, nuD = 0, rho0D = 0;
+        bool operator==(const Uniform& o) const {
+            return on == o.on && h == o.h && mF == o.mF && cF == o.cF && nuF == o.nuF && mD == o.mD && cD == o.cD &&
+                   nuD == o.nuD && rho0D == o.rho0D;
+        }
+    } uni;
+    bool uniKernels = true;
+    static Uniform uniform_of(const HostSet& f, const HostSet& dm) {
+        Uniform u;
+        if (f.size() == 0) return u;
+        u.h = f.pos[0].w; u.mF = f.vel[0].w; u.cF = f.st[0].z; u.nuF = f.st[0].w;
+        bool ok = true;
+        for (size_t k = 0; k < f.size() && ok; k++)
+            ok = f.pos[k].w == u.h && f.vel[k].w == u.mF && f.st[k].z == u.cF && f.st[k].w == u.nuF;
+        if (dm.size()) {
+            u.mD = dm.vel[0].w; u.cD = dm.st[0].z; u.nuD = dm.st[0].w; u.rho0D = dm.rho0[0];
+            for (size_t k = 0; k < dm.size() && ok; k++)
+                ok = dm.pos[k].w == u.h && dm.vel[k].w == u.mD && dm.st[k].z == u.cD && dm.st[k].w == u.nuD &&
+                     dm.rho0[k] == u.rho0D;
+        }
+        u.on = ok;
+        return u;
+    }
+    bool uni_path() const { return uni.on && uniKernels && precision != DEMSPH_PRECISION_FP64 && nM == 0; }
+    UniK uni_consts() const {
+        UniK k{};
+        const double h = uni.h, qd = (double)q;
+        k.invhq = (float)(qd / h);
+        k.K = (float)(21.0 / (16.0 * kPi * h * h * h * h));
+        k.c2q = (float)((2.0 * h / qd) * (2.0 * h / qd));
+        k.cF = (float)uni.cF;
+        k.mF2 = (float)(2.0 * uni.mF);
+        k.bF = (float)(2.0 * uni.nuF * uni.mF);
+        k.mF = (float)uni.mF;
+        k.mD = (float)uni.mD;
+        k.mD2 = (float)(2.0 * uni.mD);
+        k.bD = (float)(2.0 * (0.5 * (uni.nuF + uni.nuD)) * uni.mD);
+        k.cbarD = (float)(0.5 * (uni.cF + uni.cD));
+        k.invcD2 = uni.cD > 0 ? (float)(1.0 / (uni.cD * uni.cD)) : 0.0f;
+        k.rho0D = (float)uni.rho0D;
+        k.gq = make_float3((float)(gravity.x * qd), (float)(gravity.y * qd), (float)(gravity.z * qd));
+        return k;
+    }
 
     // Coupled DEM balls.  Each is sampled by markers (moving boundary
     // particles) on shells inside its surface; body b owns the markers
@@ -1554,6 +1853,7 @@ struct SphScene {
         d.skin = 0.0f; d.gate = nullptr;
         d.nbV = nbV.p; d.cntV = cntV.p; d.nbVD = nbVD.p; d.cntVD = cntVD.p;
         d.xb = xb.p; d.maxd2 = skinState.p ? skinState.p->maxd2 : nullptr;
+        if (uni.on) d.uk = uni_consts();
         return d;
     }
 
@@ -1656,7 +1956,7 @@ struct SphScene {
                                                        drho[D].p, id[ID].p, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p,
                                                        rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p, posf.p,
                                                        velf[Vv ^ 1].p, stf[S ^ 1].p, posq[P ^ 1].p, fCells.g.mn,
-                                                       invq, gate);
+                                                       invq, gate, packed ? 1 : 0);
         if (gate) {  // a device-side decision: copy back instead of flipping the indices
             k_sph_copy_back<<<grid_for(n, 256), 256, 0, s>>>(
                 n, gate, pos[P ^ 1].p, vel[Vv ^ 1].p, st[S ^ 1].p, rho0[R0 ^ 1].p, drho[D ^ 1].p, id[ID ^ 1].p,
@@ -1674,8 +1974,28 @@ struct SphScene {
         k_sph_shadow<<<grid_for(n, 256), 256, 0, s>>>(n, vel[Vv].p, st[S].p, nullptr, velf[Vv].p, stf[S].p, nullptr);
         k_sph_fix<<<grid_for(n, 256), 256, 0, s>>>(n, pos[P].p, fCells.g.mn, invq, posq[P].p);
         g_launches += 2;
+        if (packed) {
+            k_sph_pack<<<grid_for(n, 256), 256, 0, s>>>(n, pos[P].p, vel[Vv].p, st[S].p, posq[P].p, velf[Vv].p, 1);
+            g_launches += 1;
+        }
         DEMSPH_LAUNCH_CHECK();
         skin_force();
+    }
+    // The fluid shadows' layout follows whether the uniform-constant passes
+    // run (packed) or the general ones; called at the entry of every call
+    // that launches the passes, outside any stream capture.
+    bool packed = false;
+    void sync_mode() {
+        const bool want = ready && uni_path();
+        if (want == packed) return;
+        packed = want;
+        graph.reset();          // captured launches carry the layout
+        oneStepAfter.clear();   // and the packed passes move the buffer indices differently
+        const int n = N();
+        k_sph_pack<<<grid_for(n, 256), 256, 0, s>>>(n, pos[P].p, vel[Vv].p, st[S].p, posq[P].p, velf[Vv].p,
+                                                    packed ? 1 : 0);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
     }
     // Markers from the coupled balls' current state, in cell order.
     void place_markers() {
@@ -1793,6 +2113,10 @@ struct SphScene {
                 else k_sph_accel<float, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
             }
             g_launches += 1;
+        } else if (packed) {
+            if (skin) k_sph_accel_u<true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            else k_sph_accel_u<false><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            g_launches += 1;
         } else {
             if (skin) {
                 if (fp64) k_sph_accel<double, false, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
@@ -1826,6 +2150,18 @@ struct SphScene {
             if (fp64) k_sph_density<double, true><<<grid, kSphBlock, 0, s>>>(d, dt);
             else k_sph_density<float, true><<<grid, kSphBlock, 0, s>>>(d, dt);
             g_launches += 1;
+        } else if (packed) {
+            // the packed shadows carry rho and p: the pass writes the next
+            // buffers of positions and velocities (copies of the records, with
+            // the new rho / p in their shadows) as well
+            d.posOut = pos[P ^ 1].p;
+            d.velOut = vel[Vv ^ 1].p;
+            d.posqOut = posq[P ^ 1].p;
+            d.velfOut = velf[Vv ^ 1].p;
+            k_sph_density_u<<<grid, kSphBlock, 0, s>>>(d, dt);
+            g_launches += 1;
+            P ^= 1;
+            Vv ^= 1;
         } else {
             if (fp64) k_sph_density<double, false><<<grid, kSphBlock, 0, s>>>(d, dt);
             else k_sph_density<float, false><<<grid, kSphBlock, 0, s>>>(d, dt);
@@ -1923,6 +2259,12 @@ struct SphScene {
         long iStep;
         double time;
         int P, Vv, S, R0, D, ID, L;
+        // with the skin lists (rows, rebuild positions, rebuild state), so
+        // that the steps after a restore use the rows the steps after the
+        // snapshot used; valid while the list capacities are unchanged
+        bool lists = false;
+        int KF = 0, KD = 0;
+        bool haveLists = false;
     };
     template <class T>
     void snap_add(Snap& sn, DBuf<T>& b) {
@@ -1934,16 +2276,31 @@ struct SphScene {
         sn.bytes.push_back(b.bytes());
         sn.bufs.push_back(std::move(c));
     }
-    void take(Snap& sn) {
+    void take(Snap& sn, bool withLists = false) {
         sn.iStep = iStep; sn.time = time; sn.P = P; sn.Vv = Vv; sn.S = S; sn.R0 = R0; sn.D = D; sn.ID = ID; sn.L = L;
         snap_add(sn, pos[P]); snap_add(sn, vel[Vv]); snap_add(sn, st[S]); snap_add(sn, rho0[R0]);
         snap_add(sn, drho[D]); snap_add(sn, id[ID]);
+        sn.lists = withLists && skin_on() && nM == 0 && skinState.p;
+        if (sn.lists) {
+            sn.KF = KF; sn.KD = KD; sn.haveLists = haveLists;
+            snap_add(sn, nbV); snap_add(sn, cntV); snap_add(sn, nbVD); snap_add(sn, cntVD); snap_add(sn, xb);
+            snap_add(sn, skinState);
+            snap_add(sn, posf);
+        }
     }
     void restore(Snap& sn) {
-        for (size_t k = 0; k < sn.bufs.size(); k++)
+        const bool lists = sn.lists && sn.KF == KF && sn.KD == KD;
+        for (size_t k = 0; k < sn.bufs.size(); k++) {
+            if (!lists && k >= 6) break;  // the state records come first
             DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
+        }
         iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID; L = sn.L;
         refresh_shadows();  // the FP32 / fixed-point copies follow the restored records (and force a skin rebuild)
+        if (lists) {
+            // the restored rows and rebuild state stand: no forced rebuild
+            DEMSPH_CUDA(cudaMemsetAsync(&skinState.p->force, 0, 1, s));
+            haveLists = sn.haveLists;
+        }
     }
     // Steps without a state snapshot: a list row that overflows its capacity
     // is walked from the cell table by the passes (same neighbours), so an
@@ -1951,6 +2308,7 @@ struct SphScene {
     void run(long n) {
         if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         if (n <= 0) return;
+        sync_mode();
         clear_status();
         long k = 0;
         if (useGraphs && n >= 2) {
@@ -2164,6 +2522,7 @@ struct SphScene {
         nD = (int)hd.size();
         init_grid(mn, mx, g, timeStep, prec, hmax, uni);
         hUni = h0;
+        this->uni = uniform_of(hf, hd);
         const int n = N(), nd = ND();
         auto up4 = [&](DBuf<double4>& b, const HostVec<double4>& h) {
             DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
@@ -2289,6 +2648,7 @@ struct SphScene {
         iStep = 0;
         time = 0;
         ready = true;
+        sync_mode();
         DEMSPH_CUDA(cudaStreamSynchronize(s));
     }
 };
@@ -2395,6 +2755,7 @@ struct demsph_sph_member {
     double hmax = 0;
     float h0 = 0;
     bool uni = true;
+    SphScene::Uniform un;  // uniform constants, recorded at sealing
     DBuf<double4> fpos, fvel, fst, dpos, dvel, dst;
     DBuf<double> frho0, drh;
 };
@@ -2438,6 +2799,7 @@ int demsph_sph_member_seal(demsph_sph_member_t m) {
             }
         m->nf = (int)m->hf.size();
         m->nd = (int)m->hd.size();
+        m->un = SphScene::uniform_of(m->hf, m->hd);
         m->fpos.upload(m->hf.pos, m->s); m->fvel.upload(m->hf.vel, m->s); m->fst.upload(m->hf.st, m->s);
         m->frho0.upload(m->hf.rho0, m->s);
         if (m->nd > 0) {
@@ -2487,6 +2849,23 @@ int demsph_sph_assemble(demsph_sph_t h, int count, const demsph_sph_member_t* me
         s.nD = (int)nd;
         s.init_grid(sld3(mn, 0), sld3(mx, 0), sld3(g, 0), dt, prec, hmax, uni);
         s.hUni = (float)members[0]->h0;
+        // uniform constants: the members' fluid constants agree, and so do the
+        // dummy constants of the members that have dummies
+        SphScene::Uniform un = members[0]->un;
+        bool haveD = members[0]->nd > 0;
+        for (int k = 1; k < count && un.on; k++) {
+            const SphScene::Uniform& v = members[k]->un;
+            un.on = v.on && v.h == un.h && v.mF == un.mF && v.cF == un.cF && v.nuF == un.nuF;
+            if (members[k]->nd > 0) {
+                if (!haveD) {
+                    un.mD = v.mD; un.cD = v.cD; un.nuD = v.nuD; un.rho0D = v.rho0D;
+                    haveD = true;
+                } else {
+                    un.on = un.on && v.mD == un.mD && v.cD == un.cD && v.nuD == un.nuD && v.rho0D == un.rho0D;
+                }
+            }
+        }
+        s.uni = un;
         DBuf<double4> tp, tv, ts;
         DBuf<double> trh;
         if (nd > 0) {
@@ -2529,6 +2908,7 @@ int demsph_sph_neighbor_search(demsph_sph_t h) {
         SPH_CHECK(h);
         SphScene& s = h->sc;
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        s.sync_mode();
         s.clear_status();
         s.neighbor_search();
         DevStatus st2 = s.read_status();
@@ -2546,6 +2926,7 @@ int demsph_sph_eval_accel(demsph_sph_t h) {
         SPH_CHECK(h);
         SphScene& s = h->sc;
         if (!s.ready || !s.haveLists) throw Status(DEMSPH_ERR_NOT_READY, "no neighbour lists");
+        s.sync_mode();
         // acceleration only: kick / drift go to the scratch buffers, the state is unchanged
         SphDev d = s.dev();
         d.posOut = s.pos[s.P ^ 1].p;
@@ -2562,6 +2943,7 @@ int demsph_sph_profile_steps(demsph_sph_t h, long n, double* phaseMs) {
         SphScene& s = h->sc;
         if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         for (int k = 0; k < 5; k++) phaseMs[k] = 0.0;
+        s.sync_mode();
         s.clear_status();
         for (long k = 0; k < n; k++) s.step_profiled(phaseMs);
         DevStatus st2 = s.read_status();
@@ -2685,6 +3067,63 @@ int demsph_sph_set_skin(demsph_sph_t h, double fraction) {
         s.skinFrac = (float)fraction;
         s.graph.reset();  // the captured launches carry the skin
         s.skin_force();
+    });
+}
+int demsph_sph_set_uniform_kernels(demsph_sph_t h, int enable) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        h->sc.uniKernels = enable != 0;
+        h->sc.graph.reset();  // captured launches name the kernels
+        if (h->sc.ready) h->sc.sync_mode();
+    });
+}
+int demsph_sph_uniform_kernels(demsph_sph_t h, int* active) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!active) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        h->sc.sync_mode();
+        *active = h->sc.packed ? 1 : 0;
+    });
+}
+struct demsph_sph_snapshot {
+    demsph_sph_t scene = nullptr;
+    SphScene::Snap snap;
+};
+int demsph_sph_snapshot(demsph_sph_t h, demsph_sph_snapshot_t* out) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!out) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
+        SphScene& s = h->sc;
+        if (!s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
+        auto* sn = new struct demsph_sph_snapshot();
+        sn->scene = h;
+        try {
+            s.take(sn->snap, true);
+            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        } catch (...) {
+            delete sn;
+            throw;
+        }
+        *out = sn;
+    });
+}
+int demsph_sph_restore(demsph_sph_t h, demsph_sph_snapshot_t sn) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (!sn) throw Status(DEMSPH_ERR_INVALID, "null snapshot");
+        if (sn->scene != h) throw Status(DEMSPH_ERR_INVALID, "the snapshot belongs to another scene");
+        SphScene& s = h->sc;
+        s.sync_mode();
+        s.restore(sn->snap);
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+    });
+}
+int demsph_sph_snapshot_destroy(demsph_sph_snapshot_t sn) {
+    return guarded([&] {
+        if (!sn) return;
+        cudaStream_t st = sn->scene ? sn->scene->sc.s : 0;
+        delete sn;
+        DEMSPH_CUDA(cudaStreamSynchronize(st));
     });
 }
 int demsph_sph_diagnostics(demsph_sph_t h, double* out) {
@@ -3030,11 +3469,13 @@ int demsph_sph_couple_balls(demsph_sph_t h, demsph_dem_t dem, long n, const int*
         SPH_CHECK(h);
         if (!dem) throw Status(DEMSPH_ERR_INVALID, "null DEM scene handle");
         h->sc.add_bodies(dem, n, balls, spacing, smoothingLength, soundSpeed, viscosity, density);
+        h->sc.sync_mode();  // the general passes serve scenes with markers
     });
 }
 int demsph_sph_couple_step(demsph_sph_t h, demsph_dem_t dem, long n, int demSubsteps) {
     return guarded([&] {
         SPH_CHECK(h);
+        h->sc.sync_mode();
         h->sc.coupled_run(dem, n, demSubsteps);
     });
 }

@@ -389,6 +389,10 @@ class DEMSolver:
         return {"momentum": out[0:3], "angularMomentum": out[3:6], "kineticEnergy": out[6],
                 "rotationalEnergy": out[7], "mass": out[8], "forceSum": out[9:12]}
 
+    def snapshot(self):
+        """A device copy of the dynamic state (Snapshot.restore puts it back)."""
+        return Snapshot(self, "dem")
+
     def setBondedInteraction(self, isBonded=None, normalForce=None, torsionTorque=None, shearForce=None,
                              bendingTorque=None, normal=None, point=None):
         """Writes the bond state (getBondedInteraction's order; None keeps a field)."""
@@ -543,6 +547,21 @@ class WCSPHSolver:
              _dp(out["normal"]))
         return out
 
+    def snapshot(self):
+        """A device copy of the fluid's state (Snapshot.restore puts it back)."""
+        return Snapshot(self, "sph")
+
+    def setUniformKernels(self, enable=True):
+        """Use (default) or not the passes specialised for uniform particle
+        constants (mixed precision)."""
+        call("demsph_sph_set_uniform_kernels", self._h, int(bool(enable)))
+
+    def uniformKernels(self):
+        """Whether the specialised mixed-precision passes are in use."""
+        a = C.c_int()
+        call("demsph_sph_uniform_kernels", self._h, C.byref(a))
+        return bool(a.value)
+
     def diagnostics(self):
         """demsph_sph_diagnostics: FP64 mass, momentum, kinetic and potential
         energy, summed density change and volume of the fluid."""
@@ -676,3 +695,25 @@ class DEMSPHCoupling:
         F, T = np.zeros((nb, 3)), np.zeros((nb, 3))
         call("demsph_sph_get_coupling", self.sph._h, _ip(ball), _dp(F), _dp(T))
         return ball, F, T
+
+
+class Snapshot:
+    """A device copy of a scene's dynamic state (demsph_dem_snapshot /
+    demsph_sph_snapshot); restore() puts it back into the same scene."""
+
+    def __init__(self, solver, kind):
+        self._solver, self._kind = solver, kind
+        self._h = C.c_void_p()
+        call(f"demsph_{kind}_snapshot", solver._h, C.byref(self._h))
+
+    def restore(self):
+        call(f"demsph_{self._kind}_restore", self._solver._h, self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                getattr(_lib.lib(), f"demsph_{self._kind}_snapshot_destroy")(h)
+            except Exception:
+                pass
+            self._h = None
