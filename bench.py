@@ -15,12 +15,18 @@ kick, drift, continuity + EOS, momentum, kick.  Metric: particle-steps/s
   flushed by writing a 256 MB buffer between timed steps, outside the events.
 * e2e: the same metric through the public solver API as a user runs it:
   scene upload from host memory, K steps, final state read back, all timed.
-* roofline: the momentum kernel (the dominant one), timed live per launch.
-* stream: the serving / batching stream -- 64 seeded scenes (DEM drops and
-  WCSPH dam breaks, 1k-200k particles, 500 steps each, Poisson arrivals)
+* roofline: the momentum kernel (the dominant one), timed live per launch,
+  against the compulsory bytes of one pass of the mixed-precision design,
+  with the FP32-SIMT and instruction-issue fractions beside it.
+* dem: the plain 4,096-sphere bounce, its contact-rich form and the bonded
+  beam + clumps, each with its roofline (measured pair and bond counts).
+* reference_cuda: the reference's own CUDA kernels on the same workloads.
+* conservation_fp64: device FP64 diagnostics of the fluid around the timed steps.
+* stream: the serving / batching stream -- 2,000 seeded scenes (DEM drops
+  and WCSPH dam breaks, 1k-200k particles, 500 steps each, Poisson arrivals)
   through the continuous-batching server in mixed precision, beside the same
-  scenes run one at a time on the plain solver (FP64 and mixed); wall clock,
-  with p50 / p99 scene-step and scene latency.
+  scenes run one at a time on the plain solver (mixed; FP64 on a prefix);
+  wall clock, with p50 / p99 scene-step and scene latency, admission waits.
 * cpu_baseline: the FP64 C++ oracle on the host cores over a short sample.
 * --impl reference: the reference's step restated as the FP64 C++ oracle
   (the reference has no CPU path; its CUDA build cannot be installed as a
@@ -58,7 +64,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--stress", type=int, default=1,
                     help="1: also time the bonded beam + clumps and the coupled ice sheet (about 40 s more)")
-    ap.add_argument("--stream", type=int, default=64,
+    ap.add_argument("--stream", type=int, default=2000,
                     help="scenes in the served-stream measurement (0: skip it)")
     return ap.parse_args()
 
@@ -115,6 +121,33 @@ def workload():
     return scenes.sph_dam_break()
 
 
+def sph_bytes_8d(nf, nd, ncell):
+    """Compulsory HBM bytes of one WCSPH step of the mixed-precision design
+    (the per-step model of the hot-path measurement plan): three passes each
+    reading x, v (FP64) and rho, p, c, h, m, nu (FP32) per particle (72 B);
+    their outputs a, a, drho-rate (12 + 12 + 4 B); the integration's
+    read-modify-write of v, x, drho (48 + 48 + 16 B); the per-step re-key and
+    sort (24 + 8 + 16 B); the dummies read twice (24 B); the cell table (8 B
+    per cell).  Lists and neighbour re-reads are not counted."""
+    return 3 * nf * 72 + nf * (12 + 12 + 4) + nf * (48 + 48 + 16) + nf * (24 + 8 + 16) + nd * 24 * 2 + ncell * 8
+
+
+def momentum_bytes_8d(nf, nd):
+    """The same model for one momentum pass: each fluid particle's 72 B read
+    and its 12 B acceleration written, each dummy's 24 B read."""
+    return nf * (72 + 12) + nd * 24
+
+
+def dem_bytes_8d(n, pairs, springs, bonds):
+    """Compulsory HBM bytes of one DEM step of the mixed-precision design:
+    two force passes reading 88 B and writing 24 B per particle, 288 B of
+    integration per particle, per contact pair 8 B of ids and 48 B per active
+    spring kind read-modify-written in each pass, 192 B per bond per pass,
+    and every fifth step the rebuild (48 B per particle, the pair rows)."""
+    pair = 8 + 48 * springs
+    return 2 * n * (88 + 24) + n * 288 + 2 * pairs * pair + 2 * bonds * 192 + (n * (24 + 8 + 16) + pairs * pair) / 5
+
+
 def algorithmic_bytes_momentum(nf, nd, first):
     """Compulsory HBM bytes of one momentum launch: read each fluid particle's
     pos, vel, (rho, p, c, nu) once (3 x 32 B) and its list row count (4 B),
@@ -156,30 +189,52 @@ def timed_steps(torch, solver, steps, flush):
     return times
 
 
-def dem_bounce(torch, steps, warmup, flush):
-    """The plain DEM elastic bounce: 4,096 Hertz-Mindlin spheres
-    (r 5 mm, rho 2500, 16^3 lattice at 12 mm, +-0.5 mm seeded jitter) dropping
-    onto a 2-triangle plane, dt = 1e-5, mixed precision."""
+def dem_case(torch, name, sc, steps, flush, peak, warm=20, block=10, what=""):
+    """One DEM workload in mixed precision: `warm` steps (graph capture
+    included), then `steps` steps timed `block` at a time with CUDA events,
+    L2 flushed before each block; the roofline of the step against the
+    per-step byte model with the measured pair and bond counts."""
     from this_studio_b200 import scenes
 
-    sc = scenes.dem_drop()
     s = scenes.build_dem(sc, "mixed")
-    s.step(max(warmup, 3))
-    block = 10  # steps per timed call; the call's overflow bookkeeping amortises over them
-    times = []
-    torch.cuda.synchronize()
-    for _ in range(max(1, steps // block)):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        s.step(block)
-        e1.record()
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-    ms = float(sum(times)) / (len(times) * block)
-    return {"workload": "dem_bounce_4096", "value": sc.position.shape[0] / (ms / 1e3), "unit": METRIC,
-            "ms_per_step": ms, "precision": "mixed", "steps": steps,
-            "note": "4,096 spheres: each kernel runs 4,096 threads, bound by the latency of their dependent loads"}
+    s.step(warm)
+    ms = _event_steps(torch, s.step, steps, block, flush)
+    n = int(sc.num_moving)
+    pairs = int(s.getPairs(0)["objectPointed"].size)
+    bonds = int(s.getBondedInteraction()["isBonded"].sum()) if sc.bonded else 0
+    row = sc.hertz[0] if sc.hertz else None
+    springs = 1 + (1 if row is not None and row[5] > 0 else 0) + (1 if row is not None and row[6] > 0 else 0)
+    b = dem_bytes_8d(n, pairs, springs, bonds)
+    achieved = b / (ms / 1e3) / 1e9
+    d = s.diagnostics()
+    return {"workload": name, "value": n / (ms / 1e3), "unit": METRIC, "ms_per_step": ms, "precision": "mixed",
+            "steps": steps, "moving_particles": n, "pairs": pairs, "springs_per_pair": springs, "bonds": bonds,
+            "what": what,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_step": b, "model": "dem_bytes_8d (bench.py)"},
+            "diagnostics_fp64": {"momentum": [float(x) for x in d["momentum"]],
+                                 "kinetic_energy": float(d["kineticEnergy"]),
+                                 "rotational_energy": float(d["rotationalEnergy"])}}
+
+
+def dem_cases(torch, flush, peak, stress):
+    """The DEM rows: the plain bounce as specified (4,096 spheres, plane
+    1 mm below the lowest nominal sphere bottom: few contacts), its
+    contact-rich form (the same 4,096 spheres as a touching pack with
+    friction, rolling and torsion), and the bonded beam + clumps."""
+    from this_studio_b200 import scenes
+
+    out = {"bounce": dem_case(torch, "dem_bounce_4096", scenes.dem_drop(), 200, flush, peak,
+                              what="4,096 spheres: each kernel runs 4,096 threads, bound by the latency of their "
+                                   "dependent loads"),
+           "contact_rich": dem_case(torch, "dem_pack_4096", scenes.dem_pack(n_side=16), 200, flush, peak,
+                                    what="the 4,096 spheres touching (1.1 (r_i + r_j) lists of ~11.5k pairs), "
+                                         "friction, rolling and torsion springs")}
+    if stress:
+        out["beam_clumps"] = dem_case(torch, "bonded_beam_clumps_220k", scenes.bonded_beam_clumps(), 100, flush,
+                                      peak, warm=10,
+                                      what="20 x 20 x 400 bonded beam (462,840 bonds) + 20,000 three-sphere clumps")
+    return out
 
 
 def coupled_tank(torch, steps, warmup, flush):
@@ -216,29 +271,6 @@ def coupled_tank(torch, steps, warmup, flush):
             "balls": nb, "markers": nm, "dem_substeps": sc.dem_substeps, "precision": "mixed", "steps": steps}
 
 
-def beam_clumps(torch, steps):
-    """The bonded beam plus clumps stress scene: a 20 x 20 x 400 bonded beam of
-    r = 1 mm spheres (parallel bonds on the face contacts, one end clamped,
-    seeded tip load) beside 20,000 three-sphere clumps, dt = 1e-7, mixed
-    precision.  Particles counted: moving spheres and pebbles."""
-    from this_studio_b200 import scenes
-
-    sc = scenes.bonded_beam_clumps()
-    s = scenes.build_dem(sc, "mixed")
-    s.step(20)
-    n = int((~sc.fixed).sum()) + 3 * len(sc.clumps)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    s.step(steps)
-    e1.record()
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    nb = int(s.getBondedInteraction()["isBonded"].size)
-    return {"workload": "bonded_beam_clumps_220k", "value": n / (ms / 1e3), "unit": METRIC, "ms_per_step": ms,
-            "moving_particles": n, "bonds": nb, "clumps": len(sc.clumps), "precision": "mixed", "steps": steps}
-
-
 def ice_sheet(torch, steps):
     """The coupled ice-sheet stress scene: about 1M bonded r = 2 mm spheres
     moving into a 20,000-triangle cylinder, floating on 2M WCSPH particles
@@ -265,41 +297,46 @@ def ice_sheet(torch, steps):
             "dem_substeps": sc.dem_substeps, "precision": "mixed", "steps": steps}
 
 
-def served_stream(torch, num, seed=5, rate=30.0, steps=500, chunk=100, plain=None, warm=True):
-    """The serving / batching stream (seeded Poisson arrivals of DEM drops and
-    WCSPH dam breaks, particle counts log-uniform over 1k-200k, polydisperse
-    DEM radii, 500 steps each): the first `num` scenes served by the
-    continuous-batching server (mixed precision), then the same scenes run
-    one after another on the plain solver in FP64 and in mixed precision.
-    Wall-clock times; scenes are generated before each clock starts.
-    `plain` reuses the plain solver's values of an earlier call on the same
-    scenes (the sizes do not depend on the arrival rate)."""
+def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sample=200, warm=True):
+    """The serving / batching stream: `num` seeded scenes (DEM drops and WCSPH
+    dam breaks, particle counts log-uniform over 1k-200k, polydisperse DEM
+    radii with sigma 0.2 and max/min <= 3, 500 steps each) arriving as a
+    Poisson process at `rate` per second -- an offered load above the
+    server's capacity, so the queue builds and the throughput is the
+    server's -- served by the continuous-batching server in mixed precision
+    (batches of up to 512 members, admitted by an HBM budget); then the same
+    scenes one after another on the plain solver in mixed precision, and the
+    first `fp64_sample` of them in FP64.  Wall-clock times; scenes are
+    generated before each clock starts."""
     from this_studio_b200 import serve
 
     n_max = 200_000
     c0, dt = serve.stream_params(n_max)
-    mk = lambda: serve.make_stream(num, seed=seed, n_min=1000, n_max=n_max, rate=rate, steps=steps)
+    mk = lambda k: serve.make_stream(k, seed=seed, n_min=1000, n_max=n_max, rate=rate, steps=steps)
     # warm-up on a stream of the same sizes (another seed): kernel loads, graph
     # executables and the memory pool grown to the stream's working set, as in
     # a server that has been running
     if warm:
-        serve.SceneServer(hbm_budget=60e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt).run(
+        serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt).run(
             serve.make_stream(24, seed=1, n_min=1000, n_max=n_max, rate=1e3, steps=100))
-    reqs = mk()
+    reqs = mk(num)
     ps = serve.particle_steps(reqs, c0, dt)
-    srv = serve.SceneServer(hbm_budget=60e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt)
+    n_dem = sum(1 for r in reqs if r.kind == "dem")
+    srv = serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", max_members=512, sph_c0=c0, sph_dt=dt)
     torch.cuda.synchronize()
     m = srv.run(reqs)
-    if plain is None:
-        plain = {}
-        for prec in ("fp64", "mixed"):
-            plain[prec] = ps / serve.run_plain(mk(), prec, c0, dt)
-    return {"workload": f"served_stream_{num}", "scenes": num, "seed": seed, "arrival_rate_per_s": rate,
-            "steps_per_scene": steps, "chunk_steps": chunk, "particle_steps": ps,
-            "value": m["value"], "unit": METRIC, "makespan_s": m["makespan_s"],
-            "plain_fp64_value": plain["fp64"], "plain_mixed_value": plain["mixed"],
-            "speedup_vs_plain_fp64": m["value"] / plain["fp64"],
-            "speedup_vs_plain_mixed": m["value"] / plain["mixed"],
+    del reqs
+    plain_mixed = ps / serve.run_plain(mk(num), "mixed", c0, dt)
+    k = min(fp64_sample, num)
+    sample = mk(k)
+    ps_k = serve.particle_steps(sample, c0, dt)
+    plain_fp64 = ps_k / serve.run_plain(sample, "fp64", c0, dt)
+    return {"workload": f"served_stream_{num}", "scenes": num, "dem_scenes": n_dem, "seed": seed,
+            "arrival_rate_per_s": rate, "steps_per_scene": steps, "chunk_steps": chunk, "max_members": 512,
+            "particle_steps": ps, "value": m["value"], "unit": METRIC, "makespan_s": m["makespan_s"],
+            "plain_mixed_value": plain_mixed, "speedup_vs_plain_mixed": m["value"] / plain_mixed,
+            "plain_fp64_value": plain_fp64, "plain_fp64_what": f"the first {k} scenes of the stream",
+            "speedup_vs_plain_fp64": m["value"] / plain_fp64,
             "scene_step_latency_p50_ms": m["scene_step_latency_p50_ms"],
             "scene_step_latency_p99_ms": m["scene_step_latency_p99_ms"],
             "scene_latency_p50_s": m["scene_latency_p50_s"], "scene_latency_p99_s": m["scene_latency_p99_s"],
@@ -320,9 +357,18 @@ def native(args, rank, world, dist):
     nf, nd = sc.fluid.shape[0], sc.dummy.shape[0]
     solver = build_sph(sc, args.precision)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    # warm-up
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    peak = peaks.get("hbm_gbs", 6650.0)
+    # warm-up: the requested steps, then single steps so that the one-step
+    # graphs of both buffer states are captured before the timed region
     solver.step(max(args.warmup, 3))
+    for _ in range(4):
+        solver.step(1)
     torch.cuda.synchronize()
+    diag0 = solver.diagnostics()
     if dist:
         dist.barrier()
     clocks = ClockSampler(torch.cuda.current_device())
@@ -332,9 +378,11 @@ def native(args, rank, world, dist):
     torch.cuda.synchronize()
     launches = tsb.kernel_launches() - launches0
     clk = clocks.stop()
+    diag1 = solver.diagnostics()
     total_ms = float(sum(times))
     total_ms = max_over_ranks(torch, dist, total_ms, dev)
     value = replica_value(nf, args.steps, world, total_ms)
+    step_ms = total_ms / args.steps
 
     # per-kernel live timing for the roofline (same stream, events per phase)
     import ctypes as C
@@ -344,70 +392,71 @@ def native(args, rank, world, dist):
     _lib.call("demsph_sph_profile_steps", solver._h, nprof, phases)
     ph = list(phases)
     mom_ms = 0.5 * (ph[2] + ph[4])
-    mom_bytes = 0.5 * (algorithmic_bytes_momentum(nf, nd, True) + algorithmic_bytes_momentum(nf, nd, False))
-    peaks = {}
-    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(pk_path):
-        peaks = json.load(open(pk_path))
-    peak = peaks.get("hbm_gbs", 6650.0)
+    impl_bytes = 0.5 * (algorithmic_bytes_momentum(nf, nd, True) + algorithmic_bytes_momentum(nf, nd, False))
+    mom_bytes = momentum_bytes_8d(nf, nd)
     achieved = mom_bytes / (mom_ms / 1e3) / 1e9
-    traffic = None
-    inst = None
+    ncell = 1
+    for a, b in zip(sc.minb, sc.maxb):
+        ncell *= max(1, int((b - a) / (2.0 * 1.3 * sc.spacing * 1.04)))
+    step_bytes = sph_bytes_8d(nf, nd, ncell)
+    tj = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         tj = json.load(open(tpath))
-        traffic = tj.get("k_sph_accel_bytes_per_launch")
-        inst = tj.get("k_sph_accel_warp_instructions_per_launch")
+    traffic = tj.get("k_sph_accel_bytes_per_launch")
+    inst = tj.get("k_sph_accel_warp_instructions_per_launch")
+    flop = tj.get("k_sph_accel_fp32_flop_per_launch")
+    sm_hz = (clk.get("sm_mhz") or 1965.0) * 1e6
 
     # end to end through the public API: upload, K steps, read back.  Three
     # complete runs (each scene destroyed after its read-back), the median
     # reported: the first one also pays for mapping fresh device memory, which
     # on a shared GPU has varied from 10 ms to 300 ms; the later ones reuse
-    # the memory the library's pool keeps (its default).
-    runs_s = []
+    # the memory the library's pool keeps (its default).  Each run's time is
+    # split by host timers into scene set-up (add + initialise), the steps and
+    # the read-back.
+    runs_s, parts = [], []
     for _ in range(3):
         torch.cuda.synchronize()
         h0 = time.perf_counter()
         s2 = build_sph(sc, args.precision)
+        torch.cuda.synchronize()
+        h1 = time.perf_counter()
         s2.step(args.steps)
+        torch.cuda.synchronize()
+        h2 = time.perf_counter()
         out = s2.getSPH()
         torch.cuda.synchronize()
-        runs_s.append(time.perf_counter() - h0)
+        h3 = time.perf_counter()
+        runs_s.append(h3 - h0)
+        parts.append({"setup_ms": 1e3 * (h1 - h0), "steps_ms": 1e3 * (h2 - h1), "readback_ms": 1e3 * (h3 - h2)})
         del s2
         torch.cuda.synchronize()
-    e2e_s = sorted(runs_s)[1]
+    k = sorted(range(3), key=lambda i: runs_s[i])[1]
+    e2e_s = runs_s[k]
     h2d = (nf + nd) * (3 * 8 * 2 + 4 * 8)  # positions, velocities, 4 scalars per particle
     d2h = sum(v.nbytes for v in out.values()) + 16 * args.steps  # final state + per-step status word
     e2e = nf * args.steps * world / e2e_s
 
-    # the other precision and the DEM workload, for reference next to the headline
+    # the other precision and the DEM workloads, next to the headline
     other = "fp64" if args.precision == "mixed" else "mixed"
     s3 = build_sph(sc, other)
     s3.step(3)
+    for _ in range(4):
+        s3.step(1)
     t3 = timed_steps(torch, s3, min(args.steps, 100), flush)
     del s3
     other_value = nf / (float(sum(t3)) / len(t3) / 1e3)
-    dem = dem_bounce(torch, min(args.steps, 200), args.warmup, flush)
-    coupled = coupled_tank(torch, min(args.steps, 100), args.warmup, flush)
+    dem = dem_cases(torch, flush, peak, args.stress)
+    coupled = coupled_tank(torch, 100, args.warmup, flush)
     del flush
-    beam = beam_clumps(torch, min(args.steps, 200)) if args.stress else None
-    ice = ice_sheet(torch, min(args.steps, 40)) if args.stress else None
+    ice = ice_sheet(torch, 40) if args.stress else None
     stream = served_stream(torch, args.stream) if (args.stream > 0 and rank == 0 and world == 1) else None
-    if stream is not None:
-        # the same scenes all waiting at the start: the server's throughput
-        # without the arrival process bounding the makespan
-        sat = served_stream(torch, args.stream, rate=1e9, warm=False,
-                            plain={"fp64": stream["plain_fp64_value"], "mixed": stream["plain_mixed_value"]})
-        stream["saturated"] = {k: sat[k] for k in ("value", "makespan_s", "speedup_vs_plain_fp64",
-                                                   "speedup_vs_plain_mixed", "scene_step_latency_p50_ms",
-                                                   "scene_step_latency_p99_ms", "scene_latency_p50_s",
-                                                   "scene_latency_p99_s")}
-        stream["saturated"]["arrivals"] = "all at t = 0"
 
-
+    fp32_peak = 148 * 128 * 2 * sm_hz
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": "synthetic (seeded lattice dam break, no dataset)",
         "config": {"workload": WORKLOAD, "fluid_particles": nf, "dummy_particles": nd, "h": 1.3 * sc.spacing,
@@ -418,7 +467,6 @@ def native(args, rank, world, dist):
         "value_" + other: other_value,
         "dem": dem,
         "coupled": coupled,
-        "beam_clumps": beam,
         "ice_sheet": ice,
         "stream": stream,
         "gpu_launches": int(launches),
@@ -426,28 +474,50 @@ def native(args, rank, world, dist):
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
                 "what": "build scene from host arrays, initialise, K steps, read state back; median of 3 runs",
-                "runs_s": runs_s, "first_run_value": nf * args.steps * world / runs_s[0]},
-        "roofline": {"bound": "hbm", "kernel": "k_sph_accel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "runs_s": runs_s, "first_run_value": nf * args.steps * world / runs_s[0],
+                "median_run_parts_ms": parts[k], "setup_ms_per_scene": parts[k]["setup_ms"],
+                "readback_ms_per_scene": parts[k]["readback_ms"]},
+        # the dominant kernel against the compulsory bytes of one momentum
+        # pass of the mixed-precision design (72 B read + 12 B written per
+        # fluid particle, 24 B per dummy); the step against the per-step model
+        "roofline": {"bound": "hbm", "kernel": "k_sph_accel_u", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": mom_bytes, "ms_per_launch": mom_ms,
+                     "model": "momentum_bytes_8d (bench.py)",
+                     "implementation_bytes_per_launch": impl_bytes,
+                     "implementation_frac": impl_bytes / (mom_ms / 1e3) / 1e9 / peak,
+                     "step": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (step_ms / 1e3) / 1e9,
+                              "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak},
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s"},
-        # the bound the SPH passes actually sit at: warp-instruction issue
-        # (4 per SM per clock: 148 SMs at the sampled SM clock); instructions per
-        # launch from the committed ncu capture, time live
+        # the bounds the SPH passes actually sit at: FP32 SIMT throughput and
+        # warp-instruction issue (4 per SM per clock; 148 SMs at the sampled
+        # SM clock); flop and instruction counts per launch from the committed
+        # ncu capture, time live
+        "fp32_simt": None if not flop else {
+            "kernel": "k_sph_accel_u", "achieved": flop / (mom_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+            "peak": fp32_peak / 1e12, "frac": flop / (mom_ms / 1e3) / fp32_peak, "flop_per_launch": flop,
+            "source": "profiles/traffic.json (ncu: 2 x ffma + fadd + fmul thread instructions)"},
         "issue_roofline": None if not inst else {
-            "kernel": "k_sph_accel", "achieved": inst / (mom_ms / 1e3), "unit": "warp-instructions/s",
-            "peak": 4 * 148 * (clk.get("sm_mhz") or 1965.0) * 1e6,
-            "frac": inst / (mom_ms / 1e3) / (4 * 148 * (clk.get("sm_mhz") or 1965.0) * 1e6),
+            "kernel": "k_sph_accel_u", "achieved": inst / (mom_ms / 1e3), "unit": "warp-instructions/s",
+            "peak": 4 * 148 * sm_hz, "frac": inst / (mom_ms / 1e3) / (4 * 148 * sm_hz),
             "instructions_per_launch": inst, "source": "profiles/traffic.json (ncu smsp__inst_executed.sum)"},
         "phase_ms": {"cell_sort": ph[0], "reorder_lists": ph[1], "momentum_1": ph[2], "continuity_eos": ph[3],
                      "momentum_2": ph[4]},
+        "conservation_fp64": {
+            "what": "device diagnostics of the fluid before and after the timed steps",
+            "mass_change": diag1["mass"] - diag0["mass"],
+            "momentum_before": [float(x) for x in diag0["momentum"]],
+            "momentum_after": [float(x) for x in diag1["momentum"]],
+            "kinetic_energy": [diag0["kineticEnergy"], diag1["kineticEnergy"]],
+            "potential_energy": [diag0["potentialEnergy"], diag1["potentialEnergy"]],
+            "density_change_sum": [diag0["densityChangeSum"], diag1["densityChangeSum"]]},
     }
     if rank == 0:
         line["cpu_baseline"] = cpu_baseline(sc)
         if world == 1:
             fl = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-            mine = {"sph": total_ms / args.steps, "dem": dem["ms_per_step"],
-                    "beam": beam_only(torch, min(args.steps, 20), fl) if args.stress else None}
+            mine = {"sph": step_ms, "dem": dem["bounce"]["ms_per_step"],
+                    "beam": beam_only(torch, 20, fl) if args.stress else None}
             line["reference_cuda"] = reference_cuda_baseline(torch, sc, min(args.steps, 50), args.warmup, fl, mine)
             del fl
     return line

@@ -25,10 +25,13 @@ import numpy as np
 from . import scenes
 from .batch import DEMBatch, Member, SPHBatch
 
-# device bytes per particle (state + lists at their usual capacities)
-DEM_BYTES_PER_BALL = 2400
-SPH_BYTES_PER_FLUID = 900
-SPH_BYTES_PER_DUMMY = 200
+# device bytes per particle: state, lists at their usual capacities and the
+# step's snapshot for overflow replay (measured on a B200: 5.2 kB per ball of a
+# 195k-ball drop, 2.6 kB per fluid particle of a 195k-particle dam break with
+# as many dummies), with some headroom
+DEM_BYTES_PER_BALL = 5600
+SPH_BYTES_PER_FLUID = 1800
+SPH_BYTES_PER_DUMMY = 900
 
 
 @dataclass
