@@ -316,13 +316,18 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
     # warm-up on a stream of the same sizes (another seed): kernel loads, graph
     # executables and the memory pool grown to the stream's working set, as in
     # a server that has been running
+    # a server that has been running; the autotuner (cell size, list shape,
+    # skin, capacities per kind) runs on that warm-up stream's scenes
+    tunings, tune = None, None
     if warm:
-        serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt).run(
-            serve.make_stream(24, seed=1, n_min=1000, n_max=n_max, rate=1e3, steps=100))
+        w = serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", sph_c0=c0, sph_dt=dt, autotune=True)
+        wm = w.run(serve.make_stream(24, seed=1, n_min=1000, n_max=n_max, rate=1e3, steps=100))
+        tunings, tune = w.tunings, {"seconds": wm.get("tune_s"), **wm.get("tuning", {})}
     reqs = mk(num)
     ps = serve.particle_steps(reqs, c0, dt)
     n_dem = sum(1 for r in reqs if r.kind == "dem")
-    srv = serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", max_members=512, sph_c0=c0, sph_dt=dt)
+    srv = serve.SceneServer(hbm_budget=55e9, chunk=chunk, precision="mixed", max_members=512, sph_c0=c0, sph_dt=dt,
+                            tunings=tunings)
     torch.cuda.synchronize()
     m = srv.run(reqs)
     del reqs
@@ -341,7 +346,7 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
             "scene_step_latency_p99_ms": m["scene_step_latency_p99_ms"],
             "scene_latency_p50_s": m["scene_latency_p50_s"], "scene_latency_p99_s": m["scene_latency_p99_s"],
             "admission_wait_p50_s": m["admission_wait_p50_s"], "admission_wait_p99_s": m["admission_wait_p99_s"],
-            "per_kind": m["per_kind"]}
+            "per_kind": m["per_kind"], "autotune": tune}
 
 
 def native(args, rank, world, dist):
@@ -374,9 +379,15 @@ def native(args, rank, world, dist):
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     launches0 = tsb.kernel_launches()
+    rebuilds0 = solver.skinStats()[1]
     times = timed_steps(torch, solver, args.steps, flush)
     torch.cuda.synchronize()
-    launches = tsb.kernel_launches() - launches0
+    # the launch counter sees host-issued launches; a list rebuild inside a
+    # graph step is a conditional node whose kernels run only when the
+    # device decides to rebuild: add them per rebuild
+    cond_active, per_rebuild = solver.conditionalRebuild()
+    rebuilds = solver.skinStats()[1] - rebuilds0
+    launches = tsb.kernel_launches() - launches0 + (rebuilds * per_rebuild if cond_active else 0)
     clk = clocks.stop()
     diag1 = solver.diagnostics()
     total_ms = float(sum(times))
@@ -470,6 +481,8 @@ def native(args, rank, world, dist):
         "ice_sheet": ice,
         "stream": stream,
         "gpu_launches": int(launches),
+        "list_rebuilds": {"timed_steps": int(rebuilds), "conditional_graph_node": bool(cond_active),
+                          "kernels_per_rebuild": int(per_rebuild)},
         "clocks": clk,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,

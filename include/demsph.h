@@ -197,6 +197,12 @@ int demsph_dem_set_periodic(demsph_dem_t s, int x, int y, int z);
  * before initialize (they still grow on demand), capacity reads the current
  * ones. */
 int demsph_dem_reserve(demsph_dem_t s, int pairsPerBall, int reversePerBall, int trianglesPerBall);
+/* No counterpart in the reference (autotuner).  The ball grid's cell edge as a
+ * multiple (1 to 4) of the reference's 2 r_max (DEMSolver.h:245-263); set
+ * before initialisation.  Any factor gives the same pairs (a 27-cell stencil
+ * still covers every contact); rows come in another order, so sums differ by
+ * rounding. */
+int demsph_dem_set_cell_factor(demsph_dem_t s, double factor);
 int demsph_dem_capacity(demsph_dem_t s, int* pairsPerBall, int* reversePerBall, int* trianglesPerBall);
 int demsph_dem_initialize(demsph_dem_t s, const double* minBoundary, const double* maxBoundary,
                           const double* gravity, double timeStep, int precision);
@@ -274,10 +280,22 @@ int demsph_dem_import_wall_springs(demsph_dem_t s, long n, const int* ball, cons
  * the same material / spring configuration. */
 int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, int count, const int* srcStart, const int* dstStart,
                             const int* num, const int* triDelta, const double* shift);
+/* No counterpart in the reference (batching).  Carries the clumps and bonds
+ * of continuing members from scene src into scene dst, after
+ * demsph_dem_copy_members has carried their balls: member k's clumps
+ * [srcClump[k], +numClumps[k]) in src become [dstClump[k], ...) in dst
+ * (centroid plus shift[3k..3k+2], velocity, angular velocity, orientation)
+ * and its bonds [srcBond[k], +numBonds[k]) become [dstBond[k], ...) (intact
+ * flag, contact point plus shift, normal, accumulated forces and torques,
+ * peak stresses).  The bonds of a member must join the same member balls, in
+ * the same order, in both scenes. */
+int demsph_dem_copy_member_bodies(demsph_dem_t dst, demsph_dem_t src, int count, const int* srcClump,
+                                  const int* dstClump, const int* numClumps, const int* srcBond, const int* dstBond,
+                                  const int* numBonds, const double* shift);
 /* Batch members (no counterpart in the reference).  A member is one scene's
  * balls uploaded once to the device: create, add balls exactly as
- * demsph_dem_add_balls (no clumps), seal (validates, uploads, drops the host
- * copy).  demsph_dem_assemble_balls places `count` sealed members' balls into
+ * demsph_dem_add_balls and clumps as demsph_dem_add_clump, seal (validates,
+ * uploads, drops the host copy of the balls).  demsph_dem_assemble_balls places `count` sealed members' balls into
  * a scene that has none yet -- member k translated by offsets[3k..3k+2], its
  * material ids shifted by matOffset[k], member order kept -- as
  * demsph_dem_add_balls would from the same balls; walls, materials and the
@@ -287,6 +305,15 @@ int demsph_dem_member_destroy(demsph_dem_member_t m);
 int demsph_dem_member_add_balls(demsph_dem_member_t m, long n, const double* position, const double* velocity,
                                 const double* angularVelocity, const double* radius, const double* density,
                                 const int* materialID, int fixed);
+/* addClump (DEMSolver.h:1796-1845) into a member: its pebbles follow the
+ * member's balls added so far (member-local indices), the clump keeps its
+ * centroid, velocity, angular velocity and inverse inertia.  Assembly
+ * appends the clumps of each member, in member order, to the scene's clump
+ * table (centroids translated, pebble ranges and clump ids renumbered). */
+int demsph_dem_member_add_clump(demsph_dem_member_t m, long np, const double* point, const double* radius,
+                                const double* centroid, const double* velocity, const double* angularVelocity,
+                                double mass, const double* inertia, int materialID);
+int demsph_dem_member_num_clumps(demsph_dem_member_t m, long* n);
 int demsph_dem_member_seal(demsph_dem_member_t m);
 int demsph_dem_member_count(demsph_dem_member_t m, long* n);
 int demsph_dem_assemble_balls(demsph_dem_t s, int count, const demsph_dem_member_t* members, const double* offsets,
@@ -364,6 +391,29 @@ int demsph_sph_profile_steps(demsph_sph_t s, long numSteps, double* phaseMs);
  * The lists are unchanged by the choice (same pairs, same order). */
 int demsph_sph_tune(demsph_sph_t s, int trials, int* chosen, double* msPerShape);
 int demsph_sph_num_list_shapes(void);
+/* No counterpart in the reference (autotuner).  The grid's cell edge as a
+ * multiple (1 to 4) of 2 h_max (1 + skin); set before initialisation.  Any
+ * factor gives the same pairs; rows come in another order. */
+int demsph_sph_set_cell_factor(demsph_sph_t s, double factor);
+/* No counterpart in the reference.  In CUDA-graph steps of a scene with skin
+ * lists (and no coupled balls), the list rebuild -- cell sort, reorder, skin
+ * rows -- is the body of a conditional graph node whose condition the
+ * rebuild decision sets on the device, so steps that keep their lists launch
+ * none of its kernels (enable = 0: the rebuild's kernels are launched every
+ * step and return at once when the decision says so; results are identical).
+ * conditional_rebuild reports whether it is in use and how many kernels one
+ * rebuild runs (the library's launch counter counts them only when they run,
+ * which the host does not see: add rebuilds x launchesPerRebuild). */
+int demsph_sph_set_conditional_rebuild(demsph_sph_t s, int enable);
+int demsph_sph_conditional_rebuild(demsph_sph_t s, int* active, long* launchesPerRebuild);
+/* No counterpart in the reference (autotuner).  The neighbour rows are sized at
+ * initialisation to the longest row of one build times (1 + fraction)
+ * (default 0.125) and regrown by a quarter when a later build overflows
+ * (the step is then replayed); set before initialisation.  list_capacity
+ * reports the current row capacities of the fluid-fluid and fluid-dummy
+ * lists. */
+int demsph_sph_set_list_headroom(demsph_sph_t s, double fraction);
+int demsph_sph_list_capacity(demsph_sph_t s, int* fluidRow, int* dummyRow);
 /* Selects a list-build block shape by index (what demsph_sph_tune picks). */
 int demsph_sph_set_list_shape(demsph_sph_t s, int shape);
 

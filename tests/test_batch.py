@@ -162,3 +162,88 @@ def test_dem_assemble_matches_host_build(gpu):
     for k in ("position", "velocity", "angularVelocity"):
         np.testing.assert_array_equal(pa[k], pb[k])
     assert DEMMember is not None
+
+
+def _sorted_bonds(bo, base=0):
+    key = np.lexsort((bo["objectPointing"], bo["objectPointed"]))
+    return {k: v[key] for k, v in bo.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_dem_clumps_and_bonds_same_alone_and_in_mix(gpu, prec, tol):
+    """Members with clumps and bonds (agglomerates bonded on their initial
+    contacts, rigid 3-sphere clumps) keep their bodies across a membership
+    change: balls, pebbles, clump states and bond states after 100 steps match
+    the scene run alone."""
+    x = scenes.dem_agglomerate_drop(1500, seed=1)
+    y = scenes.dem_agglomerate_drop(2400, seed=2)
+    rng = np.random.default_rng(0)
+    for sc in (x, y):  # stress the bonds and spin the clumps from the first step
+        sc.velocity = rng.normal(0.0, 0.05, sc.position.shape)
+        for c in sc.clumps:
+            c["angularVelocity"] = tuple(rng.normal(0.0, 20.0, 3))
+    others = [scenes.dem_drop_poly(800, seed=3), scenes.dem_drop_poly(1200, seed=4),
+              scenes.dem_agglomerate_drop(900, seed=5)]
+    alone = {}
+    for k, sc in ((0, x), (1, y)):
+        s = scenes.build_dem(sc, prec)
+        s.step(100)
+        alone[k] = (s.getBall(), s.getClump(), s.getBondedInteraction())
+    b = batch.DEMBatch(prec)
+    b.members = [batch.Member(1, y), batch.Member(2, others[0]), batch.Member(0, x)]
+    b.rebuild()
+    b.step(45)
+    keep = {m.key: m for m in b.members}
+    # x and y continue at other indices; one leaves, two arrive
+    b.members = [batch.Member(3, others[1]), keep[0], batch.Member(4, others[2]), keep[1]]
+    b.rebuild()
+    b.step(55)
+    b.capture()
+    got = {m.key: m for m in b.members}
+    for k, sc in ((0, x), (1, y)):
+        st = got[k].state
+        assert got[k].steps_done == 100
+        ball, cl, bo = alone[k]
+        p0 = np.concatenate([sc.position] + [np.asarray(c["point"]) for c in sc.clumps])
+        e_pos = rel_err(st["position"] - p0, ball["position"] - p0)
+        e_clump = rel_err(st["clumps"]["position"] - np.array([c["centroid"] for c in sc.clumps]),
+                          cl["position"] - np.array([c["centroid"] for c in sc.clumps]))
+        e_q = np.abs(st["clumps"]["orientation"] - cl["orientation"]).max()
+        mine, ref = _sorted_bonds(st["bonds"]), _sorted_bonds(bo)
+        np.testing.assert_array_equal(mine["objectPointed"], ref["objectPointed"])
+        np.testing.assert_array_equal(mine["objectPointing"], ref["objectPointing"])
+        np.testing.assert_array_equal(mine["isBonded"], ref["isBonded"])
+        e_fn = np.abs(mine["normalForce"] - ref["normalForce"]).max() / np.abs(ref["normalForce"]).max()
+        print(f"{prec} member {k}: {len(sc.clumps)} clumps, {len(ref['isBonded'])} bonds; alone vs in the mix: "
+              f"displacement {e_pos:.2e}, clump displacement {e_clump:.2e}, orientation {e_q:.2e}, "
+              f"bond normal force {e_fn:.2e}")
+        assert len(ref["isBonded"]) > 0 and len(sc.clumps) > 0
+        assert e_pos < tol and e_clump < tol and e_q < tol
+        assert e_fn < (1e-7 if prec == "fp64" else 1e-3)
+
+
+@pytest.mark.gpu
+def test_server_serves_bonded_and_clump_scenes(gpu):
+    """The DEM batch of the server takes agglomerate / clump scenes beside
+    plain drops; each result equals the scene run alone."""
+    reqs = serve.make_stream(8, seed=21, n_min=1000, n_max=4000, rate=400.0, steps=40,
+                             kinds=("dem", "dem_bonded", "sph"))
+    assert any(r.kind == "dem_bonded" for r in reqs)
+    srv = serve.SceneServer(hbm_budget=2e9, chunk=20, precision="fp64", keep_states=True)
+    srv.run(reqs)
+    c0, dt = srv.sph_c0, srv.sph_dt
+    checked = 0
+    for r in reqs:
+        if r.kind != "dem_bonded":
+            continue
+        sc = r.build(c0, dt)
+        s = scenes.build_dem(sc, "fp64")
+        s.step(r.steps)
+        ref = s.getBall()["position"]
+        p0 = np.concatenate([sc.position] + [np.asarray(c["point"]) for c in sc.clumps])
+        e = rel_err(r.final["position"] - p0, ref - p0)
+        print(f"request {r.key} (dem_bonded, {r.np_} particles): served vs alone {e:.2e}")
+        assert e < 1e-9
+        checked += 1
+    assert checked > 0

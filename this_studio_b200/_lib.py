@@ -105,7 +105,15 @@ SIGNATURES = {
     "demsph_dem_member_create": [_pvp, _vp],
     "demsph_dem_member_destroy": [_vp],
     "demsph_dem_member_add_balls": [_vp, _long, _d, _d, _d, _d, _d, _i, _int],
+    "demsph_dem_member_add_clump": [_vp, _long, _d, _d, _d, _d, _d, _dbl, _d, _int],
+    "demsph_dem_member_num_clumps": [_vp, C.POINTER(_long)],
     "demsph_dem_member_seal": [_vp],
+    "demsph_dem_set_cell_factor": [_vp, _dbl],
+    "demsph_sph_set_cell_factor": [_vp, _dbl],
+    "demsph_sph_set_conditional_rebuild": [_vp, _int],
+    "demsph_sph_conditional_rebuild": [_vp, _i, C.POINTER(_long)],
+    "demsph_sph_set_list_headroom": [_vp, _dbl],
+    "demsph_sph_list_capacity": [_vp, _i, _i],
     "demsph_dem_member_count": [_vp, _l],
     "demsph_dem_assemble_balls": [_vp, _int, _pvp, _d, _i],
     "demsph_dem_set_graphs": [_vp, _int],
@@ -114,6 +122,7 @@ SIGNATURES = {
     "demsph_dem_capacity": [_vp, _i, _i, _i],
     "demsph_dem_write_vtu": [_vp, C.c_char_p, _long, _int],
     "demsph_dem_copy_members": [_vp, _vp, _int, _i, _i, _i, _i, _d],
+    "demsph_dem_copy_member_bodies": [_vp, _vp, _int, _i, _i, _i, _i, _i, _i, _d],
     "demsph_dem_get_bonds": [_vp, _i, _i, _i, _d, _d, _d, _d, _d, _d],
     "demsph_dem_get_clumps": [_vp, _d, _d, _d, _d],
     "demsph_dem_get_walls": [_vp, _d, _d, _d],

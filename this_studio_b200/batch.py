@@ -51,6 +51,11 @@ class Member:
     record: object = None      # the scene's device-resident member record (assembly source)
     range: tuple = None        # its particle index range there
     tri_range: tuple = None    # its triangle index range there (DEM)
+    clump_range: tuple = None  # its clump index range there (DEM)
+    bond_range: tuple = None   # its bond index range there (DEM)
+    # its bonds (member-local ball indices, the order the device scene holds
+    # them in), fixed at its first admission (DEM)
+    bonds: tuple = None
 
 
 @dataclass
@@ -62,6 +67,8 @@ class Prepared:
     tri_ranges: list
     offsets: list
     stream: int
+    clump_ranges: list = None  # DEM: each member's clump index range
+    bond_ranges: list = None   # DEM: each member's bond index range
 
 
 def tile_offsets(boxes, gap):
@@ -116,8 +123,11 @@ def _drop(obj):
 class _Batch:
     """Member bookkeeping shared by the DEM and WCSPH batches."""
 
-    def __init__(self, precision="mixed", stream=None, streams=None):
+    def __init__(self, precision="mixed", stream=None, streams=None, tuning=None):
         self.precision = precision
+        # an autotune.Tuning of this kind: cell size, capacities, list shape
+        # and skin of every batch scene
+        self.tuning = tuning
         # two streams: the next scene is prepared on the one the current scene
         # does not use
         self.streams = list(streams) if streams is not None else [stream, stream]
@@ -152,8 +162,24 @@ class _Batch:
         self.members = []
 
 
+def _num_balls(scene):
+    """Balls of a DEM member, its clumps' pebbles included (they follow its
+    balls, clump by clump)."""
+    return scene.position.shape[0] + sum(len(c["radius"]) for c in scene.clumps)
+
+
+def _initial_positions(scene):
+    """Initial positions of a DEM member's balls and pebbles, in device order."""
+    parts = [scene.position] + [np.asarray(c["point"], float).reshape(-1, 3) for c in scene.clumps]
+    return np.concatenate(parts, axis=0)
+
+
 class DEMBatch(_Batch):
-    """DEM members of one time step and gravity stepped together."""
+    """DEM members of one time step and gravity stepped together.  Members
+    may hold clumps (their pebbles follow the member's balls), bonds on their
+    initial contacts (the addInitialCondition hook of the bonded scenes: the
+    member's contacts in the batch's first pair list after its admission)
+    and a constant force per ball (no ramp)."""
 
     @staticmethod
     def cell_of(scene):
@@ -196,21 +222,26 @@ class DEMBatch(_Batch):
         tic = time.perf_counter()
         for m in members:
             sc = m.scene
-            assert not sc.clumps and not sc.bonded and not sc.bond_initial_contacts, \
-                "batched DEM members are balls and mesh walls"
+            if sc.periodic is not None or sc.buoyancy is not None:
+                raise ValueError("batched DEM members have no periodic boundaries or buoyancy plane")
+            if (sc.clumps or sc.bond_initial_contacts) and m.home is None and "position" in m.state:
+                raise ValueError("a member with clumps or bonds re-enters a batch only from its device scene")
         cell = max(self.cell_of(m.scene) for m in members)
         boxes = [(np.asarray(m.scene.minb), np.asarray(m.scene.maxb)) for m in members]
         offs = tile_offsets(boxes, gap=2.0 * cell)
         moffs, rows_h, rows_l, rows_b = self._materials(members)
         lo = np.full(3, np.inf)
         hi = np.full(3, -np.inf)
-        ranges, tri_ranges = [], []
+        ranges, tri_ranges, clump_ranges = [], [], []
         start = 0
         tstart = 0
+        cstart = 0
         walls = []
         for m, off, mo in zip(members, offs, moffs):
             sc = m.scene
-            n = sc.position.shape[0]
+            n = _num_balls(sc)
+            clump_ranges.append((cstart, cstart + len(sc.clumps)))
+            cstart += len(sc.clumps)
             for wl in sc.walls:
                 d = dict(wl)
                 d["position"] = np.asarray(wl["position"], float) + off
@@ -228,6 +259,8 @@ class DEMBatch(_Batch):
         hosted = [m.home is None and "position" in m.state for m in members]
         if not any(hosted):
             new = DEMSolver(self.streams[si])
+            if self.tuning is not None:
+                self.tuning.configure(new)
             for r in rows_h:
                 new.setHertzianPair(*r)
             for r in rows_l:
@@ -249,6 +282,9 @@ class DEMBatch(_Batch):
                         rec.addBalls(sc.position[sl], None if sc.velocity is None else sc.velocity[sl],
                                      None if w0 is None else w0[sl], sc.radius[sl], sc.density[sl],
                                      sc.material[sl], fixed=bool(fixed[a]))
+                    for c in sc.clumps:
+                        rec.addClump(c["point"], c["radius"], c["centroid"], c["velocity"], c["angularVelocity"],
+                                     c["mass"], c["inertia"], c["material"])
                     m.record = rec.seal()
                 recs.append(m.record)
             new.assembleBalls(recs, offs, moffs)
@@ -258,7 +294,11 @@ class DEMBatch(_Batch):
                 if "velocity" in wl:
                     new.setMeshWallMotion(k, wl["velocity"], wl.get("angularVelocity", (0, 0, 0)))
             new.initialize(tuple(lo), tuple(hi), first.gravity, first.dt, self.precision)
+            bond_ranges = self._bonds(new, members, ranges, offs)
+            self._constant_force(new, members, ranges)
         else:
+            if any(m.scene.clumps for m in members):
+                raise ValueError("a batch with members entering from a host state holds no clumps")
             pos, vel, w, rad, den, mat, fixed = [], [], [], [], [], [], []
             for m, off, mo, h in zip(members, offs, moffs, hosted):
                 sc = m.scene
@@ -280,7 +320,8 @@ class DEMBatch(_Batch):
                            bonded=rows_b, walls=walls, minb=tuple(lo), maxb=tuple(hi), gravity=first.gravity,
                            dt=first.dt)
             big.angvel = np.concatenate(w)
-            new = S.build_dem(big, self.precision, self.streams[si])
+            new = S.build_dem(big, self.precision, self.streams[si],
+                              configure=None if self.tuning is None else self.tuning.configure)
             # springs of members entering from a host state, renumbered
             A, B, SL, RO, TO = [], [], [], [], []
             WA, WT, WS, WR, WTo = [], [], [], [], []
@@ -302,8 +343,65 @@ class DEMBatch(_Batch):
             if WA:
                 new.importWallSprings(np.concatenate(WA), np.concatenate(WT), np.concatenate(WS),
                                       np.concatenate(WR), np.concatenate(WTo))
+            bond_ranges = self._bonds(new, members, ranges, offs)
+            self._constant_force(new, members, ranges)
         self.timing["initialize_s"] += time.perf_counter() - tic
-        return Prepared(new, list(members), ranges, tri_ranges, offs, si)
+        return Prepared(new, list(members), ranges, tri_ranges, offs, si, clump_ranges, bond_ranges)
+
+    @staticmethod
+    def _bonds(new, members, ranges, offs):
+        """Bonds of the members with bond_initial_contacts, added to the
+        initialised scene `new` member by member (each member's bonds one
+        block, in the order it keeps them).  A member's bonds are fixed at its
+        first admission: its contacts between balls (not pebbles) in `new`'s
+        pair list.  Returns each member's bond index range."""
+        out = [(0, 0)] * len(members)
+        if not any(m.scene.bond_initial_contacts for m in members):
+            return out
+        pairs = None
+        A, B = [], []
+        for k, (m, (b0, b1)) in enumerate(zip(members, ranges)):
+            if not m.scene.bond_initial_contacts:
+                continue
+            if m.bonds is None:
+                if pairs is None:
+                    p = new.getPairs(0)
+                    pairs = (p["objectPointed"], p["objectPointing"])
+                nb = m.scene.position.shape[0]
+                a, b = pairs
+                sel = (a >= b0) & (a < b0 + nb) & (b >= b0) & (b < b0 + nb)
+                la, lb = a[sel] - b0, b[sel] - b0
+                lo_, hi_ = np.minimum(la, lb), np.maximum(la, lb)
+                # the library keeps the first of repeated pairs, (min, max) ordered
+                _, first = np.unique(lo_.astype(np.int64) * (b1 - b0) + hi_, return_index=True)
+                keep = np.sort(first)
+                m.bonds = (lo_[keep].astype(np.int32), hi_[keep].astype(np.int32))
+            A.append(m.bonds[0] + b0)
+            B.append(m.bonds[1] + b0)
+        if not A:
+            return out
+        pos = np.zeros((ranges[-1][1], 3))
+        for m, (b0, b1), off in zip(members, ranges, offs):
+            pos[b0:b1] = _initial_positions(m.scene) + off
+        new.addBondedInteraction(np.concatenate(A), np.concatenate(B), pos)
+        start = 0
+        for k, m in enumerate(members):
+            nb = len(m.bonds[0]) if m.scene.bond_initial_contacts else 0
+            out[k] = (start, start + nb)
+            start += nb
+        return out
+
+    @staticmethod
+    def _constant_force(new, members, ranges):
+        if not any(getattr(m.scene, "constant_force", None) is not None for m in members):
+            return
+        f = np.zeros((ranges[-1][1], 3))
+        for m, (b0, b1) in zip(members, ranges):
+            cf = getattr(m.scene, "constant_force", None)
+            if cf is not None:
+                cf = np.asarray(cf, float).reshape(-1, 3)
+                f[b0:b0 + cf.shape[0]] = cf
+        new.setConstantForce(f)
 
     def commit(self, prep):
         """Carries the continuing members' state from the current device
@@ -318,8 +416,19 @@ class DEMBatch(_Batch):
             td = [prep.tri_ranges[k][0] - m.tri_range[0] for m, k in carried]
             sh = [prep.offsets[k] - m.offset for m, k in carried]
             prep.solver.copyMembers(old, ss, ds, nn, td, sh)
-        for m, r, t, off in zip(prep.members, prep.ranges, prep.tri_ranges, prep.offsets):
+            bodies = [(m, k) for m, k in carried if m.clump_range[1] > m.clump_range[0] or
+                      m.bond_range[1] > m.bond_range[0]]
+            if bodies:
+                prep.solver.copyMemberBodies(
+                    old, [m.clump_range[0] for m, k in bodies], [prep.clump_ranges[k][0] for m, k in bodies],
+                    [m.clump_range[1] - m.clump_range[0] for m, k in bodies],
+                    [m.bond_range[0] for m, k in bodies], [prep.bond_ranges[k][0] for m, k in bodies],
+                    [m.bond_range[1] - m.bond_range[0] for m, k in bodies],
+                    [prep.offsets[k] - m.offset for m, k in bodies])
+        for m, r, t, off, cr, br in zip(prep.members, prep.ranges, prep.tri_ranges, prep.offsets,
+                                        prep.clump_ranges, prep.bond_ranges):
             m.home, m.range, m.tri_range, m.offset = prep.solver, r, t, off
+            m.clump_range, m.bond_range = cr, br
         self.members = prep.members
         self.ranges, self.tri_ranges = prep.ranges, prep.tri_ranges
         self.solver = prep.solver
@@ -337,6 +446,7 @@ class DEMBatch(_Batch):
         b = self.solver.getBall()
         pp = self.solver.getPairs(0)
         wp = self.solver.getPairs(1)
+        cl = bo = None
         for m, (b0, b1), (t0, t1) in zip(self.members, self.ranges, self.tri_ranges):
             if keys is not None and m.key not in keys:
                 continue
@@ -352,6 +462,19 @@ class DEMBatch(_Batch):
             st["wall_pairs"] = {"a": wp["objectPointed"][sel] - b0, "b": wp["objectPointing"][sel] - t0,
                                 "sliding": wp["sliding"][sel], "rolling": wp["rolling"][sel],
                                 "torsion": wp["torsion"][sel]}
+            c0, c1 = m.clump_range
+            if c1 > c0:
+                if cl is None:
+                    cl = self.solver.getClump()
+                st["clumps"] = {"position": cl["position"][c0:c1] - m.offset, "velocity": cl["velocity"][c0:c1],
+                                "angularVelocity": cl["angularVelocity"][c0:c1],
+                                "orientation": cl["orientation"][c0:c1]}
+            k0, k1 = m.bond_range
+            if k1 > k0:
+                if bo is None:
+                    bo = self.solver.getBondedInteraction()
+                st["bonds"] = {k: (v[k0:k1] - (b0 if k.startswith("object") else 0)) if v.ndim == 1
+                               else (v[k0:k1] - m.offset if k == "point" else v[k0:k1]) for k, v in bo.items()}
 
     def num_particles(self):
         return sum(m.scene.num_moving for m in self.members)
@@ -372,6 +495,8 @@ class SPHBatch(_Batch):
         offs = tile_offsets(boxes, gap=2.0 * cell)
         si = 1 - self.cur_stream
         s = WCSPHSolver(self.streams[si])
+        if self.tuning is not None:
+            self.tuning.configure(s)
         lo = np.full(3, np.inf)
         hi = np.full(3, -np.inf)
         ranges = []
@@ -416,6 +541,8 @@ class SPHBatch(_Batch):
                     p[a:b] = st.get("pressure", np.zeros(b - a))
                     dr[a:b] = st.get("densityChange", np.zeros(b - a))
                 s.setSPH(density=rho, pressure=p, densityChange=dr)
+        if self.tuning is not None:
+            self.tuning.finish(s)
         self.timing["initialize_s"] += time.perf_counter() - tic
         return Prepared(s, list(members), ranges, [None] * len(members), offs, si)
 

@@ -829,11 +829,13 @@ __global__ void k_dem_ghost_sum(int n, const double4* __restrict__ FA, const dou
 
 // ------------------------------------------------------------ batching ----
 // Places one batch member's balls at [start, start + n) of the batch arrays,
-// translated by off, with material ids shifted by matOff.
-__global__ void k_dem_place(int n, int start, double3 off, int matOff, const double4* __restrict__ pos,
+// translated by off, with material ids shifted by matOff and the member's
+// clump ids (clumpLocal, -1 for a free ball; may be null) by clumpOff.
+__global__ void k_dem_place(int n, int start, double3 off, int matOff, int clumpOff, const double4* __restrict__ pos,
                             const double4* __restrict__ vel, const double4* __restrict__ angv,
-                            const int* __restrict__ mat, double4* __restrict__ pos2, double4* __restrict__ vel2,
-                            double4* __restrict__ angv2, int* __restrict__ mat2, int* __restrict__ clump2) {
+                            const int* __restrict__ mat, const int* __restrict__ clumpLocal,
+                            double4* __restrict__ pos2, double4* __restrict__ vel2, double4* __restrict__ angv2,
+                            int* __restrict__ mat2, int* __restrict__ clump2) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const double4 p = pos[t];
@@ -841,7 +843,41 @@ __global__ void k_dem_place(int n, int start, double3 off, int matOff, const dou
     vel2[start + t] = vel[t];
     angv2[start + t] = angv[t];
     mat2[start + t] = mat[t] + matOff;
-    clump2[start + t] = -1;
+    const int c = clumpLocal ? clumpLocal[t] : -1;
+    clump2[start + t] = c >= 0 ? c + clumpOff : -1;
+}
+
+// Carries the bodies of continuing batch members from another scene: clumps
+// [srcC, srcC + nC) there become [dstC, ...) here (centroid translated by
+// shift, velocity, angular velocity, orientation), bonds [srcB, srcB + nB)
+// become [dstB, ...) (intact flag, contact point translated by shift,
+// normal, the accumulated normal / shear forces and torques and the peak
+// stresses).  The pebbles and the bonds' end balls move with the member's
+// balls (k_dem_copy_member).
+__global__ void k_dem_copy_bodies(DemDev dst, DemDev src, int srcC, int dstC, int nC, int srcB, int dstB, int nB,
+                                  double3 shift) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nC) {
+        const int a = dstC + t, b = srcC + t;
+        const double4 c = src.cpos[b];
+        dst.cpos[a] = make_double4(c.x + shift.x, c.y + shift.y, c.z + shift.z, c.w);
+        dst.cvel[a] = src.cvel[b];
+        dst.cangv[a] = src.cangv[b];
+        dst.cq[a] = src.cq[b];
+    }
+    if (t < nB) {
+        const int a = dstB + t, b = srcB + t;
+        dst.bok[a] = src.bok[b];
+        const double4 p = src.bpoint[b];
+        dst.bpoint[a] = make_double4(p.x + shift.x, p.y + shift.y, p.z + shift.z, p.w);
+        dst.bnormal[a] = src.bnormal[b];
+        dst.bFs[a] = src.bFs[b];
+        dst.bTb[a] = src.bTb[b];
+        dst.bFn[a] = src.bFn[b];
+        dst.bTt[a] = src.bTt[b];
+        dst.bsmax[a] = src.bsmax[b];
+        dst.btmax[a] = src.btmax[b];
+    }
 }
 
 // Copies the state of one continuing batch member from another scene: its n
@@ -1000,6 +1036,7 @@ struct DemScene {
     int nB = 0;                // balls (the host arrays' size until a batch assembly)
     bool assembled = false;    // balls placed on the device from member records
     double assembledRmax = 0;  // their largest radius
+    double cellFactor = 1.0;   // ball grid cell = cellFactor x 2 r_max (autotuner; 1 = the reference's)
     int N() const { return nB; }
 
     DemDev dev(bool withOld) {
@@ -1610,6 +1647,7 @@ struct DemScene {
         } else {
             cell = 2.0 * assembledRmax;
         }
+        cell *= cellFactor;
         precision = prec;
         gmin = mn; gmax = mx; gravity = g; dt = timeStep;
         build_materials();
@@ -1789,6 +1827,51 @@ bool dem_block_end(demsph_dem_t h) {
 
 }  // namespace demsph
 
+// Appends the pebbles and the clump record of addClump (DEMSolver.h:1796-1845)
+// to the host tables of T (a scene or a batch member, both with the same
+// vectors): pebbles take the clump's mean density for their masses and its
+// rigid-body velocity; the clump keeps its centroid, velocity, angular
+// velocity, unit orientation and the inverse of its inertia tensor (the
+// symmetric inverse of myMat.h:163-179).  Clump cid, pebbles [ps, ps + np).
+template <class T>
+static void append_clump(T& s, int cid, int ps, long np, const double* pts, const double* rad,
+                         const double* centroid, const double* vel, const double* w, double mass, const double* I6,
+                         int mat) {
+    const int pe = ps + (int)np;
+    double3 c = ld3(centroid, 0), v = ld3(vel, 0), ww = ld3(w, 0);
+    std::vector<double3> pv(np, v);
+    double vol = 0., im = 0.;
+    if (mass > 1.e-20) {
+        im = 1.0 / mass;
+        for (long i = 0; i < np; i++) {
+            vol += 4.0 / 3.0 * kPi * std::pow(rad[i], 3.0);
+            pv[i] += cross(ww, ld3(pts, i) - c);
+        }
+    }
+    double dave = vol > 0. ? mass / vol : 0.;
+    for (long i = 0; i < np; i++) {
+        double r = rad[i];
+        double m = 4. / 3. * r * r * r * kPi * dave;
+        double pim = m > 0.0 ? 1.0 / m : 0.0;
+        s.hPos.push_back(d4(ld3(pts, i), r));
+        s.hVel.push_back(d4(pv[i], pim));
+        s.hAngv.push_back(d4(ww, 0));
+        s.hMat.push_back(mat);
+        s.hClump.push_back(cid);
+    }
+    double xx = I6[0], yy = I6[1], zz = I6[2], xy = I6[3], xz = I6[4], yz = I6[5];
+    double di = 1.0 / (xx * (yy * zz - yz * yz) + xy * (yz * xz - xy * zz) + xz * (xy * yz - yy * xz));
+    double ixx = (yy * zz - yz * yz) * di, iyy = (xx * zz - xz * xz) * di, izz = (xx * yy - xy * xy) * di;
+    double ixy = -(xy * zz - xz * yz) * di, ixz = (xy * yz - xz * yy) * di, iyz = -(xx * yz - xz * xy) * di;
+    s.hCpos.push_back(d4(c, 0));
+    s.hCvel.push_back(d4(v, 0));
+    s.hCangv.push_back(d4(ww, 0));
+    s.hCq.push_back(make_double4(1, 0, 0, 0));
+    s.hCinvIa.push_back(make_double4(ixx, iyy, izz, ixy));
+    s.hCinvIb.push_back(make_double4(ixz, iyz, 0, 0));
+    s.hCinvm.push_back(im);
+    s.hCpeb.push_back(make_int2(ps, pe));
+}
 extern "C" {
 
 int demsph_dem_create(demsph_dem_t* out, void* stream) {
@@ -1858,12 +1941,17 @@ int demsph_dem_add_balls(demsph_dem_t h, long n, const double* pos, const double
 struct demsph_dem_member {
     cudaStream_t s = 0;
     std::vector<double4> hPos, hVel, hAngv;  // staging until sealed
-    std::vector<int> hMat;
+    std::vector<int> hMat, hClump;           // hClump: member-local clump id, -1 for a free ball
+    // the member's clumps (kept on the host: assembly appends them to the
+    // scene's clump table, translated and renumbered)
+    std::vector<double4> hCpos, hCvel, hCangv, hCq, hCinvIa, hCinvIb;
+    std::vector<double> hCinvm;
+    std::vector<int2> hCpeb;
     bool sealed = false;
     int n = 0, matMax = -1;
     double rmax = 0;
     DBuf<double4> pos, vel, angv;
-    DBuf<int> mat;
+    DBuf<int> mat, clump;
 };
 int demsph_dem_member_create(demsph_dem_member_t* out, void* stream) {
     return guarded([&] {
@@ -1898,7 +1986,25 @@ int demsph_dem_member_add_balls(demsph_dem_member_t m, long n, const double* pos
             m->hVel.push_back(d4(fixed || !vel ? mk3(0, 0, 0) : ld3(vel, i), im));
             m->hAngv.push_back(d4(fixed || !w ? mk3(0, 0, 0) : ld3(w, i), 0));
             m->hMat.push_back(mat[i]);
+            m->hClump.push_back(-1);
         }
+    });
+}
+int demsph_dem_member_add_clump(demsph_dem_member_t m, long np, const double* pts, const double* rad,
+                                const double* centroid, const double* vel, const double* w, double mass,
+                                const double* I6, int mat) {
+    return guarded([&] {
+        if (!m) throw Status(DEMSPH_ERR_INVALID, "null member handle");
+        if (m->sealed) throw Status(DEMSPH_ERR_INVALID, "member already sealed");
+        if (np < 0 || (np > 0 && (!pts || !rad)) || !centroid || !vel || !w || !I6)
+            throw Status(DEMSPH_ERR_INVALID, "missing clump arrays");
+        append_clump(*m, (int)m->hCpos.size(), (int)m->hPos.size(), np, pts, rad, centroid, vel, w, mass, I6, mat);
+    });
+}
+int demsph_dem_member_num_clumps(demsph_dem_member_t m, long* n) {
+    return guarded([&] {
+        if (!m || !n) throw Status(DEMSPH_ERR_INVALID, "null argument");
+        *n = (long)m->hCpos.size();
     });
 }
 int demsph_dem_member_seal(demsph_dem_member_t m) {
@@ -1918,8 +2024,9 @@ int demsph_dem_member_seal(demsph_dem_member_t m) {
         m->n = (int)m->hPos.size();
         m->pos.upload(m->hPos, m->s); m->vel.upload(m->hVel, m->s); m->angv.upload(m->hAngv, m->s);
         m->mat.upload(m->hMat, m->s);
+        if (!m->hCpos.empty()) m->clump.upload(m->hClump, m->s);
         DEMSPH_CUDA(cudaStreamSynchronize(m->s));
-        m->hPos = {}; m->hVel = {}; m->hAngv = {}; m->hMat = {};
+        m->hPos = {}; m->hVel = {}; m->hAngv = {}; m->hMat = {}; m->hClump = {};
         m->sealed = true;
     });
 }
@@ -1953,9 +2060,23 @@ int demsph_dem_assemble_balls(demsph_dem_t h, int count, const demsph_dem_member
         int b0 = 0;
         for (int k = 0; k < count; k++) {
             const demsph_dem_member* m = members[k];
-            k_dem_place<<<grid_for(m->n, 256), 256, 0, s.s>>>(m->n, b0, ld3(offsets, k), matOffset[k], m->pos.p,
-                                                             m->vel.p, m->angv.p, m->mat.p, s.pos.p, s.vel.p,
-                                                             s.angv.p, s.mat.p, s.clump.p);
+            const int c0 = (int)s.hCpos.size();
+            k_dem_place<<<grid_for(m->n, 256), 256, 0, s.s>>>(m->n, b0, ld3(offsets, k), matOffset[k], c0, m->pos.p,
+                                                             m->vel.p, m->angv.p, m->mat.p,
+                                                             m->hCpos.empty() ? nullptr : m->clump.p, s.pos.p,
+                                                             s.vel.p, s.angv.p, s.mat.p, s.clump.p);
+            const double3 off = ld3(offsets, k);
+            for (size_t c = 0; c < m->hCpos.size(); c++) {
+                const double4 p = m->hCpos[c];
+                s.hCpos.push_back(make_double4(p.x + off.x, p.y + off.y, p.z + off.z, p.w));
+                s.hCvel.push_back(m->hCvel[c]);
+                s.hCangv.push_back(m->hCangv[c]);
+                s.hCq.push_back(m->hCq[c]);
+                s.hCinvIa.push_back(m->hCinvIa[c]);
+                s.hCinvIb.push_back(m->hCinvIb[c]);
+                s.hCinvm.push_back(m->hCinvm[c]);
+                s.hCpeb.push_back(make_int2(m->hCpeb[c].x + b0, m->hCpeb[c].y + b0));
+            }
             b0 += m->n;
         }
         g_launches += count;
@@ -1970,42 +2091,9 @@ int demsph_dem_add_clump(demsph_dem_t h, long np, const double* pts, const doubl
         SCENE_CHECK(h);
         DemScene& s = h->sc;
         if (s.ready || s.assembled) throw Status(DEMSPH_ERR_INVALID, "clumps must be added before initialisation");
-        int cid = (int)s.hCpos.size();
-        int ps = s.N(), pe = ps + (int)np;
-        double3 c = ld3(centroid, 0), v = ld3(vel, 0), ww = ld3(w, 0);
-        std::vector<double3> pv(np, v);
-        double vol = 0., im = 0.;
-        if (mass > 1.e-20) {
-            im = 1.0 / mass;
-            for (long i = 0; i < np; i++) {
-                vol += 4.0 / 3.0 * kPi * std::pow(rad[i], 3.0);
-                pv[i] += cross(ww, ld3(pts, i) - c);
-            }
-        }
-        double dave = vol > 0. ? mass / vol : 0.;
-        for (long i = 0; i < np; i++) {
-            double r = rad[i];
-            double m = 4. / 3. * r * r * r * kPi * dave;
-            double pim = m > 0.0 ? 1.0 / m : 0.0;
-            s.hPos.push_back(d4(ld3(pts, i), r));
-            s.hVel.push_back(d4(pv[i], pim));
-            s.hAngv.push_back(d4(ww, 0));
-            s.hMat.push_back(mat);
-            s.hClump.push_back(cid);
-        }
-        // inverse (myMat.h:163-179)
-        double xx = I6[0], yy = I6[1], zz = I6[2], xy = I6[3], xz = I6[4], yz = I6[5];
-        double di = 1.0 / (xx * (yy * zz - yz * yz) + xy * (yz * xz - xy * zz) + xz * (xy * yz - yy * xz));
-        double ixx = (yy * zz - yz * yz) * di, iyy = (xx * zz - xz * xz) * di, izz = (xx * yy - xy * xy) * di;
-        double ixy = -(xy * zz - xz * yz) * di, ixz = (xy * yz - xz * yy) * di, iyz = -(xx * yz - xz * xy) * di;
-        s.hCpos.push_back(d4(c, 0));
-        s.hCvel.push_back(d4(v, 0));
-        s.hCangv.push_back(d4(ww, 0));
-        s.hCq.push_back(make_double4(1, 0, 0, 0));
-        s.hCinvIa.push_back(make_double4(ixx, iyy, izz, ixy));
-        s.hCinvIb.push_back(make_double4(ixz, iyz, 0, 0));
-        s.hCinvm.push_back(im);
-        s.hCpeb.push_back(make_int2(ps, pe));
+        if (np < 0 || (np > 0 && (!pts || !rad)) || !centroid || !vel || !w || !I6)
+            throw Status(DEMSPH_ERR_INVALID, "missing clump arrays");
+        append_clump(s, (int)s.hCpos.size(), s.N(), np, pts, rad, centroid, vel, w, mass, I6, mat);
         s.nB = (int)s.hPos.size();
     });
 }
@@ -2135,6 +2223,15 @@ int demsph_dem_reserve(demsph_dem_t h, int pairsPerBall, int reversePerBall, int
         s.K = std::max(s.K, pairsPerBall);
         s.KR = std::max(s.KR, reversePerBall);
         s.KT = std::max(s.KT, std::min(trianglesPerBall, kMaxTriPerBall));
+    });
+}
+int demsph_dem_set_cell_factor(demsph_dem_t h, double factor) {
+    return guarded([&] {
+        SCENE_CHECK(h);
+        DemScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "the cell size is set before initialisation");
+        if (!(factor >= 1.0 && factor <= 4.0)) throw Status(DEMSPH_ERR_INVALID, "cell factor must be in [1, 4]");
+        s.cellFactor = factor;
     });
 }
 int demsph_dem_capacity(demsph_dem_t h, int* pairsPerBall, int* reversePerBall, int* trianglesPerBall) {
@@ -2449,6 +2546,7 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, int count, const
         DEMSPH_LAUNCH_CHECK();
         DevStatus cs = d.read_status();
         if (cs.bad_index) throw Status(DEMSPH_ERR_INVALID, "a carried pair partner or triangle left its member");
+        d.bondPairsStale = true;  // bonds look their pairs up in the carried rows
         // reverse lists for the copied rows
         const int n = d.N();
         DEMSPH_CUDA(cudaMemsetAsync(d.rcnt.p, 0, sizeof(int) * n, d.s));
@@ -2465,6 +2563,50 @@ int demsph_dem_copy_members(demsph_dem_t dst, demsph_dem_t src, int count, const
             k_dem_reverse_order<<<grid_for(n, 256), 256, 0, d.s>>>(dr);
             d.launch_count(2);
         }
+        DEMSPH_CUDA(cudaStreamSynchronize(d.s));
+    });
+}
+int demsph_dem_copy_member_bodies(demsph_dem_t dst, demsph_dem_t src, int count, const int* srcClump,
+                                  const int* dstClump, const int* numClumps, const int* srcBond, const int* dstBond,
+                                  const int* numBonds, const double* shift) {
+    return guarded([&] {
+        SCENE_CHECK(dst);
+        SCENE_CHECK(src);
+        DemScene& d = dst->sc;
+        DemScene& s = src->sc;
+        if (!d.ready || !s.ready) throw Status(DEMSPH_ERR_NOT_READY, "scenes not initialised");
+        if (count < 0 || (count > 0 && (!srcClump || !dstClump || !numClumps || !srcBond || !dstBond || !numBonds ||
+                                        !shift)))
+            throw Status(DEMSPH_ERR_INVALID, "missing member tables");
+        const long sc = (long)s.hCpos.size(), dc = (long)d.hCpos.size();
+        const long sb = (long)s.hBab.size(), db = (long)d.hBab.size();
+        for (int k = 0; k < count; k++) {
+            if (numClumps[k] < 0 || srcClump[k] < 0 || dstClump[k] < 0 || srcClump[k] + (long)numClumps[k] > sc ||
+                dstClump[k] + (long)numClumps[k] > dc)
+                throw Status(DEMSPH_ERR_INVALID, "member clump range out of bounds");
+            if (numBonds[k] < 0 || srcBond[k] < 0 || dstBond[k] < 0 || srcBond[k] + (long)numBonds[k] > sb ||
+                dstBond[k] + (long)numBonds[k] > db)
+                throw Status(DEMSPH_ERR_INVALID, "member bond range out of bounds");
+            // a carried bond must join the same two member balls on both sides
+            for (int j = 0; j < numBonds[k]; j++) {
+                const int2 a = s.hBab[srcBond[k] + j], b = d.hBab[dstBond[k] + j];
+                if (a.x - s.hBab[srcBond[k]].x != b.x - d.hBab[dstBond[k]].x ||
+                    a.y - s.hBab[srcBond[k]].x != b.y - d.hBab[dstBond[k]].x)
+                    throw Status(DEMSPH_ERR_INVALID, "carried bonds differ between the scenes");
+            }
+        }
+        DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+        d.graph.reset();  // bond pairs are looked up again
+        DemDev dd = d.dev(false), sd = s.dev(false);
+        for (int k = 0; k < count; k++) {
+            const int n = std::max(numClumps[k], numBonds[k]);
+            if (n == 0) continue;
+            k_dem_copy_bodies<<<grid_for(n, 128), 128, 0, d.s>>>(dd, sd, srcClump[k], dstClump[k], numClumps[k],
+                                                                srcBond[k], dstBond[k], numBonds[k], ld3(shift, k));
+            d.launch_count(1);
+        }
+        DEMSPH_LAUNCH_CHECK();
+        d.bondPairsStale = true;
         DEMSPH_CUDA(cudaStreamSynchronize(d.s));
     });
 }

@@ -354,7 +354,11 @@ struct SkinState {
 // when some particle has drifted more than half the skin since the last
 // rebuild (then no pair within the cutoff now was beyond cutoff + skin at
 // the rebuild).
-__global__ void __launch_bounds__(kSkinSlots) k_sph_skin_decide(SkinState* st, float half2) {
+// Inside a captured step the decision also sets the condition of the graph's
+// IF node around the rebuild (setCond = 1), so a step that keeps its lists
+// launches none of the rebuild's kernels.
+__global__ void __launch_bounds__(kSkinSlots) k_sph_skin_decide(SkinState* st, float half2,
+                                                                 cudaGraphConditionalHandle cond, int setCond) {
     __shared__ unsigned m[kSkinSlots];
     const int t = threadIdx.x;
     m[t] = st->maxd2[t];
@@ -372,6 +376,7 @@ __global__ void __launch_bounds__(kSkinSlots) k_sph_skin_decide(SkinState* st, f
             st->force = 0;
             st->rebuilds++;
         }
+        if (setCond) cudaGraphSetConditional(cond, r ? 1u : 0u);
     }
 }
 
@@ -1363,6 +1368,81 @@ __device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, co
     acc += sb * (o.v - vd) - sw * p.r;
 }
 
+// Fluid neighbours of the uniform passes with their packed records gathered
+// one pair of neighbours ahead and the row entries two pairs ahead, so the
+// next pair's gathers are in flight while the current pair is computed.
+// f(j, q_j, v_j); rows with a count (cnt >= 0) only.
+#ifndef DEMSPH_UNI_PREFETCH
+#define DEMSPH_UNI_PREFETCH 0
+#endif
+template <class F>
+__device__ __forceinline__ void quad_fluid_pf(int cnt, const int* __restrict__ nb, int K, int i,
+                                              const int4* __restrict__ posq, const float4* __restrict__ velf, F&& f) {
+    const int sub = threadIdx.x & 3;
+    const int* __restrict__ row = nb + (size_t)i * K;
+    const int kend = sub + kQuad * lane_count(cnt, sub);
+    int k = sub;
+    int a = k < kend ? __ldg(row + k) : -1;
+    int b = k + kQuad < kend ? __ldg(row + k + kQuad) : -1;
+    int an = k + 2 * kQuad < kend ? __ldg(row + k + 2 * kQuad) : -1;
+    int bn = k + 3 * kQuad < kend ? __ldg(row + k + 3 * kQuad) : -1;
+    int4 qa = make_int4(0, 0, 0, 0), qb = qa;
+    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
+    if (a >= 0) { qa = posq[a]; va = velf[a]; }
+    if (b >= 0) { qb = posq[b]; vb = velf[b]; }
+    for (; k < kend; k += 2 * kQuad) {
+        int4 qan = make_int4(0, 0, 0, 0), qbn = qan;
+        float4 van = make_float4(0.f, 0.f, 0.f, 0.f), vbn = van;
+        if (an >= 0) { qan = posq[an]; van = velf[an]; }
+        if (bn >= 0) { qbn = posq[bn]; vbn = velf[bn]; }
+        const int kk = k + 4 * kQuad;
+        const int ann = kk < kend ? __ldg(row + kk) : -1;
+        const int bnn = kk + kQuad < kend ? __ldg(row + kk + kQuad) : -1;
+        f(a, qa, va);
+        if (b >= 0) f(b, qb, vb);
+        a = an; b = bn; an = ann; bn = bnn;
+        qa = qan; qb = qbn; va = van; vb = vbn;
+    }
+}
+// The skin-row walk of skin_loop with the same prefetch: f(j, q_j, v_j)
+// returns whether the pair is kept (written to this step's rows).
+template <class F>
+__device__ __forceinline__ void skin_fluid_pf(int cnt, const int* __restrict__ nbV, int K, int i,
+                                              int* __restrict__ nbOut, int* __restrict__ cntOut,
+                                              const int4* __restrict__ posq, const float4* __restrict__ velf,
+                                              F&& f) {
+    const int sub = threadIdx.x & 3;
+    const int* __restrict__ row = nbV + (size_t)i * K;
+    int* __restrict__ out = nbOut + (size_t)i * K;
+    int w = 0;
+    int k = sub;
+    int a = k < cnt ? __ldg(row + k) : -1;
+    int b = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
+    int an = k + 2 * kQuad < cnt ? __ldg(row + k + 2 * kQuad) : -1;
+    int bn = k + 3 * kQuad < cnt ? __ldg(row + k + 3 * kQuad) : -1;
+    int4 qa = make_int4(0, 0, 0, 0), qb = qa;
+    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
+    if (a >= 0) { qa = posq[a]; va = velf[a]; }
+    if (b >= 0) { qb = posq[b]; vb = velf[b]; }
+    for (; k < cnt; k += 2 * kQuad) {
+        int4 qan = make_int4(0, 0, 0, 0), qbn = qan;
+        float4 van = make_float4(0.f, 0.f, 0.f, 0.f), vbn = van;
+        if (an >= 0) { qan = posq[an]; van = velf[an]; }
+        if (bn >= 0) { qbn = posq[bn]; vbn = velf[bn]; }
+        const int kk = k + 4 * kQuad;
+        const int ann = kk < cnt ? __ldg(row + kk) : -1;
+        const int bnn = kk + kQuad < cnt ? __ldg(row + kk + kQuad) : -1;
+        if (f(a, qa, va)) out[sub + kQuad * w++] = a;
+        if (b >= 0 && f(b, qb, vb)) out[sub + kQuad * w++] = b;
+        a = an; b = bn; an = ann; bn = bnn;
+        qa = qan; qb = qbn; va = van; vb = vbn;
+    }
+    const unsigned gm = quad_mask();
+    const int over = quad_sum(w > 127 ? 1 : 0, gm);
+    const int packed = quad_sum(w << (7 * sub), gm);
+    if (sub == 0) cntOut[i] = over ? -1 : (kLaneRows | packed);
+}
+
 template <bool kSkin>
 __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
@@ -1376,13 +1456,23 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double h
     const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
     float3 acc = make_float3(0.f, 0.f, 0.f);
     if constexpr (kSkin) {
-        skin_loop(d.cntV[i], d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
-            const int4 qj = d.posq[j];
-            const PairGeom p = pair_geom(o.q, qj, u);
-            if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
-            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
-            return true;
-        });
+        const int cv = d.cntV[i];
+        if (DEMSPH_UNI_PREFETCH && cv >= 0) {
+            skin_fluid_pf(cv, d.nbV, d.KF, i, d.nbF, d.cntF, d.posq, d.velf, [&](int j, int4 qj, float4 vj) {
+                const PairGeom p = pair_geom(o.q, qj, u);
+                if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
+                acc_fluid_u(o, p, vj, __int_as_float(qj.w), u, acc);
+                return true;
+            });
+        } else {
+            skin_loop(cv, d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
+                const int4 qj = d.posq[j];
+                const PairGeom p = pair_geom(o.q, qj, u);
+                if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
+                acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+                return true;
+            });
+        }
         if (d.ND > 0) {
             skin_loop(d.cntVD[i], d.nbVD, d.KD, i, d.nbD, d.cntD, pi4, d.g, d.dStart, d.dpos, -1, [&](int j) {
                 const PairGeom p = pair_geom(o.q, d.dposq[j], u);
@@ -1392,11 +1482,19 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double h
             });
         }
     } else {
-        quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-            const int4 qj = d.posq[j];
-            const PairGeom p = pair_geom(o.q, qj, u);
-            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
-        });
+        const int cf = d.cntF[i];
+        if (DEMSPH_UNI_PREFETCH && cf >= 0) {
+            quad_fluid_pf(cf, d.nbF, d.KF, i, d.posq, d.velf, [&](int, int4 qj, float4 vj) {
+                const PairGeom p = pair_geom(o.q, qj, u);
+                acc_fluid_u(o, p, vj, __int_as_float(qj.w), u, acc);
+            });
+        } else {
+            quad_neighbors(cf, d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+                const int4 qj = d.posq[j];
+                const PairGeom p = pair_geom(o.q, qj, u);
+                acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+            });
+        }
         if (d.ND > 0) {
             quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
                 const PairGeom p = pair_geom(o.q, d.dposq[j], u);
@@ -1437,16 +1535,21 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     const double4 s4 = d.st[i];
     const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
     float sumF = 0.f, sumD = 0.f;  // sum of (1 / rho_j) (v_i - v*) . grad W / (1/2), per kind of neighbour
-    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-        const int4 qj = d.posq[j];
+    auto fluid = [&](int4 qj, float4 vj) {  // vj = (v_j, p_j)
         const PairGeom p = pair_geom(o.q, qj, u);
-        const float4 vj = d.velf[j];  // (v_j, p_j)
         const float rhoj = __int_as_float(qj.w);
         const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
         const float rbar = 0.5f * (o.rho + rhoj);
         const float X = __fdividef(o.PL - vj.w, rbar * u.cF);
         sumF += __fdividef(p.Kdq * (dot(dv, p.r) * p.inv_r + X), rhoj);
-    });
+    };
+    const int cf = d.cntF[i];
+    if (DEMSPH_UNI_PREFETCH && cf >= 0) {
+        quad_fluid_pf(cf, d.nbF, d.KF, i, d.posq, d.velf, [&](int, int4 qj, float4 vj) { fluid(qj, vj); });
+    } else {
+        quad_neighbors(cf, d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos,
+                       [&](int j) { fluid(d.posq[j], d.velf[j]); });
+    }
     if (d.ND > 0) {
         quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
             const PairGeom p = pair_geom(o.q, d.dposq[j], u);
@@ -1705,6 +1808,7 @@ struct SphScene {
     long iStep = 0;
     double time = 0;
     int KF = 96, KD = 64, KDD = 96;
+    double listHeadroom = 0.125;  // row capacity above the initial longest row (autotuner)
     CellTable fCells, dCells;
     DBuf<double4> pos[2], vel[2], st[2];
     DBuf<double> rho0[2], drho[2];
@@ -1734,6 +1838,7 @@ struct SphScene {
     // 2 h_max (1 + skinMax) wide so that the 27-cell stencil covers the skin.
     float skinMax = 0.04f;   // fraction of 2 h_max the grid allows (fixed at initialisation)
     float skinFrac = 0.04f;  // fraction in use (0: exact lists every step)
+    double cellFactor = 1.0;  // grid cell = cellFactor x 2 h_max (1 + skin) (autotuner)
     double hmaxGrid = 0;
     DBuf<int> nbV, cntV, nbVD, cntVD;
     DBuf<double4> xb;
@@ -2036,6 +2141,10 @@ struct SphScene {
     }
     // The step's rebuild of the skin lists, gated on the device's decision.
     void skin_rebuild() {
+        if (condCapture) {
+            skin_rebuild_conditional();
+            return;
+        }
         skin_rebuild_sort();
         skin_rebuild_lists();
     }
@@ -2045,10 +2154,95 @@ struct SphScene {
         const int* gate = &skinState.p->rebuild;
         const bool move = coupling && nM > 0;
         if (move) marker_place(true);
-        k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()));
+        k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()),
+                                                   cudaGraphConditionalHandle(), 0);
         if (move) marker_sort(gate);
         fCells.build(pos[P].p, N(), s, id[ID].p, false, gate);
         g_launches += 1 + fCells.launches;
+    }
+
+    // Conditional rebuild (a scene without markers, inside a stream capture):
+    // the decision kernel, then an IF node whose body -- captured into the
+    // node's graph on a helper stream -- is the cell sort, the reorder and the
+    // skin-list build.  The body's kernels keep their device-side gate, so the
+    // body does the same work as the gated launches outside graphs; they are
+    // counted when a rebuild runs them, not per replay.
+    bool condOK = true;         // the runtime took conditional capture so far
+    bool condEnabled = true;    // demsph_sph_set_conditional_rebuild
+    bool condCapture = false;   // set while a block of steps is captured
+    long long condBodyLaunches = 0;
+    cudaStream_t condStream = nullptr;
+    bool cond_wanted() const { return condOK && condEnabled && nM == 0 && skin_on(); }
+    ~SphScene() {
+        if (condStream) cudaStreamDestroy(condStream);
+    }
+    void skin_rebuild_conditional() {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        DEMSPH_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        cudaGraphConditionalHandle h;
+        DEMSPH_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        k_sph_skin_decide<<<1, kSkinSlots, 0, s>>>(skinState.p, (float)(0.25 * skin_abs() * skin_abs()), h, 1);
+        g_launches += 1;
+        DEMSPH_LAUNCH_CHECK();
+        DEMSPH_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeIf;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        DEMSPH_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        if (!condStream) DEMSPH_CUDA(cudaStreamCreateWithFlags(&condStream, cudaStreamNonBlocking));
+        DEMSPH_CUDA(cudaStreamBeginCaptureToGraph(condStream, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        const cudaStream_t keep = s;
+        const long long l0 = g_launches.load();
+        s = condStream;
+        try {
+            const int* gate = &skinState.p->rebuild;
+            fCells.build(pos[P].p, N(), s, id[ID].p, false, gate);
+            g_launches += fCells.launches;
+            skin_rebuild_lists();
+        } catch (...) {
+            s = keep;
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(condStream, &tmp);
+            g_launches = l0;
+            throw;
+        }
+        s = keep;
+        condBodyLaunches = g_launches.load() - l0;
+        g_launches = l0;
+        cudaGraph_t out = nullptr;
+        DEMSPH_CUDA(cudaStreamEndCapture(condStream, &out));
+        DEMSPH_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    }
+    // Captures a block of steps, with conditional rebuilds when they apply; a
+    // runtime that refuses them leaves the block captured with the gated
+    // launches (and later blocks too).
+    template <class F>
+    void capture_steps(StepGraph& gr, int nsteps, F&& body) {
+        if (cond_wanted()) {
+            const std::array<int, 7> idx = {P, Vv, S, R0, D, ID, L};
+            const bool lists0 = haveLists;
+            condCapture = true;
+            try {
+                gr.capture(nsteps, s, body);
+                condCapture = false;
+                return;
+            } catch (const Status&) {
+                condCapture = false;
+                condOK = false;
+                (void)cudaGetLastError();
+                P = idx[0]; Vv = idx[1]; S = idx[2]; R0 = idx[3]; D = idx[4]; ID = idx[5]; L = idx[6];
+                haveLists = lists0;
+            }
+        }
+        gr.capture(nsteps, s, body);
     }
     // The gated reorder and skin-list build (with markers: the fluid-marker
     // skin rows and their transposed rows too).
@@ -2313,7 +2507,7 @@ struct SphScene {
         long k = 0;
         if (useGraphs && n >= 2) {
             StepGraph& gr = graph.at(index_key());
-            if (!gr.ready()) gr.capture(2, s, [&] { step_body(); step_body(); });
+            if (!gr.ready()) capture_steps(gr, 2, [&] { step_body(); step_body(); });
             for (; k + 2 <= n; k += 2) {
                 gr.launch(s);
                 iStep += 2;
@@ -2326,7 +2520,7 @@ struct SphScene {
             const int key = index_key() | kOneStepKey;
             StepGraph& gr = graph.at(key);
             if (!gr.ready()) {
-                gr.capture(1, s, [&] { step_body(); });  // moves the host's indices on
+                capture_steps(gr, 1, [&] { step_body(); });  // moves the host's indices on
                 oneStepAfter[key] = {P, Vv, S, R0, D, ID, L};
             } else {
                 const auto& a = oneStepAfter.at(key);
@@ -2559,7 +2753,7 @@ struct SphScene {
         dt = timeStep;
         uniformH = uni;
         hmaxGrid = hmax;
-        const double cell = 2.0 * hmax * (1.0 + skinMax);
+        const double cell = 2.0 * hmax * (1.0 + skinMax) * cellFactor;
         GridDesc gd{};
         if (!grid_set(gd, mn, mx, cell)) throw Status(DEMSPH_ERR_SCENE, "invalid domain or cell size");
         status.alloc(1, s, true);
@@ -2640,9 +2834,9 @@ struct SphScene {
         const DevStatus st2 = read_status();
         KF = std::max(st2.need_pairs, 1);
         KD = std::max(st2.need_aux, 1);
-        // a little headroom for compression during the run
-        KF = KF + KF / 8;
-        KD = KD + KD / 8;
+        // headroom for compression during the run
+        KF = KF + (int)std::ceil(KF * listHeadroom);
+        KD = KD + (int)std::ceil(KD * listHeadroom);
         alloc_lists();
         haveLists = false;
         iStep = 0;
@@ -3150,6 +3344,48 @@ int demsph_sph_skin_stats(demsph_sph_t h, double* fraction, long* rebuilds) {
                 *rebuilds = st.rebuilds;
             }
         }
+    });
+}
+int demsph_sph_set_conditional_rebuild(demsph_sph_t h, int enable) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        h->sc.condEnabled = enable != 0;
+        h->sc.graph.reset();
+        h->sc.oneStepAfter.clear();
+    });
+}
+int demsph_sph_conditional_rebuild(demsph_sph_t h, int* active, long* launchesPerRebuild) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        const SphScene& s = h->sc;
+        const bool on = s.cond_wanted() && s.useGraphs;
+        if (active) *active = on ? 1 : 0;
+        if (launchesPerRebuild) *launchesPerRebuild = on ? (long)s.condBodyLaunches : 0;
+    });
+}
+int demsph_sph_set_cell_factor(demsph_sph_t h, double factor) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "the cell size is set before initialisation");
+        if (!(factor >= 1.0 && factor <= 4.0)) throw Status(DEMSPH_ERR_INVALID, "cell factor must be in [1, 4]");
+        s.cellFactor = factor;
+    });
+}
+int demsph_sph_set_list_headroom(demsph_sph_t h, double fraction) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        SphScene& s = h->sc;
+        if (s.ready) throw Status(DEMSPH_ERR_INVALID, "the list headroom is set before initialisation");
+        if (!(fraction >= 0.0 && fraction <= 4.0)) throw Status(DEMSPH_ERR_INVALID, "headroom must be in [0, 4]");
+        s.listHeadroom = fraction;
+    });
+}
+int demsph_sph_list_capacity(demsph_sph_t h, int* fluidRow, int* dummyRow) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        if (fluidRow) *fluidRow = h->sc.KF;
+        if (dummyRow) *dummyRow = h->sc.KD;
     });
 }
 int demsph_sph_set_list_shape(demsph_sph_t h, int shape) {

@@ -417,6 +417,62 @@ def dem_drop_poly(n, seed, sigma=0.2, ratio=3.0, r0=0.005, density=2500.0, E=1e8
                     minb=tuple(lo), maxb=tuple(hi), dt=dt)
 
 
+def dem_agglomerate_drop(n, seed, r=0.005, density=2500.0, E=1e8, nu=0.3, restitution=0.8, mu=0.3, dt=1e-5,
+                         bond_E=1.0e7, strength=1.0e6, gap=-0.002):
+    """About n spheres of radius r dropped onto a 2-triangle plane, half in
+    bonded agglomerates (3 x 3 x 3 cubes of pitch 2r (1 + gap); the default
+    gap is a 0.2% overlap, so every face neighbour is a contact of definite
+    sign -- none starts at an overlap of rounding size -- and lies in an
+    adjacent cell of the 2 r_max grid, whatever the grid's alignment; parallel
+    bonds on these initial contacts, normal stiffness bond_E / 2r per unit area,
+    k_n / k_s = 2.5, breakable at `strength`), half in rigid 3-sphere clumps
+    (collinear pebbles 1.5 r apart, seeded orientations); agglomerates and
+    clumps alternate on a lattice of pitch 8r with seeded jitter.  Hertz-
+    Mindlin contact, the time step and gravity of dem_drop_poly, so both share
+    a DEM batch."""
+    rng = np.random.default_rng(seed)
+    cells = max(2, int(round(n / 15.0)))
+    side = max(2, int(math.ceil(cells ** (1.0 / 3.0))))
+    pitch = 8.0 * r
+    Es, Gs = hertz_params(E, nu)
+    pos = []
+    clumps = []
+    m_peb = 4.0 / 3.0 * math.pi * r ** 3 * density
+    m = 3.0 * m_peb
+    I0 = 0.4 * m_peb * r * r
+    cube = (np.stack(np.meshgrid(*([np.arange(3.0) - 1.0] * 3), indexing="ij"), -1).reshape(-1, 3)) * 2.0 * r * (1 + gap)
+    for k in range(cells):
+        i, j, l = k % side, (k // side) % side, k // (side * side)
+        c = np.array([(i + 0.5) * pitch, (j + 0.5) * pitch, 2.0 * r + (l + 0.5) * pitch])
+        c += rng.uniform(-0.25 * r, 0.25 * r, 3)
+        if k % 2 == 0:
+            pos.append(c + cube)
+        else:
+            ax = rng.normal(size=3)
+            ax /= np.linalg.norm(ax)
+            pts = c + np.outer([-1.0, 0.0, 1.0], ax) * 1.5 * r
+            off = 2.0 * m_peb * (1.5 * r) ** 2
+            Iax, Iperp = 3 * I0, 3 * I0 + off
+            If = Iperp * np.eye(3) + (Iax - Iperp) * np.outer(ax, ax)
+            clumps.append(dict(point=pts, radius=[r, r, r], centroid=c, velocity=(0.0, 0.0, 0.0),
+                               angularVelocity=(0.0, 0.0, 0.0), mass=m,
+                               inertia=(If[0, 0], If[1, 1], If[2, 2], If[0, 1], If[0, 2], If[1, 2]), material=0))
+    p = np.concatenate(pos, axis=0)
+    nb = p.shape[0]
+    L = side * pitch
+    lo = np.array([-2 * pitch, -2 * pitch, -2 * r])
+    hi = np.array([L + 2 * pitch, L + 2 * pitch, 2.0 * r + (cells // (side * side) + 1) * pitch + pitch])
+    verts = np.array([[lo[0], lo[1], 0.0], [hi[0], lo[1], 0.0], [hi[0], hi[1], 0.0], [lo[0], hi[1], 0.0]])
+    sc = DEMScene(name="dem_agglomerate_drop", position=p, radius=np.full(nb, r), density=np.full(nb, density),
+                  material=np.zeros(nb, np.int32), hertz=[(0, 0, Es, Gs, restitution, 0.0, 0.0, mu, 0.0, 0.0)],
+                  bonded=[(0, 0, 1.0, bond_E, 2.5, strength, strength, 0.0)], clumps=clumps,
+                  walls=[dict(vertices=verts, tri0=[0, 1], tri1=[1, 2], tri2=[3, 3], position=(0, 0, 0),
+                              material=0)],
+                  minb=tuple(lo), maxb=tuple(hi), dt=dt)
+    sc.bond_initial_contacts = True
+    return sc
+
+
 def bonded_beam_clumps(nx=400, ny=20, nz=20, r=0.001, n_clumps=20_000, seed=11, density=7800.0, E=2.0e11,
                        nu=0.3, restitution=0.5, mu=0.3, tip_load=0.05, dt=1.0e-7, steps=1000):
     """The bonded cantilever beam plus clumps of the DEM stress test: nx x ny x nz
@@ -645,7 +701,9 @@ def balls_in_tank(nx=24, ny=24, depth=24, dx=0.01, layers=3, balls=((0.5, 0.5, 0
 # ---------------------------------------------------------------------------
 # Loading into the solvers
 # ---------------------------------------------------------------------------
-def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
+def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True, configure=None):
+    """A DEMSolver loaded with the scene (and initialised); `configure(solver)`
+    runs before initialisation (cell size, capacities)."""
     from .solvers import DEMSolver
 
     s = DEMSolver(stream)
@@ -682,6 +740,8 @@ def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
         s.setConstantForce(scene.constant_force)
     if scene.periodic is not None:
         s.setPeriodicBoundary(*scene.periodic)
+    if configure is not None:
+        configure(s)
     if initialize:
         s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
         if scene.bond_initial_contacts:
@@ -690,12 +750,16 @@ def build_dem(scene: DEMScene, precision="mixed", stream=None, initialize=True):
     return s
 
 
-def build_sph(scene: SPHScene, precision="fp64", stream=None, initialize=True):
+def build_sph(scene: SPHScene, precision="fp64", stream=None, initialize=True, configure=None):
+    """A WCSPHSolver loaded with the scene (and initialised); `configure(solver)`
+    runs before initialisation (cell size, skin, list headroom)."""
     from .solvers import WCSPHSolver
 
     s = WCSPHSolver(stream)
     s.addSPHs(scene.fluid, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
     s.addDummies(scene.dummy, None, scene.sound_speed, scene.spacing, scene.density, scene.viscosity)
+    if configure is not None:
+        configure(s)
     if initialize:
         s.initialize(scene.minb, scene.maxb, scene.gravity, scene.dt, precision)
     return s

@@ -37,7 +37,7 @@ SPH_BYTES_PER_DUMMY = 900
 @dataclass
 class Request:
     key: int
-    kind: str          # "dem" or "sph"
+    kind: str          # "dem" (drop), "dem_bonded" (agglomerates and clumps) or "sph"
     n: int             # requested particle count
     steps: int
     arrival: float     # seconds after the stream starts
@@ -53,18 +53,26 @@ class Request:
         if self.scene is None:
             if self.kind == "dem":
                 self.scene = scenes.dem_drop_poly(self.n, self.seed)
+            elif self.kind == "dem_bonded":
+                self.scene = scenes.dem_agglomerate_drop(self.n, self.seed)
             else:
                 self.scene = scenes.sph_column(self.n, sph_c0, sph_dt)
         return self.scene
 
+    @property
+    def batch_kind(self):
+        """The batch that runs it: DEM kinds share one (same time step and gravity)."""
+        return "sph" if self.kind == "sph" else "dem"
+
     def particles(self):
+        """Moving particles: DEM balls and pebbles, SPH fluid."""
         sc = self.scene
-        return sc.position.shape[0] if self.kind == "dem" else sc.fluid.shape[0]
+        return sc.num_moving if self.batch_kind == "dem" else sc.fluid.shape[0]
 
     def bytes(self):
         sc = self.scene
-        if self.kind == "dem":
-            return sc.position.shape[0] * DEM_BYTES_PER_BALL
+        if self.batch_kind == "dem":
+            return (sc.position.shape[0] + sum(len(c["radius"]) for c in sc.clumps)) * DEM_BYTES_PER_BALL
         return sc.fluid.shape[0] * SPH_BYTES_PER_FLUID + sc.dummy.shape[0] * SPH_BYTES_PER_DUMMY
 
 
@@ -97,7 +105,7 @@ def _pct(v, q):
 
 class SceneServer:
     def __init__(self, hbm_budget=40e9, chunk=50, precision="mixed", max_members=512, sph_c0=None, sph_dt=None,
-                 keep_states=False):
+                 keep_states=False, autotune=False, tunings=None):
         import torch
 
         assert chunk % 5 == 0, "chunks are a multiple of the DEM re-sort cadence"
@@ -107,6 +115,10 @@ class SceneServer:
         self.precision = precision
         self.max_members = max_members
         self.keep_states = keep_states
+        # autotune: tune each kind before serving (autotune.py) unless
+        # `tunings` (kind -> autotune.Tuning, e.g. an earlier server's) is given
+        self.autotune = autotune
+        self.tunings = dict(tunings or {})
         self.sph_c0, self.sph_dt = sph_c0, sph_dt
         from . import _lib
 
@@ -120,8 +132,8 @@ class SceneServer:
         lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
         self.streams = {"dem": [torch.cuda.Stream(priority=hi), torch.cuda.Stream(priority=hi)],
                         "sph": [torch.cuda.Stream(priority=lo), torch.cuda.Stream(priority=lo)]}
-        self.batches = {"dem": DEMBatch(precision, streams=self.streams["dem"]),
-                        "sph": SPHBatch(precision, streams=self.streams["sph"])}
+        self.batches = {"dem": DEMBatch(precision, streams=self.streams["dem"], tuning=self.tunings.get("dem")),
+                        "sph": SPHBatch(precision, streams=self.streams["sph"], tuning=self.tunings.get("sph"))}
 
     def run(self, requests, log=None):
         """Serves the requests to completion; returns the stream's metrics.
@@ -144,8 +156,9 @@ class SceneServer:
             r.build(self.sph_c0, self.sph_dt)
             r.np_ = r.particles()
         by_key = {r.key: r for r in reqs}
+        tune_s = self._tune(reqs) if self.autotune and not self.tunings else 0.0
         lock = threading.Lock()
-        waiting = {"dem": [r for r in reqs if r.kind == "dem"], "sph": [r for r in reqs if r.kind == "sph"]}
+        waiting = {k: [r for r in reqs if r.batch_kind == k] for k in ("dem", "sph")}
         active = {"dem": {}, "sph": {}}
         used = [0.0]
         stats = {k: {"busy": 0.0, "chunks": 0, "rebuild": 0.0} for k in ("dem", "sph")}
@@ -262,7 +275,31 @@ class SceneServer:
                           sum(stats[k]["rebuild"] for k in stats))
         m["per_kind"] = {k: {"busy_s": stats[k]["busy"], "chunks": stats[k]["chunks"],
                              "commit_s": stats[k]["rebuild"], **self.batches[k].timing} for k in stats}
+        if self.tunings:
+            m["tuning"] = {k: t.as_dict() for k, t in self.tunings.items()}
+            m["tune_s"] = tune_s  # 0 when the tunings were given
         return m
+
+    def _tune(self, reqs):
+        """Autotunes each kind once, before serving, on the scene at the
+        particle-weighted median of its first requests (the size that
+        carries the kind's work; autotune.tune_dem / tune_sph); the batches
+        then build every scene with the tuning.  Returns the seconds spent."""
+        from . import autotune
+
+        tic = time.perf_counter()
+        for kind in ("dem", "sph"):
+            early = [r for r in reqs[:64] if r.kind == kind] or [r for r in reqs if r.batch_kind == kind]
+            if not early:
+                continue
+            early = sorted(early, key=lambda x: x.n)
+            w = np.cumsum([x.n for x in early])
+            r = early[int(np.searchsorted(w, 0.5 * w[-1]))]
+            t = (autotune.tune_dem(r.scene, self.precision) if kind == "dem"
+                 else autotune.tune_sph(r.scene, self.precision))
+            self.tunings[kind] = t
+            self.batches[kind].tuning = t
+        return time.perf_counter() - tic
 
     def _metrics(self, reqs, makespan, busy, chunks, rebuild_s):
         ps = sum(r.np_ * r.steps for r in reqs)
@@ -283,7 +320,7 @@ def particle_steps(requests, sph_c0, sph_dt):
     for r in requests:
         had = r.scene is not None
         sc = r.build(sph_c0, sph_dt)
-        tot += (sc.position.shape[0] if r.kind == "dem" else sc.fluid.shape[0]) * r.steps
+        tot += (sc.num_moving if r.batch_kind == "dem" else sc.fluid.shape[0]) * r.steps
         if not had:
             r.scene = None
     return tot
@@ -303,7 +340,7 @@ def run_plain(requests, precision="mixed", sph_c0=None, sph_dt=None):
     t0 = time.perf_counter()
     for r in requests:
         sc = r.scene
-        s = scenes.build_dem(sc, precision) if r.kind == "dem" else scenes.build_sph(sc, precision)
+        s = scenes.build_dem(sc, precision) if r.batch_kind == "dem" else scenes.build_sph(sc, precision)
         s.step(r.steps)
         del s
         r.scene = None

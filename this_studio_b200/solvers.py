@@ -105,6 +105,13 @@ class DEMMember:
         m = _i32(np.broadcast_to(materialID, (n,)))
         call("demsph_dem_member_add_balls", self._h, n, _dp(p), _dp(v), _dp(w), _dp(r), _dp(d), _ip(m), int(fixed))
 
+    def addClump(self, point, radius, centroidPosition, velocity, angularVelocity, mass, inertiaTensor, materialID):
+        """DEMSolver.addClump into the member: pebbles follow the balls added so far."""
+        p = _f64(point, (-1, 3))
+        call("demsph_dem_member_add_clump", self._h, p.shape[0], _dp(p), _dp(_f64(radius)),
+             _dp(_v3(centroidPosition)), _dp(_v3(velocity)), _dp(_v3(angularVelocity)), float(mass),
+             _dp(_f64(inertiaTensor, (6,))), int(materialID))
+
     def seal(self):
         call("demsph_dem_member_seal", self._h)
         return self
@@ -112,6 +119,11 @@ class DEMMember:
     def num(self):
         n = C.c_long()
         call("demsph_dem_member_count", self._h, C.byref(n))
+        return n.value
+
+    def numClumps(self):
+        n = C.c_long()
+        call("demsph_dem_member_num_clumps", self._h, C.byref(n))
         return n.value
 
 
@@ -349,9 +361,23 @@ class DEMSolver:
         call("demsph_dem_copy_members", self._h, source._h, k, _ip(_i32(srcStart)), _ip(_i32(dstStart)),
              _ip(_i32(num)), _ip(_i32(triDelta)), _dp(_f64(shift, (k, 3))))
 
+    def copyMemberBodies(self, source, srcClump, dstClump, numClumps, srcBond, dstBond, numBonds, shift):
+        """Device-side carry of continuing members' clumps and bonds from
+        `source`, after copyMembers: member k's clumps [srcClump[k],
+        +numClumps[k]) and bonds [srcBond[k], +numBonds[k]) there become
+        [dstClump[k], ...) and [dstBond[k], ...) here, positions moved by shift[k]."""
+        k = len(numClumps)
+        call("demsph_dem_copy_member_bodies", self._h, source._h, k, _ip(_i32(srcClump)), _ip(_i32(dstClump)),
+             _ip(_i32(numClumps)), _ip(_i32(srcBond)), _ip(_i32(dstBond)), _ip(_i32(numBonds)),
+             _dp(_f64(shift, (k, 3))))
+
     def setGraphs(self, enable=True):
         """Replay the step loop as CUDA graphs (default) or launch directly."""
         call("demsph_dem_set_graphs", self._h, int(bool(enable)))
+
+    def setCellFactor(self, factor):
+        """Ball grid cell edge as a multiple of 2 r_max, before initialize (autotuner)."""
+        call("demsph_dem_set_cell_factor", self._h, float(factor))
 
     def reserve(self, pairs=0, reverse=0, triangles=0):
         """Raise the initial list capacities per ball (before initialize)."""
@@ -626,6 +652,31 @@ class WCSPHSolver:
 
     def setListShape(self, shape):
         call("demsph_sph_set_list_shape", self._h, int(shape))
+
+    def setConditionalRebuild(self, enable=True):
+        """Graph steps skip the list rebuild's launches through a conditional
+        node (default) or launch them gated every step; same results."""
+        call("demsph_sph_set_conditional_rebuild", self._h, int(bool(enable)))
+
+    def conditionalRebuild(self):
+        """(in use, kernels one rebuild runs)."""
+        a, n = C.c_int(), C.c_long()
+        call("demsph_sph_conditional_rebuild", self._h, C.byref(a), C.byref(n))
+        return bool(a.value), n.value
+
+    def setCellFactor(self, factor):
+        """Grid cell edge as a multiple of 2 h_max (1 + skin), before initialize (autotuner)."""
+        call("demsph_sph_set_cell_factor", self._h, float(factor))
+
+    def setListHeadroom(self, fraction):
+        """Row capacity above the initial longest row, before initialize (autotuner)."""
+        call("demsph_sph_set_list_headroom", self._h, float(fraction))
+
+    def listCapacity(self):
+        """(fluid-fluid, fluid-dummy) row capacities."""
+        a, b = C.c_int(), C.c_int()
+        call("demsph_sph_list_capacity", self._h, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def copyMembers(self, source, srcStart, dstStart, num, shift):
         """Device-side carry of fluid state from `source` (a WCSPHSolver):
