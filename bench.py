@@ -331,7 +331,18 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
     torch.cuda.synchronize()
     m = srv.run(reqs)
     del reqs
-    plain_mixed = ps / serve.run_plain(mk(num), "mixed", c0, dt)
+    plain_kind = {}
+    plain_mixed = ps / serve.run_plain(mk(num), "mixed", c0, dt, per_kind=plain_kind)
+    # each kind's throughput on its own: served = its particle-steps over the
+    # time its batch was stepping (the kinds overlap on the device), plain =
+    # over its scenes' time on the plain solver
+    kinds = {}
+    for k, (sec, kps) in plain_kind.items():
+        pk = m["per_kind"].get(k, {})
+        served_k = pk.get("particle_steps", 0) / pk["busy_s"] if pk.get("busy_s") else None
+        kinds[k] = {"particle_steps": kps, "plain_s": sec, "plain_value": kps / sec,
+                    "served_busy_value": served_k,
+                    "served_busy_vs_plain": None if served_k is None else served_k / (kps / sec)}
     k = min(fp64_sample, num)
     sample = mk(k)
     ps_k = serve.particle_steps(sample, c0, dt)
@@ -346,7 +357,7 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
             "scene_step_latency_p99_ms": m["scene_step_latency_p99_ms"],
             "scene_latency_p50_s": m["scene_latency_p50_s"], "scene_latency_p99_s": m["scene_latency_p99_s"],
             "admission_wait_p50_s": m["admission_wait_p50_s"], "admission_wait_p99_s": m["admission_wait_p99_s"],
-            "per_kind": m["per_kind"], "autotune": tune}
+            "per_kind": m["per_kind"], "per_kind_vs_plain": kinds, "autotune": tune}
 
 
 def native(args, rank, world, dist):

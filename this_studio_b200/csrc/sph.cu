@@ -1368,81 +1368,6 @@ __device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, co
     acc += sb * (o.v - vd) - sw * p.r;
 }
 
-// Fluid neighbours of the uniform passes with their packed records gathered
-// one pair of neighbours ahead and the row entries two pairs ahead, so the
-// next pair's gathers are in flight while the current pair is computed.
-// f(j, q_j, v_j); rows with a count (cnt >= 0) only.
-#ifndef DEMSPH_UNI_PREFETCH
-#define DEMSPH_UNI_PREFETCH 0
-#endif
-template <class F>
-__device__ __forceinline__ void quad_fluid_pf(int cnt, const int* __restrict__ nb, int K, int i,
-                                              const int4* __restrict__ posq, const float4* __restrict__ velf, F&& f) {
-    const int sub = threadIdx.x & 3;
-    const int* __restrict__ row = nb + (size_t)i * K;
-    const int kend = sub + kQuad * lane_count(cnt, sub);
-    int k = sub;
-    int a = k < kend ? __ldg(row + k) : -1;
-    int b = k + kQuad < kend ? __ldg(row + k + kQuad) : -1;
-    int an = k + 2 * kQuad < kend ? __ldg(row + k + 2 * kQuad) : -1;
-    int bn = k + 3 * kQuad < kend ? __ldg(row + k + 3 * kQuad) : -1;
-    int4 qa = make_int4(0, 0, 0, 0), qb = qa;
-    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
-    if (a >= 0) { qa = posq[a]; va = velf[a]; }
-    if (b >= 0) { qb = posq[b]; vb = velf[b]; }
-    for (; k < kend; k += 2 * kQuad) {
-        int4 qan = make_int4(0, 0, 0, 0), qbn = qan;
-        float4 van = make_float4(0.f, 0.f, 0.f, 0.f), vbn = van;
-        if (an >= 0) { qan = posq[an]; van = velf[an]; }
-        if (bn >= 0) { qbn = posq[bn]; vbn = velf[bn]; }
-        const int kk = k + 4 * kQuad;
-        const int ann = kk < kend ? __ldg(row + kk) : -1;
-        const int bnn = kk + kQuad < kend ? __ldg(row + kk + kQuad) : -1;
-        f(a, qa, va);
-        if (b >= 0) f(b, qb, vb);
-        a = an; b = bn; an = ann; bn = bnn;
-        qa = qan; qb = qbn; va = van; vb = vbn;
-    }
-}
-// The skin-row walk of skin_loop with the same prefetch: f(j, q_j, v_j)
-// returns whether the pair is kept (written to this step's rows).
-template <class F>
-__device__ __forceinline__ void skin_fluid_pf(int cnt, const int* __restrict__ nbV, int K, int i,
-                                              int* __restrict__ nbOut, int* __restrict__ cntOut,
-                                              const int4* __restrict__ posq, const float4* __restrict__ velf,
-                                              F&& f) {
-    const int sub = threadIdx.x & 3;
-    const int* __restrict__ row = nbV + (size_t)i * K;
-    int* __restrict__ out = nbOut + (size_t)i * K;
-    int w = 0;
-    int k = sub;
-    int a = k < cnt ? __ldg(row + k) : -1;
-    int b = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
-    int an = k + 2 * kQuad < cnt ? __ldg(row + k + 2 * kQuad) : -1;
-    int bn = k + 3 * kQuad < cnt ? __ldg(row + k + 3 * kQuad) : -1;
-    int4 qa = make_int4(0, 0, 0, 0), qb = qa;
-    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
-    if (a >= 0) { qa = posq[a]; va = velf[a]; }
-    if (b >= 0) { qb = posq[b]; vb = velf[b]; }
-    for (; k < cnt; k += 2 * kQuad) {
-        int4 qan = make_int4(0, 0, 0, 0), qbn = qan;
-        float4 van = make_float4(0.f, 0.f, 0.f, 0.f), vbn = van;
-        if (an >= 0) { qan = posq[an]; van = velf[an]; }
-        if (bn >= 0) { qbn = posq[bn]; vbn = velf[bn]; }
-        const int kk = k + 4 * kQuad;
-        const int ann = kk < cnt ? __ldg(row + kk) : -1;
-        const int bnn = kk + kQuad < cnt ? __ldg(row + kk + kQuad) : -1;
-        if (f(a, qa, va)) out[sub + kQuad * w++] = a;
-        if (b >= 0 && f(b, qb, vb)) out[sub + kQuad * w++] = b;
-        a = an; b = bn; an = ann; bn = bnn;
-        qa = qan; qb = qbn; va = van; vb = vbn;
-    }
-    const unsigned gm = quad_mask();
-    const int over = quad_sum(w > 127 ? 1 : 0, gm);
-    const int packed = quad_sum(w << (7 * sub), gm);
-    if (sub == 0) cntOut[i] = over ? -1 : (kLaneRows | packed);
-}
-
 template <bool kSkin>
 __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
@@ -1456,23 +1381,13 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double h
     const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
     float3 acc = make_float3(0.f, 0.f, 0.f);
     if constexpr (kSkin) {
-        const int cv = d.cntV[i];
-        if (DEMSPH_UNI_PREFETCH && cv >= 0) {
-            skin_fluid_pf(cv, d.nbV, d.KF, i, d.nbF, d.cntF, d.posq, d.velf, [&](int j, int4 qj, float4 vj) {
-                const PairGeom p = pair_geom(o.q, qj, u);
-                if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
-                acc_fluid_u(o, p, vj, __int_as_float(qj.w), u, acc);
-                return true;
-            });
-        } else {
-            skin_loop(cv, d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
-                const int4 qj = d.posq[j];
-                const PairGeom p = pair_geom(o.q, qj, u);
-                if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
-                acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
-                return true;
-            });
-        }
+        skin_loop(d.cntV[i], d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
+            const int4 qj = d.posq[j];
+            const PairGeom p = pair_geom(o.q, qj, u);
+            if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
+            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+            return true;
+        });
         if (d.ND > 0) {
             skin_loop(d.cntVD[i], d.nbVD, d.KD, i, d.nbD, d.cntD, pi4, d.g, d.dStart, d.dpos, -1, [&](int j) {
                 const PairGeom p = pair_geom(o.q, d.dposq[j], u);
@@ -1482,19 +1397,11 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double h
             });
         }
     } else {
-        const int cf = d.cntF[i];
-        if (DEMSPH_UNI_PREFETCH && cf >= 0) {
-            quad_fluid_pf(cf, d.nbF, d.KF, i, d.posq, d.velf, [&](int, int4 qj, float4 vj) {
-                const PairGeom p = pair_geom(o.q, qj, u);
-                acc_fluid_u(o, p, vj, __int_as_float(qj.w), u, acc);
-            });
-        } else {
-            quad_neighbors(cf, d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
-                const int4 qj = d.posq[j];
-                const PairGeom p = pair_geom(o.q, qj, u);
-                acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
-            });
-        }
+        quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+            const int4 qj = d.posq[j];
+            const PairGeom p = pair_geom(o.q, qj, u);
+            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+        });
         if (d.ND > 0) {
             quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
                 const PairGeom p = pair_geom(o.q, d.dposq[j], u);
@@ -1535,21 +1442,16 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     const double4 s4 = d.st[i];
     const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
     float sumF = 0.f, sumD = 0.f;  // sum of (1 / rho_j) (v_i - v*) . grad W / (1/2), per kind of neighbour
-    auto fluid = [&](int4 qj, float4 vj) {  // vj = (v_j, p_j)
+    quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
+        const int4 qj = d.posq[j];
         const PairGeom p = pair_geom(o.q, qj, u);
+        const float4 vj = d.velf[j];  // (v_j, p_j)
         const float rhoj = __int_as_float(qj.w);
         const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
         const float rbar = 0.5f * (o.rho + rhoj);
         const float X = __fdividef(o.PL - vj.w, rbar * u.cF);
         sumF += __fdividef(p.Kdq * (dot(dv, p.r) * p.inv_r + X), rhoj);
-    };
-    const int cf = d.cntF[i];
-    if (DEMSPH_UNI_PREFETCH && cf >= 0) {
-        quad_fluid_pf(cf, d.nbF, d.KF, i, d.posq, d.velf, [&](int, int4 qj, float4 vj) { fluid(qj, vj); });
-    } else {
-        quad_neighbors(cf, d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos,
-                       [&](int j) { fluid(d.posq[j], d.velf[j]); });
-    }
+    });
     if (d.ND > 0) {
         quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
             const PairGeom p = pair_geom(o.q, d.dposq[j], u);

@@ -273,8 +273,10 @@ class SceneServer:
         busy = max(stats[k]["busy"] for k in stats)
         m = self._metrics(reqs, makespan, busy, sum(stats[k]["chunks"] for k in stats),
                           sum(stats[k]["rebuild"] for k in stats))
+        kind_ps = {k: sum(r.np_ * r.steps for r in reqs if r.batch_kind == k) for k in stats}
         m["per_kind"] = {k: {"busy_s": stats[k]["busy"], "chunks": stats[k]["chunks"],
-                             "commit_s": stats[k]["rebuild"], **self.batches[k].timing} for k in stats}
+                             "commit_s": stats[k]["rebuild"], "particle_steps": kind_ps[k],
+                             **self.batches[k].timing} for k in stats}
         if self.tunings:
             m["tuning"] = {k: t.as_dict() for k, t in self.tunings.items()}
             m["tune_s"] = tune_s  # 0 when the tunings were given
@@ -326,10 +328,12 @@ def particle_steps(requests, sph_c0, sph_dt):
     return tot
 
 
-def run_plain(requests, precision="mixed", sph_c0=None, sph_dt=None):
+def run_plain(requests, precision="mixed", sph_c0=None, sph_dt=None, per_kind=None):
     """Every request alone on the plain solver, one after another.  Scenes
     are generated before the clock starts, as for the server; the time covers
-    building each device scene (upload, initialisation) and its steps."""
+    building each device scene (upload, initialisation) and its steps.  With
+    a dict `per_kind`, each kind's seconds and particle-steps are added to it
+    (per_kind[kind] = [seconds, particle-steps])."""
     import torch
 
     if sph_c0 is None:
@@ -340,8 +344,14 @@ def run_plain(requests, precision="mixed", sph_c0=None, sph_dt=None):
     t0 = time.perf_counter()
     for r in requests:
         sc = r.scene
+        tk = time.perf_counter()
         s = scenes.build_dem(sc, precision) if r.batch_kind == "dem" else scenes.build_sph(sc, precision)
         s.step(r.steps)
+        if per_kind is not None:
+            torch.cuda.synchronize()
+            e = per_kind.setdefault(r.batch_kind, [0.0, 0])
+            e[0] += time.perf_counter() - tk
+            e[1] += (sc.num_moving if r.batch_kind == "dem" else sc.fluid.shape[0]) * r.steps
         del s
         r.scene = None
     torch.cuda.synchronize()
