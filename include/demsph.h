@@ -395,12 +395,15 @@ int demsph_sph_num_list_shapes(void);
  * multiple (1 to 4) of 2 h_max (1 + skin); set before initialisation.  Any
  * factor gives the same pairs; rows come in another order. */
 int demsph_sph_set_cell_factor(demsph_sph_t s, double factor);
-/* No counterpart in the reference.  In CUDA-graph steps of a scene with skin
- * lists (and no coupled balls), the list rebuild -- cell sort, reorder, skin
- * rows -- is the body of a conditional graph node whose condition the
- * rebuild decision sets on the device, so steps that keep their lists launch
- * none of its kernels (enable = 0: the rebuild's kernels are launched every
- * step and return at once when the decision says so; results are identical).
+/* No counterpart in the reference.  enable = 1: in CUDA-graph steps of a
+ * scene with skin lists (and no coupled balls), the list rebuild -- cell
+ * sort, reorder, skin rows -- is the body of a conditional graph node whose
+ * condition the rebuild decision sets on the device, so steps that keep their
+ * lists launch none of its kernels (2% off the 128k dam break's step).  Off by
+ * default: the rebuild's kernels are then launched every step and return at
+ * once when the decision says so (results are identical), because Nsight
+ * Compute does not profile the kernel nodes of graphs that hold conditional
+ * nodes.
  * conditional_rebuild reports whether it is in use and how many kernels one
  * rebuild runs (the library's launch counter counts them only when they run,
  * which the host does not see: add rebuilds x launchesPerRebuild). */

@@ -2070,7 +2070,7 @@ struct SphScene {
     // body does the same work as the gated launches outside graphs; they are
     // counted when a rebuild runs them, not per replay.
     bool condOK = true;         // the runtime took conditional capture so far
-    bool condEnabled = true;    // demsph_sph_set_conditional_rebuild
+    bool condEnabled = false;   // demsph_sph_set_conditional_rebuild (off: profilers skip such graphs' kernels)
     bool condCapture = false;   // set while a block of steps is captured
     long long condBodyLaunches = 0;
     cudaStream_t condStream = nullptr;

@@ -655,7 +655,8 @@ class WCSPHSolver:
 
     def setConditionalRebuild(self, enable=True):
         """Graph steps skip the list rebuild's launches through a conditional
-        node (default) or launch them gated every step; same results."""
+        node, or launch them gated every step (the default, which profilers
+        can see); same results."""
         call("demsph_sph_set_conditional_rebuild", self._h, int(bool(enable)))
 
     def conditionalRebuild(self):

@@ -57,6 +57,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel directly")
+    ap.add_argument("--flush-l2", action="store_true",
+                    help="one step at a time with a 256 MB write between steps (as bench.py times them)")
     a = ap.parse_args()
     s = build(a.name, a.precision)
     if a.name.startswith("coupled") or a.name.startswith("ice_sheet"):
@@ -68,7 +70,15 @@ def main():
     else:
         if a.no_graphs:
             s.setGraphs(False)
-        s.step(a.steps)
+        if a.flush_l2:
+            import torch
+
+            flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+            for _ in range(a.steps):
+                flush.zero_()
+                s.step(1)
+        else:
+            s.step(a.steps)
         s.stepIndex()
     print(f"{a.name}: {a.steps} steps done")
 
