@@ -360,6 +360,18 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
             "per_kind": m["per_kind"], "per_kind_vs_plain": kinds, "autotune": tune}
 
 
+def pipeline_traffic(tj):
+    """DRAM bytes per launch of the momentum kernel inside the step (caches as
+    the step leaves them, L2 flushed between steps): first and second pass
+    from profiles/traffic.json, or None."""
+    p = tj.get("in_pipeline")
+    if not p:
+        return None
+    a, b = p["k_sph_accel_u_first_pass"], p["k_sph_accel_u_second_pass"]
+    return {"first_pass": a["dram_read"] + a["dram_write"], "second_pass": b["dram_read"] + b["dram_write"],
+            "first_pass_note": a.get("note"), "source": "profiles/traffic.json in_pipeline"}
+
+
 def native(args, rank, world, dist):
     import torch
 
@@ -506,6 +518,8 @@ def native(args, rank, world, dist):
         # fluid particle, 24 B per dummy); the step against the per-step model
         "roofline": {"bound": "hbm", "kernel": "k_sph_accel_u", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_what": "cold L2 per launch (ncu flushes before each profiled launch)",
+                     "traffic_in_pipeline": pipeline_traffic(tj),
                      "algorithmic_bytes_per_launch": mom_bytes, "ms_per_launch": mom_ms,
                      "model": "momentum_bytes_8d (bench.py)",
                      "implementation_bytes_per_launch": impl_bytes,
