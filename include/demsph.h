@@ -366,8 +366,14 @@ int demsph_sph_add(demsph_sph_t s, int dummy, long n, const double* position, co
  * grid (cell = 2 h_max), dummy-dummy pairs and dummy wall normals. */
 int demsph_sph_initialize(demsph_sph_t s, const double* minBoundary, const double* maxBoundary, const double* gravity,
                           double timeStep, int precision);
-/* numSteps passes of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621). */
+/* numSteps passes of the WCSPHSolver::solve loop (WCSPHSolver.h:607-621),
+ * queued on the scene's stream: the call returns without waiting for the
+ * device (getters, snapshots and demsph_sph_synchronize wait).  A neighbour
+ * row that overflows during the steps is walked from the cell table (same
+ * pairs); the lists are regrown at the next call. */
 int demsph_sph_step(demsph_sph_t s, long numSteps);
+/* No counterpart in the reference.  Waits for the scene's queued work. */
+int demsph_sph_synchronize(demsph_sph_t s);
 /* No counterpart in the reference.  step() replays the step loop as CUDA
  * graphs of two steps; enable = 0 launches every kernel directly.  Both give
  * identical results. */

@@ -131,6 +131,7 @@ SIGNATURES = {
     "demsph_sph_add": [_vp, _int, _long, _d, _d, _d, _d, _d, _d],
     "demsph_sph_initialize": [_vp, _d, _d, _d, _dbl, _int],
     "demsph_sph_step": [_vp, _long],
+    "demsph_sph_synchronize": [_vp],
     "demsph_sph_neighbor_search": [_vp],
     "demsph_sph_eval_accel": [_vp],
     "demsph_sph_profile_steps": [_vp, _long, _d],

@@ -152,8 +152,11 @@ class _Batch:
         self.commit(self.prepare(self.members))
 
     def step(self, n):
+        """n steps of every member; returns when the device has done them."""
         if self.solver is not None and n > 0:
             self.solver.step(n)
+            if hasattr(self.solver, "synchronize"):
+                self.solver.synchronize()
             for m in self.members:
                 m.steps_done += n
 

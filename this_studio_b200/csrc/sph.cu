@@ -2077,6 +2077,11 @@ struct SphScene {
     bool cond_wanted() const { return condOK && condEnabled && nM == 0 && skin_on(); }
     ~SphScene() {
         if (condStream) cudaStreamDestroy(condStream);
+        if (statusEv) {
+            cudaEventSynchronize(statusEv);
+            cudaEventDestroy(statusEv);
+        }
+        if (hostStatus) cudaFreeHost(hostStatus);
     }
     void skin_rebuild_conditional() {
         cudaStreamCaptureStatus cs;
@@ -2401,11 +2406,51 @@ struct SphScene {
     // Steps without a state snapshot: a list row that overflows its capacity
     // is walked from the cell table by the passes (same neighbours), so an
     // overflow never changes results; the lists are regrown for later calls.
+    // The status of a run's steps is copied to pinned host memory when they
+    // are queued and looked at by the next call, so step() returns without
+    // waiting for the device.  Nothing in a step depends on it: a list row
+    // that overflows is walked from the cell table by the passes (same
+    // neighbours), and the lists are regrown before the next steps.  The
+    // device status keeps its flags until they are consumed, so a later
+    // copy carries every earlier overflow.
+    DevStatus* hostStatus = nullptr;
+    cudaEvent_t statusEv = nullptr;
+    bool statusPending = false;
+    void status_async() {
+        if (!hostStatus) {
+            DEMSPH_CUDA(cudaHostAlloc((void**)&hostStatus, sizeof(DevStatus), cudaHostAllocDefault));
+            DEMSPH_CUDA(cudaEventCreateWithFlags(&statusEv, cudaEventDisableTiming));
+        }
+        DEMSPH_CUDA(cudaMemcpyAsync(hostStatus, status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+        DEMSPH_CUDA(cudaEventRecord(statusEv, s));
+        statusPending = true;
+    }
+    // Acts on the last queued status once the device has written it (wait:
+    // block until then); an overflow regrows the lists and clears the flags.
+    void consume_status(bool wait) {
+        if (!statusPending) return;
+        if (wait) {
+            DEMSPH_CUDA(cudaEventSynchronize(statusEv));
+        } else {
+            const cudaError_t q = cudaEventQuery(statusEv);
+            if (q == cudaErrorNotReady) {  // still queued: a later call looks
+                if (cudaPeekAtLastError() == cudaErrorNotReady) (void)cudaGetLastError();
+                return;
+            }
+            DEMSPH_CUDA(q);
+        }
+        statusPending = false;
+        const DevStatus st2 = *hostStatus;
+        if (st2.overflow) {
+            grow(st2);
+            clear_status();
+        }
+    }
     void run(long n) {
         if (!ready) throw Status(DEMSPH_ERR_NOT_READY, "scene not initialised");
         if (n <= 0) return;
         sync_mode();
-        clear_status();
+        consume_status(false);
         long k = 0;
         if (useGraphs && n >= 2) {
             StepGraph& gr = graph.at(index_key());
@@ -2433,8 +2478,7 @@ struct SphScene {
             time += dt;
         }
         for (; k < n; k++) step_once();
-        DevStatus st2 = read_status();
-        if (st2.overflow) grow(st2);
+        status_async();
     }
     static constexpr int kOneStepKey = 1 << 10;
     std::map<int, std::array<int, 7>> oneStepAfter;  // one-step graph key -> indices after the step
@@ -2997,6 +3041,13 @@ int demsph_sph_step(demsph_sph_t h, long n) {
     return guarded([&] {
         SPH_CHECK(h);
         h->sc.run(n);
+    });
+}
+int demsph_sph_synchronize(demsph_sph_t h) {
+    return guarded([&] {
+        SPH_CHECK(h);
+        DEMSPH_CUDA(cudaStreamSynchronize(h->sc.s));
+        h->sc.consume_status(true);
     });
 }
 int demsph_sph_neighbor_search(demsph_sph_t h) {

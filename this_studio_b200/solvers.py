@@ -530,7 +530,13 @@ class WCSPHSolver:
              float(timeStep), prec)
 
     def step(self, numSteps=1):
+        """Queues numSteps steps on the scene's stream and returns (getters
+        and synchronize() wait for them)."""
         call("demsph_sph_step", self._h, int(numSteps))
+
+    def synchronize(self):
+        """Waits for the scene's queued steps."""
+        call("demsph_sph_synchronize", self._h)
 
     def solve(self, minBoundary, maxBoundary, gravity, timeStep, maximumTime, numFrame=0, dir=None, deviceID=0,
               maximumThread=256, precision="fp64"):
