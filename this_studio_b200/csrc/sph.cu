@@ -10,7 +10,8 @@
 //          cell order (double-buffered), so a cell's particles are contiguous
 //          and neighbour gathers stay in L1/L2.
 //   dummy  pos | vel | st (c,nu,rho0,-) | normal : double4, sorted once.
-//   lists  ELL, row-major: nb[i*K + k] = k-th neighbour of fluid i.
+//   lists  ELL rows, entry k of object i at row_at(i, k, K): the rows of 8
+//          consecutive objects interleaved 4 entries at a time.
 #include <array>
 #include <map>
 #include <algorithm>
@@ -602,6 +603,26 @@ struct ListShape {
 constexpr ListShape kListShapes[] = {{4, 512, 6}, {4, 384, 8}, {8, 256, 4}, {2, 512, 12}};
 constexpr int kNumListShapes = 4;
 
+// Layout of the neighbour rows (every list of this file: fluid-fluid,
+// fluid-dummy, fluid-marker, the transposed marker rows, their skin rows).
+// A pass gives each object a quad of lanes, lane `sub` taking entries sub,
+// sub + 4, ...; a warp holds the quads of 8 consecutive objects.  The rows of
+// 8 consecutive objects are therefore interleaved 4 entries at a time: the 32
+// entries a warp reads in one iteration of a pair loop (entries 4m .. 4m + 3
+// of its 8 objects) are one 128-byte line, instead of 16 bytes from each of 8
+// rows.  Entry k of object i is at row_base(i, K) + 32 (k / 4) + k % 4; an
+// array of n rows of capacity K holds row_words(n, K) entries.
+__host__ __device__ __forceinline__ size_t row_base(int i, int K) {
+    return (size_t)(i >> 3) * (size_t)((K + 3) & ~3) * 8 + (size_t)(i & 7) * 4;
+}
+__host__ __device__ __forceinline__ size_t row_at(int i, int k, int K) {
+    return row_base(i, K) + (size_t)(k >> 2) * 32 + (k & 3);
+}
+static inline size_t row_words(size_t n, int K) {
+    return ((n + 7) & ~(size_t)7) * (size_t)((std::max(K, 1) + 3) & ~3);
+}
+
+
 __device__ __forceinline__ float list_band(float cut, float eps) {
     return 4.0f * eps * (cut + 2.0f * eps) * 1.7321f + 4.0e-6f * cut * cut;
 }
@@ -712,12 +733,12 @@ __device__ __forceinline__ void cell_lists(int ps, int pe, const Stencil& st, co
                 const unsigned hB = __ballot_sync(0xffffffffu, inB);
                 if (hA) {
                     const int k = na + __popc(hA & lt);
-                    if (inA && k < K) nb[(size_t)i0 * K + k] = j;
+                    if (inA && k < K) nb[row_at(i0, k, K)] = j;
                     na += __popc(hA);
                 }
                 if (hB) {
                     const int k = nbc + __popc(hB & lt);
-                    if (inB && k < K) nb[(size_t)i1 * K + k] = j;
+                    if (inB && k < K) nb[row_at(i1, k, K)] = j;
                     nbc += __popc(hB);
                 }
             }
@@ -836,16 +857,17 @@ __device__ __forceinline__ void quad_neighbors(int cnt, const int* __restrict__ 
     if (cnt >= 0) {
         // two neighbours per iteration, their row entries loaded one
         // iteration ahead so the index load is off the gather's critical path
-        const int* __restrict__ row = nb + (size_t)i * K;
-        const int kend = sub + kQuad * lane_count(cnt, sub);
-        int k = sub;
-        int j0 = k < kend ? __ldg(row + k) : -1;
-        int j1 = k + kQuad < kend ? __ldg(row + k + kQuad) : -1;
-        for (; k < kend; k += 2 * kQuad) {
+        // (this lane's m-th entry, 4m + sub, sits at row[32 m])
+        const int* __restrict__ row = nb + row_base(i, K) + sub;
+        const int mend = lane_count(cnt, sub);
+        int m = 0;
+        int j0 = m < mend ? __ldg(row) : -1;
+        int j1 = m + 1 < mend ? __ldg(row + 32) : -1;
+        for (; m < mend; m += 2) {
             const int a = j0, b = j1;
-            const int kn = k + 2 * kQuad;
-            j0 = kn < kend ? __ldg(row + kn) : -1;
-            j1 = kn + kQuad < kend ? __ldg(row + kn + kQuad) : -1;
+            const int mn = m + 2;
+            j0 = mn < mend ? __ldg(row + 32 * mn) : -1;
+            j1 = mn + 1 < mend ? __ldg(row + 32 * (mn + 1)) : -1;
             f(a);
             if (b >= 0) f(b);
         }
@@ -1078,19 +1100,22 @@ __device__ __forceinline__ void skin_loop(int cnt, const int* __restrict__ nbV, 
         });
         return;
     }
-    const int* __restrict__ row = nbV + (size_t)i * K;
-    int* __restrict__ out = nbOut + (size_t)i * K;
+    // this lane's entries of the dense skin row (4m + sub at row[32 m]); the
+    // kept ones become its lane row of this step (w-th kept at out[32 w])
+    const int* __restrict__ row = nbV + row_base(i, K) + sub;
+    int* __restrict__ out = nbOut + row_base(i, K) + sub;
     int w = 0;  // pairs this lane kept
-    int k = sub;
-    int j0 = k < cnt ? __ldg(row + k) : -1;
-    int j1 = k + kQuad < cnt ? __ldg(row + k + kQuad) : -1;
-    for (; k < cnt; k += 2 * kQuad) {
+    const int mend = lane_count(cnt, sub);
+    int m = 0;
+    int j0 = m < mend ? __ldg(row) : -1;
+    int j1 = m + 1 < mend ? __ldg(row + 32) : -1;
+    for (; m < mend; m += 2) {
         const int a = j0, b = j1;
-        const int kn = k + 2 * kQuad;
-        j0 = kn < cnt ? __ldg(row + kn) : -1;
-        j1 = kn + kQuad < cnt ? __ldg(row + kn + kQuad) : -1;
-        if (fn(a)) out[sub + kQuad * w++] = a;
-        if (b >= 0 && fn(b)) out[sub + kQuad * w++] = b;
+        const int mn = m + 2;
+        j0 = mn < mend ? __ldg(row + 32 * mn) : -1;
+        j1 = mn + 1 < mend ? __ldg(row + 32 * (mn + 1)) : -1;
+        if (fn(a)) out[32 * w++] = a;
+        if (b >= 0 && fn(b)) out[32 * w++] = b;
     }
     const unsigned gm = quad_mask();
     const int over = quad_sum(w > 127 ? 1 : 0, gm);
@@ -1546,9 +1571,9 @@ __global__ void __launch_bounds__(kSphBlock, kMarkerForceBlocks<R>) k_sph_marker
         if (cnt >= 0) {
             // the transposed list (k_sph_marker_lists, or the first reaction's
             // exact rows on skin lists): the fluid rows' pair set
-            const int* __restrict__ row = d.nbR + (size_t)t * d.KR;
+            const int* __restrict__ row = d.nbR + row_base(t, d.KR) + sub;
             const int c = lane_count(cnt, sub);
-            for (int k = 0; k < c; k++) term(__ldg(row + sub + kQuad * k), false);
+            for (int k = 0; k < c; k++) term(__ldg(row + 32 * k), false);
         } else {
             // an overflowed row: the same pairs from the cell stencil, with the
             // cutoff test on the build-time positions
@@ -1867,26 +1892,26 @@ struct SphScene {
     void alloc_lists() {
         graph.reset();  // the captured kernels hold the old list buffers
         size_t n = (size_t)N();
-        nbF.alloc(n * KF, s, false);
+        nbF.alloc(row_words(n, KF), s, false);
         cntF.alloc(n, s, true);
-        nbD.alloc(n * std::max(KD, 1), s, false);
+        nbD.alloc(row_words(n, std::max(KD, 1)), s, false);
         cntD.alloc(n, s, true);
         if (nM > 0) {
-            nbM.alloc(n * KM, s, false);
+            nbM.alloc(row_words(n, KM), s, false);
             cntM.alloc(n, s, true);
-            nbR.alloc((size_t)nM * KR, s, false);
+            nbR.alloc(row_words((size_t)nM, KR), s, false);
             cntR.alloc(nM, s, true);
         }
         if (skinMax > 0) {
-            nbV.alloc(n * KF, s, false);
+            nbV.alloc(row_words(n, KF), s, false);
             cntV.alloc(n, s, true);
-            nbVD.alloc(n * std::max(KD, 1), s, false);
+            nbVD.alloc(row_words(n, std::max(KD, 1)), s, false);
             cntVD.alloc(n, s, true);
             if (xb.n < n) xb.alloc(n, s, true);
             if (nM > 0) {
-                nbMV.alloc(n * KM, s, false);
+                nbMV.alloc(row_words(n, KM), s, false);
                 cntMV.alloc(n, s, true);
-                nbRV.alloc((size_t)nM * KR, s, false);
+                nbRV.alloc(row_words((size_t)nM, KR), s, false);
                 cntRV.alloc(nM, s, true);
                 if (xbM.n < (size_t)nM) xbM.alloc(nM, s, true);
             }
@@ -3639,7 +3664,7 @@ int demsph_sph_get_pairs(demsph_sph_t h, int which, int* a, int* b) {
                 for (int k = 0; k < cnt[t]; k++) slots.push_back(nb[(size_t)k * rows + t]);
             } else {
                 for (int sub = 0; sub < kQuad; sub++)
-                    for (int m = 0; m < lane_count(cnt[t], sub); m++) slots.push_back(nb[(size_t)t * K + sub + kQuad * m]);
+                    for (int m = 0; m < lane_count(cnt[t], sub); m++) slots.push_back(nb[row_at(t, sub + kQuad * m, K)]);
             }
             std::sort(slots.begin(), slots.end(), [&](int x, int y) { return colKey[x] < colKey[y]; });
             for (int j : slots) {
