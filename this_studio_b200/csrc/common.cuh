@@ -1,6 +1,8 @@
 // Shared device math, status codes and device-buffer ownership for the
 // DEMSPH B200 library.
 #pragma once
+#include <cstring>
+#include <mutex>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -107,6 +109,43 @@ static void host_parallel(long n, F&& f, int threads = 8) {
         if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
     }
     for (auto& th : pool) th.join();
+}
+
+// Process-wide page-locked staging for bulk host <-> device copies of scene
+// records: copies from (or to) pageable memory run at a fraction of the
+// link's speed, so the records are copied into this buffer by several host
+// threads and moved by one DMA.  Grown on demand and kept; one user at a
+// time (lock() while filling, copying and waiting for the copy).
+struct PinnedStage {
+    std::mutex m;
+    char* p = nullptr;
+    size_t n = 0;
+    static PinnedStage& get() {
+        static PinnedStage s;
+        return s;
+    }
+    // A buffer of at least `bytes`; call with m held.
+    char* reserve(size_t bytes) {
+        if (n < bytes) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            n = 0;
+            const size_t want = bytes + bytes / 4;
+            if (cudaHostAlloc((void**)&p, want, cudaHostAllocDefault) != cudaSuccess) {
+                (void)cudaGetLastError();
+                p = nullptr;
+                return nullptr;  // the caller copies from pageable memory instead
+            }
+            n = want;
+        }
+        return p;
+    }
+};
+// memcpy of `bytes` in up to 8 host threads (one below 64 KB).
+static inline void host_copy(void* dst, const void* src, size_t bytes) {
+    host_parallel((long)bytes, [&](long a, long b) {
+        if (b > a) std::memcpy((char*)dst + a, (const char*)src + a, (size_t)(b - a));
+    });
 }
 
 template <class T>

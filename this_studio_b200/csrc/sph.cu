@@ -2670,44 +2670,108 @@ struct SphScene {
     }
 
     // Host particle sets -> device scene (WCSPHSolver::initialize, WCSPHSolver.h:578-612).
+    // One pass over a particle set in host threads: any non-finite position
+    // or non-positive h, the largest h, whether every h has the FP32 value h0,
+    // and whether every particle has the first one's constants (h, m, c, nu
+    // and, for dummies, rho0).
+    struct SetScan {
+        bool bad = false, sameH = true, sameConst = true;
+        double hmax = 0;
+    };
+    static SetScan scan_set(const HostSet& t, float h0, bool dummies) {
+        SetScan r;
+        const long n = (long)t.size();
+        if (n == 0) return r;
+        const double4 p0 = t.pos[0], v0 = t.vel[0], s0 = t.st[0];
+        const double r0 = t.rho0[0];
+        std::mutex mu;
+        host_parallel(n, [&](long a, long b) {
+            SetScan c;
+            for (long k = a; k < b; k++) {
+                const double4 p = t.pos[k];
+                if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0)) c.bad = true;
+                c.hmax = std::max(c.hmax, p.w);
+                c.sameH = c.sameH && (float)p.w == h0;
+                c.sameConst = c.sameConst && p.w == p0.w && t.vel[k].w == v0.w && t.st[k].z == s0.z &&
+                              t.st[k].w == s0.w && (!dummies || t.rho0[k] == r0);
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            r.bad = r.bad || c.bad;
+            r.hmax = std::max(r.hmax, c.hmax);
+            r.sameH = r.sameH && c.sameH;
+            r.sameConst = r.sameConst && c.sameConst;
+        });
+        return r;
+    }
     void initialize(double3 mn, double3 mx, double3 g, double timeStep, int prec) {
         if (hf.size() == 0) throw Status(DEMSPH_ERR_SCENE, "the number of fluid particles is equal to 0");
-        for (auto& p : hf.pos)
-            if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z) || !(p.w > 0))
-                throw Status(DEMSPH_ERR_SCENE, "fluid particle with non-finite position or non-positive h");
-        double hmax = 0;
-        for (auto& p : hf.pos) hmax = std::max(hmax, p.w);
-        for (auto& p : hd.pos) hmax = std::max(hmax, p.w);
         // the same h everywhere, as the list build sees it (FP32)
         const float h0 = (float)hf.pos[0].w;
-        bool uni = true;
-        for (auto& p : hf.pos) uni = uni && (float)p.w == h0;
-        for (auto& p : hd.pos) uni = uni && (float)p.w == h0;
+        const SetScan sf = scan_set(hf, h0, false), sd = scan_set(hd, h0, true);
+        if (sf.bad) throw Status(DEMSPH_ERR_SCENE, "fluid particle with non-finite position or non-positive h");
+        const double hmax = std::max(sf.hmax, sd.hmax);
+        const bool uniH = sf.sameH && sd.sameH;
         nF = (int)hf.size();
         nD = (int)hd.size();
-        init_grid(mn, mx, g, timeStep, prec, hmax, uni);
+        init_grid(mn, mx, g, timeStep, prec, hmax, uniH);
         hUni = h0;
-        this->uni = uniform_of(hf, hd);
+        // uniform constants (uniform_of): the fluid's and the dummies' own
+        // constants the same throughout, and the dummies' h the fluid's
+        Uniform u;
+        u.h = hf.pos[0].w; u.mF = hf.vel[0].w; u.cF = hf.st[0].z; u.nuF = hf.st[0].w;
+        bool on = sf.sameConst;
+        if (hd.size()) {
+            u.mD = hd.vel[0].w; u.cD = hd.st[0].z; u.nuD = hd.st[0].w; u.rho0D = hd.rho0[0];
+            on = on && sd.sameConst && hd.pos[0].w == u.h;
+        }
+        u.on = on;
+        this->uni = u;
         const int n = N(), nd = ND();
-        auto up4 = [&](DBuf<double4>& b, const HostVec<double4>& h) {
-            DEMSPH_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(double4), cudaMemcpyHostToDevice, s));
-        };
-        up4(pos[0], hf.pos); up4(vel[0], hf.vel); up4(st[0], hf.st);
-        DEMSPH_CUDA(cudaMemcpyAsync(rho0[0].p, hf.rho0.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
-        DEMSPH_CUDA(cudaMemcpyAsync(drho[0].p, hf.drho.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
-        // dummies in caller order: (pos, vel), (c, nu, rho0, 0), rho
+        // the records through the pinned staging: fluid pos, vel, st, rho0,
+        // drho; dummies in caller order (pos, vel), (c, nu, rho0, 0), rho
         DBuf<double4> tp, tv, ts;
         DBuf<double> trh;
         if (nd > 0) {
-            tp.upload(hd.pos, s); tv.upload(hd.vel, s);
-            std::vector<double4> dst4(nd);
-            std::vector<double> rh(nd);
-            for (int i = 0; i < nd; i++) {
-                dst4[i] = make_double4(hd.st[i].z, hd.st[i].w, hd.rho0[i], 0);
-                rh[i] = hd.st[i].x;
+            tp.alloc(nd, s, false); tv.alloc(nd, s, false); ts.alloc(nd, s, false); trh.alloc(nd, s, false);
+        }
+        const size_t f4 = (size_t)n * sizeof(double4), f1 = (size_t)n * sizeof(double);
+        const size_t d4 = (size_t)nd * sizeof(double4), d1 = (size_t)nd * sizeof(double);
+        const size_t total = 3 * f4 + 2 * f1 + 3 * d4 + d1;
+        std::vector<double4> dst4;
+        std::vector<double> rh;
+        {
+            PinnedStage& ps = PinnedStage::get();
+            std::lock_guard<std::mutex> lk(ps.m);
+            char* st0 = ps.reserve(total);
+            auto up = [&](void* dev, const void* host, size_t bytes, size_t& off) {
+                if (bytes == 0) return;
+                if (st0) {
+                    host_copy(st0 + off, host, bytes);
+                    DEMSPH_CUDA(cudaMemcpyAsync(dev, st0 + off, bytes, cudaMemcpyHostToDevice, s));
+                    off += bytes;
+                } else {
+                    DEMSPH_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
+                }
+            };
+            size_t off = 0;
+            up(pos[0].p, hf.pos.data(), f4, off); up(vel[0].p, hf.vel.data(), f4, off); up(st[0].p, hf.st.data(), f4, off);
+            up(rho0[0].p, hf.rho0.data(), f1, off); up(drho[0].p, hf.drho.data(), f1, off);
+            if (nd > 0) {
+                up(tp.p, hd.pos.data(), d4, off); up(tv.p, hd.vel.data(), d4, off);
+                // the dummies' (c, nu, rho0, 0) and rho, written straight into the staging
+                double4* sst = st0 ? (double4*)(st0 + off) : nullptr;
+                double* srh = st0 ? (double*)(st0 + off + d4) : nullptr;
+                if (!st0) { dst4.resize(nd); rh.resize(nd); sst = dst4.data(); srh = rh.data(); }
+                host_parallel(nd, [&](long a, long b) {
+                    for (long i = a; i < b; i++) {
+                        sst[i] = make_double4(hd.st[i].z, hd.st[i].w, hd.rho0[i], 0);
+                        srh[i] = hd.st[i].x;
+                    }
+                });
+                DEMSPH_CUDA(cudaMemcpyAsync(ts.p, sst, d4, cudaMemcpyHostToDevice, s));
+                DEMSPH_CUDA(cudaMemcpyAsync(trh.p, srh, d1, cudaMemcpyHostToDevice, s));
             }
-            ts.upload(dst4, s);
-            trh.upload(rh, s);
+            DEMSPH_CUDA(cudaStreamSynchronize(s));  // the staging is free again
         }
         init_finish(tp, tv, ts, trh);
     }
@@ -3486,12 +3550,28 @@ int demsph_sph_get(demsph_sph_t h, int dummy, double* pos, double* vel, double* 
                                                               dDr);
             g_launches += 1;
             DEMSPH_LAUNCH_CHECK();
-            auto back = [&](double* host, const double* dev, size_t len) {
-                if (host) DEMSPH_CUDA(cudaMemcpyAsync(host, dev, len * sizeof(double), cudaMemcpyDeviceToHost, s.s));
-            };
-            back(pos, dPos, w3); back(vel, dVel, w3); back(accel, dAcc, w3);
-            back(rho, dRho, n); back(p, dP, n); back(drho, dDr, n);
-            DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            // one copy into the pinned staging, then host threads to the caller's arrays
+            PinnedStage& ps = PinnedStage::get();
+            std::lock_guard<std::mutex> lk(ps.m);
+            char* st0 = ps.reserve(words * sizeof(double));
+            if (st0) {
+                DEMSPH_CUDA(cudaMemcpyAsync(st0, out.p, words * sizeof(double), cudaMemcpyDeviceToHost, s.s));
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+                const double* hq = (const double*)st0;
+                auto back = [&](double* host, size_t len) {
+                    if (!host) return;
+                    host_copy(host, hq, len * sizeof(double));
+                    hq += len;
+                };
+                back(pos, w3); back(vel, w3); back(accel, w3); back(rho, n); back(p, n); back(drho, n);
+            } else {
+                auto back = [&](double* host, const double* dev, size_t len) {
+                    if (host) DEMSPH_CUDA(cudaMemcpyAsync(host, dev, len * sizeof(double), cudaMemcpyDeviceToHost, s.s));
+                };
+                back(pos, dPos, w3); back(vel, dVel, w3); back(accel, dAcc, w3);
+                back(rho, dRho, n); back(p, dP, n); back(drho, dDr, n);
+                DEMSPH_CUDA(cudaStreamSynchronize(s.s));
+            }
         }
         if (normal) std::fill(normal, normal + w3, 0.0);
     });
