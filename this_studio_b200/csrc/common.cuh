@@ -111,6 +111,65 @@ static void host_parallel(long n, F&& f, int threads = 8) {
     for (auto& th : pool) th.join();
 }
 
+// Many device-to-device copies in one launch: a scene's snapshot is some
+// forty buffers, and one copy call each costs a few microseconds of launch
+// latency on the stream even when the buffers are small.  Buffers are the
+// library's own allocations (256-byte aligned), copied in 16-byte words; a
+// copy's last partial word goes byte by byte.
+constexpr int kCopyMax = 48;
+struct CopyList {
+    const char* src[kCopyMax];
+    char* dst[kCopyMax];
+    unsigned long long bytes[kCopyMax];
+    unsigned long long first[kCopyMax + 1];  // first 16-byte word of each copy
+    int n;
+};
+static __global__ void k_copy_list(CopyList c) {
+    const unsigned long long total = c.first[c.n];
+    for (unsigned long long w = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; w < total;
+         w += (unsigned long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = c.n - 1;
+        while (lo < hi) {  // the last copy whose first word is <= w
+            const int mid = (lo + hi + 1) >> 1;
+            if (c.first[mid] <= w) lo = mid;
+            else hi = mid - 1;
+        }
+        const unsigned long long o = (w - c.first[lo]) * 16;
+        const unsigned long long len = c.bytes[lo] - o;
+        if (len >= 16) {
+            *reinterpret_cast<int4*>(c.dst[lo] + o) = *reinterpret_cast<const int4*>(c.src[lo] + o);
+        } else {
+            for (unsigned long long b = 0; b < len; b++) c.dst[lo][o + b] = c.src[lo][o + b];
+        }
+    }
+}
+struct CopyItem {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+// Issues the copies on stream s, kCopyMax per launch; returns the launches.
+static inline int copy_list(const std::vector<CopyItem>& items, cudaStream_t s) {
+    int launches = 0;
+    for (size_t b = 0; b < items.size(); b += kCopyMax) {
+        CopyList c{};
+        for (size_t k = b; k < items.size() && c.n < kCopyMax; k++) {
+            if (items[k].bytes == 0) continue;
+            c.src[c.n] = (const char*)items[k].src;
+            c.dst[c.n] = (char*)items[k].dst;
+            c.bytes[c.n] = items[k].bytes;
+            c.first[c.n + 1] = c.first[c.n] + (items[k].bytes + 15) / 16;
+            c.n++;
+        }
+        if (c.n == 0) continue;
+        const unsigned long long words = c.first[c.n];
+        const unsigned grid = (unsigned)std::min<unsigned long long>((words + 255) / 256, 148ull * 8);
+        k_copy_list<<<grid, 256, 0, s>>>(c);
+        launches++;
+    }
+    return launches;
+}
+
 // Process-wide page-locked staging for bulk host <-> device copies of scene
 // records: copies from (or to) pageable memory run at a fraction of the
 // link's speed, so the records are copied into this buffer by several host

@@ -1525,6 +1525,9 @@ struct DemScene {
     };
     // The snapshot's device copies are kept between calls and reused while
     // they are large enough, so a step() call allocates nothing after the first.
+    // The copies are collected and issued as one copy_list launch at the end
+    // of take().
+    std::vector<CopyItem> snapCopies;
     template <class T>
     void snap_add(Snap& sn, DBuf<T>& b) {
         if (!b.p || b.n == 0) return;
@@ -1532,10 +1535,11 @@ struct DemScene {
         if (k == sn.bufs.size()) sn.bufs.push_back(std::make_unique<DBuf<char>>());
         DBuf<char>& c = *sn.bufs[k];
         if (c.n < b.bytes()) c.alloc(b.bytes(), s, false);
-        DEMSPH_CUDA(cudaMemcpyAsync(c.p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
+        snapCopies.push_back({c.p, b.p, b.bytes()});
         sn.src.push_back({(void*)&b, b.bytes()});
     }
     void take(Snap& sn) {
+        snapCopies.clear();
         sn.src.clear();
         sn.iStep = iStep; sn.time = time; sn.cur = cur; sn.wcur = wcur; sn.havePairs = havePairs;
         sn.haveWallRows = haveWallRows; sn.K = K; sn.KT = KT;
@@ -1564,15 +1568,20 @@ struct DemScene {
                 if (tors) snap_add(sn, g.spT[b]);
             }
         }
+        launch_count(copy_list(snapCopies, s));
+        DEMSPH_LAUNCH_CHECK();
     }
     Snap snap;
     void restore(Snap& sn) {
         // pair / reverse rows were regrown in place (layout k*N + A), so the
         // saved prefix is copied back into the start of each buffer.
+        snapCopies.clear();
         for (size_t k = 0; k < sn.src.size(); k++) {
             DBuf<char>* dst = (DBuf<char>*)sn.src[k].first;
-            DEMSPH_CUDA(cudaMemcpyAsync(dst->p, sn.bufs[k]->p, sn.src[k].second, cudaMemcpyDeviceToDevice, s));
+            snapCopies.push_back({dst->p, sn.bufs[k]->p, sn.src[k].second});
         }
+        launch_count(copy_list(snapCopies, s));
+        DEMSPH_LAUNCH_CHECK();
         iStep = sn.iStep; time = sn.time; cur = sn.cur; wcur = sn.wcur; havePairs = sn.havePairs;
         haveWallRows = sn.haveWallRows;
         bondPairsStale = true;
