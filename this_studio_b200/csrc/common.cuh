@@ -115,8 +115,13 @@ static void host_parallel(long n, F&& f, int threads = 8) {
 // forty buffers, and one copy call each costs a few microseconds of launch
 // latency on the stream even when the buffers are small.  Buffers are the
 // library's own allocations (256-byte aligned), copied in 16-byte words; a
-// copy's last partial word goes byte by byte.
+// copy's last partial word goes byte by byte.  Buffers of kCopyKernelMax bytes
+// or more still go to the copy engines (cudaMemcpyAsync): there the call's
+// latency is small beside the transfer, and the engines leave the SMs to
+// whatever else runs (a kernel copy of a large batch scene's snapshot took SMs
+// from the scene stepped beside it).
 constexpr int kCopyMax = 48;
+constexpr size_t kCopyKernelMax = (size_t)1 << 20;
 struct CopyList {
     const char* src[kCopyMax];
     char* dst[kCopyMax];
@@ -148,25 +153,33 @@ struct CopyItem {
     const void* src;
     size_t bytes;
 };
-// Issues the copies on stream s, kCopyMax per launch; returns the launches.
+// Issues the copies on stream s: the small ones kCopyMax per kernel launch,
+// the large ones as copy-engine transfers.  Returns the kernel launches.
 static inline int copy_list(const std::vector<CopyItem>& items, cudaStream_t s) {
     int launches = 0;
-    for (size_t b = 0; b < items.size(); b += kCopyMax) {
-        CopyList c{};
-        for (size_t k = b; k < items.size() && c.n < kCopyMax; k++) {
-            if (items[k].bytes == 0) continue;
-            c.src[c.n] = (const char*)items[k].src;
-            c.dst[c.n] = (char*)items[k].dst;
-            c.bytes[c.n] = items[k].bytes;
-            c.first[c.n + 1] = c.first[c.n] + (items[k].bytes + 15) / 16;
-            c.n++;
-        }
-        if (c.n == 0) continue;
+    CopyList c{};
+    auto flush = [&] {
+        if (c.n == 0) return;
         const unsigned long long words = c.first[c.n];
         const unsigned grid = (unsigned)std::min<unsigned long long>((words + 255) / 256, 148ull * 8);
         k_copy_list<<<grid, 256, 0, s>>>(c);
         launches++;
+        c = CopyList{};
+    };
+    for (const CopyItem& it : items) {
+        if (it.bytes == 0) continue;
+        if (it.bytes >= kCopyKernelMax) {
+            DEMSPH_CUDA(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyDeviceToDevice, s));
+            continue;
+        }
+        c.src[c.n] = (const char*)it.src;
+        c.dst[c.n] = (char*)it.dst;
+        c.bytes[c.n] = it.bytes;
+        c.first[c.n + 1] = c.first[c.n] + (it.bytes + 15) / 16;
+        c.n++;
+        if (c.n == kCopyMax) flush();
     }
+    flush();
     return launches;
 }
 

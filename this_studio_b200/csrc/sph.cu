@@ -2392,17 +2392,26 @@ struct SphScene {
         int KF = 0, KD = 0;
         bool haveLists = false;
     };
+    // The copies are collected and issued as copy_list launches at the end of
+    // take() (and of restore()).
+    std::vector<CopyItem> snapCopies;
     template <class T>
     void snap_add(Snap& sn, DBuf<T>& b) {
         if (!b.p || b.n == 0) return;
         auto c = std::make_unique<DBuf<char>>();
         c->alloc(b.bytes(), s, false);
-        DEMSPH_CUDA(cudaMemcpyAsync(c->p, b.p, b.bytes(), cudaMemcpyDeviceToDevice, s));
+        snapCopies.push_back({c->p, b.p, b.bytes()});
         sn.dst.push_back((void*)b.p);
         sn.bytes.push_back(b.bytes());
         sn.bufs.push_back(std::move(c));
     }
     void take(Snap& sn, bool withLists = false) {
+        snapCopies.clear();
+        take_buffers(sn, withLists);
+        g_launches += copy_list(snapCopies, s);
+        DEMSPH_LAUNCH_CHECK();
+    }
+    void take_buffers(Snap& sn, bool withLists) {
         sn.iStep = iStep; sn.time = time; sn.P = P; sn.Vv = Vv; sn.S = S; sn.R0 = R0; sn.D = D; sn.ID = ID; sn.L = L;
         snap_add(sn, pos[P]); snap_add(sn, vel[Vv]); snap_add(sn, st[S]); snap_add(sn, rho0[R0]);
         snap_add(sn, drho[D]); snap_add(sn, id[ID]);
@@ -2416,10 +2425,13 @@ struct SphScene {
     }
     void restore(Snap& sn) {
         const bool lists = sn.lists && sn.KF == KF && sn.KD == KD;
+        snapCopies.clear();
         for (size_t k = 0; k < sn.bufs.size(); k++) {
             if (!lists && k >= 6) break;  // the state records come first
-            DEMSPH_CUDA(cudaMemcpyAsync(sn.dst[k], sn.bufs[k]->p, sn.bytes[k], cudaMemcpyDeviceToDevice, s));
+            snapCopies.push_back({sn.dst[k], sn.bufs[k]->p, sn.bytes[k]});
         }
+        g_launches += copy_list(snapCopies, s);
+        DEMSPH_LAUNCH_CHECK();
         iStep = sn.iStep; time = sn.time; P = sn.P; Vv = sn.Vv; S = sn.S; R0 = sn.R0; D = sn.D; ID = sn.ID; L = sn.L;
         refresh_shadows();  // the FP32 / fixed-point copies follow the restored records (and force a skin rebuild)
         if (lists) {
