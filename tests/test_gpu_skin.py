@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from this_studio_b200 import DemsphError, scenes
+from this_studio_b200.scenes import build_sph
 from this_studio_b200.solvers import WCSPHSolver
 
 from .helpers import rel_err
@@ -157,3 +158,31 @@ def test_conditional_rebuild_matches_gated_launches(gpu, prec):
         for k in ("position", "velocity", "density", "pressure"):
             np.testing.assert_array_equal(s0[k], s1[k])
     print(f"{prec}: {r0} rebuilds over 59 steps, identical with and without conditional nodes")
+
+
+def test_list_overflow_regrows_at_the_next_call(gpu):
+    """Rows sized with no headroom overflow once the fluid is compressed: the
+    passes walk those particles' stencils (same pairs), the step call returns
+    without waiting, and the next call regrows the lists from the status the
+    steps left.  The trajectory matches a scene whose rows had room."""
+    sc = scenes.dam_break_reference()
+    a = build_sph(sc, "fp64", configure=lambda s: s.setListHeadroom(0.0))
+    b = build_sph(sc, "fp64", configure=lambda s: s.setListHeadroom(1.0))
+    c = sc.fluid.mean(axis=0)
+    # 10% closer: the lattice's next shells of neighbours move inside the
+    # cutoff and the skin (a few percent would add none: the shell radii are
+    # square roots of sums of three squares)
+    squeezed = c + 0.9 * (sc.fluid - c)
+    for s in (a, b):
+        s.setSPH(position=squeezed)
+    k0 = a.listCapacity()
+    for _ in range(5):
+        a.step(6)
+        b.step(6)
+    a.synchronize()
+    k1 = a.listCapacity()
+    print(f"row capacity {k0} -> {k1} (room: {b.listCapacity()})")
+    assert k1[0] > k0[0]
+    e = rel_err(a.getSPH()["position"] - squeezed, b.getSPH()["position"] - squeezed)
+    print(f"30 steps, lists regrown vs rows with room: displacement {e:.2e}")
+    assert e < 1e-9
