@@ -1358,6 +1358,14 @@ struct OwnU {
     float3 v;
     float rho, PL;
 };
+// The own particle as the pair loops use it (fixed-point position with rho,
+// FP32 velocity, rho and p).  The FP64 velocity and state records are read
+// again after the loops rather than kept, so they hold no registers there.
+__device__ __forceinline__ OwnU own_u(const SphDev& d, int i) {
+    const double4 v = d.vel[i];
+    const double4 st = d.st[i];
+    return OwnU{d.posq[i], make_float3((float)v.x, (float)v.y, (float)v.z), (float)st.x, (float)st.y};
+}
 // vj = (v_j, p_j), rhoj from the packed shadows
 __device__ __forceinline__ void acc_fluid_u(const OwnU& o, const PairGeom& p, const float4& vj, float rhoj,
                                             const UniK& u, float3& acc) {
@@ -1393,17 +1401,18 @@ __device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, co
     acc += sb * (o.v - vd) - sw * p.r;
 }
 
+// Resident blocks: the first pass (skin rows) fits 48 registers without
+// spilling and gains from the extra warps (10 blocks: 70 -> 66 us at 128k);
+// the second pass keeps 64 (at 48 it spills).
 template <bool kSkin>
-__global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
+__global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
     const unsigned gm = quad_mask();
     const UniK& u = d.uk;
     const double4 pi4 = d.pos[i];
-    const double4 vi4 = d.vel[i];
-    const double4 s4 = d.st[i];
-    const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
+    const OwnU o = own_u(d, i);
     float3 acc = make_float3(0.f, 0.f, 0.f);
     if constexpr (kSkin) {
         skin_loop(d.cntV[i], d.nbV, d.KF, i, d.nbF, d.cntF, pi4, d.g, d.fStart, d.pos, i, [&](int j) {
@@ -1439,6 +1448,8 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_accel_u(SphDev d, double h
     a.y = quad_sum(a.y, gm);
     a.z = quad_sum(a.z, gm);
     if (sub != 0) return;
+    const double4 vi4 = d.vel[i];
+    const double4 s4 = d.st[i];
     a += d.gravity;
     d.acc[i] = d4(a, 0);
     const double3 v = xyz(vi4) + hdt * a;
@@ -1463,9 +1474,7 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     const unsigned gm = quad_mask();
     const UniK& u = d.uk;
     const double4 pi4 = d.pos[i];
-    const double4 vi4 = d.vel[i];
-    const double4 s4 = d.st[i];
-    const OwnU o{d.posq[i], make_float3((float)vi4.x, (float)vi4.y, (float)vi4.z), (float)s4.x, (float)s4.y};
+    const OwnU o = own_u(d, i);
     float sumF = 0.f, sumD = 0.f;  // sum of (1 / rho_j) (v_i - v*) . grad W / (1/2), per kind of neighbour
     quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         const int4 qj = d.posq[j];
@@ -1491,6 +1500,8 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     }
     const double dsum = quad_sum(0.5 * ((double)u.mF * (double)sumF + (double)u.mD * (double)sumD), gm);
     if (sub != 0) return;
+    const double4 vi4 = d.vel[i];
+    const double4 s4 = d.st[i];
     const double dr = dsum * (2.0 * (double)o.rho);
     double ch = d.drho[i] + dr * dt;
     d.drho[i] = ch;
