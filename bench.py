@@ -315,7 +315,6 @@ def served_stream(torch, num, seed=5, rate=100.0, steps=500, chunk=100, fp64_sam
     mk = lambda k: serve.make_stream(k, seed=seed, n_min=1000, n_max=n_max, rate=rate, steps=steps)
     # warm-up on a stream of the same sizes (another seed): kernel loads, graph
     # executables and the memory pool grown to the stream's working set, as in
-    # a server that has been running
     # a server that has been running; the autotuner (cell size, list shape,
     # skin, capacities per kind) runs on that warm-up stream's scenes
     tunings, tune = None, None

@@ -10,8 +10,9 @@ thread so the two overlap on the device.  Every chunk of steps (a multiple of
 admits waiting requests whose memory estimate fits the budget, and rebuilds
 its batch with the continuing members' state carried over on the device.  Reported: aggregate particle-steps/s, p50 / p99
 of scene latency (arrival to completion) and of scene-step latency (wall time
-of the chunk a scene-step ran in, divided by the chunk's steps), and admission
-waits.
+of the chunk a scene-step ran in, divided by the chunk's steps), admission
+waits, and per kind the seconds its batch was stepping, waiting for the next
+batch scene to be prepared, and idle with nothing admitted.
 """
 from __future__ import annotations
 
@@ -161,7 +162,7 @@ class SceneServer:
         waiting = {k: [r for r in reqs if r.batch_kind == k] for k in ("dem", "sph")}
         active = {"dem": {}, "sph": {}}
         used = [0.0]
-        stats = {k: {"busy": 0.0, "chunks": 0, "rebuild": 0.0} for k in ("dem", "sph")}
+        stats = {k: {"busy": 0.0, "chunks": 0, "rebuild": 0.0, "wait": 0.0, "idle": 0.0} for k in ("dem", "sph")}
         errors = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
@@ -226,7 +227,9 @@ class SceneServer:
                             continue
                         if not pending:
                             return
+                        ti = time.perf_counter()
                         time.sleep(max(0.0, min(0.02, pending[0].arrival - now())))
+                        st["idle"] += time.perf_counter() - ti
                         continue
                     helper = None
                     out = []
@@ -250,7 +253,9 @@ class SceneServer:
                     for m in b.members:
                         by_key[m.key].step_lat.append(lat)
                     if helper is not None:
+                        tw = time.perf_counter()
                         helper.join()
+                        st["wait"] += time.perf_counter() - tw
                         if isinstance(out[0], BaseException):
                             raise out[0]
                         prep = (out[0], adm)
@@ -276,6 +281,7 @@ class SceneServer:
         kind_ps = {k: sum(r.np_ * r.steps for r in reqs if r.batch_kind == k) for k in stats}
         m["per_kind"] = {k: {"busy_s": stats[k]["busy"], "chunks": stats[k]["chunks"],
                              "commit_s": stats[k]["rebuild"], "particle_steps": kind_ps[k],
+                             "prepare_wait_s": stats[k]["wait"], "idle_s": stats[k]["idle"],
                              **self.batches[k].timing} for k in stats}
         if self.tunings:
             m["tuning"] = {k: t.as_dict() for k, t in self.tunings.items()}
