@@ -199,3 +199,41 @@ def test_balls_float_near_their_flotation_height(gpu):
           f"offsets {(mean - expect) / R} R; difference {mean[0] - mean[1]:.4f} vs {expect[0] - expect[1]:.4f}")
     assert np.all(np.abs(mean - expect) < 0.5 * R)
     assert abs((mean[0] - mean[1]) - (expect[0] - expect[1])) < 0.25 * R[0]
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-5)])
+def test_ice_sheet_form_coupled_step(gpu, oracle_lib, prec, tol):
+    """The coupled ice-sheet workload's form at a size the oracle runs in a
+    moment: a hexagonal sheet of 672 jittered Hertz-Mindlin spheres bonded at
+    their initial contacts (parallel bonds), moving at 0.5 m/s towards a
+    cylinder mesh, one centre marker per sphere, floating half submerged on a
+    two-layer water film over a dummy floor at hydrostatic pressure.  One
+    coupled step from the same state: the bond set, the balls' force and
+    torque (contacts, bonds, coupling and gravity), the coupling force on the
+    balls and the fluid's acceleration against the FP64 oracle."""
+    from .helpers import torque_err
+
+    sc = scenes.ice_sheet_on_water(n_side=24, fluid=8000, cyl_segments=(24, 6))
+    n = sc.dem.position.shape[0]
+    o_f, o_d = oracle_coupled(sc)
+    g_f, g_d, cpl = scenes.build_coupled(sc, prec)
+    rho, p, drho = hydrostatic(sc)
+    o_f.set_state(rho=rho, p=p, drho=drho)
+    g_f.setSPH(density=rho, pressure=p, densityChange=drho)
+    ob, gb = o_d.bonds(), g_d.getBondedInteraction()
+    assert len(ob["a"]) > n
+    keys = lambda a, b: np.unique(np.minimum(a, b).astype(np.int64) * n + np.maximum(a, b))
+    assert np.array_equal(keys(ob["a"], ob["b"]), keys(gb["objectPointed"], gb["objectPointing"]))
+    o_f.couple_step(o_d, 1, sc.dem_substeps)
+    cpl.step(1, sc.dem_substeps)
+    bo, bg = o_d.balls(), g_d.getBall()
+    ef = rel_err(bg["force"], bo["force"])
+    et = torque_err(bg["torque"], bo["torque"], bo["force"], sc.dem.radius)
+    _, Fo, _ = o_f.coupling(o_d, n)
+    _, Fg, _ = cpl.getForces()
+    ec = rel_err(Fg, Fo)
+    ea = rel_err(g_f.getSPH()["acceleration"], o_f.state()["acc"])
+    print(f"{prec}: ice sheet form, {n} spheres, {len(ob['a'])} bonds: ball force {ef:.2e} torque {et:.2e} "
+          f"coupling force {ec:.2e} fluid acc {ea:.2e}")
+    for e in (ef, et, ec, ea):
+        assert e < tol
