@@ -267,6 +267,39 @@ struct DBuf {
 };
 
 static inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+// Chained launches (programmatic dependent launch): a kernel launched with
+// launch_chained may be scheduled while the kernel before it on the stream
+// is still draining, so its launch and block dispatch overlap that kernel's
+// tail instead of following its completion.  Such a kernel calls
+// chain_enter() first, before any access to global memory and before any
+// early return: griddepcontrol.wait returns once every kernel it depends on
+// has completed and its writes are visible, and since every block of every
+// chained kernel waits there, each chained kernel completes after the one
+// before it, so the ordering stays transitive along the stream.
+// griddepcontrol.launch_dependents then lets the next chained kernel be
+// scheduled as soon as every block of this one has started.  Launched
+// without the attribute (chain = false), such a kernel runs after the one
+// before it as usual and its wait returns at once.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <class... P, class... A>
+inline void launch_chained(void (*kernel)(P...), unsigned grid, unsigned block, cudaStream_t s, bool chain,
+                           A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = chain ? 1 : 0;
+    DEMSPH_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
 // Keeps up to 8 GiB of freed memory in the current device's default pool,
 // once per device, unless the caller set a limit (demsph_retain_device_memory).
 void default_pool_retention();
