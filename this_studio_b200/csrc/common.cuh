@@ -12,6 +12,9 @@
 #include <vector>
 #include <memory>
 #include <thread>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
 #include <utility>
 #include <algorithm>
 
@@ -92,8 +95,82 @@ struct DefaultInitAlloc : std::allocator<T> {
 template <class T>
 using HostVec = std::vector<T, DefaultInitAlloc<T>>;
 
-// Runs f(begin, end) over [0, n) in up to `threads` host threads (one when n
-// is small).
+// Host worker threads kept for the life of the process.  host_parallel hands
+// its chunks to them instead of starting threads per call: starting and
+// joining a thread costs tens of microseconds, and a scene's set-up and
+// read-back make dozens of parallel calls.  Several callers may submit at
+// once; a caller runs chunks of its own job until none is left and then
+// waits for the chunks the workers took, so every job completes, also one
+// submitted from inside a chunk (a worker that waits there runs its own
+// job's chunks first).  The pool is never destroyed (no join at exit).
+class HostPool {
+  public:
+    static HostPool& get() {
+        static HostPool* p = new HostPool();
+        return *p;
+    }
+    // f(i) for every i in [0, k), on the workers and the calling thread.
+    template <class F>
+    void run(int k, F& f) {
+        Job j;
+        j.k = k;
+        j.ctx = &f;
+        j.call = [](void* c, int i) { (*static_cast<F*>(c))(i); };
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            q_.push_back(&j);
+        }
+        work_.notify_all();
+        for (int i = j.next.fetch_add(1); i < k; i = j.next.fetch_add(1)) {
+            j.call(j.ctx, i);
+            j.done.fetch_add(1, std::memory_order_acq_rel);
+        }
+        std::unique_lock<std::mutex> lk(m_);
+        auto it = std::find(q_.begin(), q_.end(), &j);
+        if (it != q_.end()) q_.erase(it);
+        done_.wait(lk, [&] { return j.done.load(std::memory_order_acquire) == k; });
+    }
+
+  private:
+    struct Job {
+        int k = 0;
+        std::atomic<int> next{0}, done{0};
+        void* ctx = nullptr;
+        void (*call)(void*, int) = nullptr;
+    };
+    HostPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int workers = (int)std::min(7u, hw > 1 ? hw - 1 : 1u);
+        for (int t = 0; t < workers; t++) std::thread([this] { loop(); }).detach();
+    }
+    void loop() {
+        for (;;) {
+            Job* j = nullptr;
+            int i = 0;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                work_.wait(lk, [&] { return !q_.empty(); });
+                j = q_.front();
+                i = j->next.fetch_add(1);
+                if (i >= j->k) {  // every chunk of the front job is taken
+                    q_.pop_front();
+                    continue;
+                }
+            }
+            j->call(j->ctx, i);
+            // after this increment the job may be gone: only the pool is touched
+            j->done.fetch_add(1, std::memory_order_acq_rel);
+            std::lock_guard<std::mutex> lk(m_);
+            done_.notify_all();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable work_, done_;
+    std::deque<Job*> q_;
+};
+
+// Runs f(begin, end) over [0, n) in up to `threads` chunks on the host pool
+// (one, on the calling thread, when n is small).
 template <class F>
 static void host_parallel(long n, F&& f, int threads = 8) {
     const long minChunk = 32768;
@@ -102,13 +179,12 @@ static void host_parallel(long n, F&& f, int threads = 8) {
         f(0L, n);
         return;
     }
-    std::vector<std::thread> pool;
     const long step = (n + k - 1) / k;
-    for (int t = 0; t < k; t++) {
+    auto chunk = [&](int t) {
         const long b = t * step, e = std::min(n, b + step);
-        if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
-    }
-    for (auto& th : pool) th.join();
+        if (b < e) f(b, e);
+    };
+    HostPool::get().run(k, chunk);
 }
 
 // Many device-to-device copies in one launch: a scene's snapshot is some

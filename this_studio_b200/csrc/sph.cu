@@ -2960,29 +2960,27 @@ static void add_particles(SphScene::HostSet& t, long n, const double* pos, const
     for (int ch = 0; ch < kThreads; ch++) kept[ch + 1] += kept[ch];
     const size_t b0 = t.pos.size(), m = (size_t)kept[kThreads];
     t.pos.resize(b0 + m); t.vel.resize(b0 + m); t.st.resize(b0 + m); t.rho0.resize(b0 + m); t.drho.resize(b0 + m);
-    std::vector<std::thread> pool;
-    for (int ch = 0; ch < kThreads; ch++) {
+    auto fill = [&](int ch) {
         const long lo = ch * step, hi = std::min(n, (ch + 1) * step);
-        if (lo >= hi) continue;
-        auto fill = [&, lo, hi, ch] {
-            size_t k = b0 + kept[ch];
-            for (long i = lo; i < hi; i++) {
-                const double rho = dens[i], cc = c[i], sp = spacing[i];
-                if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
-                const double mass = sp * sp * sp * rho;
-                t.pos[k] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 1.3 * sp);
-                t.vel[k] = vel ? make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], mass)
-                               : make_double4(0, 0, 0, mass);
-                t.st[k] = make_double4(rho, 0.0, cc, visc[i]);
-                t.rho0[k] = rho;
-                t.drho[k] = 0.0;
-                k++;
-            }
-        };
-        if (n < 65536) fill();
-        else pool.emplace_back(fill);
+        size_t k = b0 + kept[ch];
+        for (long i = lo; i < hi; i++) {
+            const double rho = dens[i], cc = c[i], sp = spacing[i];
+            if (rho <= 0. || cc <= 0.) continue;  // WCSPHSolver.h:525-526
+            const double mass = sp * sp * sp * rho;
+            t.pos[k] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 1.3 * sp);
+            t.vel[k] = vel ? make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], mass)
+                           : make_double4(0, 0, 0, mass);
+            t.st[k] = make_double4(rho, 0.0, cc, visc[i]);
+            t.rho0[k] = rho;
+            t.drho[k] = 0.0;
+            k++;
+        }
+    };
+    if (n < 65536) {
+        for (int ch = 0; ch < kThreads; ch++) fill(ch);
+    } else {
+        HostPool::get().run(kThreads, fill);
     }
-    for (auto& th : pool) th.join();
 }
 int demsph_sph_add(demsph_sph_t h, int dummy, long n, const double* pos, const double* vel, const double* c,
                    const double* spacing, const double* dens, const double* visc) {
