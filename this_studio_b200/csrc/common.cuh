@@ -15,6 +15,7 @@
 #include <atomic>
 #include <condition_variable>
 #include <deque>
+#include <pthread.h>
 #include <utility>
 #include <algorithm>
 
@@ -102,11 +103,25 @@ using HostVec = std::vector<T, DefaultInitAlloc<T>>;
 // once; a caller runs chunks of its own job until none is left and then
 // waits for the chunks the workers took, so every job completes, also one
 // submitted from inside a chunk (a worker that waits there runs its own
-// job's chunks first).  The pool is never destroyed (no join at exit).
+// job's chunks first).  The pool is never destroyed (no join at exit); a
+// child process made by fork() starts its own on first use (the parent's
+// workers do not exist there, and its lock may have been held at the fork).
 class HostPool {
   public:
     static HostPool& get() {
-        static HostPool* p = new HostPool();
+        static std::atomic<HostPool*> cur{nullptr};
+        static std::once_flag hook;
+        std::call_once(hook, [] { pthread_atfork(nullptr, nullptr, [] { cur.store(nullptr); }); });
+        HostPool* p = cur.load();
+        if (!p) {
+            static std::mutex make;
+            std::lock_guard<std::mutex> lk(make);
+            p = cur.load();
+            if (!p) {
+                p = new HostPool();
+                cur.store(p);
+            }
+        }
         return *p;
     }
     // f(i) for every i in [0, k), on the workers and the calling thread.
