@@ -603,8 +603,13 @@ __global__ void __launch_bounds__(128, 8) k_dem_finalize(DemDev d, double extTim
             F.z += Fbd.z;
         }
     }
-    d.force[i] = d4(F, 0);
-    d.torque[i] = d4(T, 0);
+    // integ = 1 is the first evaluation of a step with no clumps and no hook:
+    // nothing reads its force and torque before the second evaluation
+    // overwrites them, so only the second stores them (64 B per sphere less)
+    if (integ != 1) {
+        d.force[i] = d4(F, 0);
+        d.torque[i] = d4(T, 0);
+    }
     if (integ) {
         // ballVelocityAngularVelocityIntegrationKernel (ballIntegrationKernel.cu:30-56)
         double3 v = xyz(v4);
