@@ -78,3 +78,40 @@ def test_uniform_trajectory_and_pairs(gpu, oracle_lib, dam):
     a2, b2 = g2.getPairs(0)
     np.testing.assert_array_equal(pa[0], a2)
     np.testing.assert_array_equal(pa[1], b2)
+
+
+def test_uniform_passes_with_markers(gpu, oracle_lib):
+    """A coupled scene (uniform fluid and dummy constants, markers on three
+    balls) runs the specialised passes with unpacked shadows: 20 coupled
+    steps give the same ball forces, fluid and ball trajectories as the
+    general passes within the FP32 rounding of the regrouped terms, and both
+    stay within the 1e-5 target of the FP64 oracle."""
+    from .helpers import oracle_coupled
+    from .test_coupling_oracle import hydrostatic
+
+    balls = ((0.5, 0.5, 0.45, 4.0, 1200.0), (0.25, 0.3, 0.7, 2.5, 600.0), (0.75, 0.7, 0.3, 3.0, 2500.0))
+    sc = scenes.balls_in_tank(nx=16, ny=16, depth=16, balls=balls,
+                              ball_velocity=[[0.1, 0, -0.2], [0, 0.3, 0.1], [-0.2, 0, 0]])
+    rho, p, drho = hydrostatic(sc)
+    o_f, o_d = oracle_coupled(sc)
+    o_f.set_state(rho=rho, p=p, drho=drho)
+    o_f.couple_step(o_d, 20, sc.dem_substeps)
+    _, Fo, _ = o_f.coupling(o_d, 3)
+    res = {}
+    for uni in (True, False):
+        f, d, c = scenes.build_coupled(sc, "mixed")
+        f.setUniformKernels(uni)
+        f.setSPH(density=rho, pressure=p, densityChange=drho)
+        assert f.uniformKernels() == uni
+        c.step(20, sc.dem_substeps)
+        res[uni] = (f.getSPH()["position"], d.getBall()["position"], c.getForces()[1])
+    x0, b0 = sc.sph.fluid, sc.dem.position
+    ep = rel_err(res[True][0] - x0, res[False][0] - x0)
+    eb = rel_err(res[True][1] - b0, res[False][1] - b0)
+    ef = rel_err(res[True][2], res[False][2])
+    eo = rel_err(res[True][2], Fo)
+    eop = rel_err(res[True][0] - x0, o_f.state()["pos"] - x0)
+    print(f"coupled, uniform vs general passes: fluid displacement {ep:.2e} ball displacement {eb:.2e} "
+          f"force {ef:.2e}; uniform vs oracle: force {eo:.2e} fluid displacement {eop:.2e}")
+    assert ep < 1e-5 and eb < 1e-5 and ef < 1e-5
+    assert eo < 1e-5 and eop < 1e-5

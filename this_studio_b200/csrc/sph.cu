@@ -1304,8 +1304,9 @@ __global__ void __launch_bounds__(kSphBlock, kDensityBlocks<R>) k_sph_density(Sp
 }
 
 // ---------------------------------------------------------------------------
-// Mixed-precision passes for scenes with uniform particle constants (UniK),
-// without markers.  Same pair sets, same formulas as k_sph_accel /
+// Mixed-precision passes for scenes with uniform particle constants (UniK);
+// with markers (kMarkers) the shadows stay unpacked and the markers' terms
+// come from the general boundary functions.  Same pair sets, same formulas as k_sph_accel /
 // k_sph_density (updateWCSPHAccelerationKernel and
 // updateWCSPHDensityChangeKernel, WCSPHIntegrationKernel.cu:42-282), with
 // the constants hoisted and the terms regrouped:
@@ -1366,6 +1367,21 @@ __device__ __forceinline__ OwnU own_u(const SphDev& d, int i) {
     const double4 st = d.st[i];
     return OwnU{d.posq[i], make_float3((float)v.x, (float)v.y, (float)v.z), (float)st.x, (float)st.y};
 }
+// A fluid neighbour's (v, p) and rho: from the packed shadows, or in a scene
+// with markers, whose reaction kernel reads the shadows' usual w components
+// (h, m), from the velocity shadow and the FP32 state (a third gather).
+template <bool kUnpacked>
+__device__ __forceinline__ float4 nb_vp(const SphDev& d, int j, const int4& qj, float& rhoj) {
+    const float4 v = d.velf[j];
+    if constexpr (kUnpacked) {
+        const float4 sj = d.stf[j];
+        rhoj = sj.x;
+        return make_float4(v.x, v.y, v.z, sj.y);
+    } else {
+        rhoj = __int_as_float(qj.w);
+        return v;
+    }
+}
 // vj = (v_j, p_j), rhoj from the packed shadows
 __device__ __forceinline__ void acc_fluid_u(const OwnU& o, const PairGeom& p, const float4& vj, float rhoj,
                                             const UniK& u, float3& acc) {
@@ -1403,9 +1419,14 @@ __device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, co
 
 // Resident blocks: the first pass (skin rows) fits 48 registers without
 // spilling and gains from the extra warps (10 blocks: 70 -> 66 us at 128k);
-// the second pass keeps 64 (at 48 it spills).
-template <bool kSkin>
-__global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
+// the second pass keeps 64 (at 48 it spills).  kMarkers: a coupled scene
+// (unpacked shadows; the markers' terms by the general boundary functions,
+// the same pairs and terms as the general passes and the reaction kernel).
+template <bool kSkin, bool kMarkers>
+constexpr int kUniAccelBlocks = kMarkers ? 7 : (kSkin ? 10 : 8);
+template <bool kSkin, bool kMarkers = false>
+__global__ void __launch_bounds__(kSphBlock, kUniAccelBlocks<kSkin, kMarkers>)
+    k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
@@ -1419,7 +1440,9 @@ __global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDe
             const int4 qj = d.posq[j];
             const PairGeom p = pair_geom(o.q, qj, u);
             if (!cutoff_u(p.r, u, pi4, d.pos, j)) return false;
-            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+            float rhoj;
+            const float4 vj = nb_vp<kMarkers>(d, j, qj, rhoj);
+            acc_fluid_u(o, p, vj, rhoj, u, acc);
             return true;
         });
         if (d.ND > 0) {
@@ -1434,13 +1457,37 @@ __global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDe
         quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
             const int4 qj = d.posq[j];
             const PairGeom p = pair_geom(o.q, qj, u);
-            acc_fluid_u(o, p, d.velf[j], __int_as_float(qj.w), u, acc);
+            float rhoj;
+            const float4 vj = nb_vp<kMarkers>(d, j, qj, rhoj);
+            acc_fluid_u(o, p, vj, rhoj, u, acc);
         });
         if (d.ND > 0) {
             quad_neighbors(d.cntD[i], d.nbD, d.KD, i, -1, pi4, d.g, d.dStart, d.dpos, [&](int j) {
                 const PairGeom p = pair_geom(o.q, d.dposq[j], u);
                 acc_dummy_u(o, p, d.dvelf[j], d.dnormf[j], u, acc);
             });
+        }
+    }
+    if constexpr (kMarkers) {
+        // as k_sph_accel: the fluid-marker skin row with the exact test the
+        // reaction on the markers applies, or this step's rows (an overflowed
+        // row walks the marker cells at the rows' build positions)
+        const FluidOwn<float> fo = fluid_own<float>(d, i, pi4, d.vel[i], d.st[i]);
+        const BView mv = marker_view(d);
+        const float3 g = cvt<float>(d.gravity);
+        if constexpr (kSkin) {
+            skin_loop(d.cntMV[i], d.nbMV, d.KM, i, d.nbM, d.cntM, pi4, d.g, d.mStart, d.mpos, -1, [&](int j) {
+                float3 rij;
+                float hj;
+                pair_r<float>(fo.op, mv.pos, mv.posq, d.q, j, rij, hj);
+                if (!cutoff_r<float>(rij, hj, pi4, d.mpos, j)) return false;
+                boundary_acc_r<float>(d, fo, mv, j, rij, hj, g, acc);
+                return true;
+            });
+        } else {
+            const int cM = d.cntM[i];
+            quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
+                           [&](int j) { boundary_acc<float>(d, fo, mv, j, g, acc); });
         }
     }
     double3 a = up(acc);
@@ -1455,11 +1502,11 @@ __global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDe
     const double3 v = xyz(vi4) + hdt * a;
     const double4 v4 = d4(v, vi4.w);
     d.velOut[i] = v4;
-    d.velfOut[i] = velf_p(v4, s4);
+    d.velfOut[i] = kMarkers ? f4(v4) : velf_p(v4, s4);
     if (first) {
         const double4 pn = d4(xyz(pi4) + dt * v, pi4.w);
         d.posOut[i] = pn;
-        d.posqOut[i] = fixq_rho(pn, s4, d.g.mn, d.invq);
+        d.posqOut[i] = kMarkers ? fixq(pn, d.g.mn, d.invq) : fixq_rho(pn, s4, d.g.mn, d.invq);
         if constexpr (kSkin) {
             const double3 dd = xyz(pn) - xyz(d.xb[i]);
             atomicMax(d.maxd2 + (blockIdx.x & (kSkinSlots - 1)), __float_as_uint((float)dot(dd, dd)));
@@ -1467,7 +1514,8 @@ __global__ void __launch_bounds__(kSphBlock, kSkin ? 10 : 8) k_sph_accel_u(SphDe
     }
 }
 
-__global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double dt) {
+template <bool kMarkers = false>
+__global__ void __launch_bounds__(kSphBlock, kMarkers ? 7 : 8) k_sph_density_u(SphDev d, double dt) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
@@ -1479,8 +1527,8 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     quad_neighbors(d.cntF[i], d.nbF, d.KF, i, i, pi4, d.g, d.fStart, d.pos, [&](int j) {
         const int4 qj = d.posq[j];
         const PairGeom p = pair_geom(o.q, qj, u);
-        const float4 vj = d.velf[j];  // (v_j, p_j)
-        const float rhoj = __int_as_float(qj.w);
+        float rhoj;
+        const float4 vj = nb_vp<kMarkers>(d, j, qj, rhoj);  // (v_j, p_j)
         const float3 dv = o.v - make_float3(vj.x, vj.y, vj.z);
         const float rbar = 0.5f * (o.rho + rhoj);
         const float X = __fdividef(o.PL - vj.w, rbar * u.cF);
@@ -1498,7 +1546,17 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
             sumD += __fdividef(p.Kdq * (dot(dv, p.r) * p.inv_r + X), rhoj);
         });
     }
-    const double dsum = quad_sum(0.5 * ((double)u.mF * (double)sumF + (double)u.mD * (double)sumD), gm);
+    float dRhoM = 0.f;  // the markers' terms, as k_sph_density
+    if constexpr (kMarkers) {
+        const FluidOwn<float> fo = fluid_own<float>(d, i, pi4, d.vel[i], d.st[i]);
+        const BView mv = marker_view(d);
+        const float3 g = cvt<float>(d.gravity);
+        const int cM = d.cntM[i];
+        quad_neighbors(cM, d.nbM, d.KM, i, -1, cM < 0 ? d.lpos[i] : pi4, d.g, d.mStart, d.mpos,
+                       [&](int j) { boundary_drho<float>(d, fo, mv, j, g, dRhoM); });
+    }
+    const double dsum =
+        quad_sum(0.5 * ((double)u.mF * (double)sumF + (double)u.mD * (double)sumD) + (double)dRhoM, gm);
     if (sub != 0) return;
     const double4 vi4 = d.vel[i];
     const double4 s4 = d.st[i];
@@ -1510,6 +1568,7 @@ __global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double
     const double4 so = make_double4(ch + r0, s4.z * s4.z * ch, s4.z, s4.w);
     d.stOut[i] = so;
     d.stfOut[i] = f4(so);
+    if constexpr (kMarkers) return;  // unpacked shadows: the state records alone change
     // the next position / velocity buffers: the same records, their packed
     // shadows with the new rho and p
     d.posOut[i] = pi4;
@@ -1821,7 +1880,9 @@ struct SphScene {
         u.on = ok;
         return u;
     }
-    bool uni_path() const { return uni.on && uniKernels && precision != DEMSPH_PRECISION_FP64 && nM == 0; }
+    // The uniform-constant passes (mixed precision); with markers they read
+    // the unpacked shadows (packed only when nM == 0).
+    bool uni_path() const { return uni.on && uniKernels && precision != DEMSPH_PRECISION_FP64; }
     UniK uni_consts() const {
         UniK k{};
         const double h = uni.h, qd = (double)q;
@@ -2029,7 +2090,7 @@ struct SphScene {
     // that launches the passes, outside any stream capture.
     bool packed = false;
     void sync_mode() {
-        const bool want = ready && uni_path();
+        const bool want = ready && uni_path() && nM == 0;
         if (want == packed) return;
         packed = want;
         graph.reset();          // captured launches carry the layout
@@ -2242,7 +2303,10 @@ struct SphScene {
                 }
                 g_launches += 1;
             }
-            if (skin) {
+            if (uni_path()) {
+                if (skin) k_sph_accel_u<true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+                else k_sph_accel_u<false, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
+            } else if (skin) {
                 if (fp64) k_sph_accel<double, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
                 else k_sph_accel<float, true, true><<<grid, kSphBlock, 0, s>>>(d, hdt, tstep, first);
             } else {
@@ -2284,7 +2348,8 @@ struct SphScene {
         const unsigned grid = grid_for(n, kSphPerBlock);
         const bool fp64 = precision == DEMSPH_PRECISION_FP64;
         if (nM > 0) {
-            if (fp64) k_sph_density<double, true><<<grid, kSphBlock, 0, s>>>(d, dt);
+            if (uni_path()) k_sph_density_u<true><<<grid, kSphBlock, 0, s>>>(d, dt);
+            else if (fp64) k_sph_density<double, true><<<grid, kSphBlock, 0, s>>>(d, dt);
             else k_sph_density<float, true><<<grid, kSphBlock, 0, s>>>(d, dt);
             g_launches += 1;
         } else if (packed) {
@@ -2295,7 +2360,7 @@ struct SphScene {
             d.velOut = vel[Vv ^ 1].p;
             d.posqOut = posq[P ^ 1].p;
             d.velfOut = velf[Vv ^ 1].p;
-            k_sph_density_u<<<grid, kSphBlock, 0, s>>>(d, dt);
+            k_sph_density_u<false><<<grid, kSphBlock, 0, s>>>(d, dt);
             g_launches += 1;
             P ^= 1;
             Vv ^= 1;
@@ -3339,7 +3404,7 @@ int demsph_sph_uniform_kernels(demsph_sph_t h, int* active) {
         SPH_CHECK(h);
         if (!active) throw Status(DEMSPH_ERR_INVALID, "null output pointer");
         h->sc.sync_mode();
-        *active = h->sc.packed ? 1 : 0;
+        *active = h->sc.ready && h->sc.uni_path() ? 1 : 0;
     });
 }
 struct demsph_sph_snapshot {
