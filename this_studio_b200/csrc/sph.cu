@@ -1421,9 +1421,11 @@ __device__ __forceinline__ void acc_dummy_u(const OwnU& o, const PairGeom& p, co
 // spilling and gains from the extra warps (10 blocks: 70 -> 66 us at 128k);
 // the second pass keeps 64 (at 48 it spills).  kMarkers: a coupled scene
 // (unpacked shadows; the markers' terms by the general boundary functions,
-// the same pairs and terms as the general passes and the reaction kernel).
+// the same pairs and terms as the general passes and the reaction kernel),
+// at 8 blocks despite a few spills (ice sheet 5.4-5.6 ms per coupled step at
+// 7 blocks, 5.1-5.2 at 8; 6 and 9 blocks no better).
 template <bool kSkin, bool kMarkers>
-constexpr int kUniAccelBlocks = kMarkers ? 7 : (kSkin ? 10 : 8);
+constexpr int kUniAccelBlocks = kMarkers ? 8 : (kSkin ? 10 : 8);
 template <bool kSkin, bool kMarkers = false>
 __global__ void __launch_bounds__(kSphBlock, kUniAccelBlocks<kSkin, kMarkers>)
     k_sph_accel_u(SphDev d, double hdt, double dt, int first) {
@@ -1515,7 +1517,7 @@ __global__ void __launch_bounds__(kSphBlock, kUniAccelBlocks<kSkin, kMarkers>)
 }
 
 template <bool kMarkers = false>
-__global__ void __launch_bounds__(kSphBlock, kMarkers ? 7 : 8) k_sph_density_u(SphDev d, double dt) {
+__global__ void __launch_bounds__(kSphBlock, 8) k_sph_density_u(SphDev d, double dt) {
     const int i = blockIdx.x * kSphPerBlock + threadIdx.x / kQuad;
     if (i >= d.N) return;
     const int sub = threadIdx.x & 3;
