@@ -494,7 +494,8 @@ int demsph_sph_snapshot_destroy(demsph_sph_snapshot_t snapshot);
  * particles share h, m, c and nu and whose dummies share m, c, nu and rest
  * density (with the fluid's h) runs momentum and continuity passes
  * specialised for it (constants hoisted, terms regrouped; same pairs, same
- * formulas); enable = 0 keeps the general passes.  uniform_kernels reports
+ * formulas), coupled scenes included (the markers' terms as in the general
+ * passes); enable = 0 keeps the general passes.  uniform_kernels reports
  * whether the specialised passes are in use. */
 int demsph_sph_set_uniform_kernels(demsph_sph_t s, int enable);
 int demsph_sph_uniform_kernels(demsph_sph_t s, int* active);
