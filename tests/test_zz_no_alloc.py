@@ -22,6 +22,8 @@ import pytest
 
 from this_studio_b200 import _lib
 
+from .test_gpu_compat import expected
+
 pytestmark = pytest.mark.gpu
 
 MAX_KEYS = 262144  # DEMSPH_NOALLOC_MAX_KEYS in include/demsph.h
@@ -115,6 +117,9 @@ def test_noalloc_matches_allocating_entry_point(gpu):
     for (keys, ncell), out in zip(inputs, got):
         _, ref = _sort(torch, "alloc", keys, ncell)
         for a, b in zip(out, ref):
+            np.testing.assert_array_equal(a, b)
+        # and on its own against numpy: stable order, start / end of each cell
+        for a, b in zip(out, expected(keys, ncell)):
             np.testing.assert_array_equal(a, b)
 
 
