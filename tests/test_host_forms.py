@@ -64,3 +64,63 @@ def test_agglomerate_scene_geometry():
         dk = np.linalg.norm(pts - pts[k], axis=1)
         near = (dk < 2.2 * r) & (body != body[k])
         assert not near.any()
+
+
+class _FakeBatch:
+    """The batch interface without a device: a step advances the members'
+    step counts; commits are recorded with the members' total bytes."""
+
+    def __init__(self, kind, sizes, max_members, shared):
+        self.kind, self.sizes, self.max_members, self.shared = kind, sizes, max_members, shared
+        self.members = []
+        self.timing = {"initialize_s": 0.0, "carry_s": 0.0, "rebuilds": 0}
+
+    def prepare(self, members):
+        assert 0 < len(members) <= self.max_members
+        assert all(self.sizes[m.key][0] == self.kind for m in members)
+        return list(members)
+
+    def commit(self, prep):
+        self.members = prep
+        self.timing["rebuilds"] += 1
+        self.shared[self.kind] = sum(self.sizes[m.key][1] for m in prep)
+        self.shared["peak"] = max(self.shared["peak"], self.shared.get("dem", 0) + self.shared.get("sph", 0))
+
+    def step(self, n):
+        import time
+
+        for m in self.members:
+            m.steps_done += n
+        time.sleep(0.0005)
+
+    def capture(self, keys=None):
+        pass
+
+    def clear(self):
+        self.members = []
+        self.shared[self.kind] = 0
+
+
+def test_server_schedules_every_request_within_budget():
+    """The served form's scheduling on fake batches: every request runs its
+    steps to completion after it arrived, is admitted no earlier than its
+    arrival, batches hold one kind and at most max_members, and the members
+    committed at any time fit the HBM budget (every request here fits it alone)."""
+    c0, dt = serve.stream_params(3000)
+    reqs = serve.make_stream(40, seed=3, n_min=500, n_max=3000, rate=2000.0, steps=200)
+    for r in reqs:
+        r.build(c0, dt)
+    sizes = {r.key: (r.batch_kind, r.bytes()) for r in reqs}
+    budget = 4 * max(b for _, b in sizes.values())
+    shared = {"peak": 0}
+    fakes = {k: _FakeBatch(k, sizes, 6, shared) for k in ("dem", "sph")}
+    srv = serve.SceneServer(hbm_budget=budget, chunk=50, max_members=6, sph_c0=c0, sph_dt=dt, batches=fakes)
+    m = srv.run(reqs)
+    assert all(r.done is not None and r.admitted is not None for r in reqs)
+    assert all(r.admitted >= r.arrival - 1e-9 and r.done >= r.admitted for r in reqs)
+    assert shared["peak"] <= budget
+    assert m["scenes"] == 40 and m["particle_steps"] == sum(r.np_ * r.steps for r in reqs)
+    for k in ("dem", "sph"):
+        pk = m["per_kind"][k]
+        assert pk["chunks"] >= 4 and pk["rebuilds"] >= 1
+        assert {"busy_s", "prepare_wait_s", "idle_s", "commit_s"} <= set(pk)

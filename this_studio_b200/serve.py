@@ -106,11 +106,11 @@ def _pct(v, q):
 
 class SceneServer:
     def __init__(self, hbm_budget=40e9, chunk=50, precision="mixed", max_members=512, sph_c0=None, sph_dt=None,
-                 keep_states=False, autotune=False, tunings=None):
-        import torch
-
+                 keep_states=False, autotune=False, tunings=None, batches=None):
+        """batches: kind -> an object with the batch interface (members,
+        timing, prepare, commit, step, capture, clear) in place of the device
+        batches; the scheduling then runs without a GPU."""
         assert chunk % 5 == 0, "chunks are a multiple of the DEM re-sort cadence"
-        self.torch = torch
         self.budget = hbm_budget
         self.chunk = chunk
         self.precision = precision
@@ -121,6 +121,12 @@ class SceneServer:
         self.autotune = autotune
         self.tunings = dict(tunings or {})
         self.sph_c0, self.sph_dt = sph_c0, sph_dt
+        if batches is not None:
+            self.streams = {}
+            self.batches = dict(batches)
+            return
+        import torch
+
         from . import _lib
 
         # batches are re-created at membership changes: keep their memory pooled
