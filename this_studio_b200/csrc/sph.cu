@@ -3851,7 +3851,7 @@ int demsph_sph_couple_balls(demsph_sph_t h, demsph_dem_t dem, long n, const int*
         SPH_CHECK(h);
         if (!dem) throw Status(DEMSPH_ERR_INVALID, "null DEM scene handle");
         h->sc.add_bodies(dem, n, balls, spacing, smoothingLength, soundSpeed, viscosity, density);
-        h->sc.sync_mode();  // the general passes serve scenes with markers
+        h->sc.sync_mode();  // scenes with markers keep the shadows unpacked
     });
 }
 int demsph_sph_couple_step(demsph_sph_t h, demsph_dem_t dem, long n, int demSubsteps) {
