@@ -1829,7 +1829,7 @@ struct SphScene {
     DBuf<double> diagScratch;
     bool haveLists = false;
 
-    // Skin lists (fluid scenes without markers): rows hold every candidate
+    // Skin lists (coupled scenes too, with the markers' rows): rows hold every candidate
     // within cutoff + skin at the last rebuild; a step rebuilds them (cell
     // sort, reorder, list build, all gated on the device) only when some
     // particle has drifted half the skin, and its first momentum pass keeps
